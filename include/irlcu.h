@@ -1,0 +1,140 @@
+/*
+ * irlcu.h -- device-side C ABI of libirl_b200.
+ *
+ * This is the thin layer between the host C driver (IrlOsem, IrlGenprj,
+ * set-up) and the sm_100a CUDA kernels.  Every entry point takes plain
+ * pointers and sizes and returns an int status (0 = OK, otherwise an
+ * IRLCU_E* code; irlcu_error_string() gives the message).
+ *
+ * It replaces libirl's internal projector seam (irlprivate.h:461-517:
+ * InitPrj, Project, BackProject, FreePrj) and the OSEM inner loop of
+ * osemrecon.c:687-863.  Instead of one view per call it works on all the
+ * views of a subset at once: rotation, ESSE scatter source, attenuated DRF
+ * projection, ratio, DRF backprojection, unrotation, per-view clamped
+ * accumulation and the EM update run as a few batched kernels.
+ *
+ * Layouts on the device (x fastest throughout):
+ *   volume      [y][z][x]  N*Nz*N      (libirl's internal layout)
+ *   projection  [z][x]     Nz*N per view
+ *   per-view tables [view][y][z][x]    rotated frame of each view
+ *
+ * One context per process, like libirl (non-reentrant; one device).
+ */
+#ifndef IRLCU_H
+#define IRLCU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IRLCU_OK 0
+#define IRLCU_ECUDA 101     /* a CUDA call failed */
+#define IRLCU_EARG 102      /* bad argument or size */
+#define IRLCU_ESTATE 103    /* call out of order (e.g. no context) */
+#define IRLCU_ENOMEM 104    /* device allocation failed */
+
+/* problem geometry; NumRotPixs == NumPixels as in libirl (IrlSetup.c:60) */
+typedef struct {
+	int n;            /* NumPixels */
+	int nz;           /* NumSlices */
+	int nviews;       /* NumAngles */
+	int fast_rotate;  /* 1: three-shear rotation, 0: bilinear (rot3dpar) */
+	int max_batch;    /* views processed per batched launch (>= views per subset) */
+} irlcu_geom;
+
+/* DRF table as the kernels use it: every PSF zero-padded and centred in a
+   (2*halo+1)^2 grid; row_idist[view*n + row] = table index for that rotated
+   row or -1 where libirl skips the convolution (distance <= 0). */
+typedef struct {
+	int ndist;
+	int halo;                 /* max(MaxOffsX, MaxOffsY) - 1 over the table */
+	const float *psf;         /* ndist * (2*halo+1)^2, host memory */
+	const int *pad_rows;      /* per distance: min(iAxialPadLength, MaxOffsY-1) */
+	const int *row_idist;     /* nviews * n, host memory */
+	int avg_rows;             /* iAxialAvgLength, clamped to [0, nz] */
+} irlcu_drf;
+
+/* ESSE scatter model (krnlprj3d.c:349-365, 676-954) */
+typedef struct {
+	int kx, ky, kz;           /* FFT grid: offsets (x), depths (y), slices (z) */
+	int collapse;             /* SrfCollapseFac */
+	int nterms;               /* Taylor terms, 1..3 */
+	float mu0, mu_avg, pix, cntr_pix_fac;
+	const float *krnl;        /* reordered kernel, [ky][kz][kx], host */
+	const float *kmu;         /* K * (mu - mu_avg) (nterms > 1), host */
+	const float *kmu2;        /* K * (mu - mu_avg)^2 (nterms > 2), host */
+} irlcu_esse;
+
+/* per-view scalars of the OSEM update (osemrecon.c:727-827) */
+typedef struct {
+	float view_time;          /* ViewTime */
+	float sensitivity;        /* Sensitivity */
+	int scat_mode;            /* 0 none, 1 add stored estimate, 2 store
+	                             (with-SRF minus no-SRF) estimate */
+} irlcu_view_parm;
+
+int irlcu_init(const irlcu_geom *g);
+void irlcu_shutdown(void);
+const char *irlcu_error_string(void);
+
+/* rotation angles of every view (radians, as in PrjView_t.Angle) */
+int irlcu_set_angles(const float *angles);
+/* DRF tables: which = 0 projector, 1 backprojector */
+int irlcu_set_drf(int which, const irlcu_drf *d);
+int irlcu_set_esse(const irlcu_esse *e);
+/* measured-bin mask of each view: nviews*n column flags (1 measured) */
+int irlcu_set_column_mask(const unsigned char *mask);
+
+/* volume / projection buffers */
+#define IRLCU_BUF_EST 0      /* estimate, volume */
+#define IRLCU_BUF_ATN 1      /* attenuation map (per pixel), volume */
+#define IRLCU_BUF_PRJ 2      /* measured projections, nviews planes */
+#define IRLCU_BUF_SCATEST 3  /* additive scatter estimate, nviews planes */
+#define IRLCU_BUF_PRJSCAT 4  /* stored scatter projections, nviews planes */
+#define IRLCU_BUF_UPDATE 5   /* subset update image, volume */
+#define IRLCU_BUF_NORM 6     /* inverted norm image of subset `index`, volume */
+int irlcu_upload(int buf, int index, const float *host, size_t count);
+int irlcu_download(int buf, int index, float *host, size_t count);
+int irlcu_zero(int buf, int index);
+/* a volume buffer copied to the host in libirl's external layout
+   [z][y][x] (the transposition runs on the device) */
+int irlcu_download_external(int buf, float *host);
+int irlcu_alloc_norm(int nsubsets);
+
+/* Builds the per-view rotated attenuation tables from IRLCU_BUF_ATN
+   (rotated map, cumulative half-pixel sums and exp(-sum)). */
+int irlcu_prepare_attenuation(int need_srf);
+
+/* Raw projections of the estimate for views[0..nv) into host or device
+   memory dst (nv*nz*n floats), libirl Project() with fAtnFac = 1. */
+int irlcu_project(int nv, const int *views, int model, float primary_fac,
+	float *dst, int dst_on_device);
+
+/* One OSEM subset (osemrecon.c:694-852): projections, ratio against
+   IRLCU_BUF_PRJ, backprojection, clamped accumulation into UPDATE and
+   EM update of EST with NORM[subset].  model = projector model bits for
+   this iteration; bck_model = backprojector bits. */
+int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp,
+	int model, int bck_model, int subset, int use_scatest, int apply_update,
+	int accumulate_from_update);
+
+/* Normalisation image of one subset (osemrecon.c:282-320): backprojects
+   the measured-bin mask times ViewTime of each view, clamps after each,
+   inverts with a 1e-6 floor and stores it as NORM[subset]. */
+int irlcu_norm_subset(int nv, const int *views, const float *view_time,
+	int bck_model, int subset);
+
+/* Rotation of IRLCU_BUF_EST-layout volumes (libirl vShearsRotate /
+   rot3dpar): src and dst are device or host pointers of n*nz*n floats. */
+int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, int on_device);
+
+/* synchronous wall-clock of the last batched call's stages, for tracing */
+int irlcu_stage_times(float *ms, int nmax);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IRLCU_H */

@@ -1,0 +1,85 @@
+"""libirl_b200: B200-native (sm_100a) implementation of libirl's OSEM
+projector/backprojector path behind libirl's own C API.
+
+The product is the shared library libirl_b200/libirl_b200.so (host C driver
+plus CUDA kernels).  This package only locates, builds and loads it for
+Python callers (tests, benchmarks); C applications link the .so directly
+against include/irl.h.  There is no CPU fallback: loading fails loudly when
+the library is missing and every compute call fails without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import api
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(PKG, "libirl_b200.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    from .build import build as _b
+    return _b(force=force)
+
+
+def load() -> C.CDLL:
+    """Load libirl_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SO):
+        raise ImportError(f"{SO} is missing: run `python -m libirl_b200.build`")
+    lib = api.declare_irl(C.CDLL(SO))
+    _declare_irlcu(lib)
+    _lib = lib
+    return lib
+
+
+def _declare_irlcu(lib):
+    F, I, S = api.FLOAT_P, C.c_int, C.c_size_t
+    lib.irlcu_error_string.restype = C.c_char_p
+    lib.irlcu_error_string.argtypes = []
+    lib.irlcu_init.restype = I
+    lib.irlcu_init.argtypes = [C.POINTER(IrlcuGeom)]
+    lib.irlcu_shutdown.restype = None
+    lib.irlcu_shutdown.argtypes = []
+    lib.irlcu_set_angles.restype = I
+    lib.irlcu_set_angles.argtypes = [F]
+    lib.irlcu_upload.restype = I
+    lib.irlcu_upload.argtypes = [I, I, F, S]
+    lib.irlcu_download.restype = I
+    lib.irlcu_download.argtypes = [I, I, F, S]
+    lib.irlcu_download_external.restype = I
+    lib.irlcu_download_external.argtypes = [I, F]
+    lib.irlcu_rotate_volume.restype = I
+    lib.irlcu_rotate_volume.argtypes = [C.c_float, F, F, I, I]
+    lib.irlcu_prepare_attenuation.restype = I
+    lib.irlcu_prepare_attenuation.argtypes = [I]
+    lib.irlcu_project.restype = I
+    lib.irlcu_project.argtypes = [I, C.POINTER(C.c_int), I, C.c_float, F, I]
+    lib.irlcu_stage_times.restype = I
+    lib.irlcu_stage_times.argtypes = [F, I]
+    lib.irl_gendrf.restype = None
+    lib.irl_gendrf.argtypes = [C.c_float] * 8 + [I, I, C.POINTER(api.Drf)]
+    lib.irl_compute_subsets.restype = I
+    lib.irl_compute_subsets.argtypes = [I, I, C.POINTER(C.POINTER(C.c_int))]
+
+
+class IrlcuGeom(C.Structure):
+    """irlcu_geom (include/irlcu.h)."""
+
+    _fields_ = [
+        ("n", C.c_int),
+        ("nz", C.c_int),
+        ("nviews", C.c_int),
+        ("fast_rotate", C.c_int),
+        ("max_batch", C.c_int),
+    ]
+
+
+def check(lib, rc):
+    if rc != 0:
+        raise RuntimeError(f"irlcu error {rc}: {lib.irlcu_error_string().decode(errors='replace')}")

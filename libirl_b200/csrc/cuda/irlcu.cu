@@ -1,0 +1,528 @@
+// irlcu.cu -- device context and the extern "C" entry points of include/irlcu.h.
+//
+// The host C driver (IrlOsem / IrlGenprj) owns the control flow; this file
+// owns device memory and sequences the kernels of one batched stage.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "irlcu_internal.cuh"
+#include "../host/irl_geom.h"
+
+namespace irlcu {
+
+Ctx *g_ctx = nullptr;
+static char g_err[1024] = "";
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int halo_instance(int h);
+size_t forward_partial_elems(int n, int nz, int max_batch);
+void free_rotate_scratch();
+void esse_free(Ctx &c);
+
+template <class T>
+static int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return IRLCU_OK;
+  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(IRLCU_ENOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+  }
+  return IRLCU_OK;
+}
+
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+static void free_ctx(Ctx *c) {
+  if (!c) return;
+  cudaStreamSynchronize(c->st);
+  dfree(c->rot.hdr);
+  dfree(c->rot.row_sh);
+  dfree(c->rot.row_f1);
+  dfree(c->rot.row_f2);
+  dfree(c->rot.col_sh);
+  dfree(c->rot.col_f1);
+  dfree(c->rot.col_f2);
+  dfree(c->rot.sn);
+  dfree(c->rot.cs);
+  dfree(c->sup_start);
+  dfree(c->sup_end);
+  dfree(c->est);
+  dfree(c->atn);
+  dfree(c->prj);
+  dfree(c->scatest);
+  dfree(c->prjscat);
+  dfree(c->upd);
+  dfree(c->norm);
+  dfree(c->colmask);
+  dfree(c->tE);
+  dfree(c->tS);
+  dfree(c->tMu);
+  dfree(c->wrot);
+  dfree(c->wbck);
+  dfree(c->wprj);
+  dfree(c->wprj2);
+  dfree(c->wpart);
+  dfree(c->wavg);
+  dfree(c->dviews);
+  dfree(c->dvp);
+  for (int w = 0; w < 2; ++w) {
+    dfree(c->drf[w].psf);
+    dfree(c->drf[w].pad_rows);
+    dfree(c->drf[w].row_idist);
+  }
+  esse_free(*c);
+  free_rotate_scratch();
+  for (auto &e : c->ev) cudaEventDestroy(e);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_) return rc_;       \
+  } while (0)
+
+static int need_ctx() {
+  if (!g_ctx) return set_error(IRLCU_ESTATE, "irlcu_init has not been called");
+  return IRLCU_OK;
+}
+
+// internal [y][z][x] -> external [z][y][x] (irl.h layout); x stays contiguous
+__global__ void k_to_external(const float *__restrict__ in, float *__restrict__ out, int n, int nz) {
+  const size_t vox = (size_t)n * nz * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < vox; e += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(e % n);
+    const size_t r = e / n;
+    const int z = (int)(r % nz), y = (int)(r / nz);
+    out[((size_t)z * n + y) * n + x] = in[e];
+  }
+}
+
+}  // namespace irlcu
+
+using namespace irlcu;
+
+extern "C" {
+
+const char *irlcu_error_string(void) { return g_err; }
+
+int irlcu_init(const irlcu_geom *g) {
+  if (g_ctx) irlcu_shutdown();
+  if (!g || g->n <= 0 || g->nz <= 0 || g->nviews <= 0)
+    return set_error(IRLCU_EARG, "bad geometry");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(IRLCU_ECUDA, "no CUDA device is available; libirl_b200 has no CPU path");
+  Ctx *c = new Ctx();
+  c->g = *g;
+  if (c->g.max_batch <= 0) c->g.max_batch = 16;
+  if (c->g.max_batch > g->nviews) c->g.max_batch = g->nviews;
+  c->n = g->n;
+  c->nz = g->nz;
+  c->nv = g->nviews;
+  c->pln = (size_t)c->nz * c->n;
+  c->vox = c->pln * c->n;
+  g_ctx = c;
+  CU_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  for (auto &e : c->ev) CU_TRY(cudaEventCreate(&e));
+  const int n = c->n, R = 2 * c->nv;
+  TRY(dalloc(&c->rot.hdr, (size_t)4 * R));
+  TRY(dalloc(&c->rot.row_sh, (size_t)n * R));
+  TRY(dalloc(&c->rot.row_f1, (size_t)n * R));
+  TRY(dalloc(&c->rot.row_f2, (size_t)n * R));
+  TRY(dalloc(&c->rot.col_sh, (size_t)2 * n * R));
+  TRY(dalloc(&c->rot.col_f1, (size_t)2 * n * R));
+  TRY(dalloc(&c->rot.col_f2, (size_t)2 * n * R));
+  TRY(dalloc(&c->rot.sn, (size_t)R));
+  TRY(dalloc(&c->rot.cs, (size_t)R));
+  TRY(dalloc(&c->sup_start, (size_t)n));
+  TRY(dalloc(&c->sup_end, (size_t)n));
+  {
+    std::vector<int> st(n), en(n);
+    irl_shear_support(n, st.data(), en.data());
+    CU_TRY(cudaMemcpy(c->sup_start, st.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpy(c->sup_end, en.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  const int B = c->g.max_batch;
+  TRY(dalloc(&c->est, c->vox));
+  TRY(dalloc(&c->upd, c->vox));
+  TRY(dalloc(&c->prj, c->pln * c->nv));
+  TRY(dalloc(&c->colmask, (size_t)c->nv * n));
+  TRY(dalloc(&c->wrot, c->vox * B));
+  TRY(dalloc(&c->wbck, c->vox * B));
+  TRY(dalloc(&c->wprj, c->pln * B));
+  TRY(dalloc(&c->wprj2, c->pln * B * 2));
+  c->wpart_elems = forward_partial_elems(n, c->nz, B);
+  TRY(dalloc(&c->wpart, c->wpart_elems));
+  TRY(dalloc(&c->dviews, (size_t)c->nv));
+  TRY(dalloc(&c->dvp, (size_t)c->nv));
+  CU_TRY(cudaMemset(c->prj, 0, c->pln * c->nv * sizeof(float)));
+  CU_TRY(cudaMemset(c->upd, 0, c->vox * sizeof(float)));
+  std::vector<unsigned char> ones((size_t)c->nv * n, 3);
+  CU_TRY(cudaMemcpy(c->colmask, ones.data(), ones.size(), cudaMemcpyHostToDevice));
+  return IRLCU_OK;
+}
+
+void irlcu_shutdown(void) {
+  free_ctx(g_ctx);
+  g_ctx = nullptr;
+}
+
+int irlcu_set_angles(const float *angles) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  const int n = c.n, R = 2 * c.nv;
+  std::vector<int> hdr(4 * R), rsh((size_t)n * R), csh((size_t)2 * n * R);
+  std::vector<float> rf1((size_t)n * R), rf2((size_t)n * R), cf1((size_t)2 * n * R), cf2((size_t)2 * n * R);
+  std::vector<float> sn(R), cs(R);
+  for (int r = 0; r < R; ++r) {
+    const float a = angles[r % c.nv];
+    // libirl passes 0.5*M_PI+fAngle and -0.5*M_PI-fAngle (double) to a
+    // float parameter (prjbck.c:131, 409; rot3dpar: prjbck.c:135, 413)
+    const float ang = r < c.nv ? (float)(0.5 * M_PI + a) : (float)(-0.5 * M_PI - a);
+    irl_shear_tab t;
+    t.row_sh = &rsh[(size_t)r * n];
+    t.row_f1 = &rf1[(size_t)r * n];
+    t.row_f2 = &rf2[(size_t)r * n];
+    t.col_sh = &csh[(size_t)r * 2 * n];
+    t.col_f1 = &cf1[(size_t)r * 2 * n];
+    t.col_f2 = &cf2[(size_t)r * 2 * n];
+    irl_shear_table(ang, n, &t);
+    if (t.mdim > 2 * n) return set_error(IRLCU_EARG, "shear margin too large");
+    hdr[4 * r] = t.b90;
+    hdr[4 * r + 1] = t.b180;
+    hdr[4 * r + 2] = t.iadd;
+    hdr[4 * r + 3] = t.mdim;
+    const float ang3 = r < c.nv ? (float)(0.5 * M_PI + a) : (float)(-a - 0.5 * M_PI);
+    irl_rot3dpar_sincos(ang3, &sn[r], &cs[r]);
+  }
+  CU_TRY(cudaMemcpy(c.rot.hdr, hdr.data(), hdr.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_sh, rsh.data(), rsh.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_f1, rf1.data(), rf1.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_f2, rf2.data(), rf2.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_sh, csh.data(), csh.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_f1, cf1.data(), cf1.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice));
+  return IRLCU_OK;
+}
+
+int irlcu_set_drf(int which, const irlcu_drf *d) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (which < 0 || which > 1) return set_error(IRLCU_EARG, "bad DRF slot %d", which);
+  DrfDev &D = c.drf[which];
+  dfree(D.psf);
+  dfree(D.pad_rows);
+  dfree(D.row_idist);
+  D = DrfDev{};
+  if (!d) return IRLCU_OK;
+  const int H = halo_instance(d->halo);
+  if (H < 0) return set_error(IRLCU_EARG, "DRF half-width %d exceeds the direct-convolution limit (32); use FFT convolution", d->halo);
+  const int PW = 2 * H + 1, PLD = (PW + 3) & ~3, w = 2 * d->halo + 1;
+  std::vector<float> pad((size_t)d->ndist * PW * PLD, 0.f);
+  for (int i = 0; i < d->ndist; ++i)
+    for (int yy = 0; yy < w; ++yy)
+      for (int xx = 0; xx < w; ++xx)
+        pad[(size_t)i * PW * PLD + (size_t)(yy + H - d->halo) * PLD + (xx + H - d->halo)] =
+            d->psf[(size_t)i * w * w + (size_t)yy * w + xx];
+  TRY(dalloc(&D.psf, pad.size()));
+  CU_TRY(cudaMemcpy(D.psf, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice));
+  TRY(dalloc(&D.pad_rows, (size_t)d->ndist));
+  CU_TRY(cudaMemcpy(D.pad_rows, d->pad_rows, d->ndist * 4, cudaMemcpyHostToDevice));
+  TRY(dalloc(&D.row_idist, (size_t)c.nv * c.n));
+  CU_TRY(cudaMemcpy(D.row_idist, d->row_idist, (size_t)c.nv * c.n * 4, cudaMemcpyHostToDevice));
+  D.ndist = d->ndist;
+  D.halo = H;
+  D.pstride = PLD;
+  D.avg_rows = d->avg_rows;
+  return IRLCU_OK;
+}
+
+int irlcu_set_column_mask(const unsigned char *mask) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  CU_TRY(cudaMemcpy(c.colmask, mask, (size_t)c.nv * c.n, cudaMemcpyHostToDevice));
+  return IRLCU_OK;
+}
+
+static int buf_ptr(int buf, int index, float **p, size_t *count, bool alloc) {
+  Ctx &c = *g_ctx;
+  switch (buf) {
+    case IRLCU_BUF_EST: *p = c.est; *count = c.vox; return IRLCU_OK;
+    case IRLCU_BUF_UPDATE: *p = c.upd; *count = c.vox; return IRLCU_OK;
+    case IRLCU_BUF_PRJ: *p = c.prj; *count = c.pln * c.nv; return IRLCU_OK;
+    case IRLCU_BUF_ATN:
+      if (!c.atn && alloc) TRY(dalloc(&c.atn, c.vox));
+      *p = c.atn; *count = c.vox; return IRLCU_OK;
+    case IRLCU_BUF_SCATEST:
+      if (!c.scatest && alloc) TRY(dalloc(&c.scatest, c.pln * c.nv));
+      *p = c.scatest; *count = c.pln * c.nv; return IRLCU_OK;
+    case IRLCU_BUF_PRJSCAT:
+      if (!c.prjscat && alloc) {
+        TRY(dalloc(&c.prjscat, c.pln * c.nv));
+        CU_TRY(cudaMemset(c.prjscat, 0, c.pln * c.nv * 4));
+      }
+      *p = c.prjscat; *count = c.pln * c.nv; return IRLCU_OK;
+    case IRLCU_BUF_NORM:
+      if (index < 0 || index >= c.nsub) return set_error(IRLCU_EARG, "norm index %d out of range", index);
+      *p = c.norm + (size_t)index * c.vox; *count = c.vox; return IRLCU_OK;
+  }
+  return set_error(IRLCU_EARG, "unknown buffer %d", buf);
+}
+
+int irlcu_upload(int buf, int index, const float *host, size_t count) {
+  TRY(need_ctx());
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, index, &p, &cap, true));
+  if (count > cap) return set_error(IRLCU_EARG, "upload of %zu floats exceeds buffer %d (%zu)", count, buf, cap);
+  CU_TRY(cudaMemcpyAsync(p, host, count * 4, cudaMemcpyHostToDevice, g_ctx->st));
+  CU_TRY(cudaStreamSynchronize(g_ctx->st));
+  return IRLCU_OK;
+}
+
+int irlcu_download(int buf, int index, float *host, size_t count) {
+  TRY(need_ctx());
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, index, &p, &cap, false));
+  if (!p) return set_error(IRLCU_ESTATE, "buffer %d not allocated", buf);
+  if (count > cap) return set_error(IRLCU_EARG, "download of %zu floats exceeds buffer %d", count, buf);
+  CU_TRY(cudaMemcpyAsync(host, p, count * 4, cudaMemcpyDeviceToHost, g_ctx->st));
+  CU_TRY(cudaStreamSynchronize(g_ctx->st));
+  return IRLCU_OK;
+}
+
+int irlcu_zero(int buf, int index) {
+  TRY(need_ctx());
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, index, &p, &cap, true));
+  CU_TRY(cudaMemsetAsync(p, 0, cap * 4, g_ctx->st));
+  return IRLCU_OK;
+}
+
+int irlcu_download_external(int buf, float *host) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, 0, &p, &cap, false));
+  if (!p || cap != c.vox) return set_error(IRLCU_EARG, "buffer %d is not a volume", buf);
+  k_to_external<<<592, 256, 0, c.st>>>(p, c.wbck, c.n, c.nz);
+  CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(host, c.wbck, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_alloc_norm(int nsubsets) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  dfree(c.norm);
+  c.nsub = 0;
+  TRY(dalloc(&c.norm, c.vox * nsubsets));
+  c.nsub = nsubsets;
+  return IRLCU_OK;
+}
+
+static int upload_views(const int *views, int nv, const irlcu_view_parm *vp) {
+  Ctx &c = *g_ctx;
+  if (nv <= 0 || nv > c.g.max_batch) return set_error(IRLCU_EARG, "batch of %d views (max %d)", nv, c.g.max_batch);
+  for (int i = 0; i < nv; ++i)
+    if (views[i] < 0 || views[i] >= c.nv) return set_error(IRLCU_EARG, "view index %d out of range", views[i]);
+  CU_TRY(cudaMemcpyAsync(c.dviews, views, nv * sizeof(int), cudaMemcpyHostToDevice, c.st));
+  if (vp) CU_TRY(cudaMemcpyAsync(c.dvp, vp, nv * sizeof(irlcu_view_parm), cudaMemcpyHostToDevice, c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_prepare_attenuation(int need_srf) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (!c.atn) return set_error(IRLCU_ESTATE, "attenuation map not uploaded");
+  if (!c.tE) TRY(dalloc(&c.tE, c.vox * c.nv));
+  if (need_srf) {
+    if (!c.tS) TRY(dalloc(&c.tS, c.vox * c.nv));
+    if (!c.tMu) TRY(dalloc(&c.tMu, c.vox * c.nv));
+  }
+  const int B = c.g.max_batch;
+  std::vector<int> views(B);
+  for (int v0 = 0; v0 < c.nv; v0 += B) {
+    const int nb = std::min(B, c.nv - v0);
+    for (int i = 0; i < nb; ++i) views[i] = v0 + i;
+    TRY(upload_views(views.data(), nb, nullptr));
+    float *rmu = need_srf ? c.tMu + (size_t)v0 * c.vox : c.wrot;
+    TRY(launch_rotate(c, c.atn, 0, rmu, c.vox, c.dviews, nb, 0));
+    TRY(launch_atn_tables(c, rmu, c.tE + (size_t)v0 * c.vox, need_srf ? c.tS + (size_t)v0 * c.vox : nullptr, nb));
+  }
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+// rotated source of the batch in wrot (act) and, with SRF, act+scatter in src
+static int forward_batch(int nv, int model, float primary, float *out, float *out_nosrf) {
+  Ctx &c = *g_ctx;
+  TRY(launch_rotate(c, c.est, 0, c.wrot, c.vox, c.dviews, nv, 0));
+  const float *E = (model & MODEL_ATN_BIT) ? c.tE : nullptr;
+  const DrfDev *drf = (model & MODEL_DRF_BIT) ? &c.drf[0] : nullptr;
+  if (model & MODEL_SRF_BIT) {
+    if (!c.esse.on) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
+    if (!c.tS) return set_error(IRLCU_ESTATE, "scatter model needs the attenuation tables");
+    TRY(launch_esse(c, c.wrot, c.dviews, nv, primary, c.wbck));
+    TRY(launch_project(c, c.wbck, c.dviews, nv, E, drf, 1.0f, out));
+    if (out_nosrf) TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out_nosrf));
+  } else {
+    TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out));
+  }
+  return IRLCU_OK;
+}
+
+int irlcu_project(int nv, const int *views, int model, float primary_fac, float *dst, int dst_on_device) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  for (int v0 = 0; v0 < nv; v0 += c.g.max_batch) {
+    const int nb = std::min(c.g.max_batch, nv - v0);
+    TRY(upload_views(views + v0, nb, nullptr));
+    TRY(forward_batch(nb, model, primary_fac, c.wprj, nullptr));
+    CU_TRY(cudaMemcpyAsync(dst + (size_t)v0 * c.pln, c.wprj, (size_t)nb * c.pln * 4,
+                           dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.st));
+  }
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp, int model, int bck_model, int subset,
+                      int use_scatest, int apply_update, int accumulate_from_update) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (apply_update && (subset < 0 || subset >= c.nsub)) return set_error(IRLCU_EARG, "bad subset %d", subset);
+  if (use_scatest && !c.scatest) return set_error(IRLCU_ESTATE, "scatter estimate not uploaded");
+  bool need_nosrf = false, need_prjscat = false;
+  for (int i = 0; i < nv; ++i) {
+    need_nosrf |= vp[i].scat_mode == 2;
+    need_prjscat |= vp[i].scat_mode != 0;
+  }
+  if (need_prjscat && !c.prjscat) {
+    float *p;
+    size_t cap;
+    TRY(buf_ptr(IRLCU_BUF_PRJSCAT, 0, &p, &cap, true));
+  }
+  TRY(upload_views(views, nv, vp));
+  float *calc = c.wprj;
+  float *calc_nosrf = c.wprj2;
+  float *ratio = c.wprj2 + c.pln * c.g.max_batch;
+  CU_TRY(cudaEventRecord(c.ev[0], c.st));
+  TRY(forward_batch(nv, model, 1.0f, calc, need_nosrf ? calc_nosrf : nullptr));
+  CU_TRY(cudaEventRecord(c.ev[1], c.st));
+  TRY(launch_ratio(c, calc, calc_nosrf, c.dviews, c.dvp, nv, use_scatest, ratio));
+  const float *E = (bck_model & MODEL_ATN_BIT) ? c.tE : nullptr;
+  const DrfDev *drf = nullptr;
+  if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
+  TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
+  CU_TRY(cudaEventRecord(c.ev[2], c.st));
+  TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nv, c.upd, accumulate_from_update,
+                                 apply_update ? ACC_EM : 0, c.est,
+                                 apply_update ? c.norm + (size_t)subset * c.vox : nullptr));
+  CU_TRY(cudaEventRecord(c.ev[3], c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_norm_subset(int nv, const int *views, const float *view_time, int bck_model, int subset) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (subset < 0 || subset >= c.nsub) return set_error(IRLCU_EARG, "bad subset %d", subset);
+  float *norm = c.norm + (size_t)subset * c.vox;
+  CU_TRY(cudaMemsetAsync(norm, 0, c.vox * 4, c.st));
+  const int B = c.g.max_batch;
+  for (int v0 = 0; v0 < nv; v0 += B) {
+    const int nb = std::min(B, nv - v0);
+    std::vector<irlcu_view_parm> vp(nb);
+    for (int i = 0; i < nb; ++i) vp[i].view_time = view_time[v0 + i];
+    TRY(upload_views(views + v0, nb, vp.data()));
+    // the per-view times travel in dvp; the mask kernel reads view_time
+    float *planes = c.wprj2;
+    float *vt = c.wprj;  // nb floats of scratch
+    std::vector<float> vth(view_time + v0, view_time + v0 + nb);
+    CU_TRY(cudaMemcpyAsync(vt, vth.data(), nb * 4, cudaMemcpyHostToDevice, c.st));
+    TRY(launch_norm_planes(c, c.dviews, vt, nb, nullptr, planes));
+    const float *E = (bck_model & MODEL_ATN_BIT) ? c.tE : nullptr;
+    const DrfDev *drf = nullptr;
+    if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
+    TRY(launch_backproject(c, planes, c.dviews, nb, E, drf, 1.0f, c.wbck));
+    const bool last = v0 + nb >= nv;
+    TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nb, norm, 1, last ? ACC_INVERT : 0, nullptr, nullptr));
+    CU_TRY(cudaStreamSynchronize(c.st));
+  }
+  return IRLCU_OK;
+}
+
+int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, int on_device) {
+  (void)pb_flag;
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  // a one-off rotation through a temporary table slot: use view 0's slots
+  // by rebuilding them for this angle
+  const int n = c.n;
+  std::vector<int> hdr(4), rsh(n), csh(2 * n);
+  std::vector<float> rf1(n), rf2(n), cf1(2 * n), cf2(2 * n);
+  irl_shear_tab t{0, 0, 0, 0, rsh.data(), rf1.data(), rf2.data(), csh.data(), cf1.data(), cf2.data()};
+  irl_shear_table(angle, n, &t);
+  hdr = {t.b90, t.b180, t.iadd, t.mdim};
+  float sn, cs;
+  irl_rot3dpar_sincos(angle, &sn, &cs);
+  // the last unrotation slot (index 2*nv-1) is borrowed and restored by the
+  // caller through irlcu_set_angles when needed
+  const int r = 2 * c.nv - 1;
+  CU_TRY(cudaMemcpy(c.rot.hdr + 4 * r, hdr.data(), 16, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_sh + (size_t)r * n, rsh.data(), n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_f1 + (size_t)r * n, rf1.data(), n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.row_f2 + (size_t)r * n, rf2.data(), n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_sh + (size_t)r * 2 * n, csh.data(), 2 * n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_f1 + (size_t)r * 2 * n, cf1.data(), 2 * n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.col_f2 + (size_t)r * 2 * n, cf2.data(), 2 * n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.sn + r, &sn, 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.rot.cs + r, &cs, 4, cudaMemcpyHostToDevice));
+  int zero = 0;
+  TRY(upload_views(&zero, 1, nullptr));
+  const float *s = src;
+  float *d = dst;
+  if (!on_device) {
+    CU_TRY(cudaMemcpyAsync(c.wbck, src, c.vox * 4, cudaMemcpyHostToDevice, c.st));
+    s = c.wbck;
+    d = c.wrot;
+  }
+  // rot_base chosen so rot_base + views[0] == r
+  TRY(launch_rotate(c, s, 0, d, c.vox, c.dviews, 1, r));
+  if (!on_device) CU_TRY(cudaMemcpyAsync(dst, c.wrot, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_stage_times(float *ms, int nmax) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  CU_TRY(cudaEventSynchronize(c.ev[3]));
+  for (int i = 0; i < 3 && i < nmax; ++i) CU_TRY(cudaEventElapsedTime(&ms[i], c.ev[i], c.ev[i + 1]));
+  return IRLCU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// irlcu_internal.cuh -- device context and kernel launchers shared by the
+// CUDA translation units of libirl_b200.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "irlcu.h"
+
+namespace irlcu {
+
+constexpr int MODEL_ATN_BIT = 1, MODEL_DRF_BIT = 2, MODEL_SRF_BIT = 4;
+
+// Rotation tables of a batch of rotations, in device memory.  For rotation
+// r: hdr[4r..4r+3] = {b90, b180, iadd, mdim}; row tables have n entries,
+// column tables 2n; sin/cos for the bilinear rotator.
+struct RotTabs {
+  int *hdr;
+  int *row_sh;
+  float *row_f1, *row_f2;
+  int *col_sh;
+  float *col_f1, *col_f2;
+  float *sn, *cs;
+};
+
+struct DrfDev {
+  int ndist = 0, halo = -1, avg_rows = 0;
+  float *psf = nullptr;       // ndist * (2h+1) * pstride
+  int pstride = 0;            // row stride of a PSF (multiple of 4 floats)
+  int *pad_rows = nullptr;    // per distance
+  int *row_idist = nullptr;   // nviews * n
+};
+
+struct EsseDev {
+  bool on = false;
+  int kx = 0, ky = 0, kz = 0, collapse = 1, nterms = 1;
+  float mu0 = 0, mu_avg = 0, pix = 0, cntr = 0;
+  int kxh = 0;                // kx/2 + 1 complex bins along x
+  float2 *kft[3] = {nullptr, nullptr, nullptr};  // kernel spectra
+};
+
+struct Ctx {
+  irlcu_geom g{};
+  int n = 0, nz = 0, nv = 0;
+  size_t vox = 0, pln = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[16];
+  int nsub = 0;
+
+  // rotation tables: [0, nv) rotate by 0.5*pi + angle, [nv, 2nv) unrotate
+  RotTabs rot{};
+  int *sup_start = nullptr, *sup_end = nullptr;
+
+  // persistent volumes / planes
+  float *est = nullptr, *atn = nullptr, *prj = nullptr, *scatest = nullptr;
+  float *prjscat = nullptr, *upd = nullptr, *norm = nullptr;
+  unsigned char *colmask = nullptr;  // nv * n measured columns
+
+  // per-view iteration-invariant tables [view][y][z][x]
+  float *tE = nullptr;    // exp(-cumulative attenuation) at pixel centres
+  float *tS = nullptr;    // cumulative attenuation (ESSE depth), SRF only
+  float *tMu = nullptr;   // rotated attenuation map (ESSE density), SRF only
+
+  // batch work space (max_batch views)
+  float *wrot = nullptr;    // rotated activity / source, B volumes
+  float *wbck = nullptr;    // backprojected rotated volumes, B volumes
+  float *wprj = nullptr;    // B projection planes
+  float *wprj2 = nullptr;   // B projection planes (second projection)
+  float *wpart = nullptr;   // forward partial sums
+  size_t wpart_elems = 0;
+  float *wavg = nullptr;    // axial-pad average rows, B * n * 2 * n
+  int *dviews = nullptr;    // B view indices
+  irlcu_view_parm *dvp = nullptr;
+
+  DrfDev drf[2];
+  EsseDev esse;
+  float *wfft = nullptr;    // ESSE work: B * spectra
+  size_t wfft_elems = 0;
+  float *weff = nullptr;    // ESSE expanded terms, B volumes x2
+};
+
+extern Ctx *g_ctx;
+
+// error helpers
+int set_error(int code, const char *fmt, ...);
+#define CU_TRY(x)                                                         \
+  do {                                                                    \
+    cudaError_t e_ = (x);                                                 \
+    if (e_ != cudaSuccess)                                                \
+      return ::irlcu::set_error(IRLCU_ECUDA, "%s:%d %s: %s", __FILE__,    \
+                                __LINE__, #x, cudaGetErrorString(e_));    \
+  } while (0)
+
+// ---- launchers (each defined in its kernel file) ----
+
+// rotation of nv volumes: dst[v] = rotate(src[v or shared], tab rot_base+views[v])
+int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
+                  size_t dst_stride, const int *dviews, int nv, int rot_base);
+
+// cumulative attenuation tables of nv views from rotated maps in tMu-like
+// buffer `rmu` (stride vox): writes E (and S if not null)
+int launch_atn_tables(const Ctx &c, const float *rmu, float *E, float *S, int nv);
+
+// forward DRF projection: out[v] = sum_y conv(src[v][y] * E[view][y]) * scale
+int launch_project(const Ctx &c, const float *src, const int *dviews, int nv,
+                   const float *E, const DrfDev *drf, float scale, float *out);
+
+// backprojection planes: bck[v][y] = conv(plane[v] * E[view][y]) * scale
+int launch_backproject(const Ctx &c, const float *planes, const int *dviews, int nv,
+                       const float *E, const DrfDev *drf, float scale, float *bck);
+
+// unrotate nv backprojected volumes and accumulate into acc with the
+// per-view clamp; then optionally est *= acc * norm or acc = invert(acc)
+#define ACC_EM 1
+#define ACC_INVERT 2
+int launch_unrotate_accumulate(const Ctx &c, const float *bck, const int *dviews, int nv,
+                               float *acc, int start_from_acc, int mode, float *est,
+                               const float *norm);
+
+// OSEM ratio epilogue for nv views
+int launch_ratio(const Ctx &c, const float *calc, const float *calc_nosrf,
+                 const int *dviews, const irlcu_view_parm *dvp, int nv,
+                 int use_scatest, float *ratio);
+
+// norm mask planes
+int launch_norm_planes(const Ctx &c, const int *dviews, const float *vt_dev, int nv,
+                       const unsigned char *normcols, float *planes);
+
+// ESSE effective source: src[v] = rot[v]*primary + effsrc(rot[v], view)
+int esse_setup(Ctx &c, const irlcu_esse *e);
+int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary,
+                float *src);
+
+}  // namespace irlcu

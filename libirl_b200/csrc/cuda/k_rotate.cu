@@ -1,0 +1,343 @@
+// k_rotate.cu -- volume rotation kernels of libirl_b200.
+//
+//  * three-shear rotation (libirl fastrotate.c:330-563, vShearsRotate):
+//    one CTA rotates one z-slice of one view.  The slice is staged in shared
+//    memory, pass 1 (x shear) writes the intermediate image X to shared
+//    memory, and passes 2 (y shear) and 3 (x shear) are fused: each output
+//    pixel reads the four X values it depends on.  Shifts and weights come
+//    from host tables (irl_geom.c) and every product/sum is rounded exactly
+//    like libirl's float C code (no FMA contraction), so the result is
+//    bit-identical to vShearsRotate.
+//  * bilinear rotation (rot3dpar.c:19-198): one thread per output (x, y)
+//    column, looping over slices.
+//  * the per-view clamped accumulation of unrotated backprojections and the
+//    EM update / norm inversion epilogue (prjbck.c:418-426,
+//    osemrecon.c:317-320, 850-852).
+//
+// Volume layout [y][z][x]; a slice k is the set of rows y*nz*n + k*n.
+#include <cstdio>
+
+#include "irlcu_internal.cuh"
+
+namespace irlcu {
+
+__device__ __forceinline__ float lerp2(float f1, float a, float f2, float b) {
+  // f1*a + f2*b with the two products and the sum each rounded once
+  return __fadd_rn(__fmul_rn(f1, a), __fmul_rn(f2, b));
+}
+
+struct RotHdr {
+  int b90, b180, iadd, mdim;
+};
+
+// ---------------------------------------------------------------- pass 1
+// X[r][i] of one slice (r = source row j, i < mdim); `S(y, x)` reads the
+// source slice.
+template <class Src>
+__device__ __forceinline__ float shear_pass1(const Src &S, int n, const RotHdr &h, int j, int i,
+                                             int sh, float f1, float f2, int st, int en) {
+  const int iStart = st - sh, iEnd = en - sh - 1;
+  if (i < iStart + h.iadd || i >= iEnd + h.iadd) return 0.f;
+  if (h.b180 == 0) {
+    const int t = sh - h.iadd;
+    if (h.b90 == 0) return lerp2(f1, S(j, i + t), f2, S(j, i + t + 1));
+    const int jj = n - j - 1;
+    return lerp2(f1, S(i + t, jj), f2, S(i + t + 1, jj));
+  } else {
+    const int t = sh - h.iadd + 1;
+    if (h.b90 == 0) {
+      const int jj = n - j - 1;
+      return lerp2(f1, S(jj, n - i - t), f2, S(jj, n - i - t - 1));
+    }
+    return lerp2(f1, S(n - i - t, j), f2, S(n - i - t - 1, j));
+  }
+}
+
+// ------------------------------------------------------------ pass 2 + 3
+// output pixel (j, x) from the intermediate image X (rows r in [0, n)
+// correspond to rows r + iadd of libirl's mdim x mdim pfShiftedX).
+template <class Xs>
+__device__ __forceinline__ float shear_pass23(const Xs &X, int n, const RotHdr &h, int j, int x,
+                                              int sh, float f1, float f2, int st, int en,
+                                              const int *__restrict__ csh,
+                                              const float *__restrict__ cf1,
+                                              const float *__restrict__ cf2) {
+  if (x < st + 1 || x >= en - 1) return 0.f;
+  const int jj = j + h.iadd;
+  const int a = x + sh + h.iadd;
+  float y2[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int c = a + q;
+    float v = 0.f;
+    if (c >= 0 && c < h.mdim) {
+      const int jt = csh[c];
+      const int jS = max(0, -jt), jE = min(h.mdim, h.mdim - jt - 1);
+      if (jj >= jS && jj < jE) {
+        const int r0 = jj + jt - h.iadd;  // X row of ShiftedX[jj + jt]
+        const float x0 = (r0 >= 0 && r0 < n) ? X(r0, c) : 0.f;
+        const float x1 = (r0 + 1 >= 0 && r0 + 1 < n) ? X(r0 + 1, c) : 0.f;
+        v = lerp2(cf1[c], x0, cf2[c], x1);
+      }
+    }
+    y2[q] = v;
+  }
+  return lerp2(f1, y2[0], f2, y2[1]);
+}
+
+struct SmemSlice {
+  const float *p;
+  int n;
+  __device__ float operator()(int y, int x) const { return p[y * n + x]; }
+};
+struct SmemX {
+  const float *p;
+  int ld;
+  __device__ float operator()(int r, int c) const { return p[r * ld + c]; }
+};
+struct GlobSlice {  // rows y*nz*n + k*n of a volume
+  const float *__restrict__ p;
+  int n;
+  size_t rs;
+  __device__ float operator()(int y, int x) const { return __ldg(p + (size_t)y * rs + x); }
+};
+struct GlobX {
+  const float *__restrict__ p;
+  int ld;
+  __device__ float operator()(int r, int c) const { return __ldg(p + (size_t)r * ld + c); }
+};
+
+__device__ __forceinline__ RotHdr load_hdr(const RotTabs &T, int r) {
+  RotHdr h;
+  h.b90 = T.hdr[4 * r];
+  h.b180 = T.hdr[4 * r + 1];
+  h.iadd = T.hdr[4 * r + 2];
+  h.mdim = T.hdr[4 * r + 3];
+  return h;
+}
+
+// Path A: whole slice and X in shared memory.  grid (nz, nv).
+__global__ void __launch_bounds__(512) k_shear_smem(const float *__restrict__ src, size_t src_stride,
+                                                    float *__restrict__ dst, size_t dst_stride,
+                                                    const int *__restrict__ views, int rot_base,
+                                                    RotTabs T, const int *__restrict__ sup_st,
+                                                    const int *__restrict__ sup_en, int n, int nz,
+                                                    int xld) {
+  extern __shared__ float sm[];
+  float *s_slice = sm;
+  float *s_x = sm + n * n;
+  const int k = blockIdx.x, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  const float *s = src + (size_t)v * src_stride;
+  float *d = dst + (size_t)v * dst_stride;
+  const size_t rs = (size_t)nz * n;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int y = e / n, x = e - y * n;
+    s_slice[e] = __ldg(s + (size_t)y * rs + (size_t)k * n + x);
+  }
+  __syncthreads();
+  const int *rsh = T.row_sh + (size_t)r * n;
+  const float *rf1 = T.row_f1 + (size_t)r * n, *rf2 = T.row_f2 + (size_t)r * n;
+  SmemSlice S{s_slice, n};
+  for (int e = threadIdx.x; e < n * h.mdim; e += blockDim.x) {
+    const int j = e / h.mdim, i = e - j * h.mdim;
+    s_x[j * xld + i] = shear_pass1(S, n, h, j, i, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j]);
+  }
+  __syncthreads();
+  const int *csh = T.col_sh + (size_t)r * 2 * n;
+  const float *cf1 = T.col_f1 + (size_t)r * 2 * n, *cf2 = T.col_f2 + (size_t)r * 2 * n;
+  SmemX X{s_x, xld};
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int j = e / n, x = e - j * n;
+    d[(size_t)j * rs + (size_t)k * n + x] =
+        shear_pass23(X, n, h, j, x, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j], csh, cf1, cf2);
+  }
+}
+
+// Path B, for slices too large for shared memory: pass 1 into a global
+// scratch X[v][k][n][xld], then passes 2+3.  grid (nz, nv).
+__global__ void __launch_bounds__(512) k_shear_pass1_glob(const float *__restrict__ src, size_t src_stride,
+                                                          float *__restrict__ xs, const int *__restrict__ views,
+                                                          int rot_base, RotTabs T,
+                                                          const int *__restrict__ sup_st,
+                                                          const int *__restrict__ sup_en, int n, int nz, int xld) {
+  const int k = blockIdx.x, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  GlobSlice S{src + (size_t)v * src_stride + (size_t)k * n, n, (size_t)nz * n};
+  float *xo = xs + ((size_t)v * nz + k) * (size_t)n * xld;
+  const int *rsh = T.row_sh + (size_t)r * n;
+  const float *rf1 = T.row_f1 + (size_t)r * n, *rf2 = T.row_f2 + (size_t)r * n;
+  for (int e = threadIdx.x; e < n * h.mdim; e += blockDim.x) {
+    const int j = e / h.mdim, i = e - j * h.mdim;
+    xo[(size_t)j * xld + i] = shear_pass1(S, n, h, j, i, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j]);
+  }
+}
+
+__global__ void __launch_bounds__(512) k_shear_pass23_glob(const float *__restrict__ xs, float *__restrict__ dst,
+                                                           size_t dst_stride, const int *__restrict__ views,
+                                                           int rot_base, RotTabs T,
+                                                           const int *__restrict__ sup_st,
+                                                           const int *__restrict__ sup_en, int n, int nz, int xld) {
+  const int k = blockIdx.x, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  GlobX X{xs + ((size_t)v * nz + k) * (size_t)n * xld, xld};
+  float *d = dst + (size_t)v * dst_stride;
+  const size_t rs = (size_t)nz * n;
+  const int *rsh = T.row_sh + (size_t)r * n;
+  const float *rf1 = T.row_f1 + (size_t)r * n, *rf2 = T.row_f2 + (size_t)r * n;
+  const int *csh = T.col_sh + (size_t)r * 2 * n;
+  const float *cf1 = T.col_f1 + (size_t)r * 2 * n, *cf2 = T.col_f2 + (size_t)r * 2 * n;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int j = e / n, x = e - j * n;
+    d[(size_t)j * rs + (size_t)k * n + x] =
+        shear_pass23(X, n, h, j, x, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j], csh, cf1, cf2);
+  }
+}
+
+// Bilinear rotation (rot3dpar.c:19-198, non-FAST branch).  One thread per
+// output (x, y); NumPixels == NumRotPixs.  grid (ceil(n*n/256), nv).
+__global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, float *__restrict__ dst,
+                           size_t dst_stride, const int *__restrict__ views, int rot_base, RotTabs T,
+                           int n, int nz) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * n) return;
+  const int v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const float Sin = T.sn[r], Cos = T.cs[r];
+  const int NewY = e / n, NewX = e - NewY * n;
+  const int Dim = n;
+  const float Axis = 0.5f * (float)(Dim - 1);  // 0.5*(NewDim-1): exact in float
+  const float Radius = 0.5f * (float)Dim;
+  const float *s = src + (size_t)v * src_stride;
+  float *d = dst + (size_t)v * dst_stride;
+  const size_t rs = (size_t)nz * n;
+  // row extent (rot3dpar.c:98-101) with the C expression types:
+  // (Radius - NewY) is float, "- .5" and the rest double
+  const double t = __dsub_rn((double)__fsub_rn(Radius, (float)NewY), 0.5);
+  int NumPix = (int)__dadd_rn(sqrt(__dsub_rn((double)__fmul_rn(Radius, Radius), __dmul_rn(t, t))), 0.5);
+  NumPix *= 2;
+  const int Head = (int)(0.5 * (double)(Dim - NumPix));
+  const int Tail = Head + NumPix - 1;
+  if (NewX < Head || NewX > Tail) {
+    for (int z = 0; z < nz; ++z) d[(size_t)NewY * rs + (size_t)z * n + NewX] = 0.f;
+    return;
+  }
+  const float Y = (float)NewY - Axis;
+  const float X = (float)NewX - Axis;
+  const float FloatX = __fadd_rn(__fsub_rn(__fmul_rn(X, Cos), __fmul_rn(Y, Sin)), Axis);
+  const float FloatY = __fadd_rn(__fadd_rn(__fmul_rn(X, Sin), __fmul_rn(Y, Cos)), Axis);
+  const int OldX = (int)FloatX, OldY = (int)FloatY;
+  bool z0o = false, z1o = false, z2o = false, z3o = false;
+  if (OldX < 0 || OldX >= Dim) z0o = z1o = true;
+  if (OldY < 0 || OldY >= Dim) z0o = z2o = true;
+  if (OldX + 1 < 0 || OldX + 1 >= Dim) z2o = z3o = true;
+  if (OldY + 1 < 0 || OldY + 1 >= Dim) z1o = z3o = true;
+  const float fy = __fsub_rn(FloatY, (float)OldY), fx = __fsub_rn(FloatX, (float)OldX);
+  for (int z = 0; z < nz; ++z) {
+    const float z0 = z0o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX);
+    const float z1 = z1o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX);
+    const float z2 = z2o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX + 1);
+    const float z3 = z3o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX + 1);
+    float z01 = __fadd_rn(z0, __fmul_rn(fy, __fsub_rn(z1, z0)));
+    float z23 = __fadd_rn(z2, __fmul_rn(fy, __fsub_rn(z3, z2)));
+    if (FloatY < 0) {
+      z01 = z0;
+      z23 = z2;
+    }
+    float z0123 = __fadd_rn(z01, __fmul_rn(fx, __fsub_rn(z23, z01)));
+    if (FloatX < 0) z0123 = z01;
+    d[(size_t)NewY * rs + (size_t)z * n + NewX] = z0123;
+  }
+}
+
+static float *g_xscratch = nullptr;
+static size_t g_xscratch_elems = 0;
+
+int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
+                  const int *dviews, int nv, int rot_base) {
+  if (nv <= 0) return IRLCU_OK;
+  const int n = c.n, nz = c.nz;
+  if (!c.g.fast_rotate) {
+    dim3 grid((n * n + 255) / 256, nv);
+    k_rot3dpar<<<grid, 256, 0, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, n, nz);
+    CU_TRY(cudaGetLastError());
+    return IRLCU_OK;
+  }
+  const int xld = 2 * n;  // mdim < 2n always
+  const size_t smem = sizeof(float) * ((size_t)n * n + (size_t)n * xld);
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  dim3 grid(nz, nv);
+  if (smem <= (size_t)maxsm) {
+    static size_t s_configured = 0;
+    if (smem > s_configured) {
+      CU_TRY(cudaFuncSetAttribute(k_shear_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      s_configured = smem;
+    }
+    k_shear_smem<<<grid, 512, smem, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base, c.rot,
+                                            c.sup_start, c.sup_end, n, nz, xld);
+    CU_TRY(cudaGetLastError());
+    return IRLCU_OK;
+  }
+  const size_t need = (size_t)nv * nz * n * xld;
+  if (need > g_xscratch_elems) {
+    if (g_xscratch) cudaFree(g_xscratch);
+    g_xscratch = nullptr;
+    g_xscratch_elems = 0;
+    CU_TRY(cudaMalloc(&g_xscratch, need * sizeof(float)));
+    g_xscratch_elems = need;
+  }
+  k_shear_pass1_glob<<<grid, 512, 0, c.st>>>(src, src_stride, g_xscratch, dviews, rot_base, c.rot,
+                                             c.sup_start, c.sup_end, n, nz, xld);
+  CU_TRY(cudaGetLastError());
+  k_shear_pass23_glob<<<grid, 512, 0, c.st>>>(g_xscratch, dst, dst_stride, dviews, rot_base, c.rot,
+                                              c.sup_start, c.sup_end, n, nz, xld);
+  CU_TRY(cudaGetLastError());
+  return IRLCU_OK;
+}
+
+void free_rotate_scratch() {
+  if (g_xscratch) cudaFree(g_xscratch);
+  g_xscratch = nullptr;
+  g_xscratch_elems = 0;
+}
+
+// ---------------------------------------------------------- accumulation
+// acc = clamp(acc + vol[v]) for v in order (prjbck.c:418-426), then the
+// epilogue: ACC_EM est *= acc * norm (osemrecon.c:850-852) or ACC_INVERT
+// acc = acc < 1e-6 ? 0 : 1/acc (osemrecon.c:317-320).
+__global__ void k_accumulate(const float *__restrict__ vols, size_t vstride, int nv, float *__restrict__ acc,
+                             int start_from_acc, int mode, float *__restrict__ est,
+                             const float *__restrict__ norm, size_t vox) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vox; i += (size_t)gridDim.x * blockDim.x) {
+    float a = start_from_acc ? acc[i] : 0.f;
+    for (int v = 0; v < nv; ++v) {
+      a = __fadd_rn(a, __ldg(vols + (size_t)v * vstride + i));
+      if ((double)a < 1.0e-5) a = 0.f;
+    }
+    if (mode == ACC_INVERT) {
+      a = (double)a < 1e-6 ? 0.f : (float)(1.0 / (double)a);
+    } else if (mode == ACC_EM) {
+      est[i] = __fmul_rn(est[i], __fmul_rn(a, __ldg(norm + i)));
+    }
+    acc[i] = a;
+  }
+}
+
+int launch_unrotate_accumulate(const Ctx &c, const float *bck, const int *dviews, int nv, float *acc,
+                               int start_from_acc, int mode, float *est, const float *norm) {
+  // unrotate every backprojected volume in place into wrot, then accumulate
+  int rc = launch_rotate(c, bck, c.vox, c.wrot, c.vox, dviews, nv, c.nv);
+  if (rc) return rc;
+  int blocks = (int)((c.vox + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_accumulate<<<blocks, 256, 0, c.st>>>(c.wrot, c.vox, nv, acc, start_from_acc, mode, est, norm, c.vox);
+  CU_TRY(cudaGetLastError());
+  return IRLCU_OK;
+}
+
+}  // namespace irlcu

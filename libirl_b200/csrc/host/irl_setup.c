@@ -1,0 +1,792 @@
+/*
+ * irl_setup.c -- run set-up of libirl_b200 on the host: parameters, views,
+ * per-view extra data and detectors, DRF tables (read or computed GRF),
+ * ESSE kernel preparation, initial estimate, subsets.
+ *
+ * Each routine follows the libirl routine named beside it; expressions that
+ * decide integer indices or table sizes keep libirl's float/double types so
+ * the decisions are identical.
+ */
+#include <complex.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "irl_err.h"
+#include "irl_host.h"
+#include "irl_geom.h"
+#include "irlcu.h"
+
+#ifndef MAX
+#define MAX(a, b) ((a) > (b) ? (a) : (b))
+#endif
+#ifndef MIN
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+#endif
+
+/* ------------------------------------------------ extra view data / detectors */
+
+int g_irl_extra_nviews = 0;
+float *g_irl_acq_times = NULL;
+int *g_irl_det_nums = NULL;
+int g_irl_ndet = 0;
+void **g_irl_dets = NULL;
+
+/* IrlSetup.c:350-402 */
+int iSetupExtraPrjViewData(int iNumPrjViews, float *pfAcqTimes, int *piDetectorNums)
+{
+	int i, err = 0;
+	g_irl_extra_nviews = iNumPrjViews;
+	if (pfAcqTimes != NULL)
+		g_irl_acq_times = pfAcqTimes;
+	if (piDetectorNums != NULL)
+		g_irl_det_nums = piDetectorNums;
+	if (iNumPrjViews < 0)
+		err = 1;
+	if (iNumPrjViews > 0 && pfAcqTimes == NULL && piDetectorNums == NULL)
+		err = 1;
+	if (iNumPrjViews == 0 && (pfAcqTimes != NULL || piDetectorNums != NULL))
+		err = 1;
+	if (pfAcqTimes != NULL)
+		for (i = 0; i < iNumPrjViews; ++i)
+			if (pfAcqTimes[i] < 0.0)
+				err |= 2;
+	if (piDetectorNums != NULL)
+		for (i = 0; i < iNumPrjViews; ++i)
+			if (piDetectorNums[i] < 0)
+				err |= 4;
+	return err;
+}
+
+/* IrlSetup.c:415-439 */
+void *pvStoreDetectorData(float fHoleDiam, float fHoleLen, float fBackToDet, float fIntrinsicFWHM,
+	float fSensitivity, int bFFTconvolve, int bUseGrfInBck, char *pchDrfTabFname)
+{
+	irl_detector *d = (irl_detector *)calloc(1, sizeof(irl_detector));
+	if (d == NULL)
+		return NULL;
+	d->hole_diam = fHoleDiam;
+	d->hole_len = fHoleLen;
+	d->back_to_det = fBackToDet;
+	d->intrinsic_fwhm = fIntrinsicFWHM;
+	d->sensitivity = fSensitivity;
+	d->fft_convolve = bFFTconvolve;
+	d->grf_in_bck = bUseGrfInBck;
+	d->drf_fname = pchDrfTabFname;
+	d->drf = NULL;
+	return d;
+}
+
+/* IrlSetup.c:441-462 */
+int iSetupDetectors(int iNumDetectors, void **ppsDetectors)
+{
+	int err = 0;
+	g_irl_ndet = iNumDetectors;
+	g_irl_dets = ppsDetectors;
+	if (iNumDetectors < 0)
+		err = 1;
+	if (iNumDetectors > 0 && ppsDetectors == NULL)
+		err = 2;
+	if (iNumDetectors == 0 && ppsDetectors != NULL)
+		err = 4;
+	return err;
+}
+
+/* end-of-run release of caller-supplied tables (IrlSetup.c:404-413,
+   464-481): the arrays, detector records and DRF file names are freed */
+void irl_free_run_tables(void)
+{
+	int i;
+	free(g_irl_acq_times);
+	g_irl_acq_times = NULL;
+	free(g_irl_det_nums);
+	g_irl_det_nums = NULL;
+	g_irl_extra_nviews = 0;
+	if (g_irl_dets != NULL) {
+		for (i = 0; i < g_irl_ndet; ++i) {
+			irl_detector *d = (irl_detector *)g_irl_dets[i];
+			if (d == NULL)
+				continue;
+			free(d->drf_fname);
+			d->drf = irl_free_drftab(d->drf);
+			free(d);
+			g_irl_dets[i] = NULL;
+		}
+		free(g_irl_dets);
+	}
+	g_irl_dets = NULL;
+	g_irl_ndet = 0;
+}
+
+/* ------------------------------------------------------------ parameters */
+
+/* vSetupParms, IrlSetup.c:51-91 */
+void irl_setup_parms(IrlParms_t *ip, Options_t *op, float *atn, char *krnl_fname, irl_parms *p)
+{
+	int srf, drf, at;
+	memset(p, 0, sizeof(*p));
+	p->n = ip->NumPixels;
+	p->nbins = ip->NumPixels;
+	p->nviews = ip->NumViews;
+	p->nz = ip->NumSlices;
+	p->pix = ip->BinWidth;
+	p->atn_scale = ip->fAtnScaleFac;
+	p->srf_iters = ip->iNumSrfIterations;
+	p->scatest_fac = ip->fScatEstFac;
+	p->hole_len = ip->fHoleLen;
+	p->hole_diam = ip->fHoleDiam;
+	p->back_to_det = ip->fBackToDet;
+	p->max_frac_err = 0.05f;
+	p->intrinsic_fwhm = ip->fIntrinsicFWHM;
+	srf = krnl_fname == NULL ? 0 : MODEL_SRF;
+	drf = op->bModelDrf ? MODEL_DRF : 0;
+	at = atn == NULL ? 0 : MODEL_ATN;
+	p->prj_model = srf | at | drf;
+	p->bck_model = at | drf;
+	p->model = srf | at | drf;
+	p->ang_per_subset = ip->NumAngPerSubset;
+	p->norm_base = ip->pchNormImageBase;
+	p->iterations = ip->NumIterations;
+	p->start_iteration = 0;
+	p->pad_len = op->iAxialPadLength;
+	p->avg_len = op->iAxialAvgLength;
+	if (p->n <= 0 || p->nz <= 0 || p->nviews <= 0)
+		irl_fatal(IRL_E_VALUE, "SetupParms", "NumPixels, NumSlices and NumViews must be positive");
+	if (p->pix <= 0.0f)
+		irl_fatal(IRL_E_VALUE, "SetupParms", "BinWidth must be positive, not %g", p->pix);
+}
+
+/* psSetupViews, IrlSetup.c:101-144 */
+irl_view *irl_setup_views(IrlParms_t *ip, PrjView_t *pv)
+{
+	int i, n = ip->NumViews;
+	irl_view *v = (irl_view *)irl_calloc(sizeof(irl_view) * n, "views");
+	for (i = 0; i < n; ++i) {
+		v[i].angle = pv[i].Angle;
+		v[i].cfcr = pv[i].CFCR;
+		v[i].right = pv[i].Right;
+		v[i].left = pv[i].Left;
+		v[i].view_time = 1.0f;
+		v[i].sensitivity = 1.0f;
+		v[i].drf = NULL;
+		v[i].det = 0;
+	}
+	if (g_irl_acq_times != NULL) {
+		if (g_irl_extra_nviews != n)
+			irl_fatal(IRL_E_VALUE, "SetupViews", "Number of Prj Views passed to SetupExtrPrjViewData is incorrect");
+		for (i = 0; i < n; ++i)
+			v[i].view_time = g_irl_acq_times[i];
+	}
+	return v;
+}
+
+/* ------------------------------------------------------------ GRF tables */
+
+/* in-place complex FFT (double), power-of-two n, kernel exp(sign i ...) */
+static void cfft(double complex *x, int n, int stride, int sign)
+{
+	int i, j, len;
+	for (i = 1, j = 0; i < n; ++i) {
+		int bit = n >> 1;
+		for (; j & bit; bit >>= 1)
+			j ^= bit;
+		j ^= bit;
+		if (i < j) {
+			double complex t = x[(long)i * stride];
+			x[(long)i * stride] = x[(long)j * stride];
+			x[(long)j * stride] = t;
+		}
+	}
+	for (len = 2; len <= n; len <<= 1) {
+		int h = len >> 1;
+		for (j = 0; j < h; ++j) {
+			double a = sign * 2.0 * M_PI * (double)j / (double)len;
+			double complex w = cos(a) + I * sin(a);
+			for (i = j; i < n; i += len) {
+				double complex u = x[(long)i * stride], t = x[(long)(i + h) * stride] * w;
+				x[(long)i * stride] = u + t;
+				x[(long)(i + h) * stride] = u - t;
+			}
+		}
+	}
+}
+
+/* GenDPSRF, gendrf.c:44-216 (parallel-hole collimator) */
+static void gen_dpsrf(double ColToSource, double ColThick, double ColToImage, double HoleDiam,
+	double BinSize, double IntrinsicFWHM, int MatSize, float *pDPSRF, int *pAliasing)
+{
+	double intarg, samwid, normsum, normfac, alpha, beta, xfreq, yfreq, freq, delf, ftmp;
+	double PsfZero, NewBinSize;
+	int BinRatio, MyMatSize, NewMatSize, ix, iy, ix1, iy1;
+	float *ft;
+	double complex *cx;
+
+	*pAliasing = 0;
+	intarg = M_PI * M_PI * IntrinsicFWHM * IntrinsicFWHM / (4.0 * log(2.0));
+	alpha = (ColToSource + ColToImage + ColThick) / ColThick;
+	beta = M_PI * alpha * HoleDiam;
+	samwid = M_PI * BinSize;
+	BinRatio = 20.0 * BinSize / beta + 0.5;
+	BinRatio = BinRatio < 1 ? 1 : BinRatio;
+	NewBinSize = BinSize / BinRatio;
+	PsfZero = HoleDiam * (ColToSource + ColToImage + ColThick) / ColThick;
+	NewMatSize = 4.0 * PsfZero / NewBinSize;
+	MyMatSize = 2;
+	while ((MyMatSize < NewMatSize) && (MyMatSize < 1024))
+		MyMatSize *= 2;
+	ft = (float *)irl_calloc(sizeof(float) * 2 * MyMatSize * MyMatSize, "GRF spectrum");
+	delf = 1.0 / ((double)MyMatSize * NewBinSize);
+	ft[0] = 1;
+	for (ix = 0; ix <= MyMatSize / 2; ++ix) {
+		xfreq = (double)ix * delf;
+		for (iy = 0; iy <= MyMatSize / 2; ++iy) {
+			if (ix == 0 && iy == 0)
+				continue;
+			yfreq = (double)iy * delf;
+			freq = hypot(yfreq, xfreq);
+			ftmp = 2.0 * j1(beta * freq) / (beta * freq);
+			ftmp = ftmp * ftmp * exp(-freq * freq * intarg);
+			if (samwid > 0.0)
+				ftmp *= sin(samwid * freq) / (freq * samwid);
+			ft[2 * (MyMatSize * iy + ix)] = ftmp;
+			if (iy != 0)
+				ft[2 * (MyMatSize * (MyMatSize - iy) + ix)] = ftmp;
+			if (ix != 0)
+				ft[2 * (MyMatSize * iy + (MyMatSize - ix))] = ftmp;
+			if (ix != 0 && iy != 0)
+				ft[2 * (MyMatSize * (MyMatSize - iy) + (MyMatSize - ix))] = ftmp;
+		}
+	}
+	/* inverse 2D transform of the (float-stored) spectrum, in double */
+	cx = (double complex *)irl_malloc(sizeof(double complex) * MyMatSize * MyMatSize, "GRF transform");
+	for (ix = 0; ix < MyMatSize * MyMatSize; ++ix)
+		cx[ix] = ft[2 * ix] + I * ft[2 * ix + 1];
+	for (iy = 0; iy < MyMatSize; ++iy)
+		cfft(cx + (long)iy * MyMatSize, MyMatSize, 1, +1);
+	for (ix = 0; ix < MyMatSize; ++ix)
+		cfft(cx + ix, MyMatSize, MyMatSize, +1);
+	for (ix = 0; ix < MyMatSize * MyMatSize; ++ix) {
+		ft[2 * ix] = (float)(creal(cx[ix]) / ((double)MyMatSize * MyMatSize));
+		ft[2 * ix + 1] = (float)(cimag(cx[ix]) / ((double)MyMatSize * MyMatSize));
+	}
+	free(cx);
+	NewMatSize = MIN(MyMatSize / 2, BinRatio * MatSize);
+	*pAliasing = MyMatSize > 2 * MatSize;
+	for (ix = 0; ix < MyMatSize * MyMatSize; ix += 2)
+		if (ft[ix] < 0)
+			ft[ix] = 0;
+	normsum = ft[0];
+	for (ix = BinRatio; ix < NewMatSize; ix += BinRatio)
+		normsum += 2.0 * (ft[2 * ix] + ft[2 * ix * MyMatSize]);
+	for (ix = BinRatio; ix < NewMatSize; ix += BinRatio)
+		for (iy = BinRatio; iy < NewMatSize; iy += BinRatio)
+			normsum += 4.0 * ft[2 * (ix + iy * MyMatSize)];
+	normfac = 1.0 / normsum;
+	for (ix = 0; ix < MatSize * MatSize; ++ix)
+		pDPSRF[ix] = 0.0;
+	for (ix = 0, ix1 = 0; ix < NewMatSize; ix += BinRatio, ix1++)
+		for (iy = 0, iy1 = 0; iy < NewMatSize; iy += BinRatio, iy1++)
+			pDPSRF[ix1 + iy1 * MatSize] = ft[2 * (ix + iy * MyMatSize)] * normfac;
+	free(ft);
+}
+
+/* gendrf, gendrf.c:218-427 (parallel hole) */
+void irl_gendrf(float fColThick, float fHoleDiam, float fGap, float fIntrinsic, float fMaxErr,
+	float fBinSize, float fDrfSpacing, float minDist, int NumDists, int NOffs, Drf_t *tab)
+{
+	int iDist, iXOffs, iYOffs, MaxOffsX = NOffs, MaxOffsY = NOffs, alias = 0;
+	float fColToSource;
+	float *q = (float *)irl_malloc(sizeof(float) * NOffs * NOffs, "quarter DPSF");
+	double dSum, dNormFac, dMinSum = 1.0 - fMaxErr;
+
+	for (iDist = 0, fColToSource = minDist; iDist < NumDists; iDist++, fColToSource += fDrfSpacing) {
+		if (fColToSource <= 0.0) {
+			for (iXOffs = 1; iXOffs < NOffs * NOffs; ++iXOffs)
+				q[iXOffs] = 0.0;
+			q[0] = 1.0;
+		} else {
+			gen_dpsrf(fColToSource, fColThick, fGap, fHoleDiam, fBinSize, fIntrinsic, NOffs, q, &alias);
+		}
+		if (alias)
+			irl_warn("gendrf", "Possible aliasing in DRF table computation at distance %.2f", fColToSource);
+		if (fMaxErr <= 0.0) {
+			MaxOffsX = MaxOffsY = NOffs;
+			dNormFac = 1.0;
+		} else {
+			/* grow the square until the enclosed sum exceeds 1 - fMaxErr */
+			int iXT, iYT, prevX = 1;
+			dSum = q[0];
+			iYOffs = 1;
+			for (iXOffs = 1; iXOffs < NOffs; iXOffs++) {
+				if (dSum > dMinSum)
+					break;
+				dSum += 2 * q[iXOffs];
+				iYOffs = iXOffs;
+				for (iYT = 1; iYT < iYOffs; iYT++)
+					for (iXT = (prevX + 1); iXT <= iXOffs; iXT++)
+						dSum += 4 * q[iYT * NOffs + iXT];
+				for (iXT = 1; iXT <= iXOffs; iXT++)
+					dSum += 4 * q[iYOffs * NOffs + iXT];
+				dSum += 2 * q[iYOffs * NOffs];
+				iYOffs++;
+				prevX = iXOffs;
+			}
+			MaxOffsX = iXOffs;
+			MaxOffsY = iXOffs;
+			dSum = q[0];
+			for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs) {
+				dSum += q[iXOffs] * 2.0;
+				dSum += q[iXOffs * NOffs] * 2.0;
+				for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
+					dSum += 4.0 * q[iXOffs + iYOffs * NOffs];
+			}
+			dNormFac = 1.0 / dSum;
+		}
+		tab[iDist].MaxOffsX = MaxOffsX;
+		tab[iDist].MaxOffsY = MaxOffsY;
+		tab[iDist].bFFTdone = 0;
+		{
+			const int w = 2 * MaxOffsX - 1, xs = MaxOffsX - 1, ys = MaxOffsY - 1;
+			float *P = (float *)irl_calloc(sizeof(float) * (2 * MaxOffsX - 1) * (2 * MaxOffsY - 1), "PSF");
+#define PP(y, x) P[(y) * w + (x)]
+			PP(ys, xs) = q[0] * dNormFac;
+			for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
+				PP(ys + iYOffs, xs) = PP(ys - iYOffs, xs) = q[NOffs * iYOffs] * dNormFac;
+			for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs)
+				PP(ys, xs + iXOffs) = PP(ys, xs - iXOffs) = q[iXOffs] * dNormFac;
+			for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
+				for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs)
+					PP(ys + iYOffs, xs + iXOffs) = PP(ys - iYOffs, xs + iXOffs) =
+						PP(ys + iYOffs, xs - iXOffs) = PP(ys - iYOffs, xs - iXOffs) =
+							q[NOffs * iYOffs + iXOffs] * dNormFac;
+#undef PP
+			tab[iDist].Psf = P;
+		}
+	}
+	free(q);
+}
+
+/* vComputeDrfs, IrlSetup.c:243-334 */
+static void compute_drfs(DrfTab_t *t, float fPixelWidth, float fBinWidth, int iReconMatSize, float fMinDist,
+	float fMaxDist)
+{
+	int iNumDrfOffs = (int)(iReconMatSize * 0.5);
+	int iNumDists = ((fMaxDist - fMinDist) / fPixelWidth + 1 + 0.5);
+	t->psDrfs = (Drf_t *)irl_calloc(iNumDists * sizeof(Drf_t), "GRF table");
+	t->iNumDistances = iNumDists;
+	t->fStartDistance = fMinDist;
+	t->fDrfSpacing = fPixelWidth;
+	t->fPixSize = fPixelWidth;
+	t->bIncKrnl = 0;
+	irl_gendrf(t->fColThick, t->fHoleDiam, t->fGap, t->fIntrinsicFWHM, t->fMaxFracErr, fBinWidth, fPixelWidth,
+		fMinDist, iNumDists, iNumDrfOffs, t->psDrfs);
+}
+
+#define RELDIF(a, b) (2.0 * fabs((a) - (b)) / (((fabs(a) + fabs(b)) == 0.0) ? 1 : (fabs(a) + fabs(b))))
+#define CMPRFLOAT(a, b, tol) (RELDIF((a), (b)) <= tol)
+
+/* vCheckDrfTab, IrlSetup.c:202-241 */
+static void check_drftab(const DrfTab_t *t, float fPixWid, float fMinDist, float fMaxDist, const char *fname)
+{
+	float fTabMax;
+	if (!CMPRFLOAT(t->fPixSize, fPixWid, 0.01))
+		irl_fatal(IRL_E_VALUE, "vCheckDrfTab",
+			"The pixel size in Drf Table %s is %.4f, and not %.4f as needed for recon.", fname, t->fPixSize,
+			fPixWid);
+	fTabMax = t->fStartDistance + (t->iNumDistances - 1) * t->fDrfSpacing;
+	if (!(((CMPRFLOAT(fMinDist, t->fStartDistance, 0.0001) || fMinDist > t->fStartDistance) &&
+		      (CMPRFLOAT(fMaxDist, fTabMax, 0.0001) || fMaxDist < fTabMax)) ||
+		    (fMaxDist > fTabMax)))
+		irl_warn("vCheckDrfTab",
+			"The range of distances in %s is (%.2f to %.2f), reconstruction needs (%.2f to %.2f). "
+			"Approximations will be used",
+			fname, t->fStartDistance, fTabMax, fMinDist, fMaxDist);
+	if (!CMPRFLOAT(t->fDrfSpacing, fPixWid, 0.01))
+		irl_warn("vCheckDrfTab", "The distance between Drfs in %s is %.4f, not %.4f. NN interp will be used",
+			fname, t->fDrfSpacing, fPixWid);
+}
+
+/* psDrfSetup, IrlSetup.c:504-588 */
+static DrfTab_t *drf_setup(float fMinCFCR, float fMaxCFCR, float fPixelWidth, float fBinWidth, int n,
+	float fMaxFracErr, irl_detector *d)
+{
+	DrfTab_t *t = (DrfTab_t *)irl_calloc(sizeof(DrfTab_t), "DRF table");
+	float fMinDist = fMinCFCR - n / 2 * fPixelWidth + fPixelWidth / 2;
+	float fMaxDist;
+	if (fMinDist < 0)
+		fMinDist = fPixelWidth / 2;
+	fMaxDist = fMaxCFCR + n / 2 * fPixelWidth - fPixelWidth / 2;
+	t->fGap = d->back_to_det;
+	t->fHoleDiam = d->hole_diam;
+	t->fColThick = d->hole_len;
+	t->fIntrinsicFWHM = d->intrinsic_fwhm;
+	t->fMaxFracErr = fMaxFracErr;
+	if (d->drf_fname != NULL) {
+		char *title = NULL, *col = NULL;
+		DrfTab_t r = sReadDrfTab(d->drf_fname, &title, &col);
+		free(title);
+		free(col);
+		r.psBckDrfTab = NULL;
+		*t = r;
+		check_drftab(t, fPixelWidth, fMinDist, fMaxDist, d->drf_fname);
+		if (d->grf_in_bck) {
+			DrfTab_t *b = (DrfTab_t *)irl_calloc(sizeof(DrfTab_t), "GRF table");
+			b->fGap = d->back_to_det;
+			b->fHoleDiam = d->hole_diam;
+			b->fColThick = d->hole_len;
+			b->fIntrinsicFWHM = d->intrinsic_fwhm;
+			b->fMaxFracErr = fMaxFracErr;
+			compute_drfs(b, fPixelWidth, fBinWidth, n, fMinDist, fMaxDist);
+			b->psBckDrfTab = NULL;
+			b->bFFTconvolve = 0;
+			t->psBckDrfTab = b;
+		}
+	} else {
+		compute_drfs(t, fPixelWidth, fBinWidth, n, fMinDist, fMaxDist);
+	}
+	t->bFFTconvolve = d->fft_convolve;
+	return t;
+}
+
+/* vSetupDrfTables, IrlSetup.c:590-658 */
+int irl_setup_drf_tables(irl_parms *p, Options_t *op, irl_view *views, char *drf_fname, irl_detector **pdets)
+{
+	int a, k;
+	float fMin, fMax;
+	if (g_irl_ndet == 0) {
+		void **arr = (void **)irl_malloc(sizeof(void *), "detector table");
+		arr[0] = pvStoreDetectorData(p->hole_diam, p->hole_len, p->back_to_det, p->intrinsic_fwhm, 1.0f,
+			op->bFFTConvolve, op->bUseGrfInBck, drf_fname);
+		if (arr[0] == NULL)
+			irl_fatal(IRL_E_MALLOC, "vSetupDrfTables", "out of memory");
+		iSetupDetectors(1, arr);
+	}
+	fMin = fMax = views[0].cfcr;
+	for (a = 0; a < p->nviews; ++a) {
+		fMin = fMin > views[a].cfcr ? views[a].cfcr : fMin;
+		fMax = fMax < views[a].cfcr ? views[a].cfcr : fMax;
+	}
+	for (k = 0; k < g_irl_ndet; ++k) {
+		irl_detector *d = (irl_detector *)g_irl_dets[k];
+		if (p->prj_model & MODEL_DRF)
+			d->drf = drf_setup(fMin, fMax, p->pix, p->pix, p->n, p->max_frac_err, d);
+		else
+			d->drf = NULL;
+	}
+	for (a = 0; a < p->nviews; ++a) {
+		if (g_irl_det_nums == NULL) {
+			views[a].det = 0;
+			views[a].drf = ((irl_detector *)g_irl_dets[0])->drf;
+			views[a].sensitivity = 1.0f;
+		} else {
+			int dn = g_irl_det_nums[a];
+			if (dn < 0 || dn >= g_irl_ndet)
+				irl_fatal(IRL_E_VALUE, "vSetupDrfTables", "Illegal detector specified for view %d (%d)", a, dn);
+			views[a].det = dn;
+			views[a].drf = ((irl_detector *)g_irl_dets[dn])->drf;
+			views[a].sensitivity = ((irl_detector *)g_irl_dets[dn])->sensitivity;
+		}
+	}
+	*pdets = NULL;
+	return g_irl_ndet;
+}
+
+/* Concatenates the tables of all detectors, pads every PSF to the common
+   half-width and uploads the per-view row -> table index map. */
+static void upload_one(const irl_parms *p, irl_view *views, int bck)
+{
+	int ndet = g_irl_ndet, k, a, i, halo = 0, total = 0, w;
+	int *base = (int *)irl_calloc(sizeof(int) * (ndet + 1), "DRF offsets");
+	DrfTab_t **tabs = (DrfTab_t **)irl_calloc(sizeof(DrfTab_t *) * (ndet + 1), "DRF tables");
+	float *psf;
+	int *pad, *rows;
+	irlcu_drf D;
+	for (k = 0; k < ndet; ++k) {
+		DrfTab_t *t = ((irl_detector *)g_irl_dets[k])->drf;
+		if (t != NULL && bck && t->psBckDrfTab != NULL)
+			t = t->psBckDrfTab;
+		tabs[k] = t;
+		base[k] = total;
+		if (t == NULL)
+			continue;
+		if (t->bFFTconvolve)
+			irl_warn("SetupDrf", "FFT convolution requested; the direct convolution is used instead "
+				"(identical results without axial padding)");
+		for (i = 0; i < t->iNumDistances; ++i) {
+			halo = MAX(halo, t->psDrfs[i].MaxOffsX - 1);
+			halo = MAX(halo, t->psDrfs[i].MaxOffsY - 1);
+		}
+		total += t->iNumDistances;
+	}
+	w = 2 * halo + 1;
+	psf = (float *)irl_calloc(sizeof(float) * (size_t)total * w * w, "padded PSFs");
+	pad = (int *)irl_calloc(sizeof(int) * (total > 0 ? total : 1), "pad rows");
+	for (k = 0; k < ndet; ++k) {
+		DrfTab_t *t = tabs[k];
+		if (t == NULL)
+			continue;
+		for (i = 0; i < t->iNumDistances; ++i) {
+			const Drf_t *d = &t->psDrfs[i];
+			int wx = 2 * d->MaxOffsX - 1, wy = 2 * d->MaxOffsY - 1, yy, xx;
+			int oy = halo - (d->MaxOffsY - 1), ox = halo - (d->MaxOffsX - 1);
+			float *dst = psf + (size_t)(base[k] + i) * w * w;
+			for (yy = 0; yy < wy; ++yy)
+				for (xx = 0; xx < wx; ++xx)
+					dst[(size_t)(yy + oy) * w + xx + ox] = d->Psf[yy * wx + xx];
+			/* conv2d_ypad.c:54-57: iPadY = clamp(iAxialPadLength, 0, bCtrY) */
+			pad[base[k] + i] = MIN(MAX(p->pad_len, 0), d->MaxOffsY - 1);
+		}
+	}
+	rows = (int *)irl_malloc(sizeof(int) * (size_t)p->nviews * p->n, "DRF rows");
+	for (a = 0; a < p->nviews; ++a) {
+		DrfTab_t *t = tabs[views[a].det];
+		if (t == NULL) {
+			for (i = 0; i < p->n; ++i)
+				rows[(size_t)a * p->n + i] = -1;
+			continue;
+		}
+		irl_drf_rows(views[a].cfcr, p->pix, p->n, t->fStartDistance, t->fDrfSpacing, t->iNumDistances,
+			rows + (size_t)a * p->n);
+		for (i = 0; i < p->n; ++i)
+			if (rows[(size_t)a * p->n + i] >= 0)
+				rows[(size_t)a * p->n + i] += base[views[a].det];
+	}
+	D.ndist = total;
+	D.halo = halo;
+	D.psf = psf;
+	D.pad_rows = pad;
+	D.row_idist = rows;
+	D.avg_rows = MIN(MAX(p->avg_len, 0), p->nz);
+	irl_cu(irlcu_set_drf(bck, total > 0 ? &D : NULL), "SetupDrf");
+	free(psf);
+	free(pad);
+	free(rows);
+	free(base);
+	free(tabs);
+}
+
+void irl_upload_drf(const irl_parms *p, irl_view *views, int ndet, irl_detector *dets)
+{
+	int k, separate = 0;
+	(void)ndet;
+	(void)dets;
+	upload_one(p, views, 0);
+	for (k = 0; k < g_irl_ndet; ++k) {
+		DrfTab_t *t = ((irl_detector *)g_irl_dets[k])->drf;
+		if (t != NULL && t->psBckDrfTab != NULL)
+			separate = 1;
+	}
+	if (separate)
+		upload_one(p, views, 1);
+	else
+		irl_cu(irlcu_set_drf(1, NULL), "SetupDrf");
+}
+
+/* ------------------------------------------------------------------- ESSE */
+
+/* pfReorder3dKrnl, krnlprj3d.c:43-128: one-quadrant kernel -> wrap-around
+   order [depth][slice][offset] with the depth axis flipped */
+static float *reorder_krnl(const float *in, int noffs, int ndepths, int oxd, int oyd, int ozd)
+{
+	float *out = (float *)irl_calloc(sizeof(float) * (size_t)oxd * oyd * ozd, "reordered kernel");
+	int xmin = MIN(noffs, oxd / 2), ymin = MIN(noffs, oyd / 2), izin, iy, ix;
+	for (izin = 0; izin < ndepths; ++izin) {
+		int izout = ozd / 2 - izin + ndepths / 2 - 1;
+		if (izout < 0 || izout >= ozd)
+			continue;
+		izout += izout < ozd / 2 ? ozd / 2 : -ozd / 2;
+		for (iy = 0; iy < ymin; iy++) {
+			for (ix = 0; ix < xmin; ix++) {
+				float v = in[ix + noffs * (iy + noffs * izin)];
+				int yo[2] = {iy, oyd - iy}, xo[2] = {ix, oxd - ix}, a, b;
+				for (a = 0; a < (iy > 0 ? 2 : 1); ++a)
+					for (b = 0; b < (ix > 0 ? 2 : 1); ++b)
+						out[xo[b] + (size_t)oxd * (yo[a] + (size_t)oyd * izout)] = v;
+			}
+		}
+	}
+	return out;
+}
+
+/* pvInitESSEScatterModel + pvInitScatterPrj, krnlprj3d.c:956-1009, 403-547,
+   with libirl's hard-coded parameters "2 2 2 3" (IrlSetup.c:169-174):
+   xy pad 2, z pad 2, two Taylor terms, 3D geometry */
+void irl_esse_prepare(const char *fname, const irl_parms *p, int c, irl_esse_host *e)
+{
+	const float xypad = 2, zpad = 2;
+	const int nterms = 2;
+	KrnlData_t *k;
+	int nx, ny, nz;
+	size_t i, cnt;
+	float fKs = 0.0f, fKMs = 0.0f, *mu;
+	memset(e, 0, sizeof(*e));
+	if (c < 1 || c > 4)
+		irl_fatal(IRL_E_VALUE, "SrfSetup", "srf_collapse_fac = %d: must be 1 (no collapse) to 4", c);
+	k = psReadKrnlFile((char *)fname, 1);
+	if (k->fScatFac == 0.0) {
+		psFreeKrnlData(k, 1);
+		return;
+	}
+	e->on = 1;
+	e->mu0 = k->fKrnlMu0;
+	e->pix = p->pix;
+	e->cntr_pix_fac = k->fCntrPixFac;
+	e->nterms = nterms;
+	e->collapse = c;
+	nx = p->n / c;
+	ny = p->n / c;
+	nz = p->nz / c;
+	nx = (int)ceil(xypad * (float)(nx));
+	ny = (int)ceil(xypad * (float)(ny));
+	nz = (int)ceil(zpad * (float)nz);
+	e->kx = nx;
+	e->ky = ny;
+	e->kz = nz;
+	e->krnl = reorder_krnl(k->pfKrnl, k->iNumXYoffs, k->iNumDists, nx, nz, ny);
+	mu = reorder_krnl(k->pfKrnlMu, k->iNumXYoffs, k->iNumDists, nx, nz, ny);
+	cnt = (size_t)nx * ny * nz;
+	for (i = 0; i < cnt; ++i) {
+		fKs += e->krnl[i];
+		fKMs += e->krnl[i] * mu[i];
+	}
+	if (fKs == 0.0) {
+		irl_warn("InitScatterPrj", "Sum of Krnl is 0!");
+		e->mu_avg = k->fKrnlMu0;
+	} else {
+		e->mu_avg = fKMs / fKs;
+	}
+	e->kmu = (float *)irl_malloc(sizeof(float) * cnt, "K mu");
+	for (i = 0; i < cnt; ++i) {
+		mu[i] -= e->mu_avg;
+		e->kmu[i] = mu[i] * e->krnl[i];
+	}
+	free(mu);
+	if (fabs(k->fPixSize - p->pix * c) > 0.02)
+		irl_warn("vInitESSEScatterModel", "Pixel size after collapse=%.3g, Pixel size in kernel=%.3g",
+			c * p->pix, k->fPixSize);
+	if (p->n % c != 0 || p->nz % c != 0)
+		irl_fatal(IRL_E_VALUE, "CollapseByFac", "factor %d does not evenly divide image dimensions %d, %d",
+			c, p->n, p->nz);
+	psFreeKrnlData(k, 1);
+}
+
+void irl_esse_free(irl_esse_host *e)
+{
+	free(e->krnl);
+	free(e->kmu);
+	free(e->kmu2);
+	memset(e, 0, sizeof(*e));
+}
+
+/* ------------------------------------------------------ initial estimate */
+
+/* vZeroBehind, initial_est.c:160-180 */
+static void zero_behind(int nd, float fSin, float fCos, float fRadius, float *pix)
+{
+	int ix, iy;
+	float fX, fY, fR;
+	for (iy = 0; iy < nd; ++iy) {
+		fY = iy - (float)nd / 2.0;
+		for (ix = 0; ix < nd; ++ix) {
+			fX = ix - (float)nd / 2.0;
+			fR = floor(fX * fCos + fY * fSin + 0.5);
+			if (fR > fRadius)
+				pix[ix + iy * nd] = 0.0;
+		}
+	}
+}
+
+/* pfComputeInitialEstimate, initial_est.c:29-158 (internal layout) */
+float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const irl_view *views, const float *prj,
+	const float *atn, float *init)
+{
+	int n = p->n, nz = p->nz, na = p->nviews, a, s, r, c2, use_map = 0;
+	size_t i, tot = (size_t)n * nz * na;
+	float fNum = (float)(n * n * nz), fAvg, fSum = 0.0f, fMapThresh = 0.0f;
+	fNum *= M_PI / 4.0;
+	for (i = 0; i < tot; ++i)
+		fSum += prj[i];
+	fAvg = fSum / (fNum * na);
+	if (atn != NULL) {
+		fMapThresh = thresh;
+		fMapThresh *= p->pix;
+		if (fMapThresh < 0.0)
+			irl_warn("ComputeInitialEstimate", "atnmap_support_thresh must be > 0, not %.3f. Ignoring",
+				fMapThresh);
+		else
+			use_map = fMapThresh > 0.0;
+	}
+	if (!contour) {
+		for (i = 0; i < (size_t)n * nz * n; ++i)
+			init[i] = fAvg;
+	} else {
+		float *img = (float *)irl_malloc(sizeof(float) * n * n, "contour image");
+		for (i = 0; i < (size_t)n * n; ++i)
+			img[i] = fAvg;
+		for (a = 0; a < na; ++a) {
+			double d = views[a].angle;
+			zero_behind(n, (float)sin(d), (float)cos(d), views[a].cfcr / p->pix, img);
+		}
+		for (s = 0; s < nz; ++s)
+			for (r = 0; r < n; ++r)
+				for (c2 = 0; c2 < n; ++c2)
+					init[(size_t)r * nz * n + (size_t)s * n + c2] = img[c2 + r * n];
+		free(img);
+	}
+	if (use_map)
+		for (i = 0; i < (size_t)n * nz * n; ++i)
+			if (atn[i] < fMapThresh)
+				init[i] = 0.0;
+	{
+		float fRadius = (float)n * 0.5, fX, fY, fCent = fRadius;
+		for (r = 0; r < n; ++r) {
+			fY = (float)r - fCent;
+			if (fY > 0)
+				fY += 1;
+			for (c2 = 0; c2 < n; ++c2) {
+				fX = (float)c2 - fCent;
+				if (fX > 0)
+					fX += 1;
+				if (hypot(fX, fY) > fRadius)
+					for (s = 0; s < nz; ++s)
+						init[(size_t)r * nz * n + (size_t)s * n + c2] = 0.0;
+			}
+		}
+	}
+	return init;
+}
+
+/* ---------------------------------------------------------------- subsets */
+
+/* iComputeSubsets, osemrecon.c:395-456 */
+int irl_compute_subsets(int na, int per, int **angles)
+{
+	int ns, s, m, a;
+	if (per <= 0 || na % per)
+		irl_fatal(IRL_E_VALUE, "iComputeSubsets",
+			"No. of angles not an integer multiple of the no. of angles per subset\n NumAngles=%d, NumAngPerSet=%d",
+			na, per);
+	ns = na / per;
+	if (ns != 1 && ns % 2)
+		irl_fatal(IRL_E_VALUE, "iComputeSubsets", "Number of subsets (%d) for num_ang_per_set=%d is not even",
+			ns, per);
+	*angles = (int *)irl_malloc(sizeof(int) * na, "subset angles");
+	for (s = 0; s < ns; ++s) {
+		a = s / 2 + (s % 2) * ns / 2;
+		for (m = 0; m < per; ++m) {
+			(*angles)[s * per + m] = a;
+			a += ns;
+		}
+	}
+	return ns;
+}
+
+void irl_reorder(int d0, int d1, int d2, const float *in, float *out)
+{
+	int i, j, k;
+	for (j = 0; j < d1; ++j)
+		for (k = 0; k < d0; ++k)
+			for (i = 0; i < d2; ++i)
+				out[((size_t)j * d0 + k) * d2 + i] = in[((size_t)k * d1 + j) * d2 + i];
+}
