@@ -385,7 +385,7 @@ static int forward_batch(int nv, int model, float primary, float *out, float *ou
   const float *E = (model & MODEL_ATN_BIT) ? c.tE : nullptr;
   const DrfDev *drf = (model & MODEL_DRF_BIT) ? &c.drf[0] : nullptr;
   if (model & MODEL_SRF_BIT) {
-    if (!c.esse.on) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
+    if (!c.esse.on && !c.esse.zero) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
     if (!c.tS) return set_error(IRLCU_ESTATE, "scatter model needs the attenuation tables");
     TRY(launch_esse(c, c.wrot, c.dviews, nv, primary, c.wbck));
     TRY(launch_project(c, c.wbck, c.dviews, nv, E, drf, 1.0f, out));

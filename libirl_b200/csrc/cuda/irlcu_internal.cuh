@@ -34,6 +34,7 @@ struct DrfDev {
 
 struct EsseDev {
   bool on = false;
+  bool zero = false;          // kernel scatter factor 0: zero effective source
   int kx = 0, ky = 0, kz = 0, collapse = 1, nterms = 1;
   float mu0 = 0, mu_avg = 0, pix = 0, cntr = 0;
   int kxh = 0;                // kx/2 + 1 complex bins along x
