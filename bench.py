@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: ms per OSEM iteration, 128^3 / 120 views, on one B200.
+
+Workload (full128, seed 2000): 128^3 float32 volume, 0.3125 cm voxels,
+120 views on an elliptical 22 x 18 cm orbit, 8 subsets, attenuation, a
+33x33-tap DRF at every depth and ESSE scatter (collapse 2, two Taylor
+terms), Poisson data at 5e6 counts.  One step = one OSEM iteration (all
+8 subsets, 120 projections + 120 backprojections with scatter).
+
+  value      device time per iteration with everything resident in HBM,
+             CUDA events on the library's stream (IrlOsemIterate)
+  e2e        the public call IrlOsem (host buffers in, result out, set-up,
+             normalisation images and a per-iteration callback included),
+             wall time / iterations
+  roofline   the dominant stage (the DRF convolution) against its bound
+  cpu_baseline  the reference C (compiled here) on a bounded sample
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun) every rank runs an independent replica (the path does
+not shard) and rank 0 prints the job line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+# one GPU per rank: pin the visible device before any CUDA initialisation
+_LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+_WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+if _WORLD > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(_LOCAL_RANK)
+
+import numpy as np  # noqa: E402
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per OSEM iteration, 128³/120 views, 1 B200: ESSE vs learned scatter at ≤1% NRMSE"
+WORKLOAD = ("full128: 128^3 x 120 views, 8 subsets x 15 views, attenuation + 33x33 DRF + ESSE scatter "
+            "(collapse 2, 2 Taylor terms), 5e6 counts, seed 2000")
+
+
+def _dup(s):
+    libc = C.CDLL(None)
+    libc.strdup.restype = C.c_void_p
+    libc.strdup.argtypes = [C.c_char_p]
+    return C.cast(libc.strdup(s.encode()), C.c_char_p) if s else None
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while active."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# --------------------------------------------------------------- workload
+
+def make_workload(lib, tmpdir):
+    from libirl_b200 import api, workloads as W
+    case = W.full128(seed=2000)
+    files = case.write_tables(tmpdir)
+    p, o, v = case.parms(), case.options(), case.views()
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    rc = lib.IrlGenprj(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), None, None,
+                       api.fptr(act), api.fptr(atn), api.fptr(prj), 1.0, None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    meas = W.poisson_counts(prj, case.counts, 2000)
+    return case, files, meas
+
+
+def run_b200(args):
+    import torch
+    import libirl_b200 as L
+    from libirl_b200 import api
+
+    rank, world = int(os.environ.get("RANK", "0")), _WORLD
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(0)
+    L.build()
+    lib = L.load()
+    tmp = tempfile.mkdtemp(prefix="irlbench_")
+    case, files, meas = make_workload(lib, tmp)
+    K, Wm, P = args.steps, args.warmup, 1
+    n3 = case.n * case.nz * case.n
+
+    # --- device-resident timing through the session API
+    p, o, v = case.parms(), case.options(), case.views()
+    p.NumIterations = Wm + K + P
+    atn = case.atn.copy()
+    rec = np.zeros_like(case.act)
+    m = meas.copy()
+    rc = lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]),
+                          api.ITER_CB(), None, api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    stream = torch.cuda.ExternalStream(lib.irlcu_stream())
+    if lib.IrlOsemIterate(Wm):
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = lib.irlcu_launch_count()
+    with ClockSampler(gpu_index) as clk:
+        ev0.record(stream)
+        rc = lib.IrlOsemIterate(K)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    launches = lib.irlcu_launch_count() - l0
+    ms_total = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / K
+
+    # --- stage profile over one more iteration (separate from the timing)
+    lib.irlcu_profile_enable(1)
+    lib.IrlOsemIterate(P)
+    prof = L.IrlcuProfile()
+    lib.irlcu_profile_read(C.byref(prof))
+    lib.irlcu_profile_enable(0)
+    lib.IrlOsemEnd(api.fptr(rec))
+
+    # --- end to end: the public call with host buffers, E_IT iterations
+    e2e = None
+    if not args.no_e2e:
+        E_IT = 10
+        for it in (1, E_IT):  # a short warm-up call, then the timed one
+            p, o, v = case.parms(), case.options(), case.views()
+            p.NumIterations = it
+            atn = case.atn.copy()
+            rec = np.zeros_like(case.act)
+            m = meas.copy()
+            cb = api.ITER_CB(lambda i, q: None)
+            t0 = time.perf_counter()
+            rc = lib.IrlOsem(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), cb, None,
+                             api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+            wall = time.perf_counter() - t0
+            if rc:
+                raise RuntimeError(lib.pchIrlErrorString().decode())
+        h2d = (meas.nbytes + case.atn.nbytes + case.act.nbytes) / E_IT
+        d2h = (case.act.nbytes * E_IT + case.act.nbytes) / E_IT
+        e2e = {"value": round(1000.0 * wall / E_IT, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "iterations": E_IT,
+               "includes": "set-up (tables, ESSE kernel spectra, attenuation tables, 8 norm images), "
+                           "host<->device copies from pageable memory, per-iteration callback"}
+
+    clocks = clk.summary()
+    roofline = make_roofline(prof, clocks)
+    stages = {L.STAGES[i]: {"ms": round(prof.ms[i], 3), "launches": int(prof.launches[i]),
+                            "gflop": round(prof.flops[i] / 1e9, 2), "gbyte": round(prof.bytes[i] / 1e9, 3)}
+              for i in range(6)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(case, files, views=args.cpu_views)
+        except Exception as e:  # the baseline is reported, never the product
+            cpu = {"value": None, "error": str(e)[:200]}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(ms_step / world, 3), "unit": "ms", "n_gpus": world, "steps": K,
+        "warmup": Wm, "ms_per_step": round(ms_step, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson data)",
+        "config": {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2: per-view attenuation tables 2.8 GB streamed every iteration",
+                   "scatter": "ESSE (GPU); learned surrogate not part of this line"},
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "stages_ms_per_iteration": {k: {**s, "ms": round(s["ms"] / P, 3)} for k, s in stages.items()},
+    }
+    print(json.dumps(line))
+
+
+def _traffic_from_profiles():
+    """Per-launch DRAM bytes of the DRF projector kernel from the committed
+    ncu summary (profiles/drf_conv_full128.md), or None."""
+    path = os.path.join(ROOT, "profiles", "drf_conv_full128.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def make_roofline(prof, clocks):
+    """The dominant stage is the direct DRF convolution (projector +
+    backprojector), an FP32 FMA-bound kernel: its bound is the CUDA-core FP32
+    peak, 148 SMs x 128 FMA lanes x 2 FLOP x SM clock, evaluated at the
+    median SM clock measured during the timed region (neither of the
+    measured HBM / bf16-tensor peaks bounds it)."""
+    i_p, i_b = 2, 4
+    ms = prof.ms[i_p] + prof.ms[i_b]
+    fl = prof.flops[i_p] + prof.flops[i_b]
+    launches = max(1, prof.launches[i_p] + prof.launches[i_b])
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = fl / (ms * 1e-3) / 1e12 if ms > 0 else 0.0
+    hbm = None
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak, src = peaks["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        hbm_peak, src = 6650.0, "fallback"
+    # memory-bound companion: unrotation + clamped accumulation
+    if prof.ms[5] > 0:
+        gbs = prof.bytes[5] / (prof.ms[5] * 1e-3) / 1e9
+        hbm = {"stage": "unrotate_accumulate", "achieved": round(gbs, 1), "peak": hbm_peak,
+               "unit": "GB/s", "frac": round(gbs / hbm_peak, 3), "peak_source": src}
+    return {"bound": "fp32", "kernel": "k_drf_forward / k_drf_backward (direct 33x33 DRF convolution)",
+            "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 3) if peak else None,
+            "peak_source": f"FP32 FMA peak at the measured median SM clock ({mhz:.0f} MHz)",
+            "traffic": _traffic_from_profiles(),
+            "algorithmic": "2 FLOP per PSF tap per output pixel, planes at distance > 0",
+            "launch_ms": round(ms / launches, 4), "hbm_companion": hbm}
+
+
+# ------------------------------------------------------------- CPU baseline
+
+def _ref_view_timer(case, files):
+    """Returns f(view) -> seconds of one view of an OSEM iteration
+    (Project with ESSE + DRF + attenuation, BackProject with DRF +
+    attenuation) run by the reference compiled here, and the kind."""
+    from libirl_b200 import api
+    from oracle import oracle as O
+    atn_i = O.to_internal(case.atn * np.float32(case.atn_scale))
+    est_i = O.to_internal(case.act)
+    n, nz = case.n, case.nz
+    if O.have_ref():
+        ref = O.ref()
+        F, I, FL = api.FLOAT_P, C.c_int, C.c_float
+
+        class Srf(C.Structure):
+            _fields_ = [("c", C.c_int), ("line", C.c_int), ("data", C.c_void_p)]
+
+        ref.pvInitESSEScatterModel.restype = C.c_void_p
+        ref.pvInitESSEScatterModel.argtypes = [C.c_char_p, C.c_char_p, FL, I, I, I, I]
+        ref.Project.restype = None
+        ref.Project.argtypes = [I, I, I, I, FL, I, FL, FL, C.POINTER(api.DrfTab), C.POINTER(Srf), F, F, F, FL, FL,
+                                I, I, I, I, I]
+        ref.BackProject.restype = None
+        ref.BackProject.argtypes = [I, I, I, I, FL, I, FL, FL, C.POINTER(api.DrfTab), C.POINTER(Srf), F, F, F, FL,
+                                    FL, I, I, I, I]
+        title, col = C.c_char_p(), C.c_char_p()
+        tab = ref.sReadDrfTab(files["drf"].encode(), C.byref(title), C.byref(col))
+        tab.psBckDrfTab = None
+        srf = Srf(case.collapse, 0, ref.pvInitESSEScatterModel(files["krnl"].encode(), b"2 2 2 3", case.pix, n, nz,
+                                                                case.collapse, 0))
+        ref.InitPrj(nz, n, n, 7)
+        calc = np.zeros((nz, n), np.float32)
+        img = np.zeros_like(est_i)
+
+        def one(view):
+            a, r = float(case.angles[view]), float(case.cfcr[view])
+            t0 = time.perf_counter()
+            ref.Project(nz, n, n, 7, case.pix, view, a, r, C.byref(tab), C.byref(srf), api.fptr(atn_i),
+                        api.fptr(est_i), api.fptr(calc), 1.0, 1.0, 0, 0, 0, 0, 1)
+            ratio = np.where(calc > 1e-20, 1.0 / np.maximum(calc, 1e-20), 0).astype(np.float32)
+            ref.BackProject(nz, n, n, 3, case.pix, view, a, r, C.byref(tab), C.byref(srf), api.fptr(atn_i),
+                            api.fptr(ratio), api.fptr(img), 1.0, 1.0, 0, 0, 1, 1)
+            return time.perf_counter() - t0
+        return one, "reference"
+    pr = O.Problem(case)
+    calc = np.zeros((nz, n), np.float32)
+    img = np.zeros_like(est_i)
+
+    def one_port(view):
+        t0 = time.perf_counter()
+        O.orc().or_project(C.byref(pr.P), 7, view, api.fptr(est_i), api.fptr(pr.atn), 1.0, api.fptr(calc))
+        ratio = np.where(calc > 1e-20, 1.0 / np.maximum(calc, 1e-20), 0).astype(np.float32)
+        O.orc().or_backproject(C.byref(pr.P), 3, view, api.fptr(pr.atn), api.fptr(ratio), api.fptr(img))
+        return time.perf_counter() - t0
+    return one_port, "port"
+
+
+def cpu_baseline(case, files, views=2):
+    one, kind = _ref_view_timer(case, files)
+    sel = [0, case.nviews // 3, 2 * case.nviews // 3][:max(1, views)]
+    secs = [one(v) for v in sel]
+    per_view = statistics.mean(secs)
+    return {"value": round(1000.0 * per_view * case.nviews, 1), "unit": "ms", "cores": 1, "kind": kind,
+            "sample": f"{len(sel)} of {case.nviews} views of one OSEM iteration (projection with ESSE + DRF + "
+                      f"attenuation and DRF + attenuation backprojection), single-threaded reference C, "
+                      f"mean {per_view:.2f} s/view, extrapolated x{case.nviews}",
+            "threads_available": os.cpu_count()}
+
+
+def run_reference(args):
+    """Reference arm: the reference's own CPU implementation, one view per
+    step, reported as ms per OSEM iteration (x120 views)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import libirl_b200.workloads as W
+    case = W.full128(seed=2000)
+    tmp = tempfile.mkdtemp(prefix="irlbench_ref_")
+    files = case.write_tables(tmp)
+    try:
+        one, kind = _ref_view_timer(case, files)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {e}"[:300]}))
+        return
+    for i in range(args.warmup):
+        one(i % case.nviews)
+    secs = [one((7 * (i + 1)) % case.nviews) for i in range(args.steps)]
+    per_view = statistics.median(secs)
+    val = round(1000.0 * per_view * case.nviews, 1)
+    print(json.dumps({
+        "metric": METRIC, "value": val, "unit": "ms", "n_gpus": _WORLD, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson data)",
+        "config": {"workload": WORKLOAD, "parallelism": "single"}, "impl": "reference",
+        "cpu_baseline": {"value": val, "unit": "ms", "cores": 1, "kind": kind,
+                         "sample": f"each step one of {case.nviews} views of an OSEM iteration (projection with ESSE + "
+                                   f"DRF + attenuation, backprojection), median {per_view:.2f} s/view, x{case.nviews}"},
+        "e2e": {"value": val, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-views", type=int, default=2)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

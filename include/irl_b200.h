@@ -1,0 +1,46 @@
+/*
+ * irl_b200.h -- entry points of libirl_b200 beyond libirl's API.
+ *
+ * IrlOsem (irl.h) is exactly IrlOsemBegin + IrlOsemIterate(NumIterations)
+ * + IrlOsemEnd.  The split lets a caller keep a reconstruction resident on
+ * the GPU and run its iterations in steps (benchmarks, interactive use,
+ * stopping rules).  libirl has no counterpart of these three functions.
+ *
+ * One session at a time per process (the library is non-reentrant, like
+ * libirl).  The caller's arrays follow IrlOsem's contract: pfAtnMap,
+ * pfPrjImage and pfScatterEstimate are modified in place by Begin, and
+ * pfReconImage must stay valid until End (hooks see it in the internal
+ * layout, as in libirl).
+ */
+#ifndef IRL_B200_H
+#define IRL_B200_H
+
+#include "irl.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Set-up of IrlOsem (everything before the first iteration, including the
+   normalisation images and the iteration-0 callback).  Returns 0 or an
+   error code (pchIrlErrorString gives the message); on error the session
+   is closed. */
+int IrlOsemBegin(IrlParms_t *psIrlParms, Options_t *psOptions, PrjView_t *psViews,
+	char *pchDrfTabFname, char *pchScatKrnlFname,
+	void (*pIterationCallbackFunc)(int IterationNumber, float *pfCurrentEst),
+	float *pfScatterEstimate, float *pfAtnMap, float *pfPrjImage, float *pfReconImage,
+	char *pchLogFname, char *pchMessageFname);
+
+/* Runs up to iNumIterations further iterations (never past NumIterations)
+   with hooks and callbacks as in IrlOsem; returns 0 or an error code. */
+int IrlOsemIterate(int iNumIterations);
+
+/* Copies the estimate (external layout) into pfReconImage and closes the
+   session.  Always safe to call; returns the session's error code. */
+int IrlOsemEnd(float *pfReconImage);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IRL_B200_H */

@@ -54,6 +54,8 @@ typedef struct {
 	const int *pad_rows;      /* per distance: min(iAxialPadLength, MaxOffsY-1) */
 	const int *row_idist;     /* nviews * n, host memory */
 	int avg_rows;             /* iAxialAvgLength, clamped to [0, nz] */
+	const int *taps;          /* per distance: (2*MaxOffsX-1)*(2*MaxOffsY-1),
+	                             the PSF's own extent (work accounting) */
 } irlcu_drf;
 
 /* ESSE scatter model (krnlprj3d.c:349-365, 676-954) */
@@ -132,6 +134,34 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
 
 /* synchronous wall-clock of the last batched call's stages, for tracing */
 int irlcu_stage_times(float *ms, int nmax);
+
+/* The CUDA stream every kernel of the library is launched on (a
+   cudaStream_t), so callers can time or order work against it. */
+void *irlcu_stream(void);
+
+/* Kernel launches issued by the library since the context was created. */
+long long irlcu_launch_count(void);
+
+/* Stage profiling.  While enabled, every stage of irlcu_osem_subset is
+   bracketed by CUDA events on the library stream; irlcu_profile_read()
+   waits for them and returns per-stage totals since the last enable:
+   device milliseconds, launches, and the algorithmic work of the stage
+   (FLOPs for the DRF convolutions, bytes for the memory-bound stages). */
+#define IRLCU_NSTAGE 8
+#define IRLCU_ST_ROTATE 0      /* rotation of the estimate */
+#define IRLCU_ST_ESSE 1        /* effective scatter source */
+#define IRLCU_ST_PROJECT 2     /* attenuated DRF projection (conv kernel) */
+#define IRLCU_ST_REDUCE 3      /* partial-sum reduction + ratio epilogue */
+#define IRLCU_ST_BACKPROJECT 4 /* attenuated DRF backprojection (conv kernel) */
+#define IRLCU_ST_ACCUM 5       /* unrotation + clamped accumulation + EM update */
+typedef struct {
+	double ms[IRLCU_NSTAGE];
+	double flops[IRLCU_NSTAGE];
+	double bytes[IRLCU_NSTAGE];
+	long long launches[IRLCU_NSTAGE];
+} irlcu_profile;
+int irlcu_profile_enable(int on);
+int irlcu_profile_read(irlcu_profile *out);
 
 #ifdef __cplusplus
 }

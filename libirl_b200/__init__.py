@@ -66,6 +66,35 @@ def _declare_irlcu(lib):
     lib.irl_gendrf.argtypes = [C.c_float] * 8 + [I, I, C.POINTER(api.Drf)]
     lib.irl_compute_subsets.restype = I
     lib.irl_compute_subsets.argtypes = [I, I, C.POINTER(C.POINTER(C.c_int))]
+    lib.irlcu_stream.restype = C.c_void_p
+    lib.irlcu_stream.argtypes = []
+    lib.irlcu_launch_count.restype = C.c_longlong
+    lib.irlcu_launch_count.argtypes = []
+    lib.irlcu_profile_enable.restype = I
+    lib.irlcu_profile_enable.argtypes = [I]
+    lib.irlcu_profile_read.restype = I
+    lib.irlcu_profile_read.argtypes = [C.POINTER(IrlcuProfile)]
+    lib.IrlOsemBegin.restype = I
+    lib.IrlOsemBegin.argtypes = list(lib.IrlOsem.argtypes)
+    lib.IrlOsemIterate.restype = I
+    lib.IrlOsemIterate.argtypes = [I]
+    lib.IrlOsemEnd.restype = I
+    lib.IrlOsemEnd.argtypes = [F]
+
+
+NSTAGE = 8
+STAGES = ["rotate", "esse", "project", "reduce_ratio", "backproject", "unrotate_accumulate", "-", "-"]
+
+
+class IrlcuProfile(C.Structure):
+    """irlcu_profile (include/irlcu.h)."""
+
+    _fields_ = [
+        ("ms", C.c_double * NSTAGE),
+        ("flops", C.c_double * NSTAGE),
+        ("bytes", C.c_double * NSTAGE),
+        ("launches", C.c_longlong * NSTAGE),
+    ]
 
 
 class IrlcuGeom(C.Structure):

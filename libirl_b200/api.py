@@ -168,7 +168,7 @@ def declare_irl(lib: C.CDLL) -> C.CDLL:
     lib.pvStoreDetectorData.restype = C.c_void_p
     lib.pvStoreDetectorData.argtypes = [
         C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int,
-        C.c_void_p,
+        C.c_char_p,
     ]
     lib.sReadDrfTab.restype = DrfTab
     lib.sReadDrfTab.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]

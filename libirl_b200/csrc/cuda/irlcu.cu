@@ -15,7 +15,62 @@
 namespace irlcu {
 
 Ctx *g_ctx = nullptr;
+long long g_launch_count = 0;
 static char g_err[1024] = "";
+
+// ------------------------------------------------------- stage profiling
+struct ProfRec {
+  int stage;
+  cudaEvent_t a, b;
+  double flops, bytes;
+  int launches;
+};
+static bool g_prof_on = false;
+static std::vector<ProfRec> g_prof;
+static std::vector<cudaEvent_t> g_prof_pool;
+static size_t g_prof_used = 0;
+static irlcu_profile g_prof_acc;
+
+static cudaEvent_t prof_event() {
+  if (g_prof_used == g_prof_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    g_prof_pool.push_back(e);
+  }
+  return g_prof_pool[g_prof_used++];
+}
+
+// RAII bracket of one stage on stream st
+struct Stage {
+  int stage;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  long long l0;
+  double flops = 0, bytes = 0;
+  Stage(int s, cudaStream_t st_) : stage(s), st(st_), l0(g_launch_count) {
+    if (g_prof_on && (a = prof_event())) cudaEventRecord(a, st);
+  }
+  ~Stage() {
+    if (!a) return;
+    cudaEvent_t b = prof_event();
+    if (!b) return;
+    cudaEventRecord(b, st);
+    g_prof.push_back(ProfRec{stage, a, b, flops, bytes, (int)(g_launch_count - l0)});
+  }
+};
+
+// algorithmic FLOPs of the DRF convolutions of a batch (2 per tap per
+// output pixel, taps = the PSF's own extent, planes with distance > 0)
+static double drf_flops(const Ctx &c, const DrfDev *d, const int *views, int nv) {
+  if (!d || !d->psf) return 0.0;
+  double f = 0.0;
+  for (int i = 0; i < nv; ++i)
+    for (int y = 0; y < c.n; ++y) {
+      const int id = d->h_rows[(size_t)views[i] * c.n + y];
+      if (id >= 0) f += 2.0 * (double)c.pln * d->h_taps[id];
+    }
+  return f;
+}
 
 int set_error(int code, const char *fmt, ...) {
   va_list ap;
@@ -254,6 +309,9 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   D.halo = H;
   D.pstride = PLD;
   D.avg_rows = d->avg_rows;
+  D.h_rows.assign(d->row_idist, d->row_idist + (size_t)c.nv * c.n);
+  D.h_taps.resize(d->ndist);
+  for (int i = 0; i < d->ndist; ++i) D.h_taps[i] = d->taps ? d->taps[i] : w * w;
   return IRLCU_OK;
 }
 
@@ -329,7 +387,7 @@ int irlcu_download_external(int buf, float *host) {
   TRY(buf_ptr(buf, 0, &p, &cap, false));
   if (!p || cap != c.vox) return set_error(IRLCU_EARG, "buffer %d is not a volume", buf);
   k_to_external<<<592, 256, 0, c.st>>>(p, c.wbck, c.n, c.nz);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   CU_TRY(cudaMemcpyAsync(host, c.wbck, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
   CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
@@ -379,19 +437,34 @@ int irlcu_prepare_attenuation(int need_srf) {
 }
 
 // rotated source of the batch in wrot (act) and, with SRF, act+scatter in src
-static int forward_batch(int nv, int model, float primary, float *out, float *out_nosrf) {
+static int forward_batch(int nv, const int *hviews, int model, float primary, float *out, float *out_nosrf) {
   Ctx &c = *g_ctx;
-  TRY(launch_rotate(c, c.est, 0, c.wrot, c.vox, c.dviews, nv, 0));
+  {
+    Stage s(IRLCU_ST_ROTATE, c.st);
+    s.bytes = 8.0 * (double)c.vox * nv;  // read the estimate, write each rotated copy
+    TRY(launch_rotate(c, c.est, 0, c.wrot, c.vox, c.dviews, nv, 0));
+  }
   const float *E = (model & MODEL_ATN_BIT) ? c.tE : nullptr;
   const DrfDev *drf = (model & MODEL_DRF_BIT) ? &c.drf[0] : nullptr;
+  const float *src = c.wrot;
+  float scale = primary;
   if (model & MODEL_SRF_BIT) {
     if (!c.esse.on && !c.esse.zero) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
     if (!c.tS) return set_error(IRLCU_ESTATE, "scatter model needs the attenuation tables");
+    Stage s(IRLCU_ST_ESSE, c.st);
     TRY(launch_esse(c, c.wrot, c.dviews, nv, primary, c.wbck));
-    TRY(launch_project(c, c.wbck, c.dviews, nv, E, drf, 1.0f, out));
-    if (out_nosrf) TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out_nosrf));
-  } else {
-    TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out));
+    src = c.wbck;
+    scale = 1.0f;
+  }
+  for (int pass = 0; pass < (out_nosrf ? 2 : 1); ++pass) {
+    Stage s(IRLCU_ST_PROJECT, c.st);
+    s.flops = drf_flops(c, drf, hviews, nv);
+    // algorithmic bytes: source and attenuation factor of every plane
+    s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;
+    if (pass == 0)
+      TRY(launch_project(c, src, c.dviews, nv, E, drf, scale, out));
+    else
+      TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out_nosrf));
   }
   return IRLCU_OK;
 }
@@ -402,7 +475,7 @@ int irlcu_project(int nv, const int *views, int model, float primary_fac, float 
   for (int v0 = 0; v0 < nv; v0 += c.g.max_batch) {
     const int nb = std::min(c.g.max_batch, nv - v0);
     TRY(upload_views(views + v0, nb, nullptr));
-    TRY(forward_batch(nb, model, primary_fac, c.wprj, nullptr));
+    TRY(forward_batch(nb, views + v0, model, primary_fac, c.wprj, nullptr));
     CU_TRY(cudaMemcpyAsync(dst + (size_t)v0 * c.pln, c.wprj, (size_t)nb * c.pln * 4,
                            dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.st));
   }
@@ -431,17 +504,32 @@ int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp, int m
   float *calc_nosrf = c.wprj2;
   float *ratio = c.wprj2 + c.pln * c.g.max_batch;
   CU_TRY(cudaEventRecord(c.ev[0], c.st));
-  TRY(forward_batch(nv, model, 1.0f, calc, need_nosrf ? calc_nosrf : nullptr));
+  TRY(forward_batch(nv, views, model, 1.0f, calc, need_nosrf ? calc_nosrf : nullptr));
   CU_TRY(cudaEventRecord(c.ev[1], c.st));
-  TRY(launch_ratio(c, calc, calc_nosrf, c.dviews, c.dvp, nv, use_scatest, ratio));
+  {
+    Stage s(IRLCU_ST_REDUCE, c.st);
+    s.bytes = 16.0 * (double)c.pln * nv;
+    TRY(launch_ratio(c, calc, calc_nosrf, c.dviews, c.dvp, nv, use_scatest, ratio));
+  }
   const float *E = (bck_model & MODEL_ATN_BIT) ? c.tE : nullptr;
   const DrfDev *drf = nullptr;
   if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
-  TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
+  {
+    Stage s(IRLCU_ST_BACKPROJECT, c.st);
+    s.flops = drf_flops(c, drf, views, nv);
+    s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;  // attenuation factor read, plane written
+    TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
+  }
   CU_TRY(cudaEventRecord(c.ev[2], c.st));
-  TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nv, c.upd, accumulate_from_update,
-                                 apply_update ? ACC_EM : 0, c.est,
-                                 apply_update ? c.norm + (size_t)subset * c.vox : nullptr));
+  {
+    Stage s(IRLCU_ST_ACCUM, c.st);
+    // unrotation (read + write per view), accumulation read per view, and
+    // the update / estimate read-modify-write
+    s.bytes = 12.0 * (double)c.vox * nv + 16.0 * (double)c.vox;
+    TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nv, c.upd, accumulate_from_update,
+                                   apply_update ? ACC_EM : 0, c.est,
+                                   apply_update ? c.norm + (size_t)subset * c.vox : nullptr));
+  }
   CU_TRY(cudaEventRecord(c.ev[3], c.st));
   return IRLCU_OK;
 }
@@ -514,6 +602,35 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   TRY(launch_rotate(c, s, 0, d, c.vox, c.dviews, 1, r));
   if (!on_device) CU_TRY(cudaMemcpyAsync(dst, c.wrot, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
   CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+void *irlcu_stream(void) { return g_ctx ? (void *)g_ctx->st : nullptr; }
+
+long long irlcu_launch_count(void) { return g_launch_count; }
+
+int irlcu_profile_enable(int on) {
+  if (g_ctx) cudaStreamSynchronize(g_ctx->st);
+  g_prof.clear();
+  g_prof_used = 0;
+  std::memset(&g_prof_acc, 0, sizeof(g_prof_acc));
+  g_prof_on = on != 0;
+  return IRLCU_OK;
+}
+
+int irlcu_profile_read(irlcu_profile *out) {
+  for (const ProfRec &r : g_prof) {
+    float ms = 0.f;
+    CU_TRY(cudaEventSynchronize(r.b));
+    CU_TRY(cudaEventElapsedTime(&ms, r.a, r.b));
+    g_prof_acc.ms[r.stage] += ms;
+    g_prof_acc.flops[r.stage] += r.flops;
+    g_prof_acc.bytes[r.stage] += r.bytes;
+    g_prof_acc.launches[r.stage] += r.launches;
+  }
+  g_prof.clear();
+  g_prof_used = 0;
+  if (out) *out = g_prof_acc;
   return IRLCU_OK;
 }
 

@@ -6,6 +6,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "irlcu.h"
 
 namespace irlcu {
@@ -30,6 +32,8 @@ struct DrfDev {
   int pstride = 0;            // row stride of a PSF (multiple of 4 floats)
   int *pad_rows = nullptr;    // per distance
   int *row_idist = nullptr;   // nviews * n
+  std::vector<int> h_rows;    // host copy of row_idist (work accounting)
+  std::vector<int> h_taps;    // per distance: taps of the unpadded PSF
 };
 
 struct EsseDev {
@@ -91,6 +95,15 @@ int set_error(int code, const char *fmt, ...);
     if (e_ != cudaSuccess)                                                \
       return ::irlcu::set_error(IRLCU_ECUDA, "%s:%d %s: %s", __FILE__,    \
                                 __LINE__, #x, cudaGetErrorString(e_));    \
+  } while (0)
+
+// every kernel launch is followed by CU_LAUNCHED(): it counts the launch
+// (irlcu_launch_count) and checks the launch status
+extern long long g_launch_count;
+#define CU_LAUNCHED()                      \
+  do {                                     \
+    ++::irlcu::g_launch_count;             \
+    CU_TRY(cudaGetLastError());            \
   } while (0)
 
 // ---- launchers (each defined in its kernel file) ----

@@ -320,7 +320,7 @@ static int fwd_launch(const Ctx &c, FwdArgs a) {
   a.part = c.wpart;
   g_fwd_grid = G;
   k_drf_forward<H><<<(unsigned)G, C::NT, C::SMEM, c.st>>>(a);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -334,7 +334,7 @@ static int bck_launch(const Ctx &c, BckArgs a, int nv) {
   }
   dim3 grid(a.ntiles, a.n, nv);
   k_drf_backward<H><<<grid, C::NT, C::SMEM, c.st>>>(a);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -377,7 +377,7 @@ int launch_project(const Ctx &c, const float *src, const int *dviews, int nv, co
   const size_t tot = (size_t)nv * c.pln;
   k_forward_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(c.wpart, a.T, g_fwd_grid, c.n, c.nz, a.ntx,
                                                                       a.ntiles, nv, scale, out);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -436,7 +436,7 @@ __global__ void k_atn_tables(const float *__restrict__ rmu, float *__restrict__ 
 int launch_atn_tables(const Ctx &c, const float *rmu, float *E, float *S, int nv) {
   const size_t tot = (size_t)nv * c.pln;
   k_atn_tables<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(rmu, E, S, c.n, c.nz, nv);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 

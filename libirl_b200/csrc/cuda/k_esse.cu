@@ -501,7 +501,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   {
     dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nb);
     LDISPATCH(E.kx, k_fft_row_fwd, grid_, 256, 0, st, ra, g_ew.twx);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   // z lines (outer = y' < nyv) -> tmpB [nb][nyv][Kz][kxh]
   ColArgs za{};
@@ -521,7 +521,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   {
     dim3 grid_((kxh + CW - 1) / CW, nyv, nb);
     LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), st, za, g_ew.twz);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   // y lines (outer = z < Kz) -> out [nb][Ky][Kz][kxh]
   ColArgs ya{};
@@ -541,7 +541,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   {
     dim3 grid_((kxh + CW - 1) / CW, E.kz, nb);
     LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), st, ya, g_ew.twy);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   return IRLCU_OK;
 }
@@ -646,7 +646,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     // factor is 0 (krnlprj3d.c:714-722): src = act * primary
     const size_t tot = (size_t)nv * c.vox;
     k_scale_copy<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(rot, src, primary, tot);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
     return IRLCU_OK;
   }
   if (nv > w.batch) return set_error(IRLCU_EARG, "ESSE batch %d exceeds %d", nv, w.batch);
@@ -677,7 +677,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   {
     dim3 grid_((kxh + CW - 1) / CW, E.kz, nv);
     LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), c.st, ya, w.twy);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   // inverse z -> D[t] [nv][nyv][nzv][kxh]
   for (int t = 0; t < E.nterms; ++t) {
@@ -697,7 +697,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     za.s = -1.f;
     dim3 grid_((kxh + CW - 1) / CW, nyv, nv);
     LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), c.st, za, w.twz);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   // inverse x (real part, cropped, 1/(Kx Ky Kz)) -> g[t] [nv][nyv][nzv][nxv]
   RowInvArgs ri{};
@@ -714,7 +714,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   {
     dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
     LDISPATCH(E.kx, k_fft_row_inv, grid_, 256, 0, c.st, ri, w.twx);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   // expansion + smoothing (y, z), then x smoothing fused with the combine
   const int cf = E.collapse;
@@ -726,10 +726,10 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     const size_t lines = (size_t)nv * c.pln;
     k_expand_y<<<(unsigned)((lines + 255) / 256), 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n,
                                                                   c.nz, cf, nyv, nzv, nxv, nv);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
     const size_t zl = (size_t)nv * c.n * c.n;
     k_smooth_z<<<(unsigned)((zl + 255) / 256), 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, nv);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   CombineArgs ca{};
   ca.t0 = w.T[0];
@@ -751,7 +751,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   {
     dim3 grid_(c.n, (c.nz + 7) / 8, nv);
     k_smooth_x_combine<<<grid_, 256, sizeof(float) * 2 * 8 * c.n, c.st>>>(ca);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
   }
   return IRLCU_OK;
 }

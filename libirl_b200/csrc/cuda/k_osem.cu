@@ -49,7 +49,7 @@ int launch_ratio(const Ctx &c, const float *calc, const float *calc_nosrf, const
   k_ratio<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(calc, calc_nosrf, dviews, dvp, c.prj, c.scatest,
                                                             c.prjscat, c.colmask, nv, c.n, c.nz, use_scatest,
                                                             ratio);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -74,7 +74,7 @@ int launch_norm_planes(const Ctx &c, const int *dviews, const float *vt_dev, int
   const size_t tot = (size_t)nv * c.pln;
   k_norm_planes<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(dviews, vt_dev, c.prj, c.colmask, nv, c.n, c.nz,
                                                                   planes);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 

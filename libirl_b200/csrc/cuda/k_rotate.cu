@@ -263,7 +263,7 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   if (!c.g.fast_rotate) {
     dim3 grid((n * n + 255) / 256, nv);
     k_rot3dpar<<<grid, 256, 0, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, n, nz);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
     return IRLCU_OK;
   }
   const int xld = 2 * n;  // mdim < 2n always
@@ -280,7 +280,7 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
     }
     k_shear_smem<<<grid, 512, smem, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base, c.rot,
                                             c.sup_start, c.sup_end, n, nz, xld);
-    CU_TRY(cudaGetLastError());
+    CU_LAUNCHED();
     return IRLCU_OK;
   }
   const size_t need = (size_t)nv * nz * n * xld;
@@ -293,10 +293,10 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   }
   k_shear_pass1_glob<<<grid, 512, 0, c.st>>>(src, src_stride, g_xscratch, dviews, rot_base, c.rot,
                                              c.sup_start, c.sup_end, n, nz, xld);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   k_shear_pass23_glob<<<grid, 512, 0, c.st>>>(g_xscratch, dst, dst_stride, dviews, rot_base, c.rot,
                                               c.sup_start, c.sup_end, n, nz, xld);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -336,7 +336,7 @@ int launch_unrotate_accumulate(const Ctx &c, const float *bck, const int *dviews
   int blocks = (int)((c.vox + 255) / 256);
   if (blocks > 148 * 16) blocks = 148 * 16;
   k_accumulate<<<blocks, 256, 0, c.st>>>(c.wrot, c.vox, nv, acc, start_from_acc, mode, est, norm, c.vox);
-  CU_TRY(cudaGetLastError());
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 

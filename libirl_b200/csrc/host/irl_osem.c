@@ -7,6 +7,10 @@
  * include/irlcu.h: every view of a subset is projected, compared with the
  * data and backprojected in one batched stage, and the clamped accumulation
  * keeps libirl's view order.
+ *
+ * IrlOsem = IrlOsemBegin (set-up, normalisation images, iteration-0
+ * callback) + IrlOsemIterate (the iterations) + IrlOsemEnd (result copy and
+ * release); the three are exported (include/irl_b200.h).
  */
 #include <setjmp.h>
 #include <stdio.h>
@@ -15,6 +19,7 @@
 #include <time.h>
 #include <unistd.h>
 
+#include "irl_b200.h"
 #include "irl_err.h"
 #include "irl_geom.h"
 #include "irl_host.h"
@@ -52,37 +57,83 @@ static double now_s(void)
 	return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-/* host mirrors handed to hooks (osemhooks.h:18-27) */
-typedef struct {
-	sOsemData d;
-	int any;
-	size_t vox, prjn;
-	int norm_subset;
-} hook_state;
+/* ---------------------------------------------------------------- session */
 
-static void hook_call(hook_state *h, int which)
+typedef struct {
+	int open;
+	irl_parms p;
+	irl_view *views;
+	irl_esse_host esse;
+	FILE *logfp, *msgfp;
+	float *recon;            /* caller's image: internal layout during the run */
+	float *prjscat;          /* host copy of the stored scatter projections */
+	float *tmp;              /* external-layout callback image */
+	float *norm_host, *upd_host;
+	void (*cb)(int, float *);
+	int use_scatest;
+	int *ang, ns, per, max_batch;
+	int it;                  /* last completed iteration */
+	int this_srf, next_srf;
+	irlcu_view_parm *vp;
+	sOsemData hd;            /* hook data (osemhooks.h:18-27) */
+	int hook_norm;           /* subset whose norm the hooks see, or -1 */
+	size_t vox, prjn;
+} osem_session;
+
+static osem_session S;
+
+static void session_close(void)
+{
+	irlcu_shutdown();
+	irl_free_run_tables();
+	free(S.views);
+	free(S.prjscat);
+	free(S.tmp);
+	free(S.norm_host);
+	free(S.upd_host);
+	free(S.ang);
+	free(S.vp);
+	irl_esse_free(&S.esse);
+	if (S.logfp != NULL) {
+		fclose(S.logfp);
+		irl_set_log_file(NULL);
+	}
+	if (S.msgfp != NULL) {
+		fclose(S.msgfp);
+		irl_set_msg_file(NULL);
+	}
+	memset(&S, 0, sizeof(S));
+}
+
+/* copies the device state to the hook mirrors, calls the hook, copies back */
+static void hook_call(int which)
 {
 	irl_hook_fn f = g_irl_hooks[which];
 	if (f == NULL)
 		return;
-	irl_cu(irlcu_download(IRLCU_BUF_EST, 0, h->d.pfEst, h->vox), "hook");
-	irl_cu(irlcu_download(IRLCU_BUF_UPDATE, 0, h->d.pfUpdate, h->vox), "hook");
-	if (h->norm_subset >= 0)
-		irl_cu(irlcu_download(IRLCU_BUF_NORM, h->norm_subset, h->d.pfNorm, h->vox), "hook");
-	if (h->d.pfSct != NULL)
-		irl_cu(irlcu_download(IRLCU_BUF_PRJSCAT, 0, h->d.pfSct, h->prjn), "hook");
-	f(&h->d, g_irl_hook_ctx);
-	irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, h->d.pfEst, h->vox), "hook");
-	irl_cu(irlcu_upload(IRLCU_BUF_UPDATE, 0, h->d.pfUpdate, h->vox), "hook");
-	if (h->d.pfSct != NULL)
-		irl_cu(irlcu_upload(IRLCU_BUF_PRJSCAT, 0, h->d.pfSct, h->prjn), "hook");
+	irl_cu(irlcu_download(IRLCU_BUF_EST, 0, S.hd.pfEst, S.vox), "hook");
+	irl_cu(irlcu_download(IRLCU_BUF_UPDATE, 0, S.hd.pfUpdate, S.vox), "hook");
+	if (S.hook_norm >= 0)
+		irl_cu(irlcu_download(IRLCU_BUF_NORM, S.hook_norm, S.hd.pfNorm, S.vox), "hook");
+	if (S.hd.pfSct != NULL)
+		irl_cu(irlcu_download(IRLCU_BUF_PRJSCAT, 0, S.hd.pfSct, S.prjn), "hook");
+	f(&S.hd, g_irl_hook_ctx);
+	irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, S.hd.pfEst, S.vox), "hook");
+	irl_cu(irlcu_upload(IRLCU_BUF_UPDATE, 0, S.hd.pfUpdate, S.vox), "hook");
+	if (S.hd.pfSct != NULL)
+		irl_cu(irlcu_upload(IRLCU_BUF_PRJSCAT, 0, S.hd.pfSct, S.prjn), "hook");
 }
 
-static void write_norm_file(const char *base, int s, const float *img, size_t vox)
+static void norm_file(const char *base, int s, const float *img, size_t vox, int del)
 {
 	char *name = (char *)irl_malloc(strlen(base) + 40, "norm name");
 	FILE *fp;
 	sprintf(name, "%s.norm.%d.dat", base, s);
+	if (del) {
+		unlink(name);
+		free(name);
+		return;
+	}
 	fp = fopen(name, "wb");
 	if (fp == NULL) {
 		free(name);
@@ -95,131 +146,6 @@ static void write_norm_file(const char *base, int s, const float *img, size_t vo
 	}
 	fclose(fp);
 	free(name);
-}
-
-static void delete_norm_files(const char *base, int ns)
-{
-	char *name = (char *)irl_malloc(strlen(base) + 40, "norm name");
-	int s;
-	for (s = 0; s < ns; ++s) {
-		sprintf(name, "%s.norm.%d.dat", base, s);
-		unlink(name);
-	}
-	free(name);
-}
-
-/* the OSEM loop (vOsemRecon, osemrecon.c:557-897); the estimate is on the
-   device in internal layout */
-static void osem_loop(irl_parms *p, irl_view *views, int use_scatest, float *est_host, float *prjscat_host,
-	void (*cb)(int, float *), int max_batch)
-{
-	int *ang = NULL, ns, s, m, it, per = p->ang_per_subset;
-	int prj_srf = p->prj_model & MODEL_SRF, this_srf = 0, next_srf = 0;
-	int angle_hooks = g_irl_hooks[HOOK_PREV_ANGLE] || g_irl_hooks[HOOK_POST_ANGLE];
-	size_t vox = (size_t)p->n * p->nz * p->n;
-	hook_state h;
-	float *tmp = NULL, *norm_host = NULL, *upd_host = NULL;
-	irlcu_view_parm *vp = NULL;
-	float *vt = NULL;
-	double t0 = now_s();
-
-	ns = irl_compute_subsets(p->nviews, per, &ang);
-	irl_cu(irlcu_alloc_norm(ns), "OsemRecon");
-	vt = (float *)irl_malloc(sizeof(float) * per, "view times");
-	for (s = 0; s < ns; ++s) {
-		for (m = 0; m < per; ++m)
-			vt[m] = views[ang[s * per + m]].view_time;
-		irl_cu(irlcu_norm_subset(per, ang + s * per, vt, p->bck_model, s), "ComputeNormImages");
-		if (p->norm_base != NULL) {
-			if (tmp == NULL)
-				tmp = (float *)irl_malloc(sizeof(float) * vox, "norm image");
-			irl_cu(irlcu_download(IRLCU_BUF_NORM, s, tmp, vox), "ComputeNormImages");
-			write_norm_file(p->norm_base, s, tmp, vox);
-		}
-	}
-	irl_msg(5, "Done Computing Norm Matrix (%.3f s)\n", now_s() - t0);
-
-	memset(&h, 0, sizeof(h));
-	h.vox = vox;
-	h.prjn = (size_t)p->nviews * p->nz * p->n;
-	h.norm_subset = -1;
-	h.any = 0;
-	for (m = 0; m < 6; ++m)
-		h.any |= g_irl_hooks[m] != NULL;
-	if (h.any) {
-		norm_host = (float *)irl_calloc(sizeof(float) * vox, "norm mirror");
-		upd_host = (float *)irl_calloc(sizeof(float) * vox, "update mirror");
-	}
-	h.d.pfEst = est_host;
-	h.d.pfSct = prjscat_host;
-	h.d.pfNorm = norm_host;
-	h.d.pfUpdate = upd_host;
-
-	if (prj_srf)
-		next_srf = p->start_iteration + 1 <= p->srf_iters;
-	p->start_iteration = g_irl_adv.iStartIteration;
-	vp = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * per, "view parameters");
-	if (cb != NULL && tmp == NULL)
-		tmp = (float *)irl_malloc(sizeof(float) * vox, "callback image");
-
-	for (it = p->start_iteration + 1; it <= p->iterations; ++it) {
-		int model = p->prj_model, mode = 0;
-		double ti = now_s();
-		h.d.iIterationIdx = it;
-		hook_call(&h, HOOK_PREV_ITER);
-		if (prj_srf) {
-			this_srf = next_srf;
-			next_srf = (it == p->iterations) ? this_srf : (it + 1 <= p->srf_iters);
-			model = this_srf ? p->prj_model : (p->prj_model & ~MODEL_SRF);
-			mode = !this_srf ? 1 : (!next_srf ? 2 : 0);
-		}
-		for (s = 0; s < ns; ++s) {
-			const int *va = ang + s * per;
-			h.d.iSubsetIdx = s;
-			hook_call(&h, HOOK_PREV_SUBSET);
-			for (m = 0; m < per; ++m) {
-				vp[m].view_time = views[va[m]].view_time;
-				vp[m].sensitivity = views[va[m]].sensitivity;
-				vp[m].scat_mode = mode;
-			}
-			if (angle_hooks) {
-				for (m = 0; m < per; ++m) {
-					h.d.iAngleIdx = va[m];
-					hook_call(&h, HOOK_PREV_ANGLE);
-					irl_cu(irlcu_osem_subset(1, va + m, vp + m, model, p->bck_model, s, use_scatest,
-						       m == per - 1, m > 0),
-						"OsemRecon");
-					if (m == per - 1)
-						h.norm_subset = s;
-					hook_call(&h, HOOK_POST_ANGLE);
-				}
-			} else {
-				int m0;
-				for (m0 = 0; m0 < per; m0 += max_batch) {
-					int nb = per - m0 < max_batch ? per - m0 : max_batch;
-					irl_cu(irlcu_osem_subset(nb, va + m0, vp + m0, model, p->bck_model, s, use_scatest,
-						       m0 + nb >= per, m0 > 0),
-						"OsemRecon");
-				}
-				h.norm_subset = s;
-			}
-			hook_call(&h, HOOK_POST_SUBSET);
-		}
-		hook_call(&h, HOOK_POST_ITER);
-		if (cb != NULL) {
-			irl_cu(irlcu_download_external(IRLCU_BUF_EST, tmp), "OsemRecon");
-			cb(it, tmp);
-		}
-		irl_msg(4, "----Done iteration %d (%.3f s)\n", it, now_s() - ti);
-	}
-	if (p->norm_base != NULL)
-		delete_norm_files(p->norm_base, ns);
-	free(ang);
-	free(vt);
-	free(vp);
-	free(tmp);
-	free(norm_host);
-	free(upd_host);
 }
 
 /* opens the log and message files (irlosem.c:113-141) */
@@ -321,104 +247,237 @@ void irl_device_setup(irl_parms *p, irl_view *views, const float *atn_internal, 
 	free(m2);
 }
 
-int IrlOsem(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
+/* normalisation images of every subset (psComputeNormImages,
+   osemrecon.c:223-343) */
+static void compute_norms(void)
+{
+	irl_parms *p = &S.p;
+	float *vt = (float *)irl_malloc(sizeof(float) * S.per, "view times");
+	float *img = NULL;
+	int s, m;
+	double t0 = now_s();
+	irl_cu(irlcu_alloc_norm(S.ns), "OsemRecon");
+	for (s = 0; s < S.ns; ++s) {
+		for (m = 0; m < S.per; ++m)
+			vt[m] = S.views[S.ang[s * S.per + m]].view_time;
+		irl_cu(irlcu_norm_subset(S.per, S.ang + s * S.per, vt, p->bck_model, s), "ComputeNormImages");
+		if (p->norm_base != NULL) {
+			if (img == NULL)
+				img = (float *)irl_malloc(sizeof(float) * S.vox, "norm image");
+			irl_cu(irlcu_download(IRLCU_BUF_NORM, s, img, S.vox), "ComputeNormImages");
+			norm_file(p->norm_base, s, img, S.vox, 0);
+		}
+	}
+	free(vt);
+	free(img);
+	irl_msg(5, "Done Computing Norm Matrix (%.3f s)\n", now_s() - t0);
+}
+
+int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
 	void (*cb)(int, float *), float *scatest, float *atn, float *prj, float *recon, char *logname, char *msgname)
 {
 	jmp_buf env;
-	int err = 0;
-	/* static: their contents must survive the longjmp of a fatal error */
-	static irl_parms p;
-	static irl_esse_host esse;
-	irl_view *volatile views = NULL;
-	float *volatile tmp = NULL;
-	float *volatile prjscat = NULL;
-	FILE *volatile logfp = NULL;
-	FILE *volatile msgfp = NULL;
+	int err, m;
 	double t0 = now_s();
-
-	memset(&esse, 0, sizeof(esse));
+	if (S.open)
+		session_close();
+	memset(&S, 0, sizeof(S));
+	S.open = 1;
+	S.hook_norm = -1;
 	if ((err = setjmp(env)) != 0) {
 		fprintf(stderr, "FATAL ERROR Trapped: err_num=%d\nErrMsg=%s\n", err, irl_last_error());
 		irl_msg(1, "aborted\n");
-		goto abort;
+		irl_untrap();
+		session_close();
+		return err;
 	}
 	irl_trap(&env);
-	{
-		FILE *l, *m;
-		open_logs(logname, msgname, op->iMsgLevel, &l, &m);
-		logfp = l;
-		msgfp = m;
-	}
-	irl_setup_parms(ip, op, atn, krnl_fname, &p);
-	views = irl_setup_views(ip, pv);
-	if (p.model & MODEL_SRF) {
+	open_logs(logname, msgname, op->iMsgLevel, &S.logfp, &S.msgfp);
+	irl_setup_parms(ip, op, atn, krnl_fname, &S.p);
+	S.views = irl_setup_views(ip, pv);
+	if (S.p.model & MODEL_SRF) {
 		if (atn == NULL)
 			irl_fatal(IRL_E_VALUE, "SrfSetup", "scatter modelling needs an attenuation map");
-		irl_esse_prepare(krnl_fname, &p, ip->SrfCollapseFac, &esse);
+		irl_esse_prepare(krnl_fname, &S.p, ip->SrfCollapseFac, &S.esse);
 	}
 	{
 		irl_detector *d;
 		/* libirl calls vSetupDrfTables unconditionally (irlosem.c:158-160) */
-		irl_setup_drf_tables(&p, op, views, drf_fname, &d);
+		irl_setup_drf_tables(&S.p, op, S.views, drf_fname, &d);
 	}
-	{
-		size_t vox = (size_t)p.n * p.nz * p.n, prjn = (size_t)p.n * p.nz * p.nviews;
-		tmp = (float *)irl_malloc(sizeof(float) * vox, "IrlOsem:Temp");
-		if (atn != NULL) {
-			irl_reorder(p.nz, p.n, p.n, atn, tmp);
-			memcpy(atn, tmp, sizeof(float) * vox);
-		}
-		if (!op->bReconIsInitEst) {
-			irl_initial_estimate(&p, op->bUseContourSupport, op->fAtnMapThresh, views, prj, atn, recon);
-		} else {
-			irl_reorder(p.nz, p.n, p.n, recon, tmp);
-			memcpy(recon, tmp, sizeof(float) * vox);
-		}
-		zero_neg(prj, prjn);
-		if (atn != NULL) {
-			if (ip->fAtnScaleFac > 0 && ip->fAtnScaleFac != 1.0)
-				scale_f(atn, vox, ip->fAtnScaleFac);
-			zero_neg(atn, vox);
-		}
-		if (scatest != NULL) {
-			if (ip->fScatEstFac > 0 && ip->fScatEstFac != 1.0)
-				scale_f(scatest, prjn, ip->fScatEstFac);
-			zero_neg(scatest, prjn);
-		}
-		zero_neg(recon, vox);
-		if (cb != NULL) {
-			irl_reorder(p.n, p.nz, p.n, recon, tmp);
-			cb(0, tmp);
-		}
-		irl_device_setup(&p, views, atn, &esse, g_irl_adv.bFastRotate, p.ang_per_subset > 32 ? 32 : p.ang_per_subset);
-		irl_cu(irlcu_upload(IRLCU_BUF_PRJ, 0, prj, prjn), "IrlOsem");
-		irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, recon, vox), "IrlOsem");
-		if (scatest != NULL)
-			irl_cu(irlcu_upload(IRLCU_BUF_SCATEST, 0, scatest, prjn), "IrlOsem");
-		if ((p.prj_model & MODEL_SRF) && p.srf_iters > 0) {
-			prjscat = (float *)irl_calloc(sizeof(float) * prjn, "OsemRecon:PrjScatEst");
-			irl_cu(irlcu_zero(IRLCU_BUF_PRJSCAT, 0), "IrlOsem");
-		}
-		irl_msg(5, "Done Initialization (%.3f s)\n", now_s() - t0);
-		osem_loop(&p, views, scatest != NULL, recon, prjscat, cb, p.ang_per_subset > 32 ? 32 : p.ang_per_subset);
-		irl_cu(irlcu_download_external(IRLCU_BUF_EST, recon), "IrlOsem");
-		irl_msg(4, "done (%.3f s)\n", now_s() - t0);
+	S.vox = (size_t)S.p.n * S.p.nz * S.p.n;
+	S.prjn = (size_t)S.p.n * S.p.nz * S.p.nviews;
+	S.tmp = (float *)irl_malloc(sizeof(float) * S.vox, "IrlOsem:Temp");
+	if (atn != NULL) {
+		irl_reorder(S.p.nz, S.p.n, S.p.n, atn, S.tmp);
+		memcpy(atn, S.tmp, sizeof(float) * S.vox);
 	}
-abort:
+	if (!op->bReconIsInitEst) {
+		irl_initial_estimate(&S.p, op->bUseContourSupport, op->fAtnMapThresh, S.views, prj, atn, recon);
+	} else {
+		irl_reorder(S.p.nz, S.p.n, S.p.n, recon, S.tmp);
+		memcpy(recon, S.tmp, sizeof(float) * S.vox);
+	}
+	zero_neg(prj, S.prjn);
+	if (atn != NULL) {
+		if (ip->fAtnScaleFac > 0 && ip->fAtnScaleFac != 1.0)
+			scale_f(atn, S.vox, ip->fAtnScaleFac);
+		zero_neg(atn, S.vox);
+	}
+	if (scatest != NULL) {
+		if (ip->fScatEstFac > 0 && ip->fScatEstFac != 1.0)
+			scale_f(scatest, S.prjn, ip->fScatEstFac);
+		zero_neg(scatest, S.prjn);
+	}
+	zero_neg(recon, S.vox);
+	if (cb != NULL) {
+		irl_reorder(S.p.n, S.p.nz, S.p.n, recon, S.tmp);
+		cb(0, S.tmp);
+	}
+	S.per = S.p.ang_per_subset;
+	S.max_batch = S.per > 32 ? 32 : S.per;
+	S.ns = irl_compute_subsets(S.p.nviews, S.per, &S.ang);
+	irl_device_setup(&S.p, S.views, atn, &S.esse, g_irl_adv.bFastRotate, S.max_batch);
+	irl_cu(irlcu_upload(IRLCU_BUF_PRJ, 0, prj, S.prjn), "IrlOsem");
+	irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, recon, S.vox), "IrlOsem");
+	if (scatest != NULL)
+		irl_cu(irlcu_upload(IRLCU_BUF_SCATEST, 0, scatest, S.prjn), "IrlOsem");
+	S.use_scatest = scatest != NULL;
+	if ((S.p.prj_model & MODEL_SRF) && S.p.srf_iters > 0) {
+		S.prjscat = (float *)irl_calloc(sizeof(float) * S.prjn, "OsemRecon:PrjScatEst");
+		irl_cu(irlcu_zero(IRLCU_BUF_PRJSCAT, 0), "IrlOsem");
+	}
+	S.recon = recon;
+	S.cb = cb;
+	irl_msg(5, "Done Initialization (%.3f s)\n", now_s() - t0);
+	compute_norms();
+	for (m = 0; m < 6; ++m)
+		if (g_irl_hooks[m] != NULL && S.norm_host == NULL) {
+			S.norm_host = (float *)irl_calloc(sizeof(float) * S.vox, "norm mirror");
+			S.upd_host = (float *)irl_calloc(sizeof(float) * S.vox, "update mirror");
+		}
+	S.hd.pfEst = recon;
+	S.hd.pfSct = S.prjscat;
+	S.hd.pfNorm = S.norm_host;
+	S.hd.pfUpdate = S.upd_host;
+	if (S.p.prj_model & MODEL_SRF)
+		S.next_srf = S.p.start_iteration + 1 <= S.p.srf_iters;
+	S.p.start_iteration = g_irl_adv.iStartIteration;
+	S.it = S.p.start_iteration;
+	S.vp = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * S.per, "view parameters");
 	irl_untrap();
-	irlcu_shutdown();
-	irl_free_run_tables();
-	free(views);
-	free(tmp);
-	free(prjscat);
-	irl_esse_free(&esse);
-	if (logfp != NULL) {
-		fclose(logfp);
-		irl_set_log_file(NULL);
+	return 0;
+}
+
+/* one OSEM iteration: subset loop of osemrecon.c:637-883 */
+static void one_iteration(void)
+{
+	irl_parms *p = &S.p;
+	int it = S.it + 1, s, m, model = p->prj_model, mode = 0;
+	int angle_hooks = g_irl_hooks[HOOK_PREV_ANGLE] || g_irl_hooks[HOOK_POST_ANGLE];
+	double ti = now_s();
+	S.hd.iIterationIdx = it;
+	hook_call(HOOK_PREV_ITER);
+	if (p->prj_model & MODEL_SRF) {
+		S.this_srf = S.next_srf;
+		S.next_srf = (it == p->iterations) ? S.this_srf : (it + 1 <= p->srf_iters);
+		model = S.this_srf ? p->prj_model : (p->prj_model & ~MODEL_SRF);
+		mode = !S.this_srf ? 1 : (!S.next_srf ? 2 : 0);
 	}
-	if (msgfp != NULL) {
-		fclose(msgfp);
-		irl_set_msg_file(NULL);
+	for (s = 0; s < S.ns; ++s) {
+		const int *va = S.ang + s * S.per;
+		S.hd.iSubsetIdx = s;
+		hook_call(HOOK_PREV_SUBSET);
+		for (m = 0; m < S.per; ++m) {
+			S.vp[m].view_time = S.views[va[m]].view_time;
+			S.vp[m].sensitivity = S.views[va[m]].sensitivity;
+			S.vp[m].scat_mode = mode;
+		}
+		if (angle_hooks) {
+			for (m = 0; m < S.per; ++m) {
+				S.hd.iAngleIdx = va[m];
+				hook_call(HOOK_PREV_ANGLE);
+				irl_cu(irlcu_osem_subset(1, va + m, S.vp + m, model, p->bck_model, s, S.use_scatest,
+					       m == S.per - 1, m > 0),
+					"OsemRecon");
+				if (m == S.per - 1)
+					S.hook_norm = s;
+				hook_call(HOOK_POST_ANGLE);
+			}
+		} else {
+			int m0;
+			for (m0 = 0; m0 < S.per; m0 += S.max_batch) {
+				int nb = S.per - m0 < S.max_batch ? S.per - m0 : S.max_batch;
+				irl_cu(irlcu_osem_subset(nb, va + m0, S.vp + m0, model, p->bck_model, s, S.use_scatest,
+					       m0 + nb >= S.per, m0 > 0),
+					"OsemRecon");
+			}
+			S.hook_norm = s;
+		}
+		hook_call(HOOK_POST_SUBSET);
 	}
-	return err;
+	hook_call(HOOK_POST_ITER);
+	/* bCheckIfSaveIteration is true for every iteration with libirl's
+	   SaveInterval of 1 (IrlSetup.c:87-88, osemrecon.c:513-555) */
+	if (S.cb != NULL) {
+		irl_cu(irlcu_download_external(IRLCU_BUF_EST, S.tmp), "OsemRecon");
+		S.cb(it, S.tmp);
+	}
+	S.it = it;
+	irl_msg(4, "----Done iteration %d (%.3f s)\n", it, now_s() - ti);
+}
+
+int IrlOsemIterate(int niter)
+{
+	jmp_buf env;
+	int err, k;
+	if (!S.open)
+		return IRL_E_VALUE;
+	if ((err = setjmp(env)) != 0) {
+		fprintf(stderr, "FATAL ERROR Trapped: err_num=%d\nErrMsg=%s\n", err, irl_last_error());
+		irl_untrap();
+		session_close();
+		return err;
+	}
+	irl_trap(&env);
+	for (k = 0; k < niter && S.it < S.p.iterations; ++k)
+		one_iteration();
+	irl_untrap();
+	return 0;
+}
+
+int IrlOsemEnd(float *recon)
+{
+	jmp_buf env;
+	int err;
+	if (!S.open)
+		return 0;
+	if ((err = setjmp(env)) != 0) {
+		irl_untrap();
+		session_close();
+		return err;
+	}
+	irl_trap(&env);
+	if (S.p.norm_base != NULL) {
+		int s;
+		for (s = 0; s < S.ns; ++s)
+			norm_file(S.p.norm_base, s, NULL, 0, 1);
+	}
+	if (recon != NULL)
+		irl_cu(irlcu_download_external(IRLCU_BUF_EST, recon), "IrlOsem");
+	irl_untrap();
+	session_close();
+	return 0;
+}
+
+int IrlOsem(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
+	void (*cb)(int, float *), float *scatest, float *atn, float *prj, float *recon, char *logname, char *msgname)
+{
+	int err = IrlOsemBegin(ip, op, pv, drf_fname, krnl_fname, cb, scatest, atn, prj, recon, logname, msgname);
+	if (err)
+		return err;
+	err = IrlOsemIterate(S.p.iterations);
+	if (err)
+		return err;
+	return IrlOsemEnd(recon);
 }

@@ -500,7 +500,7 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 	int *base = (int *)irl_calloc(sizeof(int) * (ndet + 1), "DRF offsets");
 	DrfTab_t **tabs = (DrfTab_t **)irl_calloc(sizeof(DrfTab_t *) * (ndet + 1), "DRF tables");
 	float *psf;
-	int *pad, *rows;
+	int *pad, *rows, *taps;
 	irlcu_drf D;
 	for (k = 0; k < ndet; ++k) {
 		DrfTab_t *t = ((irl_detector *)g_irl_dets[k])->drf;
@@ -522,6 +522,7 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 	w = 2 * halo + 1;
 	psf = (float *)irl_calloc(sizeof(float) * (size_t)total * w * w, "padded PSFs");
 	pad = (int *)irl_calloc(sizeof(int) * (total > 0 ? total : 1), "pad rows");
+	taps = (int *)irl_calloc(sizeof(int) * (total > 0 ? total : 1), "PSF taps");
 	for (k = 0; k < ndet; ++k) {
 		DrfTab_t *t = tabs[k];
 		if (t == NULL)
@@ -536,6 +537,7 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 					dst[(size_t)(yy + oy) * w + xx + ox] = d->Psf[yy * wx + xx];
 			/* conv2d_ypad.c:54-57: iPadY = clamp(iAxialPadLength, 0, bCtrY) */
 			pad[base[k] + i] = MIN(MAX(p->pad_len, 0), d->MaxOffsY - 1);
+			taps[base[k] + i] = wx * wy;
 		}
 	}
 	rows = (int *)irl_malloc(sizeof(int) * (size_t)p->nviews * p->n, "DRF rows");
@@ -558,9 +560,11 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 	D.pad_rows = pad;
 	D.row_idist = rows;
 	D.avg_rows = MIN(MAX(p->avg_len, 0), p->nz);
+	D.taps = taps;
 	irl_cu(irlcu_set_drf(bck, total > 0 ? &D : NULL), "SetupDrf");
 	free(psf);
 	free(pad);
+	free(taps);
 	free(rows);
 	free(base);
 	free(tabs);

@@ -1,0 +1,111 @@
+"""The CPU oracle (oracle/src/irl_oracle.c) pinned against the reference.
+
+Golden fixtures come from the unmodified reference C compiled with the MIP
+shim (tests/golden/make_golden.py).  Where the compiled reference is
+present (oracle/_ref), further seeded cases are compared live.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, dup, golden_case, rel_l2
+from libirl_b200 import api, workloads as W
+
+
+def _rot(orc, fn, angle, vol):
+    out = np.zeros_like(vol)
+    n, nz, _ = vol.shape
+    getattr(orc.orc(), fn)(float(angle), api.fptr(vol), api.fptr(out), n, nz)
+    return out
+
+
+def test_rotations_match_golden_bit_for_bit(orc):
+    d = np.load(os.path.join(GOLDEN, "rotate.npz"))
+    vol = d["vol"]
+    for i, a in enumerate(d["angles"]):
+        assert np.array_equal(_rot(orc, "or_shears_rotate", a, vol), d["shears"][i])
+        assert np.array_equal(_rot(orc, "or_rot3dpar", a, vol), d["rot3dpar"][i])
+
+
+def test_conv2d_ypad_matches_golden_bit_for_bit(orc):
+    d = np.load(os.path.join(GOLDEN, "conv2d_ypad.npz"))
+    plane, psf = d["plane"], d["psf"]
+    ny, nx = plane.shape
+    for i, (pad, avg) in enumerate(d["pads"]):
+        out = np.zeros_like(plane)
+        orc.orc().or_conv2d_ypad(api.fptr(plane), nx, ny, api.fptr(psf), (psf.shape[1] - 1) // 2,
+                                 (psf.shape[0] - 1) // 2, int(pad), int(avg), api.fptr(out))
+        assert np.array_equal(out, d["out"][i])
+
+
+def test_genprj_osem_plain_match_golden_bit_for_bit(orc):
+    case, d = golden_case("plain16")
+    pr = orc.Problem(case)
+    assert np.array_equal(pr.genprj(), d["prj"])
+    est = pr.osem(d["meas"], case.iterations, case.nviews // case.subsets)
+    assert np.array_equal(orc.to_external(est), d["recon"])
+
+
+def test_genprj_osem_scatter_match_golden(orc):
+    # ESSE uses an FFT: the shim rounds each transform to float, the oracle
+    # convolves in double, so agreement is to float rounding
+    case, d = golden_case("srf16")
+    pr = orc.Problem(case)
+    prj = pr.genprj()
+    for v in range(case.nviews):
+        assert rel_l2(prj[v], d["prj"][v]) < 1e-6
+    est = pr.osem(d["meas"], case.iterations, case.nviews // case.subsets)
+    assert rel_l2(orc.to_external(est), d["recon"]) < 1e-5
+
+
+def test_subset_scheme_known_answer(orc):
+    # osemrecon.c:433-450: subset s starts at s/2 + (s%2)*S/2, stride S
+    import libirl_b200 as L
+    lib = L.load() if os.path.exists(L.SO) else None
+    if lib is None:
+        pytest.skip("libirl_b200.so not built")
+    p = C.POINTER(C.c_int)()
+    ns = lib.irl_compute_subsets(120, 15, C.byref(p))
+    assert ns == 8
+    got = np.ctypeslib.as_array(p, shape=(120,)).reshape(8, 15)
+    for s in range(8):
+        start = s // 2 + (s % 2) * 8 // 2
+        assert list(got[s]) == [start + 8 * m for m in range(15)]
+    assert sorted(got.ravel().tolist()) == list(range(120))
+
+
+def _have_ref(orc):
+    return os.path.exists(orc.REF_SO)
+
+
+@pytest.mark.parametrize("fast", [1, 0])
+def test_oracle_vs_reference_live_rotations(orc, fast):
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    rng = np.random.default_rng(11 + fast)
+    for n, nz in [(17, 2), (32, 3), (64, 2)]:
+        vol = rng.random((n, nz, n), dtype=np.float32)
+        for a in rng.uniform(-8, 8, 6).astype(np.float32):
+            if fast:
+                assert np.array_equal(_rot(orc, "or_shears_rotate", a, vol), orc.ref_shears_rotate(float(a), vol))
+            else:
+                assert np.array_equal(_rot(orc, "or_rot3dpar", a, vol), orc.ref_rot3dpar(float(a), vol))
+
+
+def test_oracle_vs_reference_live_osem_padding(orc):
+    """Axial padding and a non-default rotator, full IrlOsem chain."""
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    case = W.plain64(seed=1077, n=24, nviews=8, subsets=2, iterations=2)
+    files = case.write_tables("/tmp/irl_oracle_pad")
+    ref = orc.ref()
+    p, o, v = case.parms(), case.options(), case.views()
+    o.iAxialPadLength, o.iAxialAvgLength = 3, 2
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    assert ref.IrlGenprj(C.byref(p), C.byref(o), v, dup(files["drf"]), None, None, None, api.fptr(act),
+                         api.fptr(atn), api.fptr(prj), 1.0, None, None) == 0
+    pr = orc.Problem(case, pad_len=3, avg_len=2)
+    assert np.array_equal(pr.genprj(), prj)
