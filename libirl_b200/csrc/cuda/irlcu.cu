@@ -261,6 +261,7 @@ int irlcu_set_angles(const float *angles) {
     t.col_f2 = &cf2[(size_t)r * 2 * n];
     irl_shear_table(ang, n, &t);
     if (t.mdim > 2 * n) return set_error(IRLCU_EARG, "shear margin too large");
+    if (t.mdim > c.max_mdim) c.max_mdim = t.mdim;
     hdr[4 * r] = t.b90;
     hdr[4 * r + 1] = t.b180;
     hdr[4 * r + 2] = t.iadd;
@@ -574,6 +575,7 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   std::vector<float> rf1(n), rf2(n), cf1(2 * n), cf2(2 * n);
   irl_shear_tab t{0, 0, 0, 0, rsh.data(), rf1.data(), rf2.data(), csh.data(), cf1.data(), cf2.data()};
   irl_shear_table(angle, n, &t);
+  if (t.mdim > c.max_mdim) c.max_mdim = t.mdim;
   hdr = {t.b90, t.b180, t.iadd, t.mdim};
   float sn, cs;
   irl_rot3dpar_sincos(angle, &sn, &cs);

@@ -55,6 +55,7 @@ struct Ctx {
 
   // rotation tables: [0, nv) rotate by 0.5*pi + angle, [nv, 2nv) unrotate
   RotTabs rot{};
+  int max_mdim = 0;           // widest three-shear intermediate image in use
   int *sup_start = nullptr, *sup_end = nullptr;
 
   // persistent volumes / planes

@@ -287,74 +287,90 @@ __global__ void k_fft_col(ColArgs a, const float2 *__restrict__ twg) {
 
 // ------------------------------------------------- expansion / smoothing
 
-// one recursive smoothing step of ExpandByFac (krnlprj3d.c:636-670) along
-// a line held by the caller: out[k] = (sum of out[k-h..k-1] and in[k..k+h]) / (2h+1)
+// ExpandByFac's smoothing (krnlprj3d.c:636-670) walks each line once in
+// increasing order and overwrites it in place, so every output is
+//   out[k] = (out[k-h] + .. + out[k-1] + in[k] + .. + in[k+h]) / (2h+1)
+// summed left to right from 0, for h <= k < len-h (other entries keep
+// their input value), h = c/2.  The line walkers below keep the last h
+// outputs and the next h+1 inputs in registers.
+template <int H>
+struct LineSmoother {
+  float outp[H > 0 ? H : 1];   // out[k-H..k-1]
+  float in[H + 1];             // in[k..k+H]
+  // push in[k+H] after in[k..k+H-1] are loaded, return out[k]
+  __device__ __forceinline__ float step(int k, int len) {
+    float v;
+    if (k < H || k >= len - H) {
+      v = in[0];
+    } else {
+      float s = 0.f;
+#pragma unroll
+      for (int q = 0; q < H; ++q) s = __fadd_rn(s, outp[q]);
+#pragma unroll
+      for (int q = 0; q <= H; ++q) s = __fadd_rn(s, in[q]);
+      v = __fdiv_rn(s, (float)(2 * H + 1));
+    }
+#pragma unroll
+    for (int q = 0; q + 1 < H; ++q) outp[q] = outp[q + 1];
+    if (H > 0) outp[H - 1] = v;
+#pragma unroll
+    for (int q = 0; q < H; ++q) in[q] = in[q + 1];
+    return v;
+  }
+};
+
+// fine value of the expansion: coarse / c / c / c in libirl's order; for a
+// power-of-two c each division is exact and equals a multiplication
+__device__ __forceinline__ float expand_scale(float v, int c, float inv) {
+  if (inv != 0.f) return __fmul_rn(__fmul_rn(__fmul_rn(v, inv), inv), inv);
+  return __fdiv_rn(__fdiv_rn(__fdiv_rn(v, (float)c), (float)c), (float)c);
+}
 
 // expansion along y with the y smoothing: thread per (b, z, x) line of the
 // fine grid; g = cropped coarse result [B][nyv][nzv][nxv]
+template <int H>
 __global__ void k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1, float *__restrict__ t0,
-                           float *__restrict__ t1, int nt, int n, int nz, int c, int nyv, int nzv, int nxv, int nb) {
+                           float *__restrict__ t1, int nt, int n, int nz, int c, float inv, int nyv, int nzv,
+                           int nxv, int nb) {
   const size_t pln = (size_t)nz * n;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (size_t)nb * pln) return;
   const int b = (int)(e / pln);
   const int i = (int)(e - (size_t)b * pln);
   const int z = i / n, x = i - z * n;
-  const int h = c / 2, w = 2 * h + 1;
+  const size_t gs = (size_t)nzv * nxv;
   for (int t = 0; t < nt; ++t) {
-    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * nzv * nxv + (size_t)(z / c) * nxv + x / c;
+    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (size_t)(z / c) * nxv + x / c;
     float *o = (t == 0 ? t0 : t1) + (size_t)b * pln * n + i;
-    // fine value at y: g[y/c] / c / c / c (float divisions in libirl's order)
-    auto fine = [&](int y) {
-      float v = __ldg(g + (size_t)(y / c) * nzv * nxv);
-      v = __fdiv_rn(v, (float)c);
-      v = __fdiv_rn(v, (float)c);
-      return __fdiv_rn(v, (float)c);
-    };
-    if (h == 0) {
-      for (int y = 0; y < n; ++y) o[(size_t)y * pln] = fine(y);
-      continue;
-    }
-    // sliding window: prev[] holds smoothed values y-h..y-1
-    float prev[2] = {0.f, 0.f};
+    LineSmoother<H> L;
+#pragma unroll
+    for (int q = 0; q < H; ++q) L.in[q] = expand_scale(__ldg(g + (size_t)(q / c) * gs), c, inv);
     for (int y = 0; y < n; ++y) {
-      float v;
-      if (y < h || y >= n - h) {
-        v = fine(y);
-      } else {
-        float s = 0.f;
-        for (int q = h; q >= 1; --q) s = __fadd_rn(s, prev[h - q]);
-        for (int q = 0; q <= h; ++q) s = __fadd_rn(s, fine(y + q));
-        v = __fdiv_rn(s, (float)w);
-      }
-      o[(size_t)y * pln] = v;
-      // shift the window of smoothed values
-      if (h == 1) {
-        prev[0] = v;
-      } else {
-        prev[0] = prev[1];
-        prev[1] = v;
-      }
+      const int ya = min(y + H, n - 1);
+      L.in[H] = expand_scale(__ldg(g + (size_t)(ya / c) * gs), c, inv);
+      o[(size_t)y * pln] = L.step(y, n);
     }
   }
 }
 
 // recursive smoothing along z in place: thread per (b, y, x)
-__global__ void k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int nt, int n, int nz, int c, int nb) {
+template <int H>
+__global__ void k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int nt, int n, int nz, int nb) {
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t lines = (size_t)nb * n * n;
   if (e >= lines) return;
   const int b = (int)(e / ((size_t)n * n));
   const int r = (int)(e - (size_t)b * n * n);
   const int y = r / n, x = r - y * n;
-  const int h = c / 2, w = 2 * h + 1;
-  if (h == 0) return;
   for (int t = 0; t < nt; ++t) {
     float *o = (t == 0 ? t0 : t1) + (size_t)b * n * nz * n + (size_t)y * nz * n + x;
-    for (int z = h; z < nz - h; ++z) {
-      float s = 0.f;
-      for (int q = z - h; q <= z + h; ++q) s = __fadd_rn(s, o[(size_t)q * n]);
-      o[(size_t)z * n] = __fdiv_rn(s, (float)w);
+    LineSmoother<H> L;
+#pragma unroll
+    for (int q = 0; q < H; ++q) L.in[q] = o[(size_t)q * n];
+    for (int z = 0; z < nz; ++z) {
+      L.in[H] = o[(size_t)min(z + H, nz - 1) * n];
+      const float v = L.step(z, nz);
+      if (z >= H && z < nz - H) o[(size_t)z * n] = v;
     }
   }
 }
@@ -376,33 +392,45 @@ struct CombineArgs {
   float primary;
 };
 
-__global__ void k_smooth_x_combine(CombineArgs a) {
-  extern __shared__ float smx[];  // [2][8][n]
-  const int n = a.n, nz = a.nz;
-  const int y = blockIdx.x, z0 = blockIdx.y * 8, b = blockIdx.z;
-  const int rows = min(8, nz - z0);
+// CTA of 256 threads per (b, y, block of XZB z rows); rows are staged with
+// an odd stride so that one thread per row can walk x without bank
+// conflicts.
+constexpr int XZB = 32;
+
+template <int H>
+__global__ void __launch_bounds__(256) k_smooth_x_combine(CombineArgs a) {
+  extern __shared__ float smx[];  // [nt][XZB][n + 1]
+  const int n = a.n, nz = a.nz, ld = n + 1;
+  const int y = blockIdx.x, z0 = blockIdx.y * XZB, b = blockIdx.z;
+  const int rows = min(XZB, nz - z0);
   const size_t pln = (size_t)nz * n, vox = pln * n;
   const size_t base = (size_t)b * vox + (size_t)y * pln + (size_t)z0 * n;
   for (int t = 0; t < a.nt; ++t) {
     const float *src = (t == 0 ? a.t0 : a.t1) + base;
-    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) smx[t * 8 * n + e] = src[e];
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+      const int rr = e / n, xx = e - rr * n;
+      smx[(t * XZB + rr) * ld + xx] = src[e];
+    }
   }
   __syncthreads();
-  const int h = a.c / 2, w = 2 * h + 1;
-  if (h > 0 && threadIdx.x < a.nt * rows) {
-    float *row = smx + (threadIdx.x / rows) * 8 * n + (threadIdx.x % rows) * n;
-    for (int x = h; x < n - h; ++x) {
-      float s = 0.f;
-      for (int q = x - h; q <= x + h; ++q) s = __fadd_rn(s, row[q]);
-      row[x] = __fdiv_rn(s, (float)w);
+  if (H > 0 && threadIdx.x < a.nt * XZB && (int)(threadIdx.x % XZB) < rows) {
+    float *row = smx + (size_t)threadIdx.x * ld;  // (term, row) = (tid / XZB, tid % XZB)
+    LineSmoother<H> L;
+#pragma unroll
+    for (int q = 0; q < H; ++q) L.in[q] = row[q];
+    for (int x = 0; x < n; ++x) {
+      L.in[H] = row[min(x + H, n - 1)];
+      const float v = L.step(x, n);
+      row[x] = v;
     }
   }
   __syncthreads();
   const int view = a.views[b];
   const size_t tb = (size_t)view * vox + (size_t)y * pln + (size_t)z0 * n;
   for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
-    const float T0 = smx[e];
-    const float T1 = a.nt > 1 ? smx[8 * n + e] : 0.f;
+    const int rr = e / n, xx = e - rr * n;
+    const float T0 = smx[rr * ld + xx];
+    const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + xx] : 0.f;
     const float d = __fmul_rn(__ldg(a.S + tb + e), a.cnv);
     float eff = T0;
     if (a.nt > 1) eff = __fsub_rn(eff, __fmul_rn(d, T1));
@@ -724,12 +752,23 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
       CU_TRY(cudaMemcpyAsync(w.T[t], w.g[t], sizeof(float) * (size_t)nv * c.vox, cudaMemcpyDeviceToDevice, c.st));
   } else {
     const size_t lines = (size_t)nv * c.pln;
-    k_expand_y<<<(unsigned)((lines + 255) / 256), 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n,
-                                                                  c.nz, cf, nyv, nzv, nxv, nv);
-    CU_LAUNCHED();
+    const float inv = (cf & (cf - 1)) == 0 ? 1.0f / (float)cf : 0.f;  // exact for powers of two
+    const unsigned gy = (unsigned)((lines + 255) / 256);
     const size_t zl = (size_t)nv * c.n * c.n;
-    k_smooth_z<<<(unsigned)((zl + 255) / 256), 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, nv);
-    CU_LAUNCHED();
+    const unsigned gz = (unsigned)((zl + 255) / 256);
+    if (cf / 2 == 1) {
+      k_expand_y<1><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, inv, nyv, nzv,
+                                           nxv, nv);
+      CU_LAUNCHED();
+      k_smooth_z<1><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);
+      CU_LAUNCHED();
+    } else {
+      k_expand_y<2><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, inv, nyv, nzv,
+                                           nxv, nv);
+      CU_LAUNCHED();
+      k_smooth_z<2><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);
+      CU_LAUNCHED();
+    }
   }
   CombineArgs ca{};
   ca.t0 = w.T[0];
@@ -749,8 +788,21 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   ca.cnv_pix = ca.cnv / E.pix;
   ca.primary = primary;
   {
-    dim3 grid_(c.n, (c.nz + 7) / 8, nv);
-    k_smooth_x_combine<<<grid_, 256, sizeof(float) * 2 * 8 * c.n, c.st>>>(ca);
+    dim3 grid_(c.n, (c.nz + XZB - 1) / XZB, nv);
+    const size_t sm = sizeof(float) * 2 * XZB * (size_t)(c.n + 1);
+    static size_t configured = 0;
+    if (sm > 48 * 1024 && sm > configured) {
+      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      configured = sm;
+    }
+    if (cf / 2 == 0)
+      k_smooth_x_combine<0><<<grid_, 256, sm, c.st>>>(ca);
+    else if (cf / 2 == 1)
+      k_smooth_x_combine<1><<<grid_, 256, sm, c.st>>>(ca);
+    else
+      k_smooth_x_combine<2><<<grid_, 256, sm, c.st>>>(ca);
     CU_LAUNCHED();
   }
   return IRLCU_OK;

@@ -116,43 +116,126 @@ __device__ __forceinline__ RotHdr load_hdr(const RotTabs &T, int r) {
   return h;
 }
 
-// Path A: whole slice and X in shared memory.  grid (nz, nv).
-__global__ void __launch_bounds__(512) k_shear_smem(const float *__restrict__ src, size_t src_stride,
-                                                    float *__restrict__ dst, size_t dst_stride,
-                                                    const int *__restrict__ views, int rot_base,
-                                                    RotTabs T, const int *__restrict__ sup_st,
-                                                    const int *__restrict__ sup_en, int n, int nz,
-                                                    int xld) {
+// Path A: whole slice and X in shared memory, one CTA of 32 x 16 threads
+// per (slice, view).  The slice is stored with an odd row stride (n + 1) so
+// that the column walks of the 90-degree-flipped cases are free of bank
+// conflicts; the rotation's tables are copied to shared memory once.
+// grid (nz, nv).
+constexpr int SH_TX = 32, SH_TY = 16;
+
+__global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__restrict__ src, size_t src_stride,
+                                                             float *__restrict__ dst, size_t dst_stride,
+                                                             const int *__restrict__ views, int rot_base,
+                                                             RotTabs T, const int *__restrict__ sup_st,
+                                                             const int *__restrict__ sup_en, int n, int nz,
+                                                             int xld) {
   extern __shared__ float sm[];
-  float *s_slice = sm;
-  float *s_x = sm + n * n;
+  const int ld = n + 1;
+  float *s_slice = sm;                          // n * ld
+  float *s_x = s_slice + (size_t)n * ld;        // n * xld
+  int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xld);
+  int *t_st = t_rsh + n, *t_en = t_st + n;
+  float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
+  int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
+  float *t_cf1 = reinterpret_cast<float *>(t_csh + xld), *t_cf2 = t_cf1 + xld;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH_TY;
   const int k = blockIdx.x, v = blockIdx.y;
   const int r = rot_base + views[v];
   const RotHdr h = load_hdr(T, r);
-  const float *s = src + (size_t)v * src_stride;
-  float *d = dst + (size_t)v * dst_stride;
+  const float *s = src + (size_t)v * src_stride + (size_t)k * n;
+  float *d = dst + (size_t)v * dst_stride + (size_t)k * n;
   const size_t rs = (size_t)nz * n;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int y = e / n, x = e - y * n;
-    s_slice[e] = __ldg(s + (size_t)y * rs + (size_t)k * n + x);
+  for (int i = tid; i < n; i += nt) {
+    t_rsh[i] = T.row_sh[(size_t)r * n + i];
+    t_rf1[i] = T.row_f1[(size_t)r * n + i];
+    t_rf2[i] = T.row_f2[(size_t)r * n + i];
+    t_st[i] = sup_st[i];
+    t_en[i] = sup_en[i];
+  }
+  for (int i = tid; i < h.mdim; i += nt) {
+    t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
+    t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
+    t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
+  }
+  if ((n & 3) == 0) {
+    const int n4 = n >> 2;
+#pragma unroll 4
+    for (int y = ty; y < n; y += SH_TY)
+      for (int q = tx; q < n4; q += SH_TX) {
+        const float4 val = __ldg(reinterpret_cast<const float4 *>(s + (size_t)y * rs) + q);
+        float *o = s_slice + y * ld + 4 * q;
+        o[0] = val.x;
+        o[1] = val.y;
+        o[2] = val.z;
+        o[3] = val.w;
+      }
+  } else {
+    for (int y = ty; y < n; y += SH_TY)
+      for (int x = tx; x < n; x += SH_TX) s_slice[y * ld + x] = __ldg(s + (size_t)y * rs + x);
   }
   __syncthreads();
-  const int *rsh = T.row_sh + (size_t)r * n;
-  const float *rf1 = T.row_f1 + (size_t)r * n, *rf2 = T.row_f2 + (size_t)r * n;
-  SmemSlice S{s_slice, n};
-  for (int e = threadIdx.x; e < n * h.mdim; e += blockDim.x) {
-    const int j = e / h.mdim, i = e - j * h.mdim;
-    s_x[j * xld + i] = shear_pass1(S, n, h, j, i, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j]);
+  // pass 1 (x shear): X row j from source row j (or column, when flipped)
+  for (int j = ty; j < n; j += SH_TY) {
+    const int sh = t_rsh[j], st = t_st[j], en = t_en[j];
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const int lo = st - sh + h.iadd, hi = en - sh - 1 + h.iadd;
+    float *xr = s_x + (size_t)j * xld;
+    for (int i = tx; i < h.mdim; i += SH_TX) {
+      float val = 0.f;
+      if (i >= lo && i < hi) {
+        if (h.b180 == 0) {
+          const int t = i + sh - h.iadd;
+          if (h.b90 == 0)
+            val = lerp2(f1, s_slice[j * ld + t], f2, s_slice[j * ld + t + 1]);
+          else
+            val = lerp2(f1, s_slice[t * ld + (n - j - 1)], f2, s_slice[(t + 1) * ld + (n - j - 1)]);
+        } else {
+          const int t = n - i - (sh - h.iadd + 1);
+          if (h.b90 == 0)
+            val = lerp2(f1, s_slice[(n - j - 1) * ld + t], f2, s_slice[(n - j - 1) * ld + t - 1]);
+          else
+            val = lerp2(f1, s_slice[t * ld + j], f2, s_slice[(t - 1) * ld + j]);
+        }
+      }
+      xr[i] = val;
+    }
   }
   __syncthreads();
-  const int *csh = T.col_sh + (size_t)r * 2 * n;
-  const float *cf1 = T.col_f1 + (size_t)r * 2 * n, *cf2 = T.col_f2 + (size_t)r * 2 * n;
-  SmemX X{s_x, xld};
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int j = e / n, x = e - j * n;
-    d[(size_t)j * rs + (size_t)k * n + x] =
-        shear_pass23(X, n, h, j, x, rsh[j], rf1[j], rf2[j], sup_st[j], sup_en[j], csh, cf1, cf2);
+  // passes 2 + 3 (y shear, then x shear) per output pixel
+  for (int j = ty; j < n; j += SH_TY) {
+    const int sh = t_rsh[j], st = t_st[j], en = t_en[j];
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const int jj = j + h.iadd;
+    float *orow = d + (size_t)j * rs;
+    for (int x = tx; x < n; x += SH_TX) {
+      float out = 0.f;
+      if (x >= st + 1 && x < en - 1) {
+        const int a = x + sh + h.iadd;
+        float y2[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int c = a + q;
+          float yv = 0.f;
+          if (c >= 0 && c < h.mdim) {
+            const int jt = t_csh[c];
+            if (jj >= max(0, -jt) && jj < min(h.mdim, h.mdim - jt - 1)) {
+              const int r0 = jj + jt - h.iadd;
+              const float x0 = (r0 >= 0 && r0 < n) ? s_x[(size_t)r0 * xld + c] : 0.f;
+              const float x1 = (r0 + 1 >= 0 && r0 + 1 < n) ? s_x[(size_t)(r0 + 1) * xld + c] : 0.f;
+              yv = lerp2(t_cf1[c], x0, t_cf2[c], x1);
+            }
+          }
+          y2[q] = yv;
+        }
+        out = lerp2(f1, y2[0], f2, y2[1]);
+      }
+      orow[x] = out;
+    }
   }
+}
+
+static size_t shear_smem_bytes(int n, int xld) {
+  return sizeof(float) * ((size_t)n * (n + 1) + (size_t)n * xld + 5 * (size_t)n + 3 * (size_t)xld);
 }
 
 // Path B, for slices too large for shared memory: pass 1 into a global
@@ -225,31 +308,43 @@ __global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, flo
     for (int z = 0; z < nz; ++z) d[(size_t)NewY * rs + (size_t)z * n + NewX] = 0.f;
     return;
   }
+  // For odd sizes libirl's middle row gets NumPix = Dim + 1, so its loop
+  // also evaluates NewX = Dim; that store lands on x = 0 of the next slice
+  // of the same row (written earlier in the loop), and for the last slice
+  // on x = 0 of the next row (rewritten later).  The thread of x = 0
+  // reproduces the result: slices z >= 1 take the NewX = Dim value of z-1.
+  const bool spill = (NewX == 0 && Tail >= Dim);
   const float Y = (float)NewY - Axis;
-  const float X = (float)NewX - Axis;
-  const float FloatX = __fadd_rn(__fsub_rn(__fmul_rn(X, Cos), __fmul_rn(Y, Sin)), Axis);
-  const float FloatY = __fadd_rn(__fadd_rn(__fmul_rn(X, Sin), __fmul_rn(Y, Cos)), Axis);
-  const int OldX = (int)FloatX, OldY = (int)FloatY;
-  bool z0o = false, z1o = false, z2o = false, z3o = false;
-  if (OldX < 0 || OldX >= Dim) z0o = z1o = true;
-  if (OldY < 0 || OldY >= Dim) z0o = z2o = true;
-  if (OldX + 1 < 0 || OldX + 1 >= Dim) z2o = z3o = true;
-  if (OldY + 1 < 0 || OldY + 1 >= Dim) z1o = z3o = true;
-  const float fy = __fsub_rn(FloatY, (float)OldY), fx = __fsub_rn(FloatX, (float)OldX);
-  for (int z = 0; z < nz; ++z) {
-    const float z0 = z0o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX);
-    const float z1 = z1o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX);
-    const float z2 = z2o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX + 1);
-    const float z3 = z3o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX + 1);
-    float z01 = __fadd_rn(z0, __fmul_rn(fy, __fsub_rn(z1, z0)));
-    float z23 = __fadd_rn(z2, __fmul_rn(fy, __fsub_rn(z3, z2)));
-    if (FloatY < 0) {
-      z01 = z0;
-      z23 = z2;
+  for (int pass = 0; pass < (spill ? 2 : 1); ++pass) {
+    const int NX = pass == 0 ? NewX : Dim;
+    const float X = (float)NX - Axis;
+    const float FloatX = __fadd_rn(__fsub_rn(__fmul_rn(X, Cos), __fmul_rn(Y, Sin)), Axis);
+    const float FloatY = __fadd_rn(__fadd_rn(__fmul_rn(X, Sin), __fmul_rn(Y, Cos)), Axis);
+    const int OldX = (int)FloatX, OldY = (int)FloatY;
+    bool z0o = false, z1o = false, z2o = false, z3o = false;
+    if (OldX < 0 || OldX >= Dim) z0o = z1o = true;
+    if (OldY < 0 || OldY >= Dim) z0o = z2o = true;
+    if (OldX + 1 < 0 || OldX + 1 >= Dim) z2o = z3o = true;
+    if (OldY + 1 < 0 || OldY + 1 >= Dim) z1o = z3o = true;
+    const float fy = __fsub_rn(FloatY, (float)OldY), fx = __fsub_rn(FloatX, (float)OldX);
+    for (int z = 0; z < (pass == 0 ? nz : nz - 1); ++z) {
+      const float z0 = z0o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX);
+      const float z1 = z1o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX);
+      const float z2 = z2o ? 0.f : __ldg(s + (size_t)OldY * rs + (size_t)z * n + OldX + 1);
+      const float z3 = z3o ? 0.f : __ldg(s + (size_t)(OldY + 1) * rs + (size_t)z * n + OldX + 1);
+      float z01 = __fadd_rn(z0, __fmul_rn(fy, __fsub_rn(z1, z0)));
+      float z23 = __fadd_rn(z2, __fmul_rn(fy, __fsub_rn(z3, z2)));
+      if (FloatY < 0) {
+        z01 = z0;
+        z23 = z2;
+      }
+      float z0123 = __fadd_rn(z01, __fmul_rn(fx, __fsub_rn(z23, z01)));
+      if (FloatX < 0) z0123 = z01;
+      if (pass == 0)
+        d[(size_t)NewY * rs + (size_t)z * n + NewX] = z0123;
+      else
+        d[(size_t)NewY * rs + (size_t)(z + 1) * n] = z0123;
     }
-    float z0123 = __fadd_rn(z01, __fmul_rn(fx, __fsub_rn(z23, z01)));
-    if (FloatX < 0) z0123 = z01;
-    d[(size_t)NewY * rs + (size_t)z * n + NewX] = z0123;
   }
 }
 
@@ -266,8 +361,9 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
     CU_LAUNCHED();
     return IRLCU_OK;
   }
-  const int xld = 2 * n;  // mdim < 2n always
-  const size_t smem = sizeof(float) * ((size_t)n * n + (size_t)n * xld);
+  // widest intermediate image over the rotations in use (mdim < 2n)
+  const int xld = c.max_mdim > 0 ? c.max_mdim : 2 * n;
+  const size_t smem = shear_smem_bytes(n, xld);
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -278,8 +374,8 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
       CU_TRY(cudaFuncSetAttribute(k_shear_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       s_configured = smem;
     }
-    k_shear_smem<<<grid, 512, smem, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base, c.rot,
-                                            c.sup_start, c.sup_end, n, nz, xld);
+    k_shear_smem<<<grid, dim3(SH_TX, SH_TY), smem, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base,
+                                                          c.rot, c.sup_start, c.sup_end, n, nz, xld);
     CU_LAUNCHED();
     return IRLCU_OK;
   }

@@ -636,7 +636,11 @@ int or_osem(const or_problem *P, int prj_model, int bck_model, int srf_iters, in
 	if (ns != 1 && ns % 2)
 		return 2;
 	norm = (float *)calloc(vox * ns, sizeof(float));
-	if (srf && srf_iters > 0)
+	/* libirl allocates the stored scatter projections only when
+	   iNumSrfIterations > 0 (osemrecon.c:610-615) but adds them whenever
+	   scatter is not modelled in an iteration (osemrecon.c:743-745), a NULL
+	   dereference for iNumSrfIterations = 0; here they start at zero */
+	if (srf)
 		scat = (float *)calloc(pl * na, sizeof(float));
 	for (s = 0; s < ns; ++s) {
 		float *nm = norm + vox * s;
