@@ -107,9 +107,9 @@ class ClockSampler:
 
 # --------------------------------------------------------------- workload
 
-def make_workload(lib, tmpdir):
+def make_workload(lib, tmpdir, nviews=120, subsets=8):
     from libirl_b200 import api, workloads as W
-    case = W.full128(seed=2000)
+    case = W.full128(seed=2000, nviews=nviews, subsets=subsets)
     files = case.write_tables(tmpdir)
     p, o, v = case.parms(), case.options(), case.views()
     act, atn = case.act.copy(), case.atn.copy()
@@ -138,7 +138,7 @@ def run_b200(args):
     L.build()
     lib = L.load()
     tmp = tempfile.mkdtemp(prefix="irlbench_")
-    case, files, meas = make_workload(lib, tmp)
+    case, files, meas = make_workload(lib, tmp, args.nviews, args.subsets)
     K, Wm, P = args.steps, args.warmup, 1
     n3 = case.n * case.nz * case.n
 
@@ -394,6 +394,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    # reduced variants for profiling captures (the bench line uses the defaults)
+    ap.add_argument("--nviews", type=int, default=120)
+    ap.add_argument("--subsets", type=int, default=8)
     ap.add_argument("--cpu-views", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
