@@ -42,7 +42,9 @@ struct EsseDev {
   int kx = 0, ky = 0, kz = 0, collapse = 1, nterms = 1;
   float mu0 = 0, mu_avg = 0, pix = 0, cntr = 0;
   int kxh = 0;                // kx/2 + 1 complex bins along x
-  float2 *kft[3] = {nullptr, nullptr, nullptr};  // kernel spectra
+  float2 *kft[3] = {nullptr, nullptr, nullptr};  // kernel spectra [ky][kz][kxh]
+  float2 *kftT[3] = {nullptr, nullptr, nullptr}; // kx-major copies [kxh][ky][kz]
+  bool fused = false;         // y-z transforms in one shared-memory kernel
 };
 
 struct Ctx {

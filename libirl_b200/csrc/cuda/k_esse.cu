@@ -42,17 +42,17 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 mul_mis(float2 a, float s) { return make_float2(s * a.y, -s * a.x); }
 
 template <int R>
-__device__ __forceinline__ void dft_r(float2 (&v)[8], float s);  // s = +1 forward (exp(-i..)), -1 inverse
+__device__ __forceinline__ void dft_r(float2 *v, float s);  // s = +1 forward (exp(-i..)), -1 inverse
 
 template <>
-__device__ __forceinline__ void dft_r<2>(float2 (&v)[8], float) {
+__device__ __forceinline__ void dft_r<2>(float2 *v, float) {
   const float2 a = v[0], b = v[1];
   v[0] = cadd(a, b);
   v[1] = csub(a, b);
 }
 
 template <>
-__device__ __forceinline__ void dft_r<4>(float2 (&v)[8], float s) {
+__device__ __forceinline__ void dft_r<4>(float2 *v, float s) {
   const float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
   const float2 c = cadd(v[1], v[3]), d = mul_mis(csub(v[1], v[3]), s);
   v[0] = cadd(a, c);
@@ -62,9 +62,9 @@ __device__ __forceinline__ void dft_r<4>(float2 (&v)[8], float s) {
 }
 
 template <>
-__device__ __forceinline__ void dft_r<8>(float2 (&v)[8], float s) {
+__device__ __forceinline__ void dft_r<8>(float2 *v, float s) {
   // two 4-point DFTs on even and odd samples, then the radix-2 combine
-  float2 e[8] = {v[0], v[2], v[4], v[6]}, o[8] = {v[1], v[3], v[5], v[7]};
+  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
   dft_r<4>(e, s);
   dft_r<4>(o, s);
   const float h = 0.70710678118654752440f;
@@ -148,8 +148,9 @@ struct RowFwdArgs {
   int n, nz, c;         // full volume size and collapse factor
   int nyv, nzv, nxv;    // valid (collapsed) extents: rows y'<nyv, z'<nzv, x'<nxv
   size_t vox;
-  float2 *out;          // [B][nyv][zext][kxh] with zext >= nzv
+  float2 *out;          // [B][nyv][zext][kxh] with zext >= nzv, or kx-major
   int zext, kxh;
+  int kmajor;           // 1: out is [B][kxh][nyv][nzv] (planes of fixed kx)
 };
 
 template <int L>
@@ -188,15 +189,19 @@ __global__ void k_fft_row_fwd(RowFwdArgs a, const float2 *__restrict__ twg) {
     const int w = e / kxh, k = e - w * kxh, row = row0 + w;
     if (row >= nrows) continue;
     const int yy = row / a.nzv, zz = row - yy * a.nzv;
-    a.out[(((size_t)b * a.nyv + yy) * a.zext + zz) * kxh + k] = res[w * L + k];
+    if (a.kmajor)
+      a.out[(((size_t)b * kxh + k) * a.nyv + yy) * a.nzv + zz] = res[w * L + k];
+    else
+      a.out[(((size_t)b * a.nyv + yy) * a.zext + zz) * kxh + k] = res[w * L + k];
   }
 }
 
 struct RowInvArgs {
-  const float2 *in[2];  // [B][nyv][nzv][kxh] per term
+  const float2 *in[2];  // [B][nyv][nzv][kxh] per term, or kx-major [B][kxh][nyv][nzv]
   float *out[2];        // [B][nyv][nzv][nxv] per term (cropped real grid)
   int nt, nyv, nzv, nxv, kxh;
   float scale;
+  int kmajor;
 };
 
 template <int L>
@@ -214,13 +219,13 @@ __global__ void k_fft_row_inv(RowInvArgs a, const float2 *__restrict__ twg) {
       const int w = e / L, k = e - w * L, row = row0 + w;
       float2 v = make_float2(0.f, 0.f);
       if (row < nrows) {
-        const float2 *src = a.in[t] + ((size_t)b * nrows + row) * a.kxh;
-        if (k < a.kxh) {
-          v = src[k];
-        } else {
-          const float2 c = src[L - k];
-          v = make_float2(c.x, -c.y);
-        }
+        const int kk = k < a.kxh ? k : L - k;
+        float2 c;
+        if (a.kmajor)
+          c = a.in[t][((size_t)b * a.kxh + kk) * nrows + row];
+        else
+          c = a.in[t][((size_t)b * nrows + row) * a.kxh + kk];
+        v = k < a.kxh ? c : make_float2(c.x, -c.y);
       }
       sa[e] = v;
     }
@@ -282,6 +287,156 @@ __global__ void k_fft_col(ColArgs a, const float2 *__restrict__ twg) {
       if (w < wv)
         a.out[t][(size_t)b * a.out_bs + (size_t)o * a.out_os + (size_t)p * a.out_ps + kx0 + w] = res[w * L + p];
     }
+  }
+}
+
+// ------------------------------------------------ fused y-z plane kernel
+// One CTA per (view, kx) holds the whole (y, z) plane of that x-frequency
+// in shared memory: forward z and y transforms, then for each Taylor term
+// the spectral product, the inverse y transform (in chunks of lines, keeping
+// only y < nyv) and the inverse z transform (keeping z < nzv).  Planes are
+// exchanged with the x passes in kx-major layout [view][kx][y][z].
+
+constexpr int YZ_NT = 512;   // threads per CTA
+constexpr int YZ_CH = 16;    // z lines per inverse-y chunk
+
+// in-place Stockham pass over W lines of L points, point i of line w at
+// base[w*ls + i*es]; every thread stages its butterflies in registers, so
+// reads complete (barrier) before any write.  WFAST: consecutive threads
+// take consecutive lines (use when ls == 1) instead of consecutive points.
+template <int L, int R, int MAXW, bool WFAST>
+__device__ __forceinline__ void ip_pass(float2 *base, int W, int ls, int es, int Ns, const float2 *tw, float s) {
+  constexpr int JPL = L / R;
+  constexpr int MAXJ = (MAXW * JPL + YZ_NT - 1) / YZ_NT;
+  const int jobs = W * JPL;
+  float2 v[MAXJ][R];
+  int dst[MAXJ];
+  const int step = L / (Ns * R);
+#pragma unroll
+  for (int jj = 0; jj < MAXJ; ++jj) {
+    const int q = threadIdx.x + jj * YZ_NT;
+    dst[jj] = -1;
+    if (q < jobs) {
+      int w, j;
+      if (WFAST) {
+        w = q % W;
+        j = q / W;
+      } else {
+        w = q / JPL;
+        j = q - w * JPL;
+      }
+      const int k = j % Ns;
+      const float2 *src = base + w * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        float2 x = src[(j + r * JPL) * es];
+        if (r > 0 && k > 0) {
+          float2 t = tw[(r * k * step) & (L - 1)];
+          t.y *= s;
+          x = cmul(x, t);
+        }
+        v[jj][r] = x;
+      }
+      dst[jj] = w * ls + ((j / Ns) * Ns * R + k) * es;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int jj = 0; jj < MAXJ; ++jj) {
+    if (dst[jj] >= 0) {
+      dft_r<R>(v[jj], s);
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[dst[jj] + r * Ns * es] = v[jj][r];
+    }
+  }
+  __syncthreads();
+}
+
+// transforms W lines in chunks of at most MAXW lines (bounds the registers
+// that stage one pass of a chunk)
+template <int L, int MAXW, bool WFAST>
+__device__ void fft_ip(float2 *base_all, int W, int ls, int es, const float2 *tw, float s) {
+  for (int w0 = 0; w0 < W; w0 += MAXW) {
+    float2 *base = base_all + (size_t)w0 * ls;
+    const int Wc = min(MAXW, W - w0);
+    int Ns = 1;
+    while (Ns < L) {
+      const int rem = L / Ns;
+      // radix 8 while possible, 4 x 4 instead of 8 x 2 (fewer staged jobs)
+      if (rem >= 8 && rem != 16) {
+        ip_pass<L, 8, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
+        Ns *= 8;
+      } else if (rem == 4 || rem == 16) {
+        ip_pass<L, 4, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
+        Ns *= 4;
+      } else {
+        ip_pass<L, 2, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
+        Ns *= 2;
+      }
+    }
+  }
+}
+
+struct YzArgs {
+  const float2 *A;      // [B][kxh][nyv][nzv] after the forward x pass
+  const float2 *K[2];   // kernel spectra, kx-major [kxh][L(y)][L(z)]
+  float2 *D[2];         // [B][kxh][nyv][nzv] per term
+  int kxh, nyv, nzv, nt;
+};
+
+template <int L>
+__global__ void __launch_bounds__(YZ_NT, 1) k_esse_yz(YzArgs a, const float2 *__restrict__ twg) {
+  extern __shared__ __align__(16) float2 yzs[];
+  float2 *tw = yzs;                       // L
+  float2 *F = tw + L;                     // [L(y)][L(z)]
+  float2 *G = F + L * L;                  // [nyv][L(z)]
+  float2 *S = G + (size_t)a.nyv * L;      // [L(y)][YZ_CH]
+  const int kx = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+  const int nyv = a.nyv, nzv = a.nzv;
+  for (int i = tid; i < L; i += YZ_NT) tw[i] = twg[i];
+  const float2 *A = a.A + ((size_t)b * a.kxh + kx) * nyv * nzv;
+  for (int e = tid; e < L * L; e += YZ_NT) {
+    const int y = e / L, z = e - y * L;
+    F[e] = (y < nyv && z < nzv) ? A[y * nzv + z] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  constexpr int MW = L >= 128 ? 32 : L;        // lines per staged chunk
+  fft_ip<L, MW, false>(F, nyv, L, 1, tw, 1.f);  // z lines of the nonzero rows
+  fft_ip<L, MW, true>(F, L, 1, L, tw, 1.f);     // y lines of every z
+  for (int t = 0; t < a.nt; ++t) {
+    const float2 *K = a.K[t] + (size_t)kx * L * L;
+    for (int z0 = 0; z0 < L; z0 += YZ_CH) {
+      for (int e = tid; e < L * YZ_CH; e += YZ_NT) {
+        const int y = e / YZ_CH, zz = e - y * YZ_CH;
+        S[e] = cmul(F[y * L + z0 + zz], __ldg(K + (size_t)y * L + z0 + zz));
+      }
+      __syncthreads();
+      fft_ip<L, YZ_CH, true>(S, YZ_CH, 1, YZ_CH, tw, -1.f);  // inverse y
+      for (int e = tid; e < nyv * YZ_CH; e += YZ_NT) {
+        const int y = e / YZ_CH, zz = e - y * YZ_CH;
+        G[y * L + z0 + zz] = S[e];
+      }
+      __syncthreads();
+    }
+    fft_ip<L, MW, false>(G, nyv, L, 1, tw, -1.f);  // inverse z of the kept rows
+    float2 *D = a.D[t] + ((size_t)b * a.kxh + kx) * nyv * nzv;
+    for (int e = tid; e < nyv * nzv; e += YZ_NT) {
+      const int y = e / nzv, z = e - y * nzv;
+      D[e] = G[y * L + z];
+    }
+    __syncthreads();
+  }
+}
+
+static size_t yz_smem(int L, int nyv) { return sizeof(float2) * ((size_t)L + (size_t)L * L + (size_t)nyv * L + (size_t)L * YZ_CH); }
+
+// [ky][kz][kxh] -> [kxh][ky][kz]
+__global__ void k_spec_kmajor(const float2 *__restrict__ in, float2 *__restrict__ out, int ky, int kz, int kxh) {
+  const size_t tot = (size_t)ky * kz * kxh;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(e % kxh);
+    const size_t r = e / kxh;  // y * kz + z
+    out[(size_t)kx * ky * kz + r] = in[e];
   }
 }
 
@@ -575,10 +730,13 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
 }
 
 void esse_free(Ctx &c) {
-  for (int t = 0; t < 3; ++t)
+  for (int t = 0; t < 3; ++t) {
     if (c.esse.kft[t]) cudaFree(c.esse.kft[t]), c.esse.kft[t] = nullptr;
+    if (c.esse.kftT[t]) cudaFree(c.esse.kftT[t]), c.esse.kftT[t] = nullptr;
+  }
   c.esse.on = false;
   c.esse.zero = false;
+  c.esse.fused = false;
   EsseWork &w = g_ew;
   cudaFree(w.twx);
   cudaFree(w.twy);
@@ -662,9 +820,33 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     }
   }
   cudaFree(dgrid);
+  // fused y-z kernel when the plane fits in shared memory
+  {
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int L = E.ky;
+    const size_t sm = yz_smem(L, w.nyv);
+    if (E.ky == E.kz && (L == 32 || L == 64 || L == 128) && sm <= (size_t)maxsm) {
+      for (int t = 0; t < E.nterms; ++t) {
+        CU_TRY(cudaMalloc(&E.kftT[t], sizeof(float2) * spec));
+        k_spec_kmajor<<<592, 256, 0, c.st>>>(E.kft[t], E.kftT[t], E.ky, E.kz, E.kxh);
+        CU_LAUNCHED();
+      }
+      switch (L) {
+        case 32: CU_TRY(cudaFuncSetAttribute(k_esse_yz<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); break;
+        case 64: CU_TRY(cudaFuncSetAttribute(k_esse_yz<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); break;
+        default: CU_TRY(cudaFuncSetAttribute(k_esse_yz<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); break;
+      }
+      CU_TRY(cudaStreamSynchronize(c.st));
+      E.fused = true;
+    }
+  }
   E.on = true;
   return IRLCU_OK;
 }
+
+static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src);
 
 int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src) {
   EsseDev &E = c.esse;
@@ -679,6 +861,65 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   }
   if (nv > w.batch) return set_error(IRLCU_EARG, "ESSE batch %d exceeds %d", nv, w.batch);
   const int kxh = E.kxh, nyv = w.nyv, nzv = w.nzv, nxv = w.nxv;
+  if (E.fused) {
+    // x rows (collapse fused) -> A kx-major; y-z planes -> D[t]; x rows -> g[t]
+    RowFwdArgs ra{};
+    ra.rot = rot;
+    ra.n = c.n;
+    ra.nz = c.nz;
+    ra.c = E.collapse;
+    ra.nyv = nyv;
+    ra.nzv = nzv;
+    ra.nxv = nxv;
+    ra.vox = c.vox;
+    ra.out = w.A;
+    ra.zext = nzv;
+    ra.kxh = kxh;
+    ra.kmajor = 1;
+    {
+      dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
+      LDISPATCH(E.kx, k_fft_row_fwd, grid_, 256, 0, c.st, ra, w.twx);
+      CU_LAUNCHED();
+    }
+    YzArgs ya{};
+    ya.A = w.A;
+    ya.K[0] = E.kftT[0];
+    ya.K[1] = E.nterms > 1 ? E.kftT[1] : nullptr;
+    ya.D[0] = w.D[0];
+    ya.D[1] = w.D[1];
+    ya.kxh = kxh;
+    ya.nyv = nyv;
+    ya.nzv = nzv;
+    ya.nt = E.nterms;
+    {
+      dim3 grid_(kxh, nv);
+      const size_t sm = yz_smem(E.ky, nyv);
+      switch (E.ky) {
+        case 32: k_esse_yz<32><<<grid_, YZ_NT, sm, c.st>>>(ya, w.twy); break;
+        case 64: k_esse_yz<64><<<grid_, YZ_NT, sm, c.st>>>(ya, w.twy); break;
+        default: k_esse_yz<128><<<grid_, YZ_NT, sm, c.st>>>(ya, w.twy); break;
+      }
+      CU_LAUNCHED();
+    }
+    RowInvArgs ri{};
+    ri.in[0] = w.D[0];
+    ri.in[1] = w.D[1];
+    ri.out[0] = w.g[0];
+    ri.out[1] = w.g[1];
+    ri.nt = E.nterms;
+    ri.nyv = nyv;
+    ri.nzv = nzv;
+    ri.nxv = nxv;
+    ri.kxh = kxh;
+    ri.scale = (float)(1.0 / ((double)E.kx * E.ky * E.kz));
+    ri.kmajor = 1;
+    {
+      dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
+      LDISPATCH(E.kx, k_fft_row_inv, grid_, 256, 0, c.st, ri, w.twx);
+      CU_LAUNCHED();
+    }
+    return esse_expand_combine(c, rot, dviews, nv, primary, src);
+  }
   // forward: rot -> Bf (full spectrum)
   int rc = fft3_forward(c.st, E, rot, nullptr, c.n, c.nz, E.collapse, nyv, nzv, nxv, nv, w.A, w.C2[0], w.Bf);
   if (rc) return rc;
@@ -744,7 +985,14 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     LDISPATCH(E.kx, k_fft_row_inv, grid_, 256, 0, c.st, ri, w.twx);
     CU_LAUNCHED();
   }
-  // expansion + smoothing (y, z), then x smoothing fused with the combine
+  return esse_expand_combine(c, rot, dviews, nv, primary, src);
+}
+
+// expansion + smoothing (y, z), then x smoothing fused with the combine
+static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src) {
+  EsseDev &E = c.esse;
+  EsseWork &w = g_ew;
+  const int nyv = w.nyv, nzv = w.nzv, nxv = w.nxv;
   const int cf = E.collapse;
   if (cf == 1) {
     // no collapse: the cropped grid is the full-resolution term
