@@ -132,6 +132,39 @@ int irlcu_norm_subset(int nv, const int *views, const float *view_time,
    rot3dpar): src and dst are device or host pointers of n*nz*n floats. */
 int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, int on_device);
 
+/* Three-shear rotation (vShearsRotate) of one device-resident volume that
+   allocates nothing.  It has no counterpart in libirl, which mallocs its
+   mDim^2 scratch on every call (fastrotate.c:391-394).
+
+   It is for callers that must not allocate device memory: a per-angle hook
+   or a process beside a running reconstruction whose resident tables
+   already fill the device, and latency-bound callers that cannot absorb the
+   device-wide synchronisation of cudaMalloc/cudaFree.  irlcu_rotate_volume
+   lazily cudaMallocs an n*nz*mdim intermediate when a slice does not fit in
+   shared memory.
+
+   Instead this function keeps its rotation tables and that intermediate in
+   one file-scope device array of IRLCU_NOALLOC_SCRATCH_BYTES, part of the
+   library's module image.  Limits: 1 <= n <= IRLCU_NOALLOC_MAX_N and
+   nz*n*mdim floats <= IRLCU_NOALLOC_X_FLOATS, where mdim < 2n is the
+   intermediate side for this angle (n = nz = 128: at most 4.2 M floats).
+   Larger sizes return IRLCU_EARG before any device access.
+
+   src and dst are device pointers of n*nz*n floats ([y][z][x]), distinct.
+   Requires irlcu_init (the call runs on the library stream and synchronises
+   it before returning).  The results are bit-identical to
+   irlcu_rotate_volume with a fast-rotation context.
+
+   Set-up: the first call on a device looks up the array's address with
+   cudaGetSymbolAddress (which may load the module); make that first call
+   before any stream capture.  There is one scratch array per device, so
+   overlapping calls (from several host threads) race. */
+#define IRLCU_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define IRLCU_NOALLOC_TAB_BYTES (64u << 10)
+#define IRLCU_NOALLOC_X_FLOATS ((IRLCU_NOALLOC_SCRATCH_BYTES - IRLCU_NOALLOC_TAB_BYTES) / 4u)
+#define IRLCU_NOALLOC_MAX_N 1024
+int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz);
+
 /* synchronous wall-clock of the last batched call's stages, for tracing */
 int irlcu_stage_times(float *ms, int nmax);
 

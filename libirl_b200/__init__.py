@@ -56,6 +56,8 @@ def _declare_irlcu(lib):
     lib.irlcu_download_external.argtypes = [I, F]
     lib.irlcu_rotate_volume.restype = I
     lib.irlcu_rotate_volume.argtypes = [C.c_float, F, F, I, I]
+    lib.irlcu_rotate_volume_noalloc.restype = I
+    lib.irlcu_rotate_volume_noalloc.argtypes = [C.c_float, C.c_void_p, C.c_void_p, I, I]
     lib.irlcu_prepare_attenuation.restype = I
     lib.irlcu_prepare_attenuation.argtypes = [I]
     lib.irlcu_project.restype = I

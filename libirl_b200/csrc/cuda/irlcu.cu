@@ -607,6 +607,17 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   return IRLCU_OK;
 }
 
+// Allocates nothing: tables and intermediate live in a static device array
+// (k_rotate.cu), for callers that must not allocate device memory (see the
+// declaration in irlcu.h).
+int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  TRY(launch_rotate_noalloc(c.st, angle, src, dst, n, nz));
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
 void *irlcu_stream(void) { return g_ctx ? (void *)g_ctx->st : nullptr; }
 
 long long irlcu_launch_count(void) { return g_launch_count; }

@@ -115,6 +115,10 @@ extern long long g_launch_count;
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
                   size_t dst_stride, const int *dviews, int nv, int rot_base);
 
+// three-shear rotation of one device volume with every buffer in a static
+// device array (irlcu_rotate_volume_noalloc); enqueued on `st`
+int launch_rotate_noalloc(cudaStream_t st, float angle, const float *src, float *dst, int n, int nz);
+
 // cumulative attenuation tables of nv views from rotated maps in tMu-like
 // buffer `rmu` (stride vox): writes E (and S if not null)
 int launch_atn_tables(const Ctx &c, const float *rmu, float *E, float *S, int nv);

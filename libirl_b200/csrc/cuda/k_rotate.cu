@@ -18,6 +18,7 @@
 #include <cstdio>
 
 #include "irlcu_internal.cuh"
+#include "../host/irl_geom.h"
 
 namespace irlcu {
 
@@ -432,6 +433,107 @@ int launch_unrotate_accumulate(const Ctx &c, const float *bck, const int *dviews
   int blocks = (int)((c.vox + 255) / 256);
   if (blocks > 148 * 16) blocks = 148 * 16;
   k_accumulate<<<blocks, 256, 0, c.st>>>(c.wrot, c.vox, nv, acc, start_from_acc, mode, est, norm, c.vox);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+}  // namespace irlcu
+
+// ----------------------------------------------- allocation-free rotation
+// The three-shear rotation of irlcu_rotate_volume_noalloc runs the two
+// global-memory kernels above with every buffer inside this file-scope
+// array: rotation tables in the first IRLCU_NOALLOC_TAB_BYTES, then the
+// pass-1 intermediate X[k][j][i] (i < mdim) of every slice.  The array is
+// part of the module image, so the entry point calls no allocator.  Pass 2/3
+// read only X entries that pass 1 of the same call wrote (c < mdim, rows
+// < n), so nothing in it has to start at zero.
+namespace irlcu {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[IRLCU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int NA_MAXDEV = 64;
+void *g_noalloc_addr[NA_MAXDEV];  // per device, looked up on first use
+
+// host staging of the table region, laid out like the device copy (each
+// table starts at a multiple of 64 words = 256 bytes)
+constexpr int NA_SEG = 64;
+constexpr int na_round(int w) { return (w + NA_SEG - 1) / NA_SEG * NA_SEG; }
+struct NaLayout {
+  int hdr, row_sh, row_f1, row_f2, col_sh, col_f1, col_f2, sn, cs, st, en, views, words;
+};
+NaLayout na_layout(int n) {
+  NaLayout L{};
+  int w = 0;
+  L.hdr = w;    w += na_round(4);
+  L.row_sh = w; w += na_round(n);
+  L.row_f1 = w; w += na_round(n);
+  L.row_f2 = w; w += na_round(n);
+  L.col_sh = w; w += na_round(2 * n);
+  L.col_f1 = w; w += na_round(2 * n);
+  L.col_f2 = w; w += na_round(2 * n);
+  L.sn = w;     w += na_round(1);
+  L.cs = w;     w += na_round(1);
+  L.st = w;     w += na_round(n);
+  L.en = w;     w += na_round(n);
+  L.views = w;  w += na_round(1);
+  L.words = w;
+  return L;
+}
+static_assert((4 * (NA_SEG * 8 + 13 * IRLCU_NOALLOC_MAX_N)) <= (int)IRLCU_NOALLOC_TAB_BYTES,
+              "rotation tables of the largest n must fit the table region");
+uint32_t g_na_host[IRLCU_NOALLOC_TAB_BYTES / 4];
+
+}  // namespace
+
+int launch_rotate_noalloc(cudaStream_t st, float angle, const float *src, float *dst, int n, int nz) {
+  if (n < 1 || nz < 1 || n > IRLCU_NOALLOC_MAX_N)
+    return set_error(IRLCU_EARG, "irlcu_rotate_volume_noalloc: n = %d, nz = %d outside 1 <= n <= %d, nz >= 1", n,
+                     nz, IRLCU_NOALLOC_MAX_N);
+  if (src == nullptr || dst == nullptr || src == dst)
+    return set_error(IRLCU_EARG, "irlcu_rotate_volume_noalloc: src and dst must be distinct device pointers");
+  // host tables straight into the staging words (no heap)
+  const NaLayout L = na_layout(n);
+  int32_t *wi = reinterpret_cast<int32_t *>(g_na_host);
+  float *wf = reinterpret_cast<float *>(g_na_host);
+  irl_shear_tab t{0, 0, 0, 0, wi + L.row_sh, wf + L.row_f1, wf + L.row_f2, wi + L.col_sh, wf + L.col_f1, wf + L.col_f2};
+  irl_shear_table(angle, n, &t);
+  const size_t need = (size_t)nz * n * (size_t)t.mdim;
+  if (need > (size_t)IRLCU_NOALLOC_X_FLOATS)
+    return set_error(IRLCU_EARG,
+                     "irlcu_rotate_volume_noalloc: intermediate of nz*n*mdim = %d*%d*%d = %zu floats exceeds the "
+                     "static scratch of %u floats",
+                     nz, n, t.mdim, need, (unsigned)IRLCU_NOALLOC_X_FLOATS);
+  wi[L.hdr + 0] = t.b90;
+  wi[L.hdr + 1] = t.b180;
+  wi[L.hdr + 2] = t.iadd;
+  wi[L.hdr + 3] = t.mdim;
+  wf[L.sn] = 0.f;
+  wf[L.cs] = 0.f;
+  irl_shear_support(n, wi + L.st, wi + L.en);
+  wi[L.views] = 0;
+
+  int dev = -1;
+  CU_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAXDEV)
+    return set_error(IRLCU_EARG, "irlcu_rotate_volume_noalloc: device %d beyond %d", dev, NA_MAXDEV);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void *p = nullptr;
+    CU_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  unsigned char *base = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+  CU_TRY(cudaMemcpyAsync(base, g_na_host, (size_t)L.words * 4, cudaMemcpyHostToDevice, st));
+  int32_t *di = reinterpret_cast<int32_t *>(base);
+  float *df = reinterpret_cast<float *>(base);
+  RotTabs T{di + L.hdr, di + L.row_sh, df + L.row_f1, df + L.row_f2, di + L.col_sh,
+            df + L.col_f1, df + L.col_f2, df + L.sn, df + L.cs};
+  float *xs = reinterpret_cast<float *>(base + IRLCU_NOALLOC_TAB_BYTES);
+  const dim3 grid(nz, 1);
+  k_shear_pass1_glob<<<grid, 512, 0, st>>>(src, 0, xs, di + L.views, 0, T, di + L.st, di + L.en, n, nz, t.mdim);
+  CU_LAUNCHED();
+  k_shear_pass23_glob<<<grid, 512, 0, st>>>(xs, dst, 0, di + L.views, 0, T, di + L.st, di + L.en, n, nz, t.mdim);
   CU_LAUNCHED();
   return IRLCU_OK;
 }
