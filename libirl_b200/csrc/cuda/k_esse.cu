@@ -153,11 +153,16 @@ struct RowFwdArgs {
   int kmajor;           // 1: out is [B][kxh][nyv][nzv] (planes of fixed kx)
 };
 
+// rows per CTA of the x passes (host: row_wr)
+template <int L>
+__host__ __device__ constexpr int row_lines() { return (L <= 128) ? 16 : (L <= 256 ? 4 : 2); }
+
 template <int L>
 __global__ void k_fft_row_fwd(RowFwdArgs a, const float2 *__restrict__ twg) {
-  constexpr int WR = (L <= 128) ? 8 : (L <= 256 ? 4 : 2);
+  constexpr int WR = row_lines<L>();
+  constexpr int LS = L + 1;  // padded line stride: row-major walks are conflict-free
   __shared__ float2 tw[L];
-  __shared__ float2 sa[WR * L], sb[WR * L];
+  __shared__ float2 sa[WR * LS], sb[WR * LS];
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int b = blockIdx.y;
   const int row0 = blockIdx.x * WR;  // row = y' * nzv + z'
@@ -167,7 +172,21 @@ __global__ void k_fft_row_fwd(RowFwdArgs a, const float2 *__restrict__ twg) {
     float v = 0.f;
     if (row < nrows && x < a.nxv) {
       const int yy = row / a.nzv, zz = row - yy * a.nzv;
-      if (a.rot) {
+      if (a.rot && a.c == 2 && (a.n & 1) == 0) {
+        // CollapseByFac (krnlprj3d.c:549-593) for c = 2: the two x offsets
+        // of a (y, z) offset pair are one aligned float2
+        const float *r = a.rot + (size_t)b * a.vox;
+        float t = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const float2 q = __ldg(reinterpret_cast<const float2 *>(
+                r + ((size_t)(yy * 2 + k) * a.nz + (zz * 2 + j)) * a.n + x * 2));
+            t = __fadd_rn(__fadd_rn(t, q.x), q.y);
+          }
+        v = t;
+      } else if (a.rot) {
         // CollapseByFac (krnlprj3d.c:549-593): sum over y, then z, then x offsets
         const float *r = a.rot + (size_t)b * a.vox;
         float t = 0.f;
@@ -180,19 +199,25 @@ __global__ void k_fft_row_fwd(RowFwdArgs a, const float2 *__restrict__ twg) {
         v = __ldg(a.grid + ((size_t)yy * a.zext + zz) * L + x);
       }
     }
-    sa[e] = make_float2(v, 0.f);
+    sa[w * LS + x] = make_float2(v, 0.f);
   }
   __syncthreads();
-  float2 *res = fft_lines<L>(sa, sb, WR, L, tw, 1.f);
+  float2 *res = fft_lines<L>(sa, sb, WR, LS, tw, 1.f);
   const int kxh = a.kxh;
-  for (int e = threadIdx.x; e < WR * kxh; e += blockDim.x) {
-    const int w = e / kxh, k = e - w * kxh, row = row0 + w;
-    if (row >= nrows) continue;
-    const int yy = row / a.nzv, zz = row - yy * a.nzv;
-    if (a.kmajor)
-      a.out[(((size_t)b * kxh + k) * a.nyv + yy) * a.nzv + zz] = res[w * L + k];
-    else
-      a.out[(((size_t)b * a.nyv + yy) * a.zext + zz) * kxh + k] = res[w * L + k];
+  if (a.kmajor) {
+    // kx-major: consecutive threads take consecutive rows (contiguous in out)
+    for (int e = threadIdx.x; e < WR * kxh; e += blockDim.x) {
+      const int k = e / WR, w = e - k * WR, row = row0 + w;
+      if (row >= nrows) continue;
+      a.out[((size_t)b * kxh + k) * nrows + row] = res[w * LS + k];
+    }
+  } else {
+    for (int e = threadIdx.x; e < WR * kxh; e += blockDim.x) {
+      const int w = e / kxh, k = e - w * kxh, row = row0 + w;
+      if (row >= nrows) continue;
+      const int yy = row / a.nzv, zz = row - yy * a.nzv;
+      a.out[(((size_t)b * a.nyv + yy) * a.zext + zz) * kxh + k] = res[w * LS + k];
+    }
   }
 }
 
@@ -206,35 +231,47 @@ struct RowInvArgs {
 
 template <int L>
 __global__ void k_fft_row_inv(RowInvArgs a, const float2 *__restrict__ twg) {
-  constexpr int WR = (L <= 128) ? 8 : (L <= 256 ? 4 : 2);
+  constexpr int WR = row_lines<L>();
+  constexpr int LS = L + 1;  // padded line stride: row-major walks are conflict-free
   __shared__ float2 tw[L];
-  __shared__ float2 sa[WR * L], sb[WR * L];
+  __shared__ float2 sa[WR * LS], sb[WR * LS];
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int b = blockIdx.y;
   const int row0 = blockIdx.x * WR;
   const int nrows = a.nyv * a.nzv;
   for (int t = 0; t < a.nt; ++t) {
     __syncthreads();
-    for (int e = threadIdx.x; e < WR * L; e += blockDim.x) {
-      const int w = e / L, k = e - w * L, row = row0 + w;
-      float2 v = make_float2(0.f, 0.f);
-      if (row < nrows) {
-        const int kk = k < a.kxh ? k : L - k;
-        float2 c;
-        if (a.kmajor)
-          c = a.in[t][((size_t)b * a.kxh + kk) * nrows + row];
-        else
-          c = a.in[t][((size_t)b * nrows + row) * a.kxh + kk];
-        v = k < a.kxh ? c : make_float2(c.x, -c.y);
+    if (a.kmajor) {
+      // kx-major input: consecutive threads read consecutive rows; the
+      // conjugate-symmetric half is filled from shared memory below
+      for (int e = threadIdx.x; e < WR * a.kxh; e += blockDim.x) {
+        const int k = e / WR, w = e - k * WR, row = row0 + w;
+        sa[w * LS + k] = row < nrows ? a.in[t][((size_t)b * a.kxh + k) * nrows + row] : make_float2(0.f, 0.f);
       }
-      sa[e] = v;
+      __syncthreads();
+      for (int e = threadIdx.x; e < WR * (L - a.kxh); e += blockDim.x) {
+        const int w = e / (L - a.kxh), k = a.kxh + (e - w * (L - a.kxh));
+        const float2 c = sa[w * LS + (L - k)];
+        sa[w * LS + k] = make_float2(c.x, -c.y);
+      }
+    } else {
+      for (int e = threadIdx.x; e < WR * L; e += blockDim.x) {
+        const int w = e / L, k = e - w * L, row = row0 + w;
+        float2 v = make_float2(0.f, 0.f);
+        if (row < nrows) {
+          const int kk = k < a.kxh ? k : L - k;
+          const float2 c = a.in[t][((size_t)b * nrows + row) * a.kxh + kk];
+          v = k < a.kxh ? c : make_float2(c.x, -c.y);
+        }
+        sa[w * LS + k] = v;
+      }
     }
     __syncthreads();
-    float2 *res = fft_lines<L>(sa, sb, WR, L, tw, -1.f);
+    float2 *res = fft_lines<L>(sa, sb, WR, LS, tw, -1.f);
     for (int e = threadIdx.x; e < WR * a.nxv; e += blockDim.x) {
       const int w = e / a.nxv, x = e - w * a.nxv, row = row0 + w;
       if (row >= nrows) continue;
-      a.out[t][((size_t)b * nrows + row) * a.nxv + x] = res[w * L + x].x * a.scale;
+      a.out[t][((size_t)b * nrows + row) * a.nxv + x] = res[w * LS + x].x * a.scale;
     }
   }
 }
@@ -442,6 +479,29 @@ __global__ void k_spec_kmajor(const float2 *__restrict__ in, float2 *__restrict_
 
 // ------------------------------------------------- expansion / smoothing
 
+// x / D for the odd window lengths D = 2h+1 of the smoothing and for odd
+// collapse factors: q0 = x * RN(1/D), then one correction with the exact
+// residual r = x - q0*D (Markstein, IBM J. Res. Dev. 34(1), 1990).  For
+// D = 3, 5, 7 this equals the correctly rounded x / D for every finite x
+// except -0 (checked over all float inputs; tests/test_const_division.py
+// repeats it over the binades where under- and overflow could matter).
+// The sums divided here start from +0, so they are never -0.
+template <int D>
+__device__ __forceinline__ float div_const(float x) {
+  if constexpr (D == 1) {
+    return x;
+  } else if constexpr (D == 3 || D == 5 || D == 7) {
+    const float y = __int_as_float(D == 3 ? 0x3eaaaaab : (D == 5 ? 0x3e4ccccd : 0x3e124925));
+    const float q0 = __fmul_rn(x, y);
+    const float r = __fmaf_rn(-q0, (float)D, x);
+    return __fmaf_rn(r, y, q0);
+  } else if constexpr ((D & (D - 1)) == 0) {
+    return __fmul_rn(x, 1.0f / (float)D);  // exact for powers of two
+  } else {
+    return __fdiv_rn(x, (float)D);
+  }
+}
+
 // ExpandByFac's smoothing (krnlprj3d.c:636-670) walks each line once in
 // increasing order and overwrites it in place, so every output is
 //   out[k] = (out[k-h] + .. + out[k-1] + in[k] + .. + in[k+h]) / (2h+1)
@@ -463,7 +523,7 @@ struct LineSmoother {
       for (int q = 0; q < H; ++q) s = __fadd_rn(s, outp[q]);
 #pragma unroll
       for (int q = 0; q <= H; ++q) s = __fadd_rn(s, in[q]);
-      v = __fdiv_rn(s, (float)(2 * H + 1));
+      v = div_const<2 * H + 1>(s);
     }
 #pragma unroll
     for (int q = 0; q + 1 < H; ++q) outp[q] = outp[q + 1];
@@ -474,19 +534,22 @@ struct LineSmoother {
   }
 };
 
-// fine value of the expansion: coarse / c / c / c in libirl's order; for a
-// power-of-two c each division is exact and equals a multiplication
-__device__ __forceinline__ float expand_scale(float v, int c, float inv) {
-  if (inv != 0.f) return __fmul_rn(__fmul_rn(__fmul_rn(v, inv), inv), inv);
-  return __fdiv_rn(__fdiv_rn(__fdiv_rn(v, (float)c), (float)c), (float)c);
+// fine value of the expansion: coarse / c / c / c in libirl's order
+template <int C>
+__device__ __forceinline__ float expand_scale(float v) {
+  return div_const<C>(div_const<C>(div_const<C>(v)));
 }
 
+// loads issued ahead of the dependent walk along a line
+constexpr int WALK_PF = 8;
+
 // expansion along y with the y smoothing: thread per (b, z, x) line of the
-// fine grid; g = cropped coarse result [B][nyv][nzv][nxv]
-template <int H>
-__global__ void k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1, float *__restrict__ t0,
-                           float *__restrict__ t1, int nt, int n, int nz, int c, float inv, int nyv, int nzv,
-                           int nxv, int nb) {
+// fine grid; g = cropped coarse result [B][nyv][nzv][nxv]; C = collapse
+template <int C>
+__global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1,
+                                                  float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
+                                                  int nz, int nyv, int nzv, int nxv, int nb) {
+  constexpr int H = C / 2;
   const size_t pln = (size_t)nz * n;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (size_t)nb * pln) return;
@@ -495,22 +558,33 @@ __global__ void k_expand_y(const float *__restrict__ g0, const float *__restrict
   const int z = i / n, x = i - z * n;
   const size_t gs = (size_t)nzv * nxv;
   for (int t = 0; t < nt; ++t) {
-    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (size_t)(z / c) * nxv + x / c;
+    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (size_t)(z / C) * nxv + x / C;
     float *o = (t == 0 ? t0 : t1) + (size_t)b * pln * n + i;
     LineSmoother<H> L;
 #pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = expand_scale(__ldg(g + (size_t)(q / c) * gs), c, inv);
-    for (int y = 0; y < n; ++y) {
-      const int ya = min(y + H, n - 1);
-      L.in[H] = expand_scale(__ldg(g + (size_t)(ya / c) * gs), c, inv);
-      o[(size_t)y * pln] = L.step(y, n);
+    for (int q = 0; q < H; ++q) L.in[q] = expand_scale<C>(__ldg(g + (size_t)(q / C) * gs));
+    for (int y0 = 0; y0 < n; y0 += WALK_PF) {
+      float nx[WALK_PF];
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(g + (size_t)(min(y0 + q + H, n - 1) / C) * gs);
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) {
+        const int y = y0 + q;
+        if (y < n) {
+          L.in[H] = expand_scale<C>(nx[q]);
+          o[(size_t)y * pln] = L.step(y, n);
+        }
+      }
     }
   }
 }
 
-// recursive smoothing along z in place: thread per (b, y, x)
+// recursive smoothing along z in place: thread per (b, y, x).  A batch of
+// inputs is loaded before the batch's outputs are stored; the loads are at
+// z + H and beyond, which no earlier batch has overwritten.
 template <int H>
-__global__ void k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int nt, int n, int nz, int nb) {
+__global__ void __launch_bounds__(256) k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
+                                                  int nz, int nb) {
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t lines = (size_t)nb * n * n;
   if (e >= lines) return;
@@ -522,17 +596,25 @@ __global__ void k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int n
     LineSmoother<H> L;
 #pragma unroll
     for (int q = 0; q < H; ++q) L.in[q] = o[(size_t)q * n];
-    for (int z = 0; z < nz; ++z) {
-      L.in[H] = o[(size_t)min(z + H, nz - 1) * n];
-      const float v = L.step(z, nz);
-      if (z >= H && z < nz - H) o[(size_t)z * n] = v;
+    for (int z0 = 0; z0 < nz; z0 += WALK_PF) {
+      float nx[WALK_PF];
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) nx[q] = o[(size_t)min(z0 + q + H, nz - 1) * n];
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) {
+        const int z = z0 + q;
+        if (z < nz) {
+          L.in[H] = nx[q];
+          const float v = L.step(z, nz);
+          if (z >= H && z < nz - H) o[(size_t)z * n] = v;
+        }
+      }
     }
   }
 }
 
 // recursive smoothing along x (rows staged in shared memory) fused with the
-// depth/density combination and the projector source.  One CTA per
-// (b, y, block of 8 z rows).
+// depth/density combination and the projector source.
 struct CombineArgs {
   const float *t0, *t1;   // expanded terms [B][n][nz][n]
   const float *rot;       // rotated activity [B][n][nz][n]
@@ -547,54 +629,56 @@ struct CombineArgs {
   float primary;
 };
 
-// CTA of 256 threads per (b, y, block of XZB z rows); rows are staged with
-// an odd stride so that one thread per row can walk x without bank
+// CTA of 32 x CX_TY threads per (b, y, block of XZB z rows); rows are staged
+// with an odd stride so that one thread per row can walk x without bank
 // conflicts.
 constexpr int XZB = 32;
+constexpr int CX_TY = 8;
 
 template <int H>
-__global__ void __launch_bounds__(256) k_smooth_x_combine(CombineArgs a) {
+__global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) {
   extern __shared__ float smx[];  // [nt][XZB][n + 1]
   const int n = a.n, nz = a.nz, ld = n + 1;
   const int y = blockIdx.x, z0 = blockIdx.y * XZB, b = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int rows = min(XZB, nz - z0);
   const size_t pln = (size_t)nz * n, vox = pln * n;
   const size_t base = (size_t)b * vox + (size_t)y * pln + (size_t)z0 * n;
   for (int t = 0; t < a.nt; ++t) {
     const float *src = (t == 0 ? a.t0 : a.t1) + base;
-    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
-      const int rr = e / n, xx = e - rr * n;
-      smx[(t * XZB + rr) * ld + xx] = src[e];
-    }
+    float *dst = smx + (size_t)t * XZB * ld;
+    for (int rr = ty; rr < rows; rr += CX_TY)
+      for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * n + xx];
   }
   __syncthreads();
-  if (H > 0 && threadIdx.x < a.nt * XZB && (int)(threadIdx.x % XZB) < rows) {
-    float *row = smx + (size_t)threadIdx.x * ld;  // (term, row) = (tid / XZB, tid % XZB)
+  if (H > 0 && tid < a.nt * XZB && (tid % XZB) < rows) {
+    float *row = smx + (size_t)tid * ld;  // (term, row) = (tid / XZB, tid % XZB)
     LineSmoother<H> L;
 #pragma unroll
     for (int q = 0; q < H; ++q) L.in[q] = row[q];
     for (int x = 0; x < n; ++x) {
       L.in[H] = row[min(x + H, n - 1)];
-      const float v = L.step(x, n);
-      row[x] = v;
+      row[x] = L.step(x, n);
     }
   }
   __syncthreads();
   const int view = a.views[b];
   const size_t tb = (size_t)view * vox + (size_t)y * pln + (size_t)z0 * n;
-  for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
-    const int rr = e / n, xx = e - rr * n;
-    const float T0 = smx[rr * ld + xx];
-    const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + xx] : 0.f;
-    const float d = __fmul_rn(__ldg(a.S + tb + e), a.cnv);
-    float eff = T0;
-    if (a.nt > 1) eff = __fsub_rn(eff, __fmul_rn(d, T1));
-    eff = (float)((double)eff * exp((double)__fmul_rn(d, a.fmu)));
-    const float act = __ldg(a.rot + base + e);
-    if (a.cntr > 0.f) eff = __fadd_rn(eff, __fmul_rn(act, a.cntr));
-    eff = __fmul_rn(eff, __fmul_rn(__ldg(a.mu + tb + e), a.cnv_pix));
-    if (eff < 0.f) eff = 0.f;
-    a.src[base + e] = __fadd_rn(__fmul_rn(act, a.primary), eff);
+  for (int rr = ty; rr < rows; rr += CX_TY) {
+    for (int xx = tx; xx < n; xx += 32) {
+      const size_t e = (size_t)rr * n + xx;
+      const float T0 = smx[rr * ld + xx];
+      const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + xx] : 0.f;
+      const float d = __fmul_rn(__ldg(a.S + tb + e), a.cnv);
+      float eff = T0;
+      if (a.nt > 1) eff = __fsub_rn(eff, __fmul_rn(d, T1));
+      eff = (float)((double)eff * exp((double)__fmul_rn(d, a.fmu)));
+      const float act = __ldg(a.rot + base + e);
+      if (a.cntr > 0.f) eff = __fadd_rn(eff, __fmul_rn(act, a.cntr));
+      eff = __fmul_rn(eff, __fmul_rn(__ldg(a.mu + tb + e), a.cnv_pix));
+      if (eff < 0.f) eff = 0.f;
+      a.src[base + e] = __fadd_rn(__fmul_rn(act, a.primary), eff);
+    }
   }
 }
 
@@ -641,7 +725,7 @@ static int upload_twiddles(float2 **d, int L) {
     default: return set_error(IRLCU_EARG, "FFT length %d not supported", L);    \
   }
 
-static int row_wr(int L) { return (L <= 128) ? 8 : (L <= 256 ? 4 : 2); }
+static int row_wr(int L) { return (L <= 128) ? 16 : (L <= 256 ? 4 : 2); }  // row_lines<L>()
 
 static int col_smem(int L) { return (int)(sizeof(float2) * (L + 2 * CW * L)); }
 
@@ -1000,23 +1084,27 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
       CU_TRY(cudaMemcpyAsync(w.T[t], w.g[t], sizeof(float) * (size_t)nv * c.vox, cudaMemcpyDeviceToDevice, c.st));
   } else {
     const size_t lines = (size_t)nv * c.pln;
-    const float inv = (cf & (cf - 1)) == 0 ? 1.0f / (float)cf : 0.f;  // exact for powers of two
     const unsigned gy = (unsigned)((lines + 255) / 256);
     const size_t zl = (size_t)nv * c.n * c.n;
     const unsigned gz = (unsigned)((zl + 255) / 256);
-    if (cf / 2 == 1) {
-      k_expand_y<1><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, inv, nyv, nzv,
-                                           nxv, nv);
-      CU_LAUNCHED();
-      k_smooth_z<1><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);
-      CU_LAUNCHED();
-    } else {
-      k_expand_y<2><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, cf, inv, nyv, nzv,
-                                           nxv, nv);
-      CU_LAUNCHED();
-      k_smooth_z<2><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);
-      CU_LAUNCHED();
+#define EXPAND_Z(C)                                                                                          \
+  case C:                                                                                                    \
+    k_expand_y<C><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, nyv, nzv, nxv, nv); \
+    CU_LAUNCHED();                                                                                           \
+    k_smooth_z<C / 2><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);                        \
+    CU_LAUNCHED();                                                                                           \
+    break;
+    switch (cf) {
+      EXPAND_Z(2)
+      EXPAND_Z(3)
+      EXPAND_Z(4)
+      EXPAND_Z(5)
+      EXPAND_Z(6)
+      EXPAND_Z(7)
+      default:
+        return set_error(IRLCU_EARG, "ESSE collapse factor %d not supported (1..7)", cf);
     }
+#undef EXPAND_Z
   }
   CombineArgs ca{};
   ca.t0 = w.T[0];
@@ -1043,14 +1131,16 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
       CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       configured = sm;
     }
-    if (cf / 2 == 0)
-      k_smooth_x_combine<0><<<grid_, 256, sm, c.st>>>(ca);
-    else if (cf / 2 == 1)
-      k_smooth_x_combine<1><<<grid_, 256, sm, c.st>>>(ca);
-    else
-      k_smooth_x_combine<2><<<grid_, 256, sm, c.st>>>(ca);
+    const dim3 blk(32, CX_TY);
+    switch (cf / 2) {
+      case 0: k_smooth_x_combine<0><<<grid_, blk, sm, c.st>>>(ca); break;
+      case 1: k_smooth_x_combine<1><<<grid_, blk, sm, c.st>>>(ca); break;
+      case 2: k_smooth_x_combine<2><<<grid_, blk, sm, c.st>>>(ca); break;
+      default: k_smooth_x_combine<3><<<grid_, blk, sm, c.st>>>(ca); break;
+    }
     CU_LAUNCHED();
   }
   return IRLCU_OK;
