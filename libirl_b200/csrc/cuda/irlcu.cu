@@ -2,6 +2,7 @@
 //
 // The host C driver (IrlOsem / IrlGenprj) owns the control flow; this file
 // owns device memory and sequences the kernels of one batched stage.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -61,8 +62,21 @@ struct Stage {
 
 // algorithmic FLOPs of the DRF convolutions of a batch (2 per tap per
 // output pixel, taps = the PSF's own extent, planes with distance > 0)
-static double drf_flops(const Ctx &c, const DrfDev *d, const int *views, int nv) {
+// 5 L log2 L per complex line transform of length L
+static double fft5(double L) { return 5.0 * L * std::log2(L); }
+
+// algorithmic FLOPs of the DRF stage: 2 per PSF tap per output pixel for the
+// direct convolution; for the Fourier-domain engine the line transforms
+// (two real rows per complex line) and the spectral products
+static double drf_flops(const Ctx &c, const DrfDev *d, const int *views, int nv, bool forward) {
   if (!d || !d->psf) return 0.0;
+  if (d->fft.on) {
+    const DrfFft &F = d->fft;
+    const double rows = 0.5 * F.G * fft5(F.Mx), cols = F.Mxh * fft5(F.Mz), mul = 8.0 * F.Mz * F.Mxh;
+    const double inv_rows = 0.5 * c.nz * fft5(F.Mx);
+    if (forward) return (double)nv * (c.n * (rows + cols + mul) + cols + inv_rows);
+    return (double)nv * c.n * (rows + 2.0 * cols + mul + inv_rows);
+  }
   double f = 0.0;
   for (int i = 0; i < nv; ++i)
     for (int y = 0; y < c.n; ++y) {
@@ -140,7 +154,9 @@ static void free_ctx(Ctx *c) {
     dfree(c->drf[w].psf);
     dfree(c->drf[w].pad_rows);
     dfree(c->drf[w].row_idist);
+    drf_fft_free(c->drf[w]);
   }
+  drf_fft_work_free();
   esse_free(*c);
   free_rotate_scratch();
   for (auto &e : c->ev) cudaEventDestroy(e);
@@ -289,10 +305,22 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   dfree(D.psf);
   dfree(D.pad_rows);
   dfree(D.row_idist);
+  drf_fft_free(D);
   D = DrfDev{};
   if (!d) return IRLCU_OK;
-  const int H = halo_instance(d->halo);
-  if (H < 0) return set_error(IRLCU_EARG, "DRF half-width %d exceeds the direct-convolution limit (32); use FFT convolution", d->halo);
+  // engine: the direct kernels take half-widths up to 32; the Fourier-domain
+  // engine any that fits its grid.  IRLCU_DRF_ENGINE = direct | fft | auto
+  // (auto: Fourier domain from half-width 8 on, where it needs fewer FLOPs)
+  const int Hd = halo_instance(d->halo);
+  const char *eng = getenv("IRLCU_DRF_ENGINE");
+  bool use_fft = Hd < 0 || Hd >= 8;
+  if (eng && !strcmp(eng, "direct")) {
+    if (Hd < 0) return set_error(IRLCU_EARG, "DRF half-width %d exceeds the direct-convolution limit (32)", d->halo);
+    use_fft = false;
+  } else if (eng && !strcmp(eng, "fft")) {
+    use_fft = true;
+  }
+  const int H = Hd >= 0 ? Hd : d->halo;
   const int PW = 2 * H + 1, PLD = (PW + 3) & ~3, w = 2 * d->halo + 1;
   std::vector<float> pad((size_t)d->ndist * PW * PLD, 0.f);
   for (int i = 0; i < d->ndist; ++i)
@@ -313,6 +341,12 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   D.h_rows.assign(d->row_idist, d->row_idist + (size_t)c.nv * c.n);
   D.h_taps.resize(d->ndist);
   for (int i = 0; i < d->ndist; ++i) D.h_taps[i] = d->taps ? d->taps[i] : w * w;
+  if (use_fft) {
+    int max_pad = 0;
+    if (d->avg_rows > 0)
+      for (int i = 0; i < d->ndist; ++i) max_pad = std::max(max_pad, d->pad_rows[i]);
+    TRY(drf_fft_setup(c, D, max_pad));
+  }
   return IRLCU_OK;
 }
 
@@ -459,7 +493,7 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
   }
   for (int pass = 0; pass < (out_nosrf ? 2 : 1); ++pass) {
     Stage s(IRLCU_ST_PROJECT, c.st);
-    s.flops = drf_flops(c, drf, hviews, nv);
+    s.flops = drf_flops(c, drf, hviews, nv, true);
     // algorithmic bytes: source and attenuation factor of every plane
     s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;
     if (pass == 0)
@@ -517,7 +551,7 @@ int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp, int m
   if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
   {
     Stage s(IRLCU_ST_BACKPROJECT, c.st);
-    s.flops = drf_flops(c, drf, views, nv);
+    s.flops = drf_flops(c, drf, views, nv, false);
     s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;  // attenuation factor read, plane written
     TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
   }

@@ -26,6 +26,17 @@ struct RotTabs {
   float *sn, *cs;
 };
 
+// Fourier-domain form of a DRF table (k_drf_fft.cu): planes on an Mz x Mx
+// grid, plane row z at grid row z + P; spectra of the quadrant-swapped PSFs
+// plus an identity spectrum for rows without DRF, scaled by 1/(Mz Mx).
+struct DrfFft {
+  bool on = false;
+  int Mz = 0, Mx = 0, Mxh = 0;  // grid; Mxh = Mx/2 + 1 half-spectrum bins
+  int P = 0, G = 0;             // row offset; rows that can be nonzero
+  float2 *H = nullptr;          // [ndist + 1][Mz][Mxh]
+  float2 *twx = nullptr, *twz = nullptr;
+};
+
 struct DrfDev {
   int ndist = 0, halo = -1, avg_rows = 0;
   float *psf = nullptr;       // ndist * (2h+1) * pstride
@@ -34,6 +45,7 @@ struct DrfDev {
   int *row_idist = nullptr;   // nviews * n
   std::vector<int> h_rows;    // host copy of row_idist (work accounting)
   std::vector<int> h_taps;    // per distance: taps of the unpadded PSF
+  DrfFft fft;                 // on: the convolution runs in the Fourier domain
 };
 
 struct EsseDev {
@@ -130,6 +142,15 @@ int launch_project(const Ctx &c, const float *src, const int *dviews, int nv,
 // backprojection planes: bck[v][y] = conv(plane[v] * E[view][y]) * scale
 int launch_backproject(const Ctx &c, const float *planes, const int *dviews, int nv,
                        const float *E, const DrfDev *drf, float scale, float *bck);
+
+// Fourier-domain DRF engine (k_drf_fft.cu); max_pad: the largest axial pad
+int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad);
+void drf_fft_free(DrfDev &D);
+void drf_fft_work_free();
+int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
+                       float scale, float *out);
+int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,
+                           const DrfDev &D, float scale, float *bck);
 
 // unrotate nv backprojected volumes and accumulate into acc with the
 // per-view clamp; then optionally est *= acc * norm or acc = invert(acc)

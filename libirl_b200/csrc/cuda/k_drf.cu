@@ -298,6 +298,12 @@ int halo_instance(int h) {
 
 static long long g_fwd_grid = 0;
 
+#define TRY_FFT(x)           \
+  do {                       \
+    int rc_ = (x);           \
+    if (rc_) return rc_;     \
+  } while (0)
+
 template <int H>
 static int fwd_launch(const Ctx &c, FwdArgs a) {
   using C = Cfg<H>;
@@ -356,6 +362,10 @@ static int backward_dispatch(int h, const Ctx &c, BckArgs a, int nv) { DISPATCH_
 int launch_project(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev *drf,
                    float scale, float *out) {
   if (nv <= 0) return IRLCU_OK;
+  if (drf && drf->psf && drf->fft.on) {
+    TRY_FFT(launch_project_fft(c, src, dviews, nv, E, *drf, scale, out));
+    return IRLCU_OK;
+  }
   FwdArgs a{};
   a.src = src;
   a.E = E;
@@ -384,6 +394,7 @@ int launch_project(const Ctx &c, const float *src, const int *dviews, int nv, co
 int launch_backproject(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,
                        const DrfDev *drf, float scale, float *bck) {
   if (nv <= 0) return IRLCU_OK;
+  if (drf && drf->psf && drf->fft.on) return launch_backproject_fft(c, planes, dviews, nv, E, *drf, scale, bck);
   BckArgs a{};
   a.planes = planes;
   a.E = E;

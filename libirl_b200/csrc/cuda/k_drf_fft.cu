@@ -1,0 +1,604 @@
+// k_drf_fft.cu -- the depth-dependent DRF convolution of the projector and
+// backprojector evaluated in the Fourier domain.
+//
+// Both of libirl's convolution paths compute, per rotated row y (a z-by-x
+// plane), a linear "same" convolution of the attenuated plane with the PSF
+// of the row's distance:
+//   * conv2d_ypad (conv2d_ypad.c:39-108): x zero padded, z padded by up to
+//     pady rows holding the mean of the avgy end rows (pad2d.c:21-141);
+//   * conv2dPsfFFT (conv2dPsfFFT.c:53-117): the plane zero padded into the
+//     upper-left corner of a 2N x 2Nz grid, the PSF quadrant-swapped
+//     (padswap.c:21-119), a circular convolution and the upper-left crop --
+//     for a PSF half-width h <= N the same linear convolution with no axial
+//     padding (the FFT-flagged tables are uploaded with pady = 0).
+// Here every plane is placed in an Mz x Mx grid (products of 2, 3, 5, 7)
+// with its row z at grid row z + P, P the largest axial pad of the table,
+// Mx >= n + h and Mz >= nz + P + h, so the circular convolution on the grid
+// equals the linear one on every output pixel.  The PSF spectra H[d] (plus
+// an identity spectrum for rows without DRF, prjbck.c:233) are computed
+// once per table and carry the 1/(Mz Mx) normalisation.
+//
+// Forward (Project, prjbck.c:217-240), per batch of views:
+//   rows:    R2C along x of every grid row of every plane (two real rows per
+//            complex line) -> S[b][y][g][kx], g < G = nz + 2P;
+//   columns: per (view, kx chunk, plane group) FFT along g, multiply by
+//            H[d(y)], accumulate over the group's planes -> partial sums;
+//   finish:  per (view, kx chunk) the partial sums in group order, inverse
+//            FFT along g, rows P..P+nz-1 -> Y[b][z][kx];
+//   rows:    C2R along x, crop x < n, times the projector scale.
+// Backward (BackProject, prjbck.c:340-408), per batch of views:
+//   rows:    R2C of ratio * E(y) for every plane y -> S;
+//   columns: per (view, plane, kx chunk) FFT, multiply by H[d(y)], inverse
+//            FFT, rows P..P+nz-1 written back in place;
+//   rows:    C2R, crop, scale -> the backprojected volume [b][y][z][x].
+// Work per plane is O(Mz Mx log(Mz Mx)) instead of O(nz n (2h+1)^2); results
+// agree with the direct convolution to FP32 FFT rounding.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <vector>
+
+#include "fft_core.cuh"
+#include "irlcu_internal.cuh"
+
+namespace irlcu {
+
+constexpr int FT_NT = 256;
+
+#define TRY_RC(x)            \
+  do {                       \
+    int rc_ = (x);           \
+    if (rc_) return rc_;     \
+  } while (0)
+
+// row pairs per CTA of the x passes, columns per CTA of the z passes
+template <int L>
+__host__ __device__ constexpr int rows_pairs() { return L <= 256 ? 8 : (L <= 512 ? 4 : 2); }
+template <int L>
+__host__ __device__ constexpr int col_chunk() { return L <= 256 ? 16 : (L <= 512 ? 8 : 4); }
+template <int L>
+__host__ __device__ constexpr size_t col_smem() { return sizeof(float2) * ((size_t)2 * col_chunk<L>() * (L + 1) + L); }
+
+// ------------------------------------------------------------ x passes
+
+struct RowSrc {
+  // MODE_PLANE: grid row g of plane (b, y) holds row z = g - P of
+  //   a[b*a_bs + y*a_ys] * E[view][y] (x < n), or the averaged pad rows
+  // MODE_PSF:   grid row g of "plane" d holds the quadrant-swapped PSF d
+  //   (d == ndist: the identity)
+  int mode;
+  const float *a;
+  size_t a_bs, a_ys;
+  const float *E;
+  const int *views;
+  const int *row_idist;
+  const int *pad_rows;
+  int avgy;
+  const float *psf;   // padded tables: ndist * (2h+1) * pstride
+  int h, pstride, ndist;
+  int n, nz, P, G;    // G: grid rows that can be nonzero
+  int Mz;
+  float2 *out;        // [b][plane][G][Mxh]
+  int Mxh, nplanes;
+};
+constexpr int MODE_PLANE = 0, MODE_PSF = 1;
+
+__device__ __forceinline__ float plane_in(const float *a, const float *e, int i) {
+  const float v = __ldg(a + i);
+  return e ? __fmul_rn(v, __ldg(e + i)) : v;
+}
+
+// value of the attenuated, axially padded plane at (z, x), x < n
+__device__ __forceinline__ float plane_pad_val(const float *a, const float *e, int z, int x, int n, int nz,
+                                               int pady, int avgy) {
+  if (z >= 0 && z < nz) return plane_in(a, e, z * n + x);
+  if (pady <= 0 || avgy <= 0 || z < -pady || z >= nz + pady) return 0.f;
+  // pfAvgRows (pad2d.c:92-122): row sum in order, divided when > 1 row
+  const int r0 = z < 0 ? 0 : nz - avgy;
+  float s = 0.f;
+  for (int r = 0; r < avgy; ++r) s = __fadd_rn(s, plane_in(a, e, (r0 + r) * n + x));
+  return avgy > 1 ? __fdiv_rn(s, (float)avgy) : s;
+}
+
+// index of grid offset g in a centred (2h+1) table, or -1
+__device__ __forceinline__ int centred(int g, int M, int h) {
+  if (g <= h) return h + g;
+  if (g >= M - h) return h + g - M;
+  return -1;
+}
+
+template <int L>
+__global__ void __launch_bounds__(FT_NT) k_dfft_rows_fwd(RowSrc a, const float2 *__restrict__ twg) {
+  constexpr int PR = rows_pairs<L>(), LS = L + 1;
+  __shared__ float2 tw[L];
+  __shared__ float2 sa[PR * LS], sb[PR * LS];
+  for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
+  const int b = blockIdx.z, y = blockIdx.y, g0 = blockIdx.x * 2 * PR;
+  const int G = a.G, n = a.n;
+  const float *ap = nullptr, *ep = nullptr;
+  int pady = 0;
+  const float *psf = nullptr;
+  if (a.mode == MODE_PLANE) {
+    const int view = a.views[b];
+    const size_t pln = (size_t)a.nz * n;
+    ap = a.a + (size_t)b * a.a_bs + (size_t)y * a.a_ys;
+    ep = a.E ? a.E + ((size_t)view * n + y) * pln : nullptr;
+    const int idist = a.row_idist ? a.row_idist[(size_t)view * n + y] : -1;
+    pady = (idist >= 0 && a.pad_rows) ? a.pad_rows[idist] : 0;
+  } else if (y < a.ndist) {
+    psf = a.psf + (size_t)y * (2 * a.h + 1) * a.pstride;
+  }
+  for (int e = threadIdx.x; e < PR * L; e += FT_NT) {
+    const int w = e / L, x = e - w * L;
+    float v[2] = {0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int g = g0 + 2 * w + q;
+      if (g >= G) continue;
+      if (a.mode == MODE_PLANE) {
+        if (x < n) v[q] = plane_pad_val(ap, ep, g - a.P, x, n, a.nz, pady, a.avgy);
+      } else if (psf) {
+        const int py = centred(g, a.Mz, a.h), px = centred(x, L, a.h);
+        if (py >= 0 && px >= 0) v[q] = __ldg(psf + (size_t)py * a.pstride + px);
+      } else {
+        v[q] = (g == 0 && x == 0) ? 1.f : 0.f;
+      }
+    }
+    sa[w * LS + x] = make_float2(v[0], v[1]);
+  }
+  __syncthreads();
+  const float2 *res = fft_lines<L>(sa, sb, PR, LS, tw, 1.f);
+  // two real rows from one complex line: A = (Z[k] + conj Z[L-k]) / 2,
+  // B = (Z[k] - conj Z[L-k]) / 2i
+  const int Mxh = a.Mxh;
+  for (int e = threadIdx.x; e < PR * Mxh; e += FT_NT) {
+    const int w = e / Mxh, k = e - w * Mxh;
+    const int g = g0 + 2 * w;
+    if (g >= G) continue;
+    const float2 zk = res[w * LS + k];
+    const float2 zm = res[w * LS + (k == 0 ? 0 : L - k)];
+    float2 *o = a.out + (((size_t)b * a.nplanes + y) * G + g) * Mxh + k;
+    o[0] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    if (g + 1 < G) o[Mxh] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+  }
+}
+
+// C2R along x of row pairs: row (b, p, z) of the input at
+//   in[((b*np + p)*rs + r0 + z)*Mxh]; output x < n at out[((b*np + p)*nz + z)*n]
+struct RowInv {
+  const float2 *in;
+  int np, rs, r0, Mxh;
+  float *out;
+  int n, nz;
+  float scale;
+};
+
+template <int L>
+__global__ void __launch_bounds__(FT_NT) k_dfft_rows_inv(RowInv a, const float2 *__restrict__ twg) {
+  constexpr int PR = rows_pairs<L>(), LS = L + 1;
+  __shared__ float2 tw[L];
+  __shared__ float2 sa[PR * LS], sb[PR * LS];
+  for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
+  const int b = blockIdx.z, p = blockIdx.y, z0 = blockIdx.x * 2 * PR;
+  const int Mxh = a.Mxh, nz = a.nz;
+  const size_t rbase = ((size_t)b * a.np + p) * a.rs + a.r0;
+  // Z = A + iB from the half spectra of rows z (A) and z+1 (B)
+  for (int e = threadIdx.x; e < PR * Mxh; e += FT_NT) {
+    const int w = e / Mxh, k = e - w * Mxh;
+    const int z = z0 + 2 * w;
+    float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+    if (z < nz) A = a.in[(rbase + z) * Mxh + k];
+    if (z + 1 < nz) B = a.in[(rbase + z + 1) * Mxh + k];
+    sa[w * LS + k] = make_float2(A.x - B.y, A.y + B.x);
+    if (k > 0 && L - k >= Mxh) sa[w * LS + L - k] = make_float2(A.x + B.y, B.x - A.y);
+  }
+  __syncthreads();
+  const float2 *res = fft_lines<L>(sa, sb, PR, LS, tw, -1.f);
+  const int n = a.n;
+  for (int e = threadIdx.x; e < PR * 2 * n; e += FT_NT) {
+    const int w = e / (2 * n), r = e - w * 2 * n, q = r / n, x = r - q * n;
+    const int z = z0 + 2 * w + q;
+    if (z >= nz) continue;
+    const float2 v = res[w * LS + x];
+    a.out[(((size_t)b * a.np + p) * nz + z) * n + x] = (q ? v.y : v.x) * a.scale;
+  }
+}
+
+// ------------------------------------------------------------ z passes
+
+// column chunk [c][g] of lines c < CK (kx = k0 + c), g < L, from rows
+// [g][kx] of `src` (row stride Mxh); rows g >= valid are zero
+template <int L>
+__device__ __forceinline__ void load_cols(float2 *s, const float2 *src, int k0, int Mxh, int valid) {
+  constexpr int CK = col_chunk<L>(), LS = L + 1;
+  for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
+    const int c = e % CK, g = e / CK, k = k0 + c;
+    s[c * LS + g] = (g < valid && k < Mxh) ? src[(size_t)g * Mxh + k] : make_float2(0.f, 0.f);
+  }
+}
+
+struct ColArgsD {
+  const float2 *in;    // rows [b][plane][G][Mxh]
+  float2 *out;
+  const float2 *H;     // [ndist+1][Mz][Mxh]
+  const int *views;
+  const int *row_idist;
+  int ndist, nplanes, G, P, nz, Mxh;
+  float hscale;        // COL_H: normalisation of the spectra
+  float2 *part;        // COL_FWD partial sums [pg][b][Mz][Mxh]
+  int npg, nb;
+};
+constexpr int COL_H = 0, COL_BCK = 1;
+
+__device__ __forceinline__ int spectrum_of(const ColArgsD &a, int b, int y) {
+  const int view = a.views[b];
+  const int d = a.row_idist ? a.row_idist[(size_t)view * a.nplanes + y] : -1;
+  return d >= 0 ? d : a.ndist;
+}
+
+// COL_H: H[d] = FFT_g(rows) * hscale (all rows).  COL_BCK: per plane FFT,
+// multiply by H[d(y)], inverse FFT, rows P..P+nz-1 back in place.
+template <int L>
+__global__ void __launch_bounds__(FT_NT) k_dfft_cols(ColArgsD a, int mode, const float2 *__restrict__ twg) {
+  constexpr int CK = col_chunk<L>(), LS = L + 1;
+  extern __shared__ __align__(16) float2 cs[];
+  float2 *tw = cs, *s0 = cs + L, *s1 = s0 + CK * LS;
+  for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
+  const int k0 = blockIdx.x * CK, y = blockIdx.y, b = blockIdx.z;
+  const int Mxh = a.Mxh;
+  const size_t plane = ((size_t)b * a.nplanes + y) * a.G;
+  load_cols<L>(s0, a.in + plane * Mxh, k0, Mxh, a.G);
+  __syncthreads();
+  float2 *res = fft_lines<L>(s0, s1, CK, LS, tw, 1.f);
+  if (mode == COL_H) {
+    for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
+      const int c = e % CK, g = e / CK, k = k0 + c;
+      if (k < Mxh) a.out[(plane + g) * Mxh + k] = cscale(res[c * LS + g], a.hscale);
+    }
+    return;
+  }
+  const float2 *Hd = a.H + (size_t)spectrum_of(a, b, y) * L * Mxh;
+  for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
+    const int c = e % CK, g = e / CK, k = k0 + c;
+    if (k < Mxh) res[c * LS + g] = cmul(res[c * LS + g], __ldg(Hd + (size_t)g * Mxh + k));
+  }
+  __syncthreads();
+  float2 *other = res == s0 ? s1 : s0;
+  res = fft_lines<L>(res, other, CK, LS, tw, -1.f);
+  for (int e = threadIdx.x; e < CK * a.nz; e += FT_NT) {
+    const int c = e % CK, z = e / CK, k = k0 + c;
+    if (k < Mxh) a.out[(plane + a.P + z) * Mxh + k] = res[c * LS + a.P + z];
+  }
+}
+
+// forward: per (kx chunk, view, plane group) sum over the group's planes of
+// FFT_g(plane) * H[d(y)] -> part[pg][b][g][kx]
+template <int L>
+__global__ void __launch_bounds__(FT_NT) k_dfft_cols_fwd(ColArgsD a, const float2 *__restrict__ twg) {
+  constexpr int CK = col_chunk<L>(), LS = L + 1;
+  constexpr int NE = (CK * L + FT_NT - 1) / FT_NT;
+  extern __shared__ __align__(16) float2 cs[];
+  float2 *tw = cs, *s0 = cs + L, *s1 = s0 + CK * LS;
+  for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
+  const int k0 = blockIdx.x * CK, b = blockIdx.y, pg = blockIdx.z;
+  const int Mxh = a.Mxh;
+  const int per = (a.nplanes + a.npg - 1) / a.npg;
+  const int y0 = pg * per, y1 = min(a.nplanes, y0 + per);
+  float2 acc[NE];
+#pragma unroll
+  for (int i = 0; i < NE; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (int y = y0; y < y1; ++y) {
+    const size_t plane = ((size_t)b * a.nplanes + y) * a.G;
+    __syncthreads();
+    load_cols<L>(s0, a.in + plane * Mxh, k0, Mxh, a.G);
+    __syncthreads();
+    const float2 *res = fft_lines<L>(s0, s1, CK, LS, tw, 1.f);
+    const float2 *Hd = a.H + (size_t)spectrum_of(a, b, y) * L * Mxh;
+#pragma unroll
+    for (int i = 0; i < NE; ++i) {
+      const int e = threadIdx.x + i * FT_NT;
+      const int c = e % CK, g = e / CK, k = k0 + c;
+      if (e < CK * L && k < Mxh) {
+        const float2 v = cmul(res[c * LS + g], __ldg(Hd + (size_t)g * Mxh + k));
+        acc[i] = cadd(acc[i], v);
+      }
+    }
+  }
+  float2 *P = a.part + ((size_t)pg * a.nb + b) * L * Mxh;
+#pragma unroll
+  for (int i = 0; i < NE; ++i) {
+    const int e = threadIdx.x + i * FT_NT;
+    const int c = e % CK, g = e / CK, k = k0 + c;
+    if (e < CK * L && k < Mxh) P[(size_t)g * Mxh + k] = acc[i];
+  }
+}
+
+// forward: partial sums in group order, inverse FFT along g, rows
+// P..P+nz-1 -> out[b][z][kx]
+template <int L>
+__global__ void __launch_bounds__(FT_NT) k_dfft_fwd_finish(ColArgsD a, const float2 *__restrict__ twg) {
+  constexpr int CK = col_chunk<L>(), LS = L + 1;
+  extern __shared__ __align__(16) float2 cs[];
+  float2 *tw = cs, *s0 = cs + L, *s1 = s0 + CK * LS;
+  for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
+  const int k0 = blockIdx.x * CK, b = blockIdx.y;
+  const int Mxh = a.Mxh;
+  for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
+    const int c = e % CK, g = e / CK, k = k0 + c;
+    float2 v = make_float2(0.f, 0.f);
+    if (k < Mxh)
+      for (int pg = 0; pg < a.npg; ++pg) v = cadd(v, a.part[(((size_t)pg * a.nb + b) * L + g) * Mxh + k]);
+    s0[c * LS + g] = v;
+  }
+  __syncthreads();
+  const float2 *res = fft_lines<L>(s0, s1, CK, LS, tw, -1.f);
+  for (int e = threadIdx.x; e < CK * a.nz; e += FT_NT) {
+    const int c = e % CK, z = e / CK, k = k0 + c;
+    if (k < Mxh) a.out[((size_t)b * a.nz + z) * Mxh + k] = res[c * LS + a.P + z];
+  }
+}
+
+// -------------------------------------------------------------- host side
+
+// grid lengths with instantiated kernels
+static const int kLens[] = {16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 640, 768, 1024};
+
+static int grid_len(int need) {
+  for (int L : kLens)
+    if (L >= need) return L;
+  return -1;
+}
+
+#define DFFT_DISPATCH(L, ...)                                                       \
+  switch (L) {                                                                     \
+    case 16: { constexpr int LL = 16; __VA_ARGS__; } break;                       \
+    case 24: { constexpr int LL = 24; __VA_ARGS__; } break;                       \
+    case 32: { constexpr int LL = 32; __VA_ARGS__; } break;                       \
+    case 40: { constexpr int LL = 40; __VA_ARGS__; } break;                       \
+    case 48: { constexpr int LL = 48; __VA_ARGS__; } break;                       \
+    case 64: { constexpr int LL = 64; __VA_ARGS__; } break;                       \
+    case 80: { constexpr int LL = 80; __VA_ARGS__; } break;                       \
+    case 96: { constexpr int LL = 96; __VA_ARGS__; } break;                       \
+    case 128: { constexpr int LL = 128; __VA_ARGS__; } break;                     \
+    case 160: { constexpr int LL = 160; __VA_ARGS__; } break;                     \
+    case 192: { constexpr int LL = 192; __VA_ARGS__; } break;                     \
+    case 256: { constexpr int LL = 256; __VA_ARGS__; } break;                     \
+    case 320: { constexpr int LL = 320; __VA_ARGS__; } break;                     \
+    case 384: { constexpr int LL = 384; __VA_ARGS__; } break;                     \
+    case 512: { constexpr int LL = 512; __VA_ARGS__; } break;                     \
+    case 640: { constexpr int LL = 640; __VA_ARGS__; } break;                     \
+    case 768: { constexpr int LL = 768; __VA_ARGS__; } break;                     \
+    case 1024: { constexpr int LL = 1024; __VA_ARGS__; } break;                   \
+    default: return set_error(IRLCU_EARG, "DRF FFT length %d not supported", L);   \
+  }
+
+template <int L>
+static int set_col_attrs() {
+  static bool done = false;
+  if (done) return IRLCU_OK;
+  const int sm = (int)col_smem<L>();
+  CU_TRY(cudaFuncSetAttribute(k_dfft_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_dfft_cols_fwd<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_dfft_fwd_finish<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  done = true;
+  return IRLCU_OK;
+}
+
+// work buffers shared by both tables, sized for the largest request
+struct DfftWork {
+  float2 *S = nullptr;     // row spectra of a batch of planes
+  size_t s_elems = 0;
+  float2 *part = nullptr;  // forward partial sums
+  size_t part_elems = 0;
+  float2 *Y = nullptr;     // forward column results
+  size_t y_elems = 0;
+};
+static DfftWork g_dw;
+
+static int grow(float2 **p, size_t *have, size_t need) {
+  if (need <= *have) return IRLCU_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  CU_TRY(cudaMalloc(p, need * sizeof(float2)));
+  *have = need;
+  return IRLCU_OK;
+}
+
+void drf_fft_free(DrfDev &D) {
+  if (D.fft.H) cudaFree(D.fft.H);
+  if (D.fft.twx) cudaFree(D.fft.twx);
+  if (D.fft.twz) cudaFree(D.fft.twz);
+  D.fft = DrfFft{};
+}
+
+void drf_fft_work_free() {
+  if (g_dw.S) cudaFree(g_dw.S);
+  if (g_dw.part) cudaFree(g_dw.part);
+  if (g_dw.Y) cudaFree(g_dw.Y);
+  g_dw = DfftWork{};
+}
+
+// plane groups of the forward column pass
+static int fwd_groups(int nplanes) { return nplanes < 16 ? nplanes : 16; }
+
+int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
+  drf_fft_free(D);
+  const int n = c.n, nz = c.nz, h = D.halo;
+  const int Mx = grid_len(n + h), Mz = grid_len(nz + max_pad + h);
+  if (Mx < 0 || Mz < 0 || Mx < 2 * h + 1 || Mz < 2 * h + 1)
+    return set_error(IRLCU_EARG, "DRF FFT grid for n=%d nz=%d h=%d pad=%d exceeds %d", n, nz, h, max_pad, 1024);
+  DrfFft &F = D.fft;
+  F.Mx = Mx;
+  F.Mz = Mz;
+  F.Mxh = Mx / 2 + 1;
+  F.P = max_pad;
+  F.G = nz + 2 * max_pad;
+  if (F.G > Mz) F.G = Mz;
+  TRY_RC(upload_twiddle_table(&F.twx, Mx));
+  TRY_RC(upload_twiddle_table(&F.twz, Mz));
+  const int nspec = D.ndist + 1;
+  CU_TRY(cudaMalloc(&F.H, sizeof(float2) * (size_t)nspec * Mz * F.Mxh));
+  // work: row spectra for max_batch views (also holds the PSF rows here)
+  const int B = c.g.max_batch;
+  TRY_RC(grow(&g_dw.S, &g_dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
+  TRY_RC(grow(&g_dw.part, &g_dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
+  TRY_RC(grow(&g_dw.Y, &g_dw.y_elems, (size_t)B * nz * F.Mxh));
+  // spectra of the quadrant-swapped PSFs (and the identity), 1/(Mz Mx)
+  RowSrc r{};
+  r.mode = MODE_PSF;
+  r.psf = D.psf;
+  r.h = h;
+  r.pstride = D.pstride;
+  r.ndist = D.ndist;
+  r.n = n;
+  r.nz = nz;
+  r.G = Mz;
+  r.Mz = Mz;
+  r.out = g_dw.S;
+  r.Mxh = F.Mxh;
+  r.nplanes = nspec;
+  DFFT_DISPATCH(Mx, {
+    dim3 grid((Mz + 2 * rows_pairs<LL>() - 1) / (2 * rows_pairs<LL>()), nspec, 1);
+    k_dfft_rows_fwd<LL><<<grid, FT_NT, 0, c.st>>>(r, F.twx);
+    CU_LAUNCHED();
+  });
+  ColArgsD ca{};
+  ca.in = g_dw.S;
+  ca.out = F.H;
+  ca.nplanes = nspec;
+  ca.G = Mz;
+  ca.Mxh = F.Mxh;
+  ca.hscale = (float)(1.0 / ((double)Mz * Mx));
+  DFFT_DISPATCH(Mz, {
+    TRY_RC(set_col_attrs<LL>());
+    dim3 grid((F.Mxh + col_chunk<LL>() - 1) / col_chunk<LL>(), nspec, 1);
+    k_dfft_cols<LL><<<grid, FT_NT, col_smem<LL>(), c.st>>>(ca, COL_H, F.twz);
+    CU_LAUNCHED();
+  });
+  CU_TRY(cudaStreamSynchronize(c.st));
+  F.on = true;
+  return IRLCU_OK;
+}
+
+static RowSrc plane_rows(const Ctx &c, const DrfDev &D, const float *a, size_t a_bs, size_t a_ys, const float *E,
+                         const int *dviews) {
+  RowSrc r{};
+  r.mode = MODE_PLANE;
+  r.a = a;
+  r.a_bs = a_bs;
+  r.a_ys = a_ys;
+  r.E = E;
+  r.views = dviews;
+  r.row_idist = D.row_idist;
+  r.pad_rows = D.pad_rows;
+  r.avgy = D.avg_rows;
+  r.n = c.n;
+  r.nz = c.nz;
+  r.P = D.fft.P;
+  r.G = D.fft.G;
+  r.Mz = D.fft.Mz;
+  r.out = g_dw.S;
+  r.Mxh = D.fft.Mxh;
+  r.nplanes = c.n;
+  return r;
+}
+
+static ColArgsD col_args(const Ctx &c, const DrfDev &D, const int *dviews, int nv) {
+  ColArgsD a{};
+  a.in = g_dw.S;
+  a.H = D.fft.H;
+  a.views = dviews;
+  a.row_idist = D.row_idist;
+  a.ndist = D.ndist;
+  a.nplanes = c.n;
+  a.G = D.fft.G;
+  a.P = D.fft.P;
+  a.nz = c.nz;
+  a.Mxh = D.fft.Mxh;
+  a.part = g_dw.part;
+  a.npg = fwd_groups(c.n);
+  a.nb = nv;
+  return a;
+}
+
+int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
+                       float scale, float *out) {
+  const DrfFft &F = D.fft;
+  if ((size_t)nv * c.n * F.G * F.Mxh > g_dw.s_elems || (size_t)nv * c.nz * F.Mxh > g_dw.y_elems ||
+      (size_t)fwd_groups(c.n) * nv * F.Mz * F.Mxh > g_dw.part_elems)
+    return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
+  const RowSrc r = plane_rows(c, D, src, c.vox, c.pln, E, dviews);
+  DFFT_DISPATCH(F.Mx, {
+    dim3 grid((F.G + 2 * rows_pairs<LL>() - 1) / (2 * rows_pairs<LL>()), c.n, nv);
+    k_dfft_rows_fwd<LL><<<grid, FT_NT, 0, c.st>>>(r, F.twx);
+    CU_LAUNCHED();
+  });
+  ColArgsD a = col_args(c, D, dviews, nv);
+  a.out = g_dw.Y;
+  DFFT_DISPATCH(F.Mz, {
+    TRY_RC(set_col_attrs<LL>());
+    const int nch = (F.Mxh + col_chunk<LL>() - 1) / col_chunk<LL>();
+    k_dfft_cols_fwd<LL><<<dim3(nch, nv, a.npg), FT_NT, col_smem<LL>(), c.st>>>(a, F.twz);
+    CU_LAUNCHED();
+    k_dfft_fwd_finish<LL><<<dim3(nch, nv, 1), FT_NT, col_smem<LL>(), c.st>>>(a, F.twz);
+    CU_LAUNCHED();
+  });
+  RowInv ri{};
+  ri.in = g_dw.Y;
+  ri.np = 1;
+  ri.rs = c.nz;
+  ri.r0 = 0;
+  ri.Mxh = F.Mxh;
+  ri.out = out;
+  ri.n = c.n;
+  ri.nz = c.nz;
+  ri.scale = scale;
+  DFFT_DISPATCH(F.Mx, {
+    dim3 grid((c.nz + 2 * rows_pairs<LL>() - 1) / (2 * rows_pairs<LL>()), 1, nv);
+    k_dfft_rows_inv<LL><<<grid, FT_NT, 0, c.st>>>(ri, F.twx);
+    CU_LAUNCHED();
+  });
+  return IRLCU_OK;
+}
+
+int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,
+                           const DrfDev &D, float scale, float *bck) {
+  const DrfFft &F = D.fft;
+  if ((size_t)nv * c.n * F.G * F.Mxh > g_dw.s_elems)
+    return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
+  const RowSrc r = plane_rows(c, D, planes, c.pln, 0, E, dviews);
+  DFFT_DISPATCH(F.Mx, {
+    dim3 grid((F.G + 2 * rows_pairs<LL>() - 1) / (2 * rows_pairs<LL>()), c.n, nv);
+    k_dfft_rows_fwd<LL><<<grid, FT_NT, 0, c.st>>>(r, F.twx);
+    CU_LAUNCHED();
+  });
+  ColArgsD a = col_args(c, D, dviews, nv);
+  a.out = g_dw.S;
+  DFFT_DISPATCH(F.Mz, {
+    TRY_RC(set_col_attrs<LL>());
+    const int nch = (F.Mxh + col_chunk<LL>() - 1) / col_chunk<LL>();
+    k_dfft_cols<LL><<<dim3(nch, c.n, nv), FT_NT, col_smem<LL>(), c.st>>>(a, COL_BCK, F.twz);
+    CU_LAUNCHED();
+  });
+  RowInv ri{};
+  ri.in = g_dw.S;
+  ri.np = c.n;
+  ri.rs = F.G;
+  ri.r0 = F.P;
+  ri.Mxh = F.Mxh;
+  ri.out = bck;
+  ri.n = c.n;
+  ri.nz = c.nz;
+  ri.scale = scale;
+  DFFT_DISPATCH(F.Mx, {
+    dim3 grid((c.nz + 2 * rows_pairs<LL>() - 1) / (2 * rows_pairs<LL>()), c.n, nv);
+    k_dfft_rows_inv<LL><<<grid, FT_NT, 0, c.st>>>(ri, F.twx);
+    CU_LAUNCHED();
+  });
+  return IRLCU_OK;
+}
+
+}  // namespace irlcu

@@ -20,121 +20,16 @@
 // (libirl uses an external FFT library), so the source agrees with libirl to
 // FFT rounding rather than bit for bit.
 //
-// FFT: batched complex line transforms in shared memory, Stockham autosort
-// with radix-8/4/2 passes and twiddles from a double-accurate table.  Line
-// lengths are powers of two from 8 to 1024.
+// FFT: batched line transforms of fft_core.cuh; the ESSE grids are powers
+// of two from 8 to 1024.
 #include <cmath>
 #include <cstdio>
 #include <vector>
 
+#include "fft_core.cuh"
 #include "irlcu_internal.cuh"
 
 namespace irlcu {
-
-// ------------------------------------------------------------ FFT core
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-// multiply by -i*s (s = +1 forward, -1 inverse): (x, y) -> (s*y, -s*x)
-__device__ __forceinline__ float2 mul_mis(float2 a, float s) { return make_float2(s * a.y, -s * a.x); }
-
-template <int R>
-__device__ __forceinline__ void dft_r(float2 *v, float s);  // s = +1 forward (exp(-i..)), -1 inverse
-
-template <>
-__device__ __forceinline__ void dft_r<2>(float2 *v, float) {
-  const float2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
-}
-
-template <>
-__device__ __forceinline__ void dft_r<4>(float2 *v, float s) {
-  const float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-  const float2 c = cadd(v[1], v[3]), d = mul_mis(csub(v[1], v[3]), s);
-  v[0] = cadd(a, c);
-  v[2] = csub(a, c);
-  v[1] = cadd(b, d);
-  v[3] = csub(b, d);
-}
-
-template <>
-__device__ __forceinline__ void dft_r<8>(float2 *v, float s) {
-  // two 4-point DFTs on even and odd samples, then the radix-2 combine
-  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
-  dft_r<4>(e, s);
-  dft_r<4>(o, s);
-  const float h = 0.70710678118654752440f;
-  // W8^k = exp(-i*s*pi*k/4)
-  const float2 w1 = make_float2(h, -s * h), w3 = make_float2(-h, -s * h);
-  const float2 o1 = cmul(o[1], w1), o2 = mul_mis(o[2], s), o3 = cmul(o[3], w3);
-  v[0] = cadd(e[0], o[0]);
-  v[4] = csub(e[0], o[0]);
-  v[1] = cadd(e[1], o1);
-  v[5] = csub(e[1], o1);
-  v[2] = cadd(e[2], o2);
-  v[6] = csub(e[2], o2);
-  v[3] = cadd(e[3], o3);
-  v[7] = csub(e[3], o3);
-}
-
-// one Stockham pass of radix R over W lines of length L held in shared
-// memory (element (w, i) at base[w*lstride + i]); tw[m] = exp(-2 pi i m / L)
-template <int L, int R>
-__device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int W, int lstride, int Ns,
-                                              const float2 *tw, float s) {
-  const int jobs = W * (L / R);
-  for (int q = threadIdx.x; q < jobs; q += blockDim.x) {
-    const int w = q / (L / R), j = q - w * (L / R);
-    const float2 *src = in + w * lstride;
-    float2 v[8];
-    const int k = j % Ns;
-    const int step = L / (Ns * R);  // twiddle index stride
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      float2 x = src[j + r * (L / R)];
-      if (r > 0 && k > 0) {
-        float2 t = tw[(r * k * step) & (L - 1)];
-        t.y *= s;  // conjugate for the inverse
-        x = cmul(x, t);
-      }
-      v[r] = x;
-    }
-    dft_r<R>(v, s);
-    float2 *dst = out + w * lstride;
-    const int idxD = (j / Ns) * Ns * R + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) dst[idxD + r * Ns] = v[r];
-  }
-}
-
-// full transform; returns the buffer holding the result (a or b)
-template <int L>
-__device__ float2 *fft_lines(float2 *a, float2 *b, int W, int lstride, const float2 *tw, float s) {
-  int Ns = 1;
-  float2 *in = a, *out = b;
-  while (Ns < L) {
-    const int rem = L / Ns;
-    if (rem >= 8) {
-      stockham_pass<L, 8>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 8;
-    } else if (rem == 4) {
-      stockham_pass<L, 4>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 4;
-    } else {
-      stockham_pass<L, 2>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 2;
-    }
-    __syncthreads();
-    float2 *t = in;
-    in = out;
-    out = t;
-  }
-  return in;
-}
 
 // ----------------------------------------------------------- pass kernels
 
@@ -701,7 +596,7 @@ static EsseWork g_ew;
 
 static bool pow2_ok(int v) { return v >= 8 && v <= 1024 && (v & (v - 1)) == 0; }
 
-static int upload_twiddles(float2 **d, int L) {
+int upload_twiddle_table(float2 **d, int L) {
   std::vector<float2> h(L);
   for (int m = 0; m < L; ++m) {
     const double a = -2.0 * M_PI * (double)m / (double)L;
@@ -711,6 +606,8 @@ static int upload_twiddles(float2 **d, int L) {
   CU_TRY(cudaMemcpy(*d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
   return IRLCU_OK;
 }
+
+static int upload_twiddles(float2 **d, int L) { return upload_twiddle_table(d, L); }
 
 #define LDISPATCH(L, KERNEL, GRID, BLOCK, SMEM, ST, ...)                         \
   switch (L) {                                                                   \

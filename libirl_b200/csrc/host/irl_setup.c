@@ -510,9 +510,6 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 		base[k] = total;
 		if (t == NULL)
 			continue;
-		if (t->bFFTconvolve)
-			irl_warn("SetupDrf", "FFT convolution requested; the direct convolution is used instead "
-				"(identical results without axial padding)");
 		for (i = 0; i < t->iNumDistances; ++i) {
 			halo = MAX(halo, t->psDrfs[i].MaxOffsX - 1);
 			halo = MAX(halo, t->psDrfs[i].MaxOffsY - 1);
@@ -535,8 +532,9 @@ static void upload_one(const irl_parms *p, irl_view *views, int bck)
 			for (yy = 0; yy < wy; ++yy)
 				for (xx = 0; xx < wx; ++xx)
 					dst[(size_t)(yy + oy) * w + xx + ox] = d->Psf[yy * wx + xx];
-			/* conv2d_ypad.c:54-57: iPadY = clamp(iAxialPadLength, 0, bCtrY) */
-			pad[base[k] + i] = MIN(MAX(p->pad_len, 0), d->MaxOffsY - 1);
+			/* conv2d_ypad.c:54-57: iPadY = clamp(iAxialPadLength, 0, bCtrY);
+			   conv2dPsfFFT zero pads instead (convolve_ypad.c:63-94) */
+			pad[base[k] + i] = t->bFFTconvolve ? 0 : MIN(MAX(p->pad_len, 0), d->MaxOffsY - 1);
 			taps[base[k] + i] = wx * wy;
 		}
 	}
