@@ -152,6 +152,8 @@ def run_b200(args):
                           api.ITER_CB(), None, api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
     if rc:
         raise RuntimeError(lib.pchIrlErrorString().decode())
+    grids = (C.c_int * 5)()
+    lib.irlcu_grids(grids)
     stream = torch.cuda.ExternalStream(lib.irlcu_stream())
     if lib.IrlOsemIterate(Wm):
         raise RuntimeError(lib.pchIrlErrorString().decode())
@@ -189,28 +191,32 @@ def run_b200(args):
     e2e = None
     if not args.no_e2e:
         E_IT = 10
+        msgs = os.path.join(tmp, "e2e_messages.txt")
         for it in (1, E_IT):  # a short warm-up call, then the timed one
             p, o, v = case.parms(), case.options(), case.views()
             p.NumIterations = it
+            o.iMsgLevel = 5  # the library's own phase timings, to a file
             atn = case.atn.copy()
             rec = np.zeros_like(case.act)
             m = meas.copy()
             cb = api.ITER_CB(lambda i, q: None)
             t0 = time.perf_counter()
             rc = lib.IrlOsem(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), cb, None,
-                             api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+                             api.fptr(atn), api.fptr(m), api.fptr(rec), None, msgs.encode())
             wall = time.perf_counter() - t0
             if rc:
                 raise RuntimeError(lib.pchIrlErrorString().decode())
+        phases = _message_phases(msgs)
         h2d = (meas.nbytes + case.atn.nbytes + case.act.nbytes) / E_IT
         d2h = (case.act.nbytes * E_IT + case.act.nbytes) / E_IT
         e2e = {"value": round(1000.0 * wall / E_IT, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "iterations": E_IT,
                "includes": "set-up (tables, ESSE kernel spectra, attenuation tables, 8 norm images), "
-                           "host<->device copies from pageable memory, per-iteration callback"}
+                           "host<->device copies from pageable memory, per-iteration callback",
+               "phases_s": phases}
 
     clocks = clk.summary()
-    roofline = make_roofline(prof, clocks)
+    roofline = make_roofline(prof, case, list(grids))
     stages = {L.STAGES[i]: {"ms": round(prof.ms[i], 3), "launches": int(prof.launches[i]),
                             "gflop": round(prof.flops[i] / 1e9, 2), "gbyte": round(prof.bytes[i] / 1e9, 3)}
               for i in range(6)}
@@ -238,50 +244,90 @@ def run_b200(args):
     print(json.dumps(line))
 
 
-def _traffic_from_profiles():
-    """Per-launch DRAM bytes of the DRF projector kernel from the committed
-    ncu summary (profiles/drf_conv_full128.md), or None."""
-    path = os.path.join(ROOT, "profiles", "drf_conv_full128.md")
+def _message_phases(path):
+    """Set-up and per-iteration wall times the library itself logged."""
+    out = {"setup": None, "norms": None, "iterations": []}
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith("Done Initialization"):
+                out["setup"] = float(line.split("(")[1].split()[0])
+            elif line.startswith("Done Computing Norm Matrix"):
+                out["norms"] = float(line.split("(")[1].split()[0])
+            elif "Done iteration" in line:
+                out["iterations"].append(float(line.split("(")[1].split()[0]))
+    except (OSError, ValueError, IndexError):
+        pass
+    return out
+
+
+def _traffic_from_profiles(name, key):
+    """DRAM bytes (ncu dram__bytes_read + write) recorded in a committed
+    profile summary under profiles/, or None."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
-    except OSError:
+    except (OSError, ValueError):
         pass
     return None
 
 
-def make_roofline(prof, clocks):
-    """The dominant stage is the direct DRF convolution (projector +
-    backprojector), an FP32 FMA-bound kernel: its bound is the CUDA-core FP32
-    peak, 148 SMs x 128 FMA lanes x 2 FLOP x SM clock, evaluated at the
-    median SM clock measured during the timed region (neither of the
-    measured HBM / bf16-tensor peaks bounds it)."""
-    i_p, i_b = 2, 4
-    ms = prof.ms[i_p] + prof.ms[i_b]
-    fl = prof.flops[i_p] + prof.flops[i_b]
-    launches = max(1, prof.launches[i_p] + prof.launches[i_b])
-    mhz = clocks.get("sm_mhz") or 1965.0
-    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    achieved = fl / (ms * 1e-3) / 1e12 if ms > 0 else 0.0
-    hbm = None
+def _hbm_peak():
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        hbm_peak, src = peaks["hbm_gbs"], "measured"
+        return float(peaks["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
-        hbm_peak, src = 6650.0, "fallback"
-    # memory-bound companion: unrotation + clamped accumulation
-    if prof.ms[5] > 0:
-        gbs = prof.bytes[5] / (prof.ms[5] * 1e-3) / 1e9
-        hbm = {"stage": "unrotate_accumulate", "achieved": round(gbs, 1), "peak": hbm_peak,
-               "unit": "GB/s", "frac": round(gbs / hbm_peak, 3), "peak_source": src}
-    return {"bound": "fp32", "kernel": "k_drf_forward / k_drf_backward (direct 33x33 DRF convolution)",
-            "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
-            "frac": round(achieved / peak, 3) if peak else None,
-            "peak_source": f"FP32 FMA peak at the measured median SM clock ({mhz:.0f} MHz)",
-            "traffic": _traffic_from_profiles(),
-            "algorithmic": "2 FLOP per PSF tap per output pixel, planes at distance > 0",
-            "launch_ms": round(ms / launches, 4), "hbm_companion": hbm}
+        return 6650.0, "fallback"
+
+
+def make_roofline(prof, case, grids):
+    """Roofline of the dominant stage of an OSEM iteration.  Both candidate
+    stages are FFT work that the per-unit figures bound by HBM traffic:
+
+      DRF (Fourier-domain engine, projector + backprojector): per plane one
+        2D transform forward and two backward, each 2 passes (rows, columns)
+        of >= 2 x 4 bytes x Mz*Mx (the transform grid);
+      ESSE: per view three 3D transforms (one forward, two inverse) of
+        3 passes each of >= 2 x 4 bytes x Kx*Ky*Kz, plus 3 x 4 bytes x voxels
+        for the depth / density combination.
+
+    achieved = those bytes per subset / the stage's device time per subset
+    (CUDA events around the stage on the library stream); peak = the
+    measured HBM copy bandwidth."""
+    peak, src = _hbm_peak()
+    n, nz = case.n, case.nz
+    vox = n * nz * n
+    mz, mx, kx, ky, kz = grids
+    per_view = {}
+    if mz and mx:
+        per_view["drf"] = n * 3 * 2 * (2 * 4 * mz * mx)
+    if kx:
+        per_view["esse"] = 3 * 3 * (2 * 4 * kx * ky * kz) + 3 * 4 * vox
+    idx = {"drf": (2, 4), "esse": (1,)}
+    names = {"drf": "k_dfft_rows_fwd / k_dfft_cols_fwd / k_dfft_cols / k_dfft_rows_inv (Fourier-domain DRF)",
+             "esse": "k_fft_row_fwd / k_esse_yz / k_fft_row_inv / k_expand_y / k_smooth_z / k_smooth_x_combine (ESSE)"}
+    traffic_keys = {"drf": ("drf_fft_full128.md", "traffic_bytes_per_subset"),
+                    "esse": ("esse_full128.md", "traffic_bytes_per_subset")}
+    subsets = case.subsets
+    per = case.nviews // subsets
+    out = []
+    for k, bytes_view in per_view.items():
+        ms = sum(prof.ms[i] for i in idx[k]) / subsets
+        if ms <= 0:
+            continue
+        b = bytes_view * per
+        gbs = b / (ms * 1e-3) / 1e9
+        tr = _traffic_from_profiles(*traffic_keys[k])
+        out.append({"stage": k, "kernel": names[k], "bound": "hbm", "achieved": round(gbs, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(gbs / peak, 3), "peak_source": src,
+                    "traffic": tr, "algorithmic_bytes_per_launch": int(b), "launch_ms": round(ms, 4),
+                    "launch": f"one subset ({per} views)"})
+    if not out:
+        return None
+    out.sort(key=lambda r: -r["launch_ms"])
+    top = dict(out[0])
+    top["other_stages"] = out[1:]
+    return top
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -389,7 +435,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -172,6 +172,11 @@ int irlcu_stage_times(float *ms, int nmax);
    cudaStream_t), so callers can time or order work against it. */
 void *irlcu_stream(void);
 
+/* Transform grids in use (0 where not set up): out[0..1] = Mz, Mx of the
+   projector's Fourier-domain DRF engine (0, 0: direct convolution),
+   out[2..4] = Kx, Ky, Kz of the ESSE grid. */
+int irlcu_grids(int out[5]);
+
 /* Kernel launches issued by the library since the context was created. */
 long long irlcu_launch_count(void);
 

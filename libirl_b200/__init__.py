@@ -68,6 +68,8 @@ def _declare_irlcu(lib):
     lib.irl_gendrf.argtypes = [C.c_float] * 8 + [I, I, C.POINTER(api.Drf)]
     lib.irl_compute_subsets.restype = I
     lib.irl_compute_subsets.argtypes = [I, I, C.POINTER(C.POINTER(C.c_int))]
+    lib.irlcu_grids.restype = I
+    lib.irlcu_grids.argtypes = [C.POINTER(C.c_int)]
     lib.irlcu_stream.restype = C.c_void_p
     lib.irlcu_stream.argtypes = []
     lib.irlcu_launch_count.restype = C.c_longlong

@@ -652,6 +652,18 @@ int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n
   return IRLCU_OK;
 }
 
+int irlcu_grids(int out[5]) {
+  TRY(need_ctx());
+  const Ctx &c = *g_ctx;
+  const DrfFft &F = c.drf[0].fft;
+  out[0] = F.on ? F.Mz : 0;
+  out[1] = F.on ? F.Mx : 0;
+  out[2] = c.esse.on ? c.esse.kx : 0;
+  out[3] = c.esse.on ? c.esse.ky : 0;
+  out[4] = c.esse.on ? c.esse.kz : 0;
+  return IRLCU_OK;
+}
+
 void *irlcu_stream(void) { return g_ctx ? (void *)g_ctx->st : nullptr; }
 
 long long irlcu_launch_count(void) { return g_launch_count; }

@@ -106,6 +106,23 @@ def ref_rot3dpar(angle, vol, pb_flag=0):
     return out
 
 
+def ref_conv2d_fft(plane, psf):
+    """The reference's FFT convolution branch as ConvolveDrfYpad runs it
+    (convolve_ypad.c:63-94): PadSwap the PSF into a 2N x 2Nz grid, realft3d,
+    conv2dPsfFFT."""
+    lib = ref()
+    plane = _arr(plane)
+    psf = _arr(psf)
+    ny, nx = plane.shape
+    py, px = psf.shape
+    grid = np.zeros((2 * ny, 2 * nx), np.float32)
+    lib.PadSwap(api.fptr(psf), px, py, api.fptr(grid), 2 * nx, 2 * ny)
+    lib.realft3d(api.fptr(grid), 2 * nx, 2 * ny, 1)
+    out = np.zeros_like(plane)
+    lib.conv2dPsfFFT(api.fptr(plane), nx, ny, api.fptr(grid), 2 * nx, 2 * ny, api.fptr(out))
+    return out
+
+
 def ref_conv2d_ypad(plane, psf, pad=0, avg=0):
     lib = ref()
     plane = _arr(plane)

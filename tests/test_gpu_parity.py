@@ -89,7 +89,7 @@ def test_rotation_bit_exact(product, orc, n, nz, fast):
 
 # -------------------------------------------------------------- projection
 
-@pytest.mark.parametrize("variant", ["atn", "atn_drf", "drf_pad", "srf_c2", "srf_c1", "srf_primary0"])
+@pytest.mark.parametrize("variant", ["atn", "atn_drf", "drf_pad", "fft_table", "srf_c2", "srf_c1", "srf_primary0"])
 def test_genprj_per_view(product, orc, tmp_path, variant):
     if variant.startswith("srf"):
         c = 1 if variant == "srf_c1" else 2
@@ -97,8 +97,13 @@ def test_genprj_per_view(product, orc, tmp_path, variant):
     else:
         case = W.plain64(seed=1100, n=48, nviews=12, subsets=2, iterations=2)
     files = case.write_tables(str(tmp_path))
-    pad = (3, 2) if variant == "drf_pad" else (0, 0)
+    pad = (3, 2) if variant in ("drf_pad", "fft_table") else (0, 0)
     opts = {"iAxialPadLength": pad[0], "iAxialAvgLength": pad[1]}
+    if variant == "fft_table":
+        # libirl's FFT convolution path ignores the axial pad
+        # (convolve_ypad.c:63-94): the oracle runs without it
+        opts["bFFTConvolve"] = 1
+        pad = (0, 0)
     prim = 0.0 if variant == "srf_primary0" else 1.0
     use_drf = variant != "atn"
     got = gpu_genprj(product, case, files, primary=prim, opts=opts, model_drf=use_drf)
@@ -106,6 +111,39 @@ def test_genprj_per_view(product, orc, tmp_path, variant):
     want = pr.genprj(primary=prim)
     for vi in range(case.nviews):
         assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (variant, vi, rel_l2(got[vi], want[vi]))
+
+
+@pytest.mark.parametrize("engine", ["direct", "fft"])
+def test_genprj_drf_engines(product, orc, tmp_path, monkeypatch, engine):
+    """Both DRF engines (direct convolution kernels and the Fourier-domain
+    engine) against the oracle on a 33 x 33 DRF with axial padding."""
+    monkeypatch.setenv("IRLCU_DRF_ENGINE", engine)
+    case = W.full128(seed=2150, n=48, nviews=6, subsets=2, iterations=1, drf_max_offs=17, with_srf=False)
+    files = case.write_tables(str(tmp_path))
+    opts = {"iAxialPadLength": 4, "iAxialAvgLength": 3}
+    got = gpu_genprj(product, case, files, opts=opts, krnl=False)
+    want = orc.Problem(case, with_srf=False, pad_len=4, avg_len=3).genprj()
+    for vi in range(case.nviews):
+        assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (engine, vi, rel_l2(got[vi], want[vi]))
+
+
+def test_drf_half_width_beyond_direct_limit(product, orc, tmp_path, monkeypatch):
+    """A 73 x 73 DRF (half-width 36) runs on the Fourier-domain engine only;
+    the direct engine refuses it."""
+    case = W.full128(seed=2160, n=40, nviews=3, subsets=1, iterations=1, drf_max_offs=37, with_srf=False)
+    files = case.write_tables(str(tmp_path))
+    monkeypatch.setenv("IRLCU_DRF_ENGINE", "direct")
+    p, o, v = case.parms(), case.options(), case.views()
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    rc = product.IrlGenprj(C.byref(p), C.byref(o), v, dup(files["drf"]), None, None, None, api.fptr(act),
+                           api.fptr(atn), api.fptr(prj), 1.0, None, None)
+    assert rc != 0 and b"limit" in product.pchIrlErrorString()
+    monkeypatch.setenv("IRLCU_DRF_ENGINE", "auto")
+    got = gpu_genprj(product, case, files, krnl=False)
+    want = orc.Problem(case, with_srf=False).genprj()
+    for vi in range(case.nviews):
+        assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (vi, rel_l2(got[vi], want[vi]))
 
 
 def test_genprj_golden_fixture(product, tmp_path):

@@ -109,3 +109,41 @@ def test_oracle_vs_reference_live_osem_padding(orc):
                          api.fptr(atn), api.fptr(prj), 1.0, None, None) == 0
     pr = orc.Problem(case, pad_len=3, avg_len=2)
     assert np.array_equal(pr.genprj(), prj)
+
+
+def test_reference_fft_convolution_is_zero_padded_direct(orc):
+    """libirl's FFT convolution branch (PadSwap + realft3d + conv2dPsfFFT on a
+    2N x 2Nz grid) equals the direct "same" convolution with no axial
+    padding: the axial pad is ignored and, for h <= N, the circular
+    convolution never wraps onto the cropped output."""
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    rng = np.random.default_rng(31)
+    for ny, nx, h in [(12, 16, 3), (17, 20, 6), (32, 32, 16), (9, 40, 8)]:
+        plane = rng.random((ny, nx), dtype=np.float32)
+        psf = rng.random((2 * h + 1, 2 * h + 1)).astype(np.float32)
+        psf /= psf.sum()
+        fft = orc.ref_conv2d_fft(plane, psf)
+        direct = orc.ref_conv2d_ypad(plane, psf, pad=0, avg=0)
+        assert rel_l2(fft, direct) <= 1e-6, (ny, nx, h, rel_l2(fft, direct))
+        padded = orc.ref_conv2d_ypad(plane, psf, pad=min(3, h), avg=2)
+        assert rel_l2(padded, direct) > 1e-4  # the pad would have mattered
+
+
+def test_reference_fft_table_genprj_matches_oracle_without_pad(orc):
+    """Full IrlGenprj chain with bFFTConvolve: the reference's projections
+    equal the oracle's direct convolution with the axial pad switched off."""
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    case = W.plain64(seed=1078, n=24, nviews=6, subsets=2, iterations=1)
+    files = case.write_tables("/tmp/irl_oracle_fft")
+    ref = orc.ref()
+    p, o, v = case.parms(), case.options(), case.views()
+    o.iAxialPadLength, o.iAxialAvgLength, o.bFFTConvolve = 3, 2, 1
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    assert ref.IrlGenprj(C.byref(p), C.byref(o), v, dup(files["drf"]), None, None, None, api.fptr(act),
+                         api.fptr(atn), api.fptr(prj), 1.0, None, None) == 0
+    want = orc.Problem(case, pad_len=0, avg_len=0).genprj()
+    for vi in range(case.nviews):
+        assert rel_l2(prj[vi], want[vi]) <= 1e-6, (vi, rel_l2(prj[vi], want[vi]))
