@@ -7,7 +7,7 @@
  * stopping rules).  libirl has no counterpart of these three functions.
  *
  * One session at a time per process (the library is non-reentrant, like
- * libirl).  The caller's arrays follow IrlOsem's contract: pfAtnMap,
+ * libirl); IrlOsemBatch runs several side by side internally.  The caller's arrays follow IrlOsem's contract: pfAtnMap,
  * pfPrjImage and pfScatterEstimate are modified in place by Begin, and
  * pfReconImage must stay valid until End (hooks see it in the internal
  * layout, as in libirl).
@@ -38,6 +38,30 @@ int IrlOsemIterate(int iNumIterations);
 /* Copies the estimate (external layout) into pfReconImage and closes the
    session.  Always safe to call; returns the session's error code. */
 int IrlOsemEnd(float *pfReconImage);
+
+/* One reconstruction of a batch: IrlOsem's arguments without the
+   callback, log and message files.  iStatus receives its return code. */
+typedef struct {
+	IrlParms_t *psIrlParms;
+	Options_t *psOptions;
+	PrjView_t *psViews;
+	char *pchDrfTabFname;       /* malloc'd; freed by the library, as in IrlOsem */
+	char *pchScatKrnlFname;
+	float *pfScatterEstimate;
+	float *pfAtnMap;
+	float *pfPrjImage;
+	float *pfReconImage;
+	int iStatus;
+} IrlOsemProblem_t;
+
+/* Runs nprob independent OSEM reconstructions, each exactly as IrlOsem
+   would run it alone (same results), resident together on the device:
+   every problem has its own device context and stream, and the host
+   enqueues their iterations round-robin so that small problems overlap on
+   the GPU.  Not allowed with hooks, or with iSetupExtraPrjViewData /
+   iSetupDetectors data pending (those are per-call state of IrlOsem).
+   Returns 0, or the first non-zero iStatus. */
+int IrlOsemBatch(int nprob, IrlOsemProblem_t *psProblems);
 
 #ifdef __cplusplus
 }

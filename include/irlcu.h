@@ -122,6 +122,27 @@ int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp,
 	int model, int bck_model, int subset, int use_scatest, int apply_update,
 	int accumulate_from_update);
 
+/* Views of every subset for irlcu_osem_iteration: views[s*per + m] and the
+   per-view ViewTime / Sensitivity in vp (its scat_mode is ignored); kept on
+   the device. */
+int irlcu_set_subsets(int nsub, int per, const int *views, const irlcu_view_parm *vp);
+
+/* One OSEM iteration over every subset set by irlcu_set_subsets: the
+   subset loop of osemrecon.c:687-863 without hooks, each subset as
+   irlcu_osem_subset in batches of max_batch views, scat_mode for every
+   view.  The first call with a given (model, bck_model, use_scatest,
+   scat_mode) runs eagerly; later ones replay a CUDA graph captured from the
+   second (set IRLCU_GRAPHS=0 to always run eagerly).  Asynchronous: returns
+   once the work is enqueued on the library stream. */
+int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mode);
+
+/* Several device contexts per process (one per reconstruction of a batch):
+   irlcu_ctx_detach returns the current context and leaves none current, so
+   that the next irlcu_init creates a new one; irlcu_ctx_attach makes a
+   detached context current again (none may be current). */
+void *irlcu_ctx_detach(void);
+int irlcu_ctx_attach(void *ctx);
+
 /* Normalisation image of one subset (osemrecon.c:282-320): backprojects
    the measured-bin mask times ViewTime of each view, clamps after each,
    inverts with a 1e-6 floor and stores it as NORM[subset]. */
@@ -176,6 +197,11 @@ void *irlcu_stream(void);
    projector's Fourier-domain DRF engine (0, 0: direct convolution),
    out[2..4] = Kx, Ky, Kz of the ESSE grid. */
 int irlcu_grids(int out[5]);
+
+/* The DRF engine autotuner's last measurement (ms for one projection plus
+   backprojection of a subset batch): ms[0] direct kernels, ms[1] the
+   Fourier-domain engine; zeros before the first tuning. */
+int irlcu_drf_tuning(float ms[2]);
 
 /* Kernel launches issued by the library since the context was created. */
 long long irlcu_launch_count(void);

@@ -68,6 +68,8 @@ def _declare_irlcu(lib):
     lib.irl_gendrf.argtypes = [C.c_float] * 8 + [I, I, C.POINTER(api.Drf)]
     lib.irl_compute_subsets.restype = I
     lib.irl_compute_subsets.argtypes = [I, I, C.POINTER(C.POINTER(C.c_int))]
+    lib.irlcu_drf_tuning.restype = I
+    lib.irlcu_drf_tuning.argtypes = [C.POINTER(C.c_float)]
     lib.irlcu_grids.restype = I
     lib.irlcu_grids.argtypes = [C.POINTER(C.c_int)]
     lib.irlcu_stream.restype = C.c_void_p
@@ -84,6 +86,16 @@ def _declare_irlcu(lib):
     lib.IrlOsemIterate.argtypes = [I]
     lib.IrlOsemEnd.restype = I
     lib.IrlOsemEnd.argtypes = [F]
+    lib.IrlOsemBatch.restype = I
+    lib.IrlOsemBatch.argtypes = [I, C.POINTER(api.OsemProblem)]
+    lib.irlcu_set_subsets.restype = I
+    lib.irlcu_set_subsets.argtypes = [I, I, C.POINTER(C.c_int), C.c_void_p]
+    lib.irlcu_osem_iteration.restype = I
+    lib.irlcu_osem_iteration.argtypes = [I, I, I, I]
+    lib.irlcu_ctx_detach.restype = C.c_void_p
+    lib.irlcu_ctx_detach.argtypes = []
+    lib.irlcu_ctx_attach.restype = I
+    lib.irlcu_ctx_attach.argtypes = [C.c_void_p]
 
 
 NSTAGE = 8

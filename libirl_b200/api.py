@@ -134,6 +134,22 @@ def bstr(s):
     return None if s is None else (s.encode() if isinstance(s, str) else s)
 
 
+class OsemProblem(C.Structure):
+    """IrlOsemProblem_t (include/irl_b200.h): one reconstruction of a batch."""
+    _fields_ = [
+        ("psIrlParms", C.POINTER(IrlParms)),
+        ("psOptions", C.POINTER(Options)),
+        ("psViews", C.POINTER(PrjView)),
+        ("pchDrfTabFname", C.c_void_p),     # malloc'd (the library frees it)
+        ("pchScatKrnlFname", C.c_void_p),
+        ("pfScatterEstimate", FLOAT_P),
+        ("pfAtnMap", FLOAT_P),
+        ("pfPrjImage", FLOAT_P),
+        ("pfReconImage", FLOAT_P),
+        ("iStatus", C.c_int),
+    ]
+
+
 def declare_irl(lib: C.CDLL) -> C.CDLL:
     """Declare the libirl entry points (irl.h, osemhooks.h) on a CDLL."""
     lib.IrlOsem.restype = C.c_int

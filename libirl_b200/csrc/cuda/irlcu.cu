@@ -96,7 +96,7 @@ int set_error(int code, const char *fmt, ...) {
 
 int halo_instance(int h);
 size_t forward_partial_elems(int n, int nz, int max_batch);
-void free_rotate_scratch();
+void free_rotate_scratch(Ctx &c);
 void esse_free(Ctx &c);
 
 template <class T>
@@ -117,9 +117,19 @@ static void dfree(T *&p) {
   p = nullptr;
 }
 
+static void graphs_clear(Ctx &c) {
+  for (GraphRec &g : c.graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  c.graphs.clear();
+  c.graph_seen.clear();
+}
+
 static void free_ctx(Ctx *c) {
   if (!c) return;
   cudaStreamSynchronize(c->st);
+  graphs_clear(*c);
+  dfree(c->dviews_all);
+  dfree(c->dvp_all);
   dfree(c->rot.hdr);
   dfree(c->rot.row_sh);
   dfree(c->rot.row_f1);
@@ -156,9 +166,9 @@ static void free_ctx(Ctx *c) {
     dfree(c->drf[w].row_idist);
     drf_fft_free(c->drf[w]);
   }
-  drf_fft_work_free();
+  drf_fft_work_free(*c);
   esse_free(*c);
-  free_rotate_scratch();
+  free_rotate_scratch(*c);
   for (auto &e : c->ev) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -297,6 +307,61 @@ int irlcu_set_angles(const float *angles) {
   return IRLCU_OK;
 }
 
+// ------------------------------------------------------------ autotuner
+// DRF engine per table: the direct kernels and the Fourier-domain engine
+// compute the same convolution; which is faster depends on the PSF size,
+// the plane size and the batch.  One projection plus backprojection of a
+// subset batch (views 0 .. B-1 of this geometry) is timed with each, after
+// one untimed run, and the faster is kept.  Decisions are cached per
+// (n, nz, half-width, distances, pad, batch, views) for the process.
+enum { ENGINE_TUNE = 0, ENGINE_DIRECT = 1, ENGINE_FFT = 2 };
+
+struct TuneKey {
+  int n, nz, halo, ndist, pad, batch, nv;
+  bool operator==(const TuneKey &o) const {
+    return n == o.n && nz == o.nz && halo == o.halo && ndist == o.ndist && pad == o.pad && batch == o.batch &&
+           nv == o.nv;
+  }
+};
+static std::vector<std::pair<TuneKey, bool>> g_tune_cache;
+static float g_tune_ms[2] = {0.f, 0.f};  // last timing: direct, Fourier domain
+
+static int upload_views(const int *views, int nv, const irlcu_view_parm *vp);
+
+static int time_drf(Ctx &c, const DrfDev &D, int B, float *ms) {
+  for (int rep = 0; rep < 2; ++rep) {
+    if (rep == 1) CU_TRY(cudaEventRecord(c.ev[4], c.st));
+    TRY(launch_project(c, c.wrot, c.dviews, B, nullptr, &D, 1.0f, c.wprj));
+    TRY(launch_backproject(c, c.wprj, c.dviews, B, nullptr, &D, 1.0f, c.wbck));
+  }
+  CU_TRY(cudaEventRecord(c.ev[5], c.st));
+  CU_TRY(cudaEventSynchronize(c.ev[5]));
+  CU_TRY(cudaEventElapsedTime(ms, c.ev[4], c.ev[5]));
+  return IRLCU_OK;
+}
+
+static int drf_autotune(Ctx &c, DrfDev &D, int max_pad, bool *fft) {
+  const int B = std::min(c.g.max_batch, c.nv);
+  const TuneKey key{c.n, c.nz, D.halo, D.ndist, max_pad, B, c.nv};
+  for (const auto &e : g_tune_cache)
+    if (e.first == key) {
+      *fft = e.second;
+      return IRLCU_OK;
+    }
+  std::vector<int> views(B);
+  for (int i = 0; i < B; ++i) views[i] = i;
+  TRY(upload_views(views.data(), B, nullptr));
+  CU_TRY(cudaMemsetAsync(c.wrot, 0, sizeof(float) * c.vox * B, c.st));
+  D.fft.on = false;
+  TRY(time_drf(c, D, B, &g_tune_ms[0]));
+  D.fft.on = true;
+  TRY(time_drf(c, D, B, &g_tune_ms[1]));
+  *fft = g_tune_ms[1] < g_tune_ms[0];
+  D.fft.on = *fft;
+  g_tune_cache.push_back({key, *fft});
+  return IRLCU_OK;
+}
+
 int irlcu_set_drf(int which, const irlcu_drf *d) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
@@ -308,17 +373,18 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   drf_fft_free(D);
   D = DrfDev{};
   if (!d) return IRLCU_OK;
-  // engine: the direct kernels take half-widths up to 32; the Fourier-domain
-  // engine any that fits its grid.  IRLCU_DRF_ENGINE = direct | fft | auto
-  // (auto: Fourier domain from half-width 8 on, where it needs fewer FLOPs)
+  // engine: the direct kernels take half-widths up to 32, the Fourier-domain
+  // engine any that fits its grid.  IRLCU_DRF_ENGINE = direct | fft | auto;
+  // auto (the default) times both on this table and keeps the faster
   const int Hd = halo_instance(d->halo);
   const char *eng = getenv("IRLCU_DRF_ENGINE");
-  bool use_fft = Hd < 0 || Hd >= 8;
-  if (eng && !strcmp(eng, "direct")) {
-    if (Hd < 0) return set_error(IRLCU_EARG, "DRF half-width %d exceeds the direct-convolution limit (32)", d->halo);
-    use_fft = false;
-  } else if (eng && !strcmp(eng, "fft")) {
-    use_fft = true;
+  int mode = ENGINE_TUNE;
+  if (eng && !strcmp(eng, "direct")) mode = ENGINE_DIRECT;
+  if (eng && !strcmp(eng, "fft")) mode = ENGINE_FFT;
+  if (Hd < 0) {
+    if (mode == ENGINE_DIRECT)
+      return set_error(IRLCU_EARG, "DRF half-width %d exceeds the direct-convolution limit (32)", d->halo);
+    mode = ENGINE_FFT;
   }
   const int H = Hd >= 0 ? Hd : d->halo;
   const int PW = 2 * H + 1, PLD = (PW + 3) & ~3, w = 2 * d->halo + 1;
@@ -341,11 +407,16 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   D.h_rows.assign(d->row_idist, d->row_idist + (size_t)c.nv * c.n);
   D.h_taps.resize(d->ndist);
   for (int i = 0; i < d->ndist; ++i) D.h_taps[i] = d->taps ? d->taps[i] : w * w;
-  if (use_fft) {
+  if (mode != ENGINE_DIRECT) {
     int max_pad = 0;
     if (d->avg_rows > 0)
       for (int i = 0; i < d->ndist; ++i) max_pad = std::max(max_pad, d->pad_rows[i]);
     TRY(drf_fft_setup(c, D, max_pad));
+    if (mode == ENGINE_TUNE) {
+      bool fft = true;
+      TRY(drf_autotune(c, D, max_pad, &fft));
+      if (!fft) drf_fft_free(D);
+    }
   }
   return IRLCU_OK;
 }
@@ -518,6 +589,52 @@ int irlcu_project(int nv, const int *views, int model, float primary_fac, float 
   return IRLCU_OK;
 }
 
+// the device work of one subset batch whose views and parameters are at
+// c.dviews / c.dvp; hviews: the same view indices on the host (accounting)
+static int osem_subset_body(int nv, const int *hviews, bool need_nosrf, int model, int bck_model, int subset,
+                            int use_scatest, int apply_update, int accumulate_from_update) {
+  Ctx &c = *g_ctx;
+  float *calc = c.wprj;
+  float *calc_nosrf = c.wprj2;
+  float *ratio = c.wprj2 + c.pln * c.g.max_batch;
+  if (!c.capturing) CU_TRY(cudaEventRecord(c.ev[0], c.st));
+  TRY(forward_batch(nv, hviews, model, 1.0f, calc, need_nosrf ? calc_nosrf : nullptr));
+  if (!c.capturing) CU_TRY(cudaEventRecord(c.ev[1], c.st));
+  {
+    Stage s(IRLCU_ST_REDUCE, c.st);
+    s.bytes = 16.0 * (double)c.pln * nv;
+    TRY(launch_ratio(c, calc, calc_nosrf, c.dviews, c.dvp, nv, use_scatest, ratio));
+  }
+  const float *E = (bck_model & MODEL_ATN_BIT) ? c.tE : nullptr;
+  const DrfDev *drf = nullptr;
+  if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
+  {
+    Stage s(IRLCU_ST_BACKPROJECT, c.st);
+    s.flops = drf_flops(c, drf, hviews, nv, false);
+    s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;  // attenuation factor read, plane written
+    TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
+  }
+  if (!c.capturing) CU_TRY(cudaEventRecord(c.ev[2], c.st));
+  {
+    Stage s(IRLCU_ST_ACCUM, c.st);
+    // unrotation (read + write per view), accumulation read per view, and
+    // the update / estimate read-modify-write
+    s.bytes = 12.0 * (double)c.vox * nv + 16.0 * (double)c.vox;
+    TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nv, c.upd, accumulate_from_update,
+                                   apply_update ? ACC_EM : 0, c.est,
+                                   apply_update ? c.norm + (size_t)subset * c.vox : nullptr));
+  }
+  if (!c.capturing) CU_TRY(cudaEventRecord(c.ev[3], c.st));
+  return IRLCU_OK;
+}
+
+static int need_prjscat_buffer(Ctx &c) {
+  if (c.prjscat) return IRLCU_OK;
+  float *p;
+  size_t cap;
+  return buf_ptr(IRLCU_BUF_PRJSCAT, 0, &p, &cap, true);
+}
+
 int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp, int model, int bck_model, int subset,
                       int use_scatest, int apply_update, int accumulate_from_update) {
   TRY(need_ctx());
@@ -529,43 +646,119 @@ int irlcu_osem_subset(int nv, const int *views, const irlcu_view_parm *vp, int m
     need_nosrf |= vp[i].scat_mode == 2;
     need_prjscat |= vp[i].scat_mode != 0;
   }
-  if (need_prjscat && !c.prjscat) {
-    float *p;
-    size_t cap;
-    TRY(buf_ptr(IRLCU_BUF_PRJSCAT, 0, &p, &cap, true));
-  }
+  if (need_prjscat) TRY(need_prjscat_buffer(c));
   TRY(upload_views(views, nv, vp));
-  float *calc = c.wprj;
-  float *calc_nosrf = c.wprj2;
-  float *ratio = c.wprj2 + c.pln * c.g.max_batch;
-  CU_TRY(cudaEventRecord(c.ev[0], c.st));
-  TRY(forward_batch(nv, views, model, 1.0f, calc, need_nosrf ? calc_nosrf : nullptr));
-  CU_TRY(cudaEventRecord(c.ev[1], c.st));
-  {
-    Stage s(IRLCU_ST_REDUCE, c.st);
-    s.bytes = 16.0 * (double)c.pln * nv;
-    TRY(launch_ratio(c, calc, calc_nosrf, c.dviews, c.dvp, nv, use_scatest, ratio));
+  return osem_subset_body(nv, views, need_nosrf, model, bck_model, subset, use_scatest, apply_update,
+                          accumulate_from_update);
+}
+
+int irlcu_set_subsets(int nsub, int per, const int *views, const irlcu_view_parm *vp) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (nsub <= 0 || per <= 0 || nsub > c.nsub) return set_error(IRLCU_EARG, "bad subsets %d x %d", nsub, per);
+  const size_t tot = (size_t)nsub * per;
+  for (size_t i = 0; i < tot; ++i)
+    if (views[i] < 0 || views[i] >= c.nv) return set_error(IRLCU_EARG, "view index %d out of range", views[i]);
+  graphs_clear(c);
+  dfree(c.dviews_all);
+  dfree(c.dvp_all);
+  TRY(dalloc(&c.dviews_all, tot));
+  TRY(dalloc(&c.dvp_all, tot));
+  c.h_views_all.assign(views, views + tot);
+  c.h_vp_all.assign(vp, vp + tot);
+  for (auto &q : c.h_vp_all) q.scat_mode = 0;
+  c.vp_scat_mode = 0;
+  CU_TRY(cudaMemcpy(c.dviews_all, views, tot * sizeof(int), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c.dvp_all, c.h_vp_all.data(), tot * sizeof(irlcu_view_parm), cudaMemcpyHostToDevice));
+  c.nsub_all = nsub;
+  c.per_all = per;
+  return IRLCU_OK;
+}
+
+// every subset of one iteration, in batches of max_batch views
+static int run_subsets(Ctx &c, int model, int bck_model, int use_scatest, int scat_mode) {
+  int *dv0 = c.dviews;
+  irlcu_view_parm *dp0 = c.dvp;
+  int rc = IRLCU_OK;
+  const int per = c.per_all, B = c.g.max_batch;
+  for (int s = 0; s < c.nsub_all && !rc; ++s)
+    for (int m0 = 0; m0 < per && !rc; m0 += B) {
+      const int nb = std::min(B, per - m0);
+      const size_t off = (size_t)s * per + m0;
+      c.dviews = c.dviews_all + off;
+      c.dvp = c.dvp_all + off;
+      rc = osem_subset_body(nb, c.h_views_all.data() + off, scat_mode == 2, model, bck_model, s, use_scatest,
+                            m0 + nb >= per, m0 > 0);
+    }
+  c.dviews = dv0;
+  c.dvp = dp0;
+  return rc;
+}
+
+int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mode) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (!c.dviews_all) return set_error(IRLCU_ESTATE, "irlcu_set_subsets has not been called");
+  if (use_scatest && !c.scatest) return set_error(IRLCU_ESTATE, "scatter estimate not uploaded");
+  if (scat_mode < 0 || scat_mode > 2) return set_error(IRLCU_EARG, "bad scatter mode %d", scat_mode);
+  if (scat_mode != 0) TRY(need_prjscat_buffer(c));
+  if (scat_mode != c.vp_scat_mode) {  // ordered on the stream before this iteration's kernels
+    for (auto &q : c.h_vp_all) q.scat_mode = scat_mode;
+    CU_TRY(cudaMemcpyAsync(c.dvp_all, c.h_vp_all.data(), c.h_vp_all.size() * sizeof(irlcu_view_parm),
+                           cudaMemcpyHostToDevice, c.st));
+    c.vp_scat_mode = scat_mode;
   }
-  const float *E = (bck_model & MODEL_ATN_BIT) ? c.tE : nullptr;
-  const DrfDev *drf = nullptr;
-  if (bck_model & MODEL_DRF_BIT) drf = c.drf[1].psf ? &c.drf[1] : &c.drf[0];
-  {
-    Stage s(IRLCU_ST_BACKPROJECT, c.st);
-    s.flops = drf_flops(c, drf, views, nv, false);
-    s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;  // attenuation factor read, plane written
-    TRY(launch_backproject(c, ratio, c.dviews, nv, E, drf, 1.0f, c.wbck));
+  // stage profiling needs the eager launches (events around every stage)
+  if (g_prof_on) return run_subsets(c, model, bck_model, use_scatest, scat_mode);
+  const int key = (model & 15) | (bck_model & 15) << 4 | (use_scatest ? 1 : 0) << 8 | scat_mode << 9;
+  for (const GraphRec &g : c.graphs)
+    if (g.key == key) {
+      CU_TRY(cudaGraphLaunch(g.exec, c.st));
+      g_launch_count += g.kernels;
+      return IRLCU_OK;
+    }
+  const char *env = getenv("IRLCU_GRAPHS");
+  const bool graphs = !(env && !strcmp(env, "0"));
+  bool seen = false;
+  for (int k : c.graph_seen) seen |= k == key;
+  if (!graphs || !seen) {
+    if (!seen) c.graph_seen.push_back(key);
+    return run_subsets(c, model, bck_model, use_scatest, scat_mode);
   }
-  CU_TRY(cudaEventRecord(c.ev[2], c.st));
-  {
-    Stage s(IRLCU_ST_ACCUM, c.st);
-    // unrotation (read + write per view), accumulation read per view, and
-    // the update / estimate read-modify-write
-    s.bytes = 12.0 * (double)c.vox * nv + 16.0 * (double)c.vox;
-    TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nv, c.upd, accumulate_from_update,
-                                   apply_update ? ACC_EM : 0, c.est,
-                                   apply_update ? c.norm + (size_t)subset * c.vox : nullptr));
+  // capture the iteration once, then replay it
+  CU_TRY(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+  const long long l0 = g_launch_count;
+  c.capturing = true;
+  const int rc = run_subsets(c, model, bck_model, use_scatest, scat_mode);
+  c.capturing = false;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(c.st, &graph);
+  const long long kernels = g_launch_count - l0;
+  g_launch_count = l0;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
   }
-  CU_TRY(cudaEventRecord(c.ev[3], c.st));
+  if (ce != cudaSuccess) return set_error(IRLCU_ECUDA, "iteration capture: %s", cudaGetErrorString(ce));
+  GraphRec g{key, nullptr, kernels};
+  const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return set_error(IRLCU_ECUDA, "iteration graph: %s", cudaGetErrorString(ie));
+  c.graphs.push_back(g);
+  CU_TRY(cudaGraphLaunch(g.exec, c.st));
+  g_launch_count += g.kernels;
+  return IRLCU_OK;
+}
+
+void *irlcu_ctx_detach(void) {
+  Ctx *c = g_ctx;
+  g_ctx = nullptr;
+  return c;
+}
+
+int irlcu_ctx_attach(void *ctx) {
+  if (g_ctx && g_ctx != ctx) return set_error(IRLCU_ESTATE, "another context is current; detach it first");
+  g_ctx = static_cast<Ctx *>(ctx);
   return IRLCU_OK;
 }
 
@@ -661,6 +854,12 @@ int irlcu_grids(int out[5]) {
   out[2] = c.esse.on ? c.esse.kx : 0;
   out[3] = c.esse.on ? c.esse.ky : 0;
   out[4] = c.esse.on ? c.esse.kz : 0;
+  return IRLCU_OK;
+}
+
+int irlcu_drf_tuning(float ms[2]) {
+  ms[0] = g_tune_ms[0];
+  ms[1] = g_tune_ms[1];
   return IRLCU_OK;
 }
 

@@ -59,6 +59,33 @@ struct EsseDev {
   bool fused = false;         // y-z transforms in one shared-memory kernel
 };
 
+// ESSE work buffers of one context (k_esse.cu)
+struct EsseWork {
+  float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;
+  float2 *A = nullptr, *Bf = nullptr, *C2[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
+  float *g[2] = {nullptr, nullptr};
+  float *T[2] = {nullptr, nullptr};
+  int batch = 0;
+  int nxv = 0, nyv = 0, nzv = 0;
+};
+
+// Fourier-domain DRF work buffers of one context, sized for the largest
+// table (k_drf_fft.cu)
+struct DfftWork {
+  float2 *S = nullptr;     // row spectra of a batch of planes
+  size_t s_elems = 0;
+  float2 *part = nullptr;  // forward partial sums
+  size_t part_elems = 0;
+  float2 *Y = nullptr;     // forward column results
+  size_t y_elems = 0;
+};
+
+struct GraphRec {
+  int key;                  // model bits, scatter estimate, scatter mode
+  cudaGraphExec_t exec;
+  long long kernels;        // kernel launches in the graph
+};
+
 struct Ctx {
   irlcu_geom g{};
   int n = 0, nz = 0, nv = 0;
@@ -98,6 +125,22 @@ struct Ctx {
   float *wfft = nullptr;    // ESSE work: B * spectra
   size_t wfft_elems = 0;
   float *weff = nullptr;    // ESSE expanded terms, B volumes x2
+  EsseWork ew;
+  DfftWork dw;
+
+  // every subset's views and per-view parameters (irlcu_set_subsets) and
+  // the CUDA graphs of whole iterations (irlcu_osem_iteration)
+  int *dviews_all = nullptr;
+  irlcu_view_parm *dvp_all = nullptr;
+  std::vector<int> h_views_all;
+  std::vector<irlcu_view_parm> h_vp_all;
+  int nsub_all = 0, per_all = 0, vp_scat_mode = 0;
+  std::vector<GraphRec> graphs;
+  std::vector<int> graph_seen;   // keys run eagerly once
+  bool capturing = false;
+  // three-shear intermediate for slices beyond shared memory, grown on use
+  mutable float *xscratch = nullptr;
+  mutable size_t xscratch_elems = 0;
 };
 
 extern Ctx *g_ctx;
@@ -146,7 +189,7 @@ int launch_backproject(const Ctx &c, const float *planes, const int *dviews, int
 // Fourier-domain DRF engine (k_drf_fft.cu); max_pad: the largest axial pad
 int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad);
 void drf_fft_free(DrfDev &D);
-void drf_fft_work_free();
+void drf_fft_work_free(Ctx &c);
 int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
                        float scale, float *out);
 int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,

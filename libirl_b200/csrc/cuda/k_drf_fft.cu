@@ -386,16 +386,7 @@ static int set_col_attrs() {
   return IRLCU_OK;
 }
 
-// work buffers shared by both tables, sized for the largest request
-struct DfftWork {
-  float2 *S = nullptr;     // row spectra of a batch of planes
-  size_t s_elems = 0;
-  float2 *part = nullptr;  // forward partial sums
-  size_t part_elems = 0;
-  float2 *Y = nullptr;     // forward column results
-  size_t y_elems = 0;
-};
-static DfftWork g_dw;
+
 
 static int grow(float2 **p, size_t *have, size_t need) {
   if (need <= *have) return IRLCU_OK;
@@ -414,11 +405,11 @@ void drf_fft_free(DrfDev &D) {
   D.fft = DrfFft{};
 }
 
-void drf_fft_work_free() {
-  if (g_dw.S) cudaFree(g_dw.S);
-  if (g_dw.part) cudaFree(g_dw.part);
-  if (g_dw.Y) cudaFree(g_dw.Y);
-  g_dw = DfftWork{};
+void drf_fft_work_free(Ctx &c) {
+  if (c.dw.S) cudaFree(c.dw.S);
+  if (c.dw.part) cudaFree(c.dw.part);
+  if (c.dw.Y) cudaFree(c.dw.Y);
+  c.dw = DfftWork{};
 }
 
 // plane groups of the forward column pass
@@ -443,9 +434,9 @@ int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
   CU_TRY(cudaMalloc(&F.H, sizeof(float2) * (size_t)nspec * Mz * F.Mxh));
   // work: row spectra for max_batch views (also holds the PSF rows here)
   const int B = c.g.max_batch;
-  TRY_RC(grow(&g_dw.S, &g_dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
-  TRY_RC(grow(&g_dw.part, &g_dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
-  TRY_RC(grow(&g_dw.Y, &g_dw.y_elems, (size_t)B * nz * F.Mxh));
+  TRY_RC(grow(&c.dw.S, &c.dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
+  TRY_RC(grow(&c.dw.part, &c.dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
+  TRY_RC(grow(&c.dw.Y, &c.dw.y_elems, (size_t)B * nz * F.Mxh));
   // spectra of the quadrant-swapped PSFs (and the identity), 1/(Mz Mx)
   RowSrc r{};
   r.mode = MODE_PSF;
@@ -457,7 +448,7 @@ int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
   r.nz = nz;
   r.G = Mz;
   r.Mz = Mz;
-  r.out = g_dw.S;
+  r.out = c.dw.S;
   r.Mxh = F.Mxh;
   r.nplanes = nspec;
   DFFT_DISPATCH(Mx, {
@@ -466,7 +457,7 @@ int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
     CU_LAUNCHED();
   });
   ColArgsD ca{};
-  ca.in = g_dw.S;
+  ca.in = c.dw.S;
   ca.out = F.H;
   ca.nplanes = nspec;
   ca.G = Mz;
@@ -500,7 +491,7 @@ static RowSrc plane_rows(const Ctx &c, const DrfDev &D, const float *a, size_t a
   r.P = D.fft.P;
   r.G = D.fft.G;
   r.Mz = D.fft.Mz;
-  r.out = g_dw.S;
+  r.out = c.dw.S;
   r.Mxh = D.fft.Mxh;
   r.nplanes = c.n;
   return r;
@@ -508,7 +499,7 @@ static RowSrc plane_rows(const Ctx &c, const DrfDev &D, const float *a, size_t a
 
 static ColArgsD col_args(const Ctx &c, const DrfDev &D, const int *dviews, int nv) {
   ColArgsD a{};
-  a.in = g_dw.S;
+  a.in = c.dw.S;
   a.H = D.fft.H;
   a.views = dviews;
   a.row_idist = D.row_idist;
@@ -518,7 +509,7 @@ static ColArgsD col_args(const Ctx &c, const DrfDev &D, const int *dviews, int n
   a.P = D.fft.P;
   a.nz = c.nz;
   a.Mxh = D.fft.Mxh;
-  a.part = g_dw.part;
+  a.part = c.dw.part;
   a.npg = fwd_groups(c.n);
   a.nb = nv;
   return a;
@@ -527,8 +518,8 @@ static ColArgsD col_args(const Ctx &c, const DrfDev &D, const int *dviews, int n
 int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
                        float scale, float *out) {
   const DrfFft &F = D.fft;
-  if ((size_t)nv * c.n * F.G * F.Mxh > g_dw.s_elems || (size_t)nv * c.nz * F.Mxh > g_dw.y_elems ||
-      (size_t)fwd_groups(c.n) * nv * F.Mz * F.Mxh > g_dw.part_elems)
+  if ((size_t)nv * c.n * F.G * F.Mxh > c.dw.s_elems || (size_t)nv * c.nz * F.Mxh > c.dw.y_elems ||
+      (size_t)fwd_groups(c.n) * nv * F.Mz * F.Mxh > c.dw.part_elems)
     return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
   const RowSrc r = plane_rows(c, D, src, c.vox, c.pln, E, dviews);
   DFFT_DISPATCH(F.Mx, {
@@ -537,7 +528,7 @@ int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv
     CU_LAUNCHED();
   });
   ColArgsD a = col_args(c, D, dviews, nv);
-  a.out = g_dw.Y;
+  a.out = c.dw.Y;
   DFFT_DISPATCH(F.Mz, {
     TRY_RC(set_col_attrs<LL>());
     const int nch = (F.Mxh + col_chunk<LL>() - 1) / col_chunk<LL>();
@@ -547,7 +538,7 @@ int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv
     CU_LAUNCHED();
   });
   RowInv ri{};
-  ri.in = g_dw.Y;
+  ri.in = c.dw.Y;
   ri.np = 1;
   ri.rs = c.nz;
   ri.r0 = 0;
@@ -567,7 +558,7 @@ int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv
 int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,
                            const DrfDev &D, float scale, float *bck) {
   const DrfFft &F = D.fft;
-  if ((size_t)nv * c.n * F.G * F.Mxh > g_dw.s_elems)
+  if ((size_t)nv * c.n * F.G * F.Mxh > c.dw.s_elems)
     return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
   const RowSrc r = plane_rows(c, D, planes, c.pln, 0, E, dviews);
   DFFT_DISPATCH(F.Mx, {
@@ -576,7 +567,7 @@ int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews,
     CU_LAUNCHED();
   });
   ColArgsD a = col_args(c, D, dviews, nv);
-  a.out = g_dw.S;
+  a.out = c.dw.S;
   DFFT_DISPATCH(F.Mz, {
     TRY_RC(set_col_attrs<LL>());
     const int nch = (F.Mxh + col_chunk<LL>() - 1) / col_chunk<LL>();
@@ -584,7 +575,7 @@ int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews,
     CU_LAUNCHED();
   });
   RowInv ri{};
-  ri.in = g_dw.S;
+  ri.in = c.dw.S;
   ri.np = c.n;
   ri.rs = F.G;
   ri.r0 = F.P;

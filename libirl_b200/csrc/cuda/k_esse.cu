@@ -584,15 +584,7 @@ __global__ void k_scale_copy(const float *__restrict__ in, float *__restrict__ o
 
 // -------------------------------------------------------------- host side
 
-struct EsseWork {
-  float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;
-  float2 *A = nullptr, *Bf = nullptr, *C2[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
-  float *g[2] = {nullptr, nullptr};
-  float *T[2] = {nullptr, nullptr};
-  int batch = 0;
-  int nxv = 0, nyv = 0, nzv = 0;
-};
-static EsseWork g_ew;
+
 
 static bool pow2_ok(int v) { return v >= 8 && v <= 1024 && (v & (v - 1)) == 0; }
 
@@ -664,7 +656,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   ra.kxh = kxh;
   {
     dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nb);
-    LDISPATCH(E.kx, k_fft_row_fwd, grid_, 256, 0, st, ra, g_ew.twx);
+    LDISPATCH(E.kx, k_fft_row_fwd, grid_, 256, 0, st, ra, g_ctx->ew.twx);
     CU_LAUNCHED();
   }
   // z lines (outer = y' < nyv) -> tmpB [nb][nyv][Kz][kxh]
@@ -684,7 +676,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   za.s = 1.f;
   {
     dim3 grid_((kxh + CW - 1) / CW, nyv, nb);
-    LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), st, za, g_ew.twz);
+    LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), st, za, g_ctx->ew.twz);
     CU_LAUNCHED();
   }
   // y lines (outer = z < Kz) -> out [nb][Ky][Kz][kxh]
@@ -704,7 +696,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   ya.s = 1.f;
   {
     dim3 grid_((kxh + CW - 1) / CW, E.kz, nb);
-    LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), st, ya, g_ew.twy);
+    LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), st, ya, g_ctx->ew.twy);
     CU_LAUNCHED();
   }
   return IRLCU_OK;
@@ -718,7 +710,7 @@ void esse_free(Ctx &c) {
   c.esse.on = false;
   c.esse.zero = false;
   c.esse.fused = false;
-  EsseWork &w = g_ew;
+  EsseWork &w = c.ew;
   cudaFree(w.twx);
   cudaFree(w.twy);
   cudaFree(w.twz);
@@ -730,7 +722,7 @@ void esse_free(Ctx &c) {
     cudaFree(w.g[t]);
     cudaFree(w.T[t]);
   }
-  g_ew = EsseWork{};
+  c.ew = EsseWork{};
 }
 
 int esse_setup(Ctx &c, const irlcu_esse *e) {
@@ -756,7 +748,7 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
   E.mu_avg = e->mu_avg;
   E.pix = e->pix;
   E.cntr = e->cntr_pix_fac;
-  EsseWork &w = g_ew;
+  EsseWork &w = c.ew;
   w.nxv = c.n / E.collapse;
   w.nyv = c.n / E.collapse;
   w.nzv = c.nz / E.collapse;
@@ -831,7 +823,7 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
 
 int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src) {
   EsseDev &E = c.esse;
-  EsseWork &w = g_ew;
+  EsseWork &w = c.ew;
   if (!E.on) {
     // libirl returns a zero effective source when the kernel's scatter
     // factor is 0 (krnlprj3d.c:714-722): src = act * primary
@@ -972,7 +964,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
 // expansion + smoothing (y, z), then x smoothing fused with the combine
 static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src) {
   EsseDev &E = c.esse;
-  EsseWork &w = g_ew;
+  EsseWork &w = c.ew;
   const int nyv = w.nyv, nzv = w.nzv, nxv = w.nxv;
   const int cf = E.collapse;
   if (cf == 1) {

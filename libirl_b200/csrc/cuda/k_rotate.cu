@@ -349,8 +349,6 @@ __global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, flo
   }
 }
 
-static float *g_xscratch = nullptr;
-static size_t g_xscratch_elems = 0;
 
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
                   const int *dviews, int nv, int rot_base) {
@@ -381,26 +379,26 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
     return IRLCU_OK;
   }
   const size_t need = (size_t)nv * nz * n * xld;
-  if (need > g_xscratch_elems) {
-    if (g_xscratch) cudaFree(g_xscratch);
-    g_xscratch = nullptr;
-    g_xscratch_elems = 0;
-    CU_TRY(cudaMalloc(&g_xscratch, need * sizeof(float)));
-    g_xscratch_elems = need;
+  if (need > c.xscratch_elems) {
+    if (c.xscratch) cudaFree(c.xscratch);
+    c.xscratch = nullptr;
+    c.xscratch_elems = 0;
+    CU_TRY(cudaMalloc(&c.xscratch, need * sizeof(float)));
+    c.xscratch_elems = need;
   }
-  k_shear_pass1_glob<<<grid, 512, 0, c.st>>>(src, src_stride, g_xscratch, dviews, rot_base, c.rot,
+  k_shear_pass1_glob<<<grid, 512, 0, c.st>>>(src, src_stride, c.xscratch, dviews, rot_base, c.rot,
                                              c.sup_start, c.sup_end, n, nz, xld);
   CU_LAUNCHED();
-  k_shear_pass23_glob<<<grid, 512, 0, c.st>>>(g_xscratch, dst, dst_stride, dviews, rot_base, c.rot,
+  k_shear_pass23_glob<<<grid, 512, 0, c.st>>>(c.xscratch, dst, dst_stride, dviews, rot_base, c.rot,
                                               c.sup_start, c.sup_end, n, nz, xld);
   CU_LAUNCHED();
   return IRLCU_OK;
 }
 
-void free_rotate_scratch() {
-  if (g_xscratch) cudaFree(g_xscratch);
-  g_xscratch = nullptr;
-  g_xscratch_elems = 0;
+void free_rotate_scratch(Ctx &c) {
+  if (c.xscratch) cudaFree(c.xscratch);
+  c.xscratch = nullptr;
+  c.xscratch_elems = 0;
 }
 
 // ---------------------------------------------------------- accumulation

@@ -62,6 +62,17 @@ irl_view *irl_setup_views(IrlParms_t *ip, PrjView_t *pv);
 int irl_setup_drf_tables(irl_parms *p, Options_t *op, irl_view *views, char *drf_fname,
 	irl_detector **pdets);
 void irl_free_run_tables(void);
+
+/* the per-call run tables (detectors, extra view data) of one
+   reconstruction, parked while another one is current */
+typedef struct {
+	void **dets;
+	int ndet, extra_nviews;
+	float *acq_times;
+	int *det_nums;
+} irl_run_tables;
+void irl_run_tables_park(irl_run_tables *t);
+void irl_run_tables_unpark(const irl_run_tables *t);
 DrfTab_t *irl_free_drftab(DrfTab_t *t);
 void irl_esse_prepare(const char *krnl_fname, const irl_parms *p, int collapse, irl_esse_host *e);
 void irl_esse_free(irl_esse_host *e);

@@ -351,6 +351,18 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 	S.cb = cb;
 	irl_msg(5, "Done Initialization (%.3f s)\n", now_s() - t0);
 	compute_norms();
+	{
+		/* every subset's views on the device, for whole-iteration launches */
+		const int tot = S.ns * S.per;
+		irlcu_view_parm *all = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * tot, "subset views");
+		int i;
+		for (i = 0; i < tot; ++i) {
+			all[i].view_time = S.views[S.ang[i]].view_time;
+			all[i].sensitivity = S.views[S.ang[i]].sensitivity;
+		}
+		irl_cu(irlcu_set_subsets(S.ns, S.per, S.ang, all), "OsemRecon");
+		free(all);
+	}
 	for (m = 0; m < 6; ++m)
 		if (g_irl_hooks[m] != NULL && S.norm_host == NULL) {
 			S.norm_host = (float *)irl_calloc(sizeof(float) * S.vox, "norm mirror");
@@ -373,7 +385,7 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 static void one_iteration(void)
 {
 	irl_parms *p = &S.p;
-	int it = S.it + 1, s, m, model = p->prj_model, mode = 0;
+	int it = S.it + 1, s = 0, m, model = p->prj_model, mode = 0;
 	int angle_hooks = g_irl_hooks[HOOK_PREV_ANGLE] || g_irl_hooks[HOOK_POST_ANGLE];
 	double ti = now_s();
 	S.hd.iIterationIdx = it;
@@ -384,7 +396,14 @@ static void one_iteration(void)
 		model = S.this_srf ? p->prj_model : (p->prj_model & ~MODEL_SRF);
 		mode = !S.this_srf ? 1 : (!S.next_srf ? 2 : 0);
 	}
-	for (s = 0; s < S.ns; ++s) {
+	if (!angle_hooks && !g_irl_hooks[HOOK_PREV_SUBSET] && !g_irl_hooks[HOOK_POST_SUBSET]) {
+		/* no host work between subsets: the whole iteration in one call
+		   (replayed from a CUDA graph after its first runs) */
+		irl_cu(irlcu_osem_iteration(model, p->bck_model, S.use_scatest, mode), "OsemRecon");
+		S.hook_norm = S.ns - 1;
+		s = S.ns;
+	}
+	for (s = s == S.ns ? S.ns : 0; s < S.ns; ++s) {
 		const int *va = S.ang + s * S.per;
 		S.hd.iSubsetIdx = s;
 		hook_call(HOOK_PREV_SUBSET);
@@ -468,6 +487,100 @@ int IrlOsemEnd(float *recon)
 	irl_untrap();
 	session_close();
 	return 0;
+}
+
+/* ----------------------------------------------------------------- batch */
+
+/* a reconstruction set aside while another one is current: its host
+   session, its device context and its per-call run tables */
+typedef struct {
+	osem_session s;
+	void *dev;
+	irl_run_tables run;
+} parked_session;
+
+static parked_session *session_park(void)
+{
+	parked_session *h = (parked_session *)irl_malloc(sizeof(parked_session), "batch session");
+	h->s = S;
+	memset(&S, 0, sizeof(S));
+	h->dev = irlcu_ctx_detach();
+	irl_run_tables_park(&h->run);
+	return h;
+}
+
+static void session_unpark(parked_session *h)
+{
+	S = h->s;
+	(void)irlcu_ctx_attach(h->dev);  /* every other context is parked */
+	irl_run_tables_unpark(&h->run);
+	free(h);
+}
+
+int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
+{
+	jmp_buf env;
+	parked_session **h = NULL;
+	int p, m, err = 0, left;
+	if ((err = setjmp(env)) != 0) {
+		irl_untrap();
+		return err;
+	}
+	irl_trap(&env);
+	if (nprob <= 0 || pp == NULL)
+		irl_fatal(IRL_E_VALUE, "IrlOsemBatch", "no problems given");
+	for (m = 0; m < 6; ++m)
+		if (g_irl_hooks[m] != NULL)
+			irl_fatal(IRL_E_VALUE, "IrlOsemBatch", "hooks are not supported in a batch");
+	if (g_irl_extra_nviews > 0 || g_irl_dets != NULL || g_irl_acq_times != NULL || g_irl_det_nums != NULL)
+		irl_fatal(IRL_E_VALUE, "IrlOsemBatch",
+			"per-call view or detector data (iSetupExtraPrjViewData / iSetupDetectors) is pending");
+	if (S.open)
+		irl_fatal(IRL_E_VALUE, "IrlOsemBatch", "an IrlOsemBegin session is open");
+	h = (parked_session **)irl_calloc(sizeof(parked_session *) * nprob, "batch sessions");
+	irl_untrap();
+	for (p = 0; p < nprob && !err; ++p) {
+		IrlOsemProblem_t *q = pp + p;
+		q->iStatus = IrlOsemBegin(q->psIrlParms, q->psOptions, q->psViews, q->pchDrfTabFname,
+			q->pchScatKrnlFname, NULL, q->pfScatterEstimate, q->pfAtnMap, q->pfPrjImage, q->pfReconImage,
+			NULL, NULL);
+		if (q->iStatus)
+			err = q->iStatus;
+		else
+			h[p] = session_park();
+	}
+	/* iterations round-robin: each call only enqueues device work */
+	do {
+		left = 0;
+		for (p = 0; p < nprob && !err; ++p) {
+			if (h[p] == NULL)
+				continue;
+			session_unpark(h[p]);
+			h[p] = NULL;
+			if (S.it < S.p.iterations) {
+				const int e = IrlOsemIterate(1);
+				if (e) {  /* IrlOsemIterate closed the session */
+					pp[p].iStatus = err = e;
+					continue;
+				}
+			}
+			left |= S.it < S.p.iterations;
+			h[p] = session_park();
+		}
+	} while (left && !err);
+	for (p = 0; p < nprob; ++p) {
+		int e;
+		if (h[p] == NULL)
+			continue;
+		session_unpark(h[p]);
+		e = IrlOsemEnd(err ? NULL : pp[p].pfReconImage);
+		if (!pp[p].iStatus)
+			pp[p].iStatus = e;
+		if (!err)
+			err = e;
+	}
+	free(h);
+	return err;
 }
 
 int IrlOsem(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,

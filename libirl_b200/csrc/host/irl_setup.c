@@ -119,6 +119,29 @@ void irl_free_run_tables(void)
 	g_irl_ndet = 0;
 }
 
+void irl_run_tables_park(irl_run_tables *t)
+{
+	t->dets = g_irl_dets;
+	t->ndet = g_irl_ndet;
+	t->extra_nviews = g_irl_extra_nviews;
+	t->acq_times = g_irl_acq_times;
+	t->det_nums = g_irl_det_nums;
+	g_irl_dets = NULL;
+	g_irl_ndet = 0;
+	g_irl_extra_nviews = 0;
+	g_irl_acq_times = NULL;
+	g_irl_det_nums = NULL;
+}
+
+void irl_run_tables_unpark(const irl_run_tables *t)
+{
+	g_irl_dets = t->dets;
+	g_irl_ndet = t->ndet;
+	g_irl_extra_nviews = t->extra_nviews;
+	g_irl_acq_times = t->acq_times;
+	g_irl_det_nums = t->det_nums;
+}
+
 /* ------------------------------------------------------------ parameters */
 
 /* vSetupParms, IrlSetup.c:51-91 */
