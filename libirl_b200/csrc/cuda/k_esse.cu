@@ -586,7 +586,6 @@ __global__ void k_scale_copy(const float *__restrict__ in, float *__restrict__ o
 
 
 
-static bool pow2_ok(int v) { return v >= 8 && v <= 1024 && (v & (v - 1)) == 0; }
 
 int upload_twiddle_table(float2 **d, int L) {
   std::vector<float2> h(L);
@@ -601,18 +600,47 @@ int upload_twiddle_table(float2 **d, int L) {
 
 static int upload_twiddles(float2 **d, int L) { return upload_twiddle_table(d, L); }
 
-#define LDISPATCH(L, KERNEL, GRID, BLOCK, SMEM, ST, ...)                         \
-  switch (L) {                                                                   \
-    case 8: KERNEL<8><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;            \
-    case 16: KERNEL<16><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;          \
-    case 32: KERNEL<32><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;          \
-    case 64: KERNEL<64><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;          \
-    case 128: KERNEL<128><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;        \
-    case 256: KERNEL<256><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;        \
-    case 512: KERNEL<512><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;        \
-    case 1024: KERNEL<1024><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;      \
-    default: return set_error(IRLCU_EARG, "FFT length %d not supported", L);    \
+// ESSE grid sides with instantiated kernels: products of 2, 3, 5, 7 that
+// ceil(2 N / c) takes for the usual volume sizes and collapse factors
+#define ESSE_LENS(X) X(8) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(112) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(512) X(1024)
+
+#define LDISPATCH(L, KERNEL, GRID, BLOCK, SMEM, ST, ...)                        \
+  switch (L) {                                                                  \
+    LCASES(KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__)                           \
+    default: return set_error(IRLCU_EARG, "FFT length %d not supported", L);   \
   }
+#define LCASE_1(L, KERNEL, GRID, BLOCK, SMEM, ST, ...) \
+  case L: KERNEL<L><<<GRID, BLOCK, SMEM, ST>>>(__VA_ARGS__); break;
+#define LCASES(KERNEL, GRID, BLOCK, SMEM, ST, ...) \
+  LCASE_1(8, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(16, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(24, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(32, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(40, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(48, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(64, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(80, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(96, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(112, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(128, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(160, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(192, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(224, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(256, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(320, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(384, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(512, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__) \
+  LCASE_1(1024, KERNEL, GRID, BLOCK, SMEM, ST, __VA_ARGS__)
+
+static bool esse_len_ok(int L) {
+  switch (L) {
+#define LOK(L) case L:
+    ESSE_LENS(LOK)
+#undef LOK
+    return true;
+    default: return false;
+  }
+}
 
 static int row_wr(int L) { return (L <= 128) ? 16 : (L <= 256 ? 4 : 2); }  // row_lines<L>()
 
@@ -621,14 +649,12 @@ static int col_smem(int L) { return (int)(sizeof(float2) * (L + 2 * CW * L)); }
 static int set_col_attr(int L) {
   const int sm = col_smem(L);
   switch (L) {
-    case 8: CU_TRY(cudaFuncSetAttribute(k_fft_col<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 16: CU_TRY(cudaFuncSetAttribute(k_fft_col<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 32: CU_TRY(cudaFuncSetAttribute(k_fft_col<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 64: CU_TRY(cudaFuncSetAttribute(k_fft_col<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 128: CU_TRY(cudaFuncSetAttribute(k_fft_col<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 256: CU_TRY(cudaFuncSetAttribute(k_fft_col<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 512: CU_TRY(cudaFuncSetAttribute(k_fft_col<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
-    case 1024: CU_TRY(cudaFuncSetAttribute(k_fft_col<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); break;
+#define LATTR(L)                                                                                  \
+  case L:                                                                                         \
+    CU_TRY(cudaFuncSetAttribute(k_fft_col<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)); \
+    break;
+    ESSE_LENS(LATTR)
+#undef LATTR
     default: return set_error(IRLCU_EARG, "FFT length %d not supported", L);
   }
   return IRLCU_OK;
@@ -732,9 +758,10 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     return IRLCU_OK;
   }
   EsseDev &E = c.esse;
-  if (!pow2_ok(e->kx) || !pow2_ok(e->ky) || !pow2_ok(e->kz) || e->ky > 512 || e->kz > 512)
+  if (!esse_len_ok(e->kx) || !esse_len_ok(e->ky) || !esse_len_ok(e->kz) || e->ky > 512 || e->kz > 512)
     return set_error(IRLCU_EARG,
-                     "ESSE FFT grid %d x %d x %d: sides must be powers of two, 8..1024 along x and 8..512 along y, z",
+                     "ESSE FFT grid %d x %d x %d: sides must be one of 8..1024 with factors 2, 3, 5, 7 "
+                     "(instantiated lengths) and at most 512 along y, z",
                      e->kx, e->ky, e->kz);
   if (e->nterms < 1 || e->nterms > 2)
     return set_error(IRLCU_EARG, "ESSE with %d Taylor terms is not supported (1 or 2)", e->nterms);

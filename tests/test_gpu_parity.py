@@ -146,6 +146,18 @@ def test_drf_half_width_beyond_direct_limit(product, orc, tmp_path, monkeypatch)
         assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (vi, rel_l2(got[vi], want[vi]))
 
 
+@pytest.mark.parametrize("n,collapse", [(40, 2), (48, 2), (24, 1)])
+def test_genprj_esse_mixed_radix_grid(product, orc, tmp_path, n, collapse):
+    """ESSE grids of ceil(2 N / c) that are not powers of two (40 = 8*5,
+    48 = 16*3) run on the mixed-radix transforms."""
+    case = W.full128(seed=2170 + n, n=n, nviews=6, subsets=2, iterations=1, collapse=collapse, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    got = gpu_genprj(product, case, files)
+    want = orc.Problem(case).genprj()
+    for vi in range(case.nviews):
+        assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (n, collapse, vi, rel_l2(got[vi], want[vi]))
+
+
 def test_genprj_golden_fixture(product, tmp_path):
     """The GPU path against the reference's own outputs."""
     for name in ("plain16", "srf16"):
