@@ -63,6 +63,20 @@ typedef struct {
    Returns 0, or the first non-zero iStatus. */
 int IrlOsemBatch(int nprob, IrlOsemProblem_t *psProblems);
 
+/* Learned scatter surrogate for the following IrlOsem / IrlOsemBegin /
+   IrlOsemBatch calls (128^3 volumes with the ESSE scatter model).
+   pchWeightsFname is a weights file written by the training in
+   libirl_b200/surrogate (NULL switches the surrogate off).  The first
+   scatter iteration runs ESSE on every view; then each view's NRMSE of the
+   surrogate against ESSE (||s - e|| / ||e|| of the scatter projection, on
+   the estimate at that point) is measured, views above fFallbackNrmse
+   (default 0.02) keep ESSE and the others use the network. */
+int IrlSetScatterSurrogate(const char *pchWeightsFname, float fFallbackNrmse);
+
+/* Those per-view NRMSEs of the open session (after its first scatter
+   iteration); returns 0 or an error code. */
+int IrlGetScatterSurrogateNrmse(float *pfNrmse, int iNumViews);
+
 #ifdef __cplusplus
 }
 #endif

@@ -193,6 +193,46 @@ int irlcu_stage_times(float *ms, int nmax);
    cudaStream_t), so callers can time or order work against it. */
 void *irlcu_stream(void);
 
+/* ---- learned scatter surrogate (no libirl counterpart) ----
+   A 3D-conv encoder / 2D decoder (1,653,153 parameters, BF16 weights and
+   activations, FP32 accumulation) that maps a view's rotated activity,
+   attenuation and depth, 4x4x4-pooled to 32^3 x 3 channels, to the view's
+   ESSE scatter projection, 128 x 128 (N = Nz = 128 only).  Input and target
+   are divided by the view's mean rotated activity.  Training and inference
+   run on hand-written kernels; the GPU ESSE path generates the targets and
+   stays the fallback. */
+typedef struct irlcu_sur irlcu_sur;
+/* network for batches of up to max_batch views, weights He-initialised from seed */
+int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **net);
+void irlcu_sur_destroy(irlcu_sur *net);
+size_t irlcu_sur_nparams(const irlcu_sur *net);
+/* FP32 parameter vector (per layer: weights [co][k] then bias [co]) */
+int irlcu_sur_get_weights(irlcu_sur *net, float *host, size_t n);
+int irlcu_sur_set_weights(irlcu_sur *net, const float *host, size_t n);
+/* x: device BF16 [B][32][32][32][3] (channels last); y, t: device FP32 [B][128*128] */
+int irlcu_sur_forward(irlcu_sur *net, int B, const void *x, float *y);
+/* mean squared error against t and its gradient (grad_host: nparams floats, or NULL) */
+int irlcu_sur_gradient(irlcu_sur *net, int B, const void *x, const float *t, float *loss, float *grad_host);
+/* one Adam step (beta 0.9 / 0.999) at learning rate lr; *loss before the step */
+int irlcu_sur_train_step(irlcu_sur *net, int B, const void *x, const float *t, float lr, float *loss);
+
+/* Training pairs of views[0..nv) from the current context's estimate (the
+   phantom): x_out the network inputs (device BF16 [nv][32][32][32][3]),
+   t_out the ESSE scatter projections divided by the view's activity mean
+   (device FP32 [nv][Nz*N]), scale_out those means (device FP32 [nv]).
+   model: projector bits with the scatter model (attenuation 1, DRF 2,
+   scatter 4). */
+int irlcu_sur_pairs(int nv, const int *views, int model, void *x_out, float *t_out, float *scale_out);
+
+/* Use net in place of the ESSE projector for every view whose flag is 0
+   (flags: nviews bytes, 1 = keep ESSE for that view, NULL = none);
+   net == NULL switches back to ESSE.  The network must outlive its use. */
+int irlcu_set_surrogate(irlcu_sur *net, const unsigned char *flags);
+
+/* Per-view NRMSE (||surrogate - ESSE|| / ||ESSE|| of the scatter
+   projection) of views[0..nv) on the current estimate, into nrmse[nv]. */
+int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *nrmse);
+
 /* Transform grids in use (0 where not set up): out[0..1] = Mz, Mx of the
    projector's Fourier-domain DRF engine (0, 0: direct convolution),
    out[2..4] = Kx, Ky, Kz of the ESSE grid. */

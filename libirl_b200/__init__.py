@@ -86,6 +86,33 @@ def _declare_irlcu(lib):
     lib.IrlOsemIterate.argtypes = [I]
     lib.IrlOsemEnd.restype = I
     lib.IrlOsemEnd.argtypes = [F]
+    V = C.c_void_p
+    lib.irlcu_sur_create.restype = I
+    lib.irlcu_sur_create.argtypes = [I, C.c_ulonglong, C.POINTER(V)]
+    lib.irlcu_sur_destroy.restype = None
+    lib.irlcu_sur_destroy.argtypes = [V]
+    lib.irlcu_sur_nparams.restype = S
+    lib.irlcu_sur_nparams.argtypes = [V]
+    lib.irlcu_sur_get_weights.restype = I
+    lib.irlcu_sur_get_weights.argtypes = [V, F, S]
+    lib.irlcu_sur_set_weights.restype = I
+    lib.irlcu_sur_set_weights.argtypes = [V, F, S]
+    lib.irlcu_sur_forward.restype = I
+    lib.irlcu_sur_forward.argtypes = [V, I, V, V]
+    lib.irlcu_sur_gradient.restype = I
+    lib.irlcu_sur_gradient.argtypes = [V, I, V, V, C.POINTER(C.c_float), F]
+    lib.irlcu_sur_train_step.restype = I
+    lib.irlcu_sur_train_step.argtypes = [V, I, V, V, C.c_float, C.POINTER(C.c_float)]
+    lib.irlcu_sur_pairs.restype = I
+    lib.irlcu_sur_pairs.argtypes = [I, C.POINTER(C.c_int), I, V, V, V]
+    lib.irlcu_set_surrogate.restype = I
+    lib.irlcu_set_surrogate.argtypes = [V, V]
+    lib.irlcu_sur_check.restype = I
+    lib.irlcu_sur_check.argtypes = [V, I, C.POINTER(C.c_int), I, F]
+    lib.IrlSetScatterSurrogate.restype = I
+    lib.IrlSetScatterSurrogate.argtypes = [C.c_char_p, C.c_float]
+    lib.IrlGetScatterSurrogateNrmse.restype = I
+    lib.IrlGetScatterSurrogateNrmse.argtypes = [F, I]
     lib.IrlOsemBatch.restype = I
     lib.IrlOsemBatch.argtypes = [I, C.POINTER(api.OsemProblem)]
     lib.irlcu_set_subsets.restype = I

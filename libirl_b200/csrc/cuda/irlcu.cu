@@ -128,6 +128,7 @@ static void free_ctx(Ctx *c) {
   if (!c) return;
   cudaStreamSynchronize(c->st);
   graphs_clear(*c);
+  dfree(c->sur_scale);
   dfree(c->dviews_all);
   dfree(c->dvp_all);
   dfree(c->rot.hdr);
@@ -543,6 +544,14 @@ int irlcu_prepare_attenuation(int need_srf) {
 }
 
 // rotated source of the batch in wrot (act) and, with SRF, act+scatter in src
+// any view of the batch kept on ESSE
+static bool sur_flagged(const Ctx &c, const int *hviews, int nv) {
+  if (c.sur_flags.empty()) return false;
+  for (int i = 0; i < nv; ++i)
+    if (c.sur_flags[hviews[i]]) return true;
+  return false;
+}
+
 static int forward_batch(int nv, const int *hviews, int model, float primary, float *out, float *out_nosrf) {
   Ctx &c = *g_ctx;
   {
@@ -554,6 +563,23 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
   const DrfDev *drf = (model & MODEL_DRF_BIT) ? &c.drf[0] : nullptr;
   const float *src = c.wrot;
   float scale = primary;
+  if ((model & MODEL_SRF_BIT) && c.sur && c.esse.on && !sur_flagged(c, hviews, nv)) {
+    // learned scatter: primary projection + the network's scatter projection
+    {
+      Stage s(IRLCU_ST_PROJECT, c.st);
+      s.flops = drf_flops(c, drf, hviews, nv, true);
+      s.bytes = (E ? 8.0 : 4.0) * (double)c.vox * nv;
+      TRY(launch_project(c, c.wrot, c.dviews, nv, E, drf, primary, out));
+    }
+    if (out_nosrf)
+      CU_TRY(cudaMemcpyAsync(out_nosrf, out, sizeof(float) * c.pln * nv, cudaMemcpyDeviceToDevice, c.st));
+    Stage s(IRLCU_ST_ESSE, c.st);
+    TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, c.sur_scale,
+                          sur_input(c.sur)));
+    const float *y = nullptr;
+    TRY(sur_infer(c.sur, c.st, nv, &y));
+    return launch_scale_views(c.st, y, c.sur_scale, out, (int)c.pln, nv, 1);
+  }
   if (model & MODEL_SRF_BIT) {
     if (!c.esse.on && !c.esse.zero) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
     if (!c.tS) return set_error(IRLCU_ESTATE, "scatter model needs the attenuation tables");
@@ -747,6 +773,104 @@ int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mod
   c.graphs.push_back(g);
   CU_TRY(cudaGraphLaunch(g.exec, c.st));
   g_launch_count += g.kernels;
+  return IRLCU_OK;
+}
+
+// ------------------------------------------------ learned scatter surrogate
+
+static int sur_geometry(const Ctx &c, irlcu_sur *net, int model) {
+  if (!net) return set_error(IRLCU_EARG, "surrogate: null network");
+  if (c.n != 128 || c.nz != 128)
+    return set_error(IRLCU_EARG, "surrogate: the network takes 128^3 volumes (here %d x %d)", c.n, c.nz);
+  if (!(model & MODEL_SRF_BIT) || !c.esse.on || !c.tS || !c.tMu)
+    return set_error(IRLCU_ESTATE, "surrogate: the scatter model (ESSE) must be set up");
+  return IRLCU_OK;
+}
+
+// ESSE scatter projections of a batch (views at c.dviews) into t; the
+// rotated activity stays in c.wrot
+static int esse_scatter(Ctx &c, int nv, const int *hviews, int model, float *t) {
+  irlcu_sur *keep = c.sur;
+  c.sur = nullptr;  // the targets come from ESSE
+  const int rc = forward_batch(nv, hviews, model, 1.0f, c.wprj, c.wprj2);
+  c.sur = keep;
+  TRY(rc);
+  return launch_sub(c.st, c.wprj, c.wprj2, t, c.pln * nv);
+}
+
+int irlcu_sur_pairs(int nv, const int *views, int model, void *x_out, float *t_out, float *scale_out) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (nv < 1 || nv > c.g.max_batch)
+    return set_error(IRLCU_EARG, "surrogate pairs: batch %d outside 1..%d", nv, c.g.max_batch);
+  if (c.n != 128 || c.nz != 128) return set_error(IRLCU_EARG, "surrogate pairs: 128^3 volumes only");
+  if (!(model & MODEL_SRF_BIT) || !c.esse.on || !c.tS || !c.tMu)
+    return set_error(IRLCU_ESTATE, "surrogate pairs: ESSE is not set up");
+  TRY(upload_views(views, nv, nullptr));
+  TRY(esse_scatter(c, nv, views, model, c.wprj));
+  TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, scale_out, x_out));
+  TRY(launch_div_views(c.st, c.wprj, scale_out, t_out, (int)c.pln, nv));
+  CU_TRY(cudaStreamSynchronize(c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *nrmse) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  TRY(sur_geometry(c, net, model));
+  const int B = std::min(sur_max_batch(net), c.g.max_batch);
+  float *scale = nullptr;
+  TRY(dalloc(&scale, (size_t)B));
+  std::vector<float> y(c.pln * B), t(c.pln * B);
+  int rc = IRLCU_OK;
+  for (int v0 = 0; v0 < nv && !rc; v0 += B) {
+    const int nb = std::min(B, nv - v0);
+    if ((rc = upload_views(views + v0, nb, nullptr))) break;
+    if ((rc = esse_scatter(c, nb, views + v0, model, c.wprj))) break;
+    if ((rc = launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nb, c.n, c.vox, scale, sur_input(net))))
+      break;
+    const float *yd = nullptr;
+    if ((rc = sur_infer(net, c.st, nb, &yd))) break;
+    if ((rc = launch_scale_views(c.st, yd, scale, c.wprj2, (int)c.pln, nb, 0))) break;
+    if (cudaMemcpyAsync(y.data(), c.wprj2, sizeof(float) * c.pln * nb, cudaMemcpyDeviceToHost, c.st) ||
+        cudaMemcpyAsync(t.data(), c.wprj, sizeof(float) * c.pln * nb, cudaMemcpyDeviceToHost, c.st) ||
+        cudaStreamSynchronize(c.st)) {
+      rc = set_error(IRLCU_ECUDA, "surrogate check: copy failed");
+      break;
+    }
+    for (int b = 0; b < nb; ++b) {
+      double e2 = 0.0, t2 = 0.0;
+      for (size_t i = 0; i < c.pln; ++i) {
+        const double d = (double)y[b * c.pln + i] - t[b * c.pln + i];
+        e2 += d * d;
+        t2 += (double)t[b * c.pln + i] * t[b * c.pln + i];
+      }
+      nrmse[v0 + b] = (float)(t2 > 0 ? std::sqrt(e2 / t2) : (e2 > 0 ? 1.0 : 0.0));
+    }
+  }
+  dfree(scale);
+  return rc;
+}
+
+int irlcu_set_surrogate(irlcu_sur *net, const unsigned char *flags) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  graphs_clear(c);  // captured iterations may hold the other projector
+  if (!net) {
+    c.sur = nullptr;
+    c.sur_flags.clear();
+    return IRLCU_OK;
+  }
+  TRY(sur_geometry(c, net, MODEL_SRF_BIT));
+  if (sur_max_batch(net) < c.g.max_batch)
+    return set_error(IRLCU_EARG, "surrogate: network batch %d below the context's %d", sur_max_batch(net),
+                     c.g.max_batch);
+  if (!c.sur_scale) TRY(dalloc(&c.sur_scale, (size_t)c.g.max_batch));
+  c.sur = net;
+  if (flags)
+    c.sur_flags.assign(flags, flags + c.nv);
+  else
+    c.sur_flags.clear();
   return IRLCU_OK;
 }
 

@@ -138,6 +138,11 @@ struct Ctx {
   std::vector<GraphRec> graphs;
   std::vector<int> graph_seen;   // keys run eagerly once
   bool capturing = false;
+
+  // learned scatter surrogate in place of ESSE (irlcu_set_surrogate)
+  irlcu_sur *sur = nullptr;
+  std::vector<unsigned char> sur_flags;   // per view: 1 = ESSE for that view
+  float *sur_scale = nullptr;             // max_batch activity means
   // three-shear intermediate for slices beyond shared memory, grown on use
   mutable float *xscratch = nullptr;
   mutable size_t xscratch_elems = 0;
@@ -211,6 +216,16 @@ int launch_ratio(const Ctx &c, const float *calc, const float *calc_nosrf,
 // norm mask planes
 int launch_norm_planes(const Ctx &c, const int *dviews, const float *vt_dev, int nv,
                        const unsigned char *normcols, float *planes);
+
+// learned scatter surrogate (k_surrogate.cu)
+int sur_max_batch(const irlcu_sur *s);
+void *sur_input(irlcu_sur *s);
+int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y);
+int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
+                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out);
+int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size_t n);
+int launch_scale_views(cudaStream_t st, const float *x, const float *s, float *y, int P, int nb, int accumulate);
+int launch_div_views(cudaStream_t st, const float *a, const float *s, float *out, int P, int nb);
 
 // ESSE effective source: src[v] = rot[v]*primary + effsrc(rot[v], view)
 int esse_setup(Ctx &c, const irlcu_esse *e);

@@ -1,0 +1,930 @@
+// k_surrogate.cu -- the learned scatter surrogate: a small 3D-conv encoder
+// and 2D decoder that maps a view's rotated activity and attenuation to the
+// view's ESSE scatter projection (the difference between the projection with
+// and without the scatter model, osemrecon.c:757-786).
+//
+// Network (BF16 weights and activations, FP32 accumulation), per view:
+//   input  [32][32][32][3]: the rotated activity, mu and exp(-depth) of the
+//          128^3 view frame, each 4x4x4 average-pooled ([y][z][x][c],
+//          channels last); activity and target are divided by the view's
+//          mean activity s (the scatter projection is linear in activity)
+//   E1 conv3d 3->32  k3 s1 + ReLU       [32][32][32][32]
+//   E2 conv3d 32->32 k3 s2 + ReLU       [16][16][16][32]
+//   E3 conv3d 32->64 k3 s2 + ReLU       [8][8][8][64]
+//   fold depth into channels            [8][8][512]
+//   D1 conv2d 512->256 k3 + ReLU, x2 nearest upsample   [16][16][256]
+//   D2 conv2d 256->128 k3 + ReLU, x2                    [32][32][128]
+//   D3 conv2d 128->64  k3 + ReLU, x2                    [64][64][64]
+//   D4 conv2d 64->32   k3 + ReLU, x2                    [128][128][32]
+//   D5 conv2d 32->1    k3 (linear)                      [128][128]
+// 1,653,153 parameters.  Every convolution is an explicit im2col followed by
+// a BF16 tensor-core GEMM (mma.sync m16n8k16, FP32 accumulate) with the bias
+// and ReLU in its epilogue; backward uses the same GEMM for the weight and
+// input gradients (split over K where the reduction is long, summed in a
+// fixed order) and a gather-form col2im, so results are deterministic.
+// Training: Adam on FP32 master weights, BF16 copies for the GEMMs.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "irlcu_internal.cuh"
+
+namespace irlcu {
+
+typedef __nv_bfloat16 bf16;
+
+// ------------------------------------------------------------------ GEMM
+// C(m, n) = sum_k A(m, k) B(k, n) over BF16 operands with FP32
+// accumulation; A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn].
+// Epilogue: + bias[n] (optional), ReLU (optional), then C = v (FP32 and/or
+// BF16 output at C[m*scm + n*scn]).
+struct GemmArgs {
+  const bf16 *A, *B;
+  long long sam, sak, sbk, sbn;
+  int M, N, K;
+  const float *bias;
+  int relu;
+  float *Cf;       // FP32 output or null
+  bf16 *Cb;        // BF16 output or null
+  long long scm, scn;
+  // split-K: grid.z slices of kper each write raw sums to ws[z][M][N];
+  // k_splitk_reduce adds them in slice order and applies the epilogue
+  int splits, kper;
+  float *ws;
+};
+
+constexpr int GBM = 64, GBN = 64, GBK = 32, GPAD = 8, GNT = 128;
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// tile [64 rows][GBK] of a strided operand into shared memory (k
+// contiguous); entries outside rows x [.., K) are zero
+__device__ __forceinline__ void load_tile(bf16 (*s)[GBK + GPAD], const bf16 *src, long long s_row, long long s_k,
+                                          int row0, int k0, int rows, int K) {
+  const bf16 zero = __float2bfloat16(0.f);
+  if (s_k == 1 && (K & 7) == 0 && (s_row & 7) == 0 && ((uintptr_t)src & 15) == 0) {
+    // 8 consecutive k per 16-byte load (k0 and K are multiples of 8)
+    for (int e = threadIdx.x; e < GBM * (GBK / 8); e += GNT) {
+      const int r = e / (GBK / 8), kk = (e % (GBK / 8)) * 8;
+      const int row = row0 + r, k = k0 + kk;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (row < rows && k < K) v = *reinterpret_cast<const uint4 *>(src + row * s_row + k);
+      *reinterpret_cast<uint4 *>(&s[r][kk]) = v;
+    }
+  } else if (s_row == 1) {
+    // transposed operand: consecutive threads take consecutive rows
+    for (int e = threadIdx.x; e < GBM * GBK; e += GNT) {
+      const int r = e % GBM, kk = e / GBM;
+      const int row = row0 + r, k = k0 + kk;
+      s[r][kk] = (row < rows && k < K) ? src[row + k * s_k] : zero;
+    }
+  } else {
+    for (int e = threadIdx.x; e < GBM * GBK; e += GNT) {
+      const int r = e / GBK, kk = e % GBK;
+      const int row = row0 + r, k = k0 + kk;
+      s[r][kk] = (row < rows && k < K) ? src[row * s_row + k * s_k] : zero;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(GNT) k_gemm_bf16(GemmArgs a) {
+  __shared__ __align__(16) bf16 As[GBM][GBK + GPAD];
+  __shared__ __align__(16) bf16 Bs[GBN][GBK + GPAD];  // [n][k]
+  const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int g = lane >> 2, t = lane & 3;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+  const int kb = a.splits > 1 ? blockIdx.z * a.kper : 0;
+  const int ke = a.splits > 1 ? min(a.K, kb + a.kper) : a.K;
+  for (int k0 = kb; k0 < ke; k0 += GBK) {
+    __syncthreads();
+    load_tile(As, a.A, a.sam, a.sak, m0, k0, a.M, ke);
+    load_tile(Bs, a.B, a.sbn, a.sbk, n0, k0, a.N, ke);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 16) {
+      uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + g;
+        af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t]);
+        af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t]);
+        af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t + 8]);
+        af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = wn + j * 8 + g;
+        bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][kk + 2 * t]);
+        bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm + i * 16 + g + (q >= 2 ? 8 : 0);
+        const int n = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if (m >= a.M || n >= a.N) continue;
+        float v = acc[i][j][q];
+        if (a.splits > 1) {
+          a.ws[((size_t)blockIdx.z * a.M + m) * a.N + n] = v;
+          continue;
+        }
+        if (a.bias) v += a.bias[n];
+        if (a.relu) v = fmaxf(v, 0.f);
+        const long long o = (long long)m * a.scm + (long long)n * a.scn;
+        if (a.Cf) a.Cf[o] = v;
+        if (a.Cb) a.Cb[o] = __float2bfloat16(v);
+      }
+}
+
+__global__ void k_splitk_reduce(GemmArgs a) {
+  const size_t tot = (size_t)a.M * a.N;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const int m = (int)(e / a.N), n = (int)(e % a.N);
+    float v = 0.f;
+    for (int z = 0; z < a.splits; ++z) v += a.ws[(size_t)z * tot + e];
+    if (a.bias) v += a.bias[n];
+    if (a.relu) v = fmaxf(v, 0.f);
+    const long long o = (long long)m * a.scm + (long long)n * a.scn;
+    if (a.Cf) a.Cf[o] = v;
+    if (a.Cb) a.Cb[o] = __float2bfloat16(v);
+  }
+}
+
+// split-K workspace of a network (FP32 elements)
+constexpr size_t GEMM_WS_ELEMS = (size_t)16 << 20;
+
+static int gemm(cudaStream_t st, GemmArgs a, float *ws) {
+  if (a.M <= 0 || a.N <= 0 || a.K <= 0) return IRLCU_OK;
+  const int tiles_m = (a.M + GBM - 1) / GBM, tiles_n = (a.N + GBN - 1) / GBN;
+  if (tiles_m > 65535) return set_error(IRLCU_EARG, "GEMM with M = %d too large", a.M);
+  // split the reduction when the tile grid is small and K long
+  const long long tiles = (long long)tiles_m * tiles_n;
+  long long sp = std::min<long long>(592 / std::max<long long>(tiles, 1), a.K / 512);
+  int splits = (int)std::max<long long>(1, std::min<long long>(sp, 64));
+  while (splits > 1 && (size_t)splits * a.M * a.N > GEMM_WS_ELEMS) --splits;
+  a.splits = 1;
+  a.kper = a.K;
+  if (splits > 1) {
+    a.kper = ((a.K + splits - 1) / splits + GBK - 1) / GBK * GBK;
+    a.splits = (a.K + a.kper - 1) / a.kper;  // slices actually populated
+    a.ws = ws;
+  }
+  const dim3 grid(tiles_n, tiles_m, a.splits);
+  k_gemm_bf16<<<grid, GNT, 0, st>>>(a);
+  CU_LAUNCHED();
+  if (a.splits > 1) {
+    const size_t tot = (size_t)a.M * a.N;
+    k_splitk_reduce<<<(unsigned)std::min<size_t>((tot + 255) / 256, 148 * 32), 256, 0, st>>>(a);
+    CU_LAUNCHED();
+  }
+  return IRLCU_OK;
+}
+
+// ---------------------------------------------------------- conv helpers
+// activations are channels-last: [b][d][h][w][c]; 2D layers use d = 1.
+struct ConvGeom {
+  int b, di, hi, wi, ci;   // input
+  int kd, kh, kw, s;       // kernel (odd sides, "same" padding k/2), stride
+  int dout, hout, wout, co;
+};
+
+__host__ __device__ inline int conv_out(int in, int k, int s) { return (in + 2 * (k / 2) - k) / s + 1; }
+
+// im2col: row m = output position (b, od, oh, ow), column k = tap*ci + c
+// with tap = (td*kh + th)*kw + tw
+__global__ void k_im2col(ConvGeom g, const bf16 *__restrict__ x, bf16 *__restrict__ col) {
+  const long long K = (long long)g.kd * g.kh * g.kw * g.ci;
+  const long long M = (long long)g.b * g.dout * g.hout * g.wout;
+  const long long tot = M * K;
+  const bf16 zero = __float2bfloat16(0.f);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long m = e / K;
+    const int k = (int)(e - m * K);
+    const int c = k % g.ci, tap = k / g.ci;
+    const int tw = tap % g.kw, th = (tap / g.kw) % g.kh, td = tap / (g.kw * g.kh);
+    long long r = m;
+    const int ow = (int)(r % g.wout); r /= g.wout;
+    const int oh = (int)(r % g.hout); r /= g.hout;
+    const int od = (int)(r % g.dout);
+    const int b = (int)(r / g.dout);
+    const int id = od * g.s + td - g.kd / 2, ih = oh * g.s + th - g.kh / 2, iw = ow * g.s + tw - g.kw / 2;
+    bf16 v = zero;
+    if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
+      v = x[((((long long)b * g.di + id) * g.hi + ih) * g.wi + iw) * g.ci + c];
+    col[e] = v;
+  }
+}
+
+// col2im in gather form: dx(b, id, ih, iw, c) = sum over the taps whose
+// output position lies on the stride grid of dcol(m, tap*ci + c)
+__global__ void k_col2im(ConvGeom g, const float *__restrict__ dcol, float *__restrict__ dx) {
+  const long long K = (long long)g.kd * g.kh * g.kw * g.ci;
+  const long long tot = (long long)g.b * g.di * g.hi * g.wi * g.ci;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const int c = (int)(r % g.ci); r /= g.ci;
+    const int iw = (int)(r % g.wi); r /= g.wi;
+    const int ih = (int)(r % g.hi); r /= g.hi;
+    const int id = (int)(r % g.di);
+    const int b = (int)(r / g.di);
+    float s = 0.f;
+    for (int td = 0; td < g.kd; ++td) {
+      const int nd = id - td + g.kd / 2;
+      if (nd < 0 || nd % g.s) continue;
+      const int od = nd / g.s;
+      if (od >= g.dout) continue;
+      for (int th = 0; th < g.kh; ++th) {
+        const int nh = ih - th + g.kh / 2;
+        if (nh < 0 || nh % g.s) continue;
+        const int oh = nh / g.s;
+        if (oh >= g.hout) continue;
+        for (int tw = 0; tw < g.kw; ++tw) {
+          const int nw = iw - tw + g.kw / 2;
+          if (nw < 0 || nw % g.s) continue;
+          const int ow = nw / g.s;
+          if (ow >= g.wout) continue;
+          const long long m = (((long long)b * g.dout + od) * g.hout + oh) * g.wout + ow;
+          const int tap = (td * g.kh + th) * g.kw + tw;
+          s += dcol[m * K + (long long)tap * g.ci + c];
+        }
+      }
+    }
+    dx[e] = s;
+  }
+}
+
+// gradient through ReLU: g = dy * (y > 0), to BF16 for the next GEMMs
+__global__ void k_relu_grad(const float *__restrict__ dy, const bf16 *__restrict__ y, bf16 *__restrict__ g,
+                            long long n, int relu) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    float v = dy[e];
+    if (relu && !(__bfloat162float(y[e]) > 0.f)) v = 0.f;
+    g[e] = __float2bfloat16(v);
+  }
+}
+
+// bias gradient: column sums of g [M][N], fixed order
+__global__ void k_bias_grad(const bf16 *__restrict__ g, long long M, int N, float *__restrict__ db) {
+  const int n = blockIdx.x;
+  __shared__ float red[256];
+  float s = 0.f;
+  for (long long m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(g[m * N + n]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) db[n] = red[0];
+}
+
+// fold depth into channels: [b][d][h][w][c] -> [b][h][w][d*c]; and the
+// gradient back
+__global__ void k_fold(const bf16 *__restrict__ x, bf16 *__restrict__ y, int b, int d, int h, int w, int c) {
+  const long long tot = (long long)b * d * h * w * c;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const int cc = (int)(r % c); r /= c;
+    const int ww = (int)(r % w); r /= w;
+    const int hh = (int)(r % h); r /= h;
+    const int dd = (int)(r % d);
+    const int bb = (int)(r / d);
+    y[(((long long)bb * h + hh) * w + ww) * (d * c) + dd * c + cc] = x[e];
+  }
+}
+__global__ void k_unfold_f(const float *__restrict__ y, float *__restrict__ x, int b, int d, int h, int w, int c) {
+  const long long tot = (long long)b * d * h * w * c;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const int cc = (int)(r % c); r /= c;
+    const int ww = (int)(r % w); r /= w;
+    const int hh = (int)(r % h); r /= h;
+    const int dd = (int)(r % d);
+    const int bb = (int)(r / d);
+    x[e] = y[(((long long)bb * h + hh) * w + ww) * (d * c) + dd * c + cc];
+  }
+}
+
+// x2 nearest upsampling of [b][h][w][c] and its gradient (sum of 4)
+__global__ void k_up2(const bf16 *__restrict__ x, bf16 *__restrict__ y, int b, int h, int w, int c) {
+  const long long tot = (long long)b * 4 * h * w * c;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const int cc = (int)(r % c); r /= c;
+    const int X = (int)(r % (2 * w)); r /= 2 * w;
+    const int Y = (int)(r % (2 * h));
+    const int bb = (int)(r / (2 * h));
+    y[e] = x[(((long long)bb * h + Y / 2) * w + X / 2) * c + cc];
+  }
+}
+__global__ void k_up2_grad(const float *__restrict__ dy, float *__restrict__ dx, int b, int h, int w, int c) {
+  const long long tot = (long long)b * h * w * c;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const int cc = (int)(r % c); r /= c;
+    const int xx = (int)(r % w); r /= w;
+    const int yy = (int)(r % h);
+    const int bb = (int)(r / h);
+    float s = 0.f;
+    for (int q = 0; q < 4; ++q) {
+      const int Y = 2 * yy + (q >> 1), X = 2 * xx + (q & 1);
+      s += dy[(((long long)bb * 2 * h + Y) * 2 * w + X) * c + cc];
+    }
+    dx[e] = s;
+  }
+}
+
+// mean squared error over [B][P]: grad = 2 (y - t) / (B P); per-sample
+// squared-error sums in part[b] (fixed-order block reduction)
+__global__ void k_mse(const float *__restrict__ y, const float *__restrict__ t, float *__restrict__ grad,
+                      float *__restrict__ part, int P, float inv_count) {
+  const int b = blockIdx.x;
+  __shared__ float red[256];
+  float s = 0.f;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    const float d = y[(size_t)b * P + i] - t[(size_t)b * P + i];
+    grad[(size_t)b * P + i] = 2.f * d * inv_count;
+    s += d * d;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[b] = red[0];
+}
+
+// Adam on FP32 master weights; refreshes the BF16 copy
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       bf16 *__restrict__ wb, long long n, float lr, float b1, float b2, float c1, float c2, float eps) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const float gg = g[e];
+    const float mm = b1 * m[e] + (1.f - b1) * gg;
+    const float vv = b2 * v[e] + (1.f - b2) * gg * gg;
+    m[e] = mm;
+    v[e] = vv;
+    const float nw = w[e] - lr * (mm * c1) / (sqrtf(vv * c2) + eps);
+    w[e] = nw;
+    wb[e] = __float2bfloat16(nw);
+  }
+}
+
+__global__ void k_to_bf16(const float *__restrict__ x, bf16 *__restrict__ y, long long n) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    y[e] = __float2bfloat16(x[e]);
+}
+
+// network input from the rotated volumes of a batch: 4x4x4 means of the
+// activity / s, mu * 10 (per pixel -> order 1) and exp(-S), channels last;
+// s = scale[b], the view's mean activity
+__global__ void k_pool_inputs(const float *__restrict__ act, size_t act_stride, const float *__restrict__ mu,
+                              const float *__restrict__ S, const int *__restrict__ views, size_t vox, int n,
+                              const float *__restrict__ scale, bf16 *__restrict__ out) {
+  const int P = n / 4;
+  const long long tot = (long long)P * P * P;
+  const int b = blockIdx.y;
+  const int view = views[b];
+  const float inv_s = scale[b] > 0.f ? 1.f / scale[b] : 0.f;
+  const float *a = act + (size_t)b * act_stride;
+  const float *m = mu + (size_t)view * vox;
+  const float *sd = S + (size_t)view * vox;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int px = (int)(e % P), pz = (int)((e / P) % P), py = (int)(e / ((long long)P * P));
+    float sa = 0.f, sm = 0.f, se = 0.f;
+    for (int dy = 0; dy < 4; ++dy)
+      for (int dz = 0; dz < 4; ++dz)
+        for (int dx = 0; dx < 4; ++dx) {
+          const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px + dx;
+          sa += a[i];
+          sm += m[i];
+          se += __expf(-sd[i]);
+        }
+    bf16 *o = out + ((size_t)b * tot + e) * 3;
+    o[0] = __float2bfloat16(sa * (1.f / 64.f) * inv_s);
+    o[1] = __float2bfloat16(sm * (10.f / 64.f));
+    o[2] = __float2bfloat16(se * (1.f / 64.f));
+  }
+}
+
+// mean of each view's rotated activity (the input / target normalisation)
+__global__ void k_view_mean(const float *__restrict__ act, size_t stride, size_t vox, float *__restrict__ mean) {
+  const int b = blockIdx.x;
+  __shared__ double red[256];
+  double s = 0.0;
+  for (size_t i = threadIdx.x; i < vox; i += blockDim.x) s += act[(size_t)b * stride + i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) mean[b] = (float)(red[0] / (double)vox);
+}
+
+// out = a - c, elementwise
+__global__ void k_sub(const float *__restrict__ a, const float *__restrict__ c, float *__restrict__ out, size_t n) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = a[e] - c[e];
+}
+
+// y[b] = x[b] * s[b] (+ y[b] when accumulate)
+__global__ void k_scale_views(const float *__restrict__ x, const float *__restrict__ s, float *__restrict__ y,
+                              int P, int nb, int accumulate) {
+  const size_t tot = (size_t)nb * P;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const float v = x[e] * s[e / P];
+    y[e] = accumulate ? y[e] + v : v;
+  }
+}
+
+// out[b] = a[b] / s[b]
+__global__ void k_div_views(const float *__restrict__ a, const float *__restrict__ s, float *__restrict__ out, int P,
+                            int nb) {
+  const size_t tot = (size_t)nb * P;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const float sc = s[e / P];
+    out[e] = sc > 0.f ? a[e] / sc : 0.f;
+  }
+}
+
+static unsigned grid_for(long long n) {
+  long long g = (n + 255) / 256;
+  return (unsigned)(g > 148 * 64 ? 148 * 64 : (g < 1 ? 1 : g));
+}
+
+struct Layer {
+  ConvGeom g;
+  bool relu, up;           // ReLU; x2 upsampling after the layer (decoder)
+  size_t woff, boff;       // weights [co][K] and bias [co] in the parameter vector
+  long long K;
+};
+
+}  // namespace irlcu
+
+struct irlcu_sur {
+  int max_batch = 0;
+  std::vector<irlcu::Layer> L;
+  size_t nparams = 0;
+  float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // FP32 master, gradient, Adam moments
+  irlcu::bf16 *wb = nullptr;                                     // BF16 weights
+  long long step = 0;
+  // act[0] = input, act[i+1] = output of layer i after ReLU (before any
+  // upsampling); upa[i] its upsampled copy; fold = E3 output, depth folded
+  std::vector<irlcu::bf16 *> act, upa;
+  irlcu::bf16 *fold = nullptr;
+  irlcu::bf16 *col = nullptr;     // im2col buffer (largest layer)
+  float *dcol = nullptr;          // input-gradient columns
+  float *gf = nullptr, *gf2 = nullptr;   // FP32 activation gradients
+  irlcu::bf16 *gb = nullptr;      // BF16 gradient of the current layer output
+  float *out = nullptr;           // network output [B][128*128]
+  float *dout = nullptr;
+  float *loss_part = nullptr;
+  float *ws = nullptr;            // split-K workspace
+  cudaStream_t st = nullptr;      // stream of the current work
+  cudaStream_t own = nullptr;     // the network's own stream
+};
+
+namespace irlcu {
+
+static void build_layers(irlcu_sur &s) {
+  struct Spec {
+    int di, hi, wi, ci, k3d, s, co;
+    bool relu, up;
+  };
+  const Spec sp[] = {
+      {32, 32, 32, 3, 1, 1, 32, true, false},  {32, 32, 32, 32, 1, 2, 32, true, false},
+      {16, 16, 16, 32, 1, 2, 64, true, false}, {1, 8, 8, 512, 0, 1, 256, true, true},
+      {1, 16, 16, 256, 0, 1, 128, true, true}, {1, 32, 32, 128, 0, 1, 64, true, true},
+      {1, 64, 64, 64, 0, 1, 32, true, true},   {1, 128, 128, 32, 0, 1, 1, false, false}};
+  size_t off = 0;
+  s.L.clear();
+  for (const Spec &p : sp) {
+    Layer l{};
+    l.g.di = p.di;
+    l.g.hi = p.hi;
+    l.g.wi = p.wi;
+    l.g.ci = p.ci;
+    l.g.kd = p.k3d ? 3 : 1;
+    l.g.kh = 3;
+    l.g.kw = 3;
+    l.g.s = p.s;
+    l.g.dout = conv_out(p.di, l.g.kd, p.s);
+    l.g.hout = conv_out(p.hi, 3, p.s);
+    l.g.wout = conv_out(p.wi, 3, p.s);
+    l.g.co = p.co;
+    l.relu = p.relu;
+    l.up = p.up;
+    l.K = (long long)l.g.kd * 9 * p.ci;
+    l.woff = off;
+    off += (size_t)l.K * p.co;
+    l.boff = off;
+    off += p.co;
+    s.L.push_back(l);
+  }
+  s.nparams = off;
+}
+
+// He-uniform initialisation from a seed (splitmix64), biases zero
+static void init_weights(const irlcu_sur &s, unsigned long long seed, std::vector<float> &w) {
+  w.assign(s.nparams, 0.f);
+  unsigned long long x = seed;
+  auto next = [&]() {
+    x += 0x9E3779B97F4A7C15ULL;
+    unsigned long long z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+  };
+  for (const Layer &l : s.L) {
+    const double bound = std::sqrt(6.0 / (double)l.K);
+    for (long long i = 0; i < l.K * l.g.co; ++i) {
+      const double u = (double)(next() >> 11) / 9007199254740992.0;  // [0, 1)
+      w[l.woff + i] = (float)((2.0 * u - 1.0) * bound);
+    }
+  }
+}
+
+static size_t layer_in_elems(const Layer &l, int B) { return (size_t)B * l.g.di * l.g.hi * l.g.wi * l.g.ci; }
+static size_t layer_out_elems(const Layer &l, int B) {
+  return (size_t)B * l.g.dout * l.g.hout * l.g.wout * l.g.co;
+}
+
+template <class T>
+static int dmalloc(T **p, size_t n) {
+  *p = nullptr;
+  if (cudaMalloc(p, sizeof(T) * (n ? n : 1)) != cudaSuccess)
+    return set_error(IRLCU_ENOMEM, "surrogate: device allocation of %zu bytes failed", sizeof(T) * n);
+  return IRLCU_OK;
+}
+
+static void sur_free(irlcu_sur *s) {
+  if (!s) return;
+  cudaFree(s->w);
+  cudaFree(s->g);
+  cudaFree(s->m);
+  cudaFree(s->v);
+  cudaFree(s->wb);
+  for (auto p : s->act) cudaFree(p);
+  for (auto p : s->upa) cudaFree(p);
+  cudaFree(s->fold);
+  cudaFree(s->col);
+  cudaFree(s->dcol);
+  cudaFree(s->gf);
+  cudaFree(s->gf2);
+  cudaFree(s->gb);
+  cudaFree(s->out);
+  cudaFree(s->dout);
+  cudaFree(s->loss_part);
+  cudaFree(s->ws);
+  if (s->own) cudaStreamDestroy(s->own);
+  delete s;
+}
+
+#define STRY(x)            \
+  do {                     \
+    int rc_ = (x);         \
+    if (rc_) return rc_;   \
+  } while (0)
+
+// input of layer i as im2col sees it
+static const bf16 *layer_input(const irlcu_sur &s, int i) {
+  if (i == 3) return s.fold;
+  if (i > 3 && s.L[i - 1].up) return s.upa[i - 1];
+  return s.act[i];
+}
+
+// forward over the B samples in act[0]; FP32 output [B][128*128] in s.out
+static int sur_forward(irlcu_sur &s, int B) {
+  const int nl = (int)s.L.size();
+  for (int i = 0; i < nl; ++i) {
+    Layer l = s.L[i];
+    l.g.b = B;
+    if (i == 3) {  // fold the encoder's depth into channels
+      const Layer &p = s.L[2];
+      k_fold<<<grid_for((long long)layer_out_elems(p, B)), 256, 0, s.st>>>(s.act[3], s.fold, B, p.g.dout, p.g.hout,
+                                                                            p.g.wout, p.g.co);
+      CU_LAUNCHED();
+    }
+    const long long M = (long long)B * l.g.dout * l.g.hout * l.g.wout;
+    k_im2col<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
+    CU_LAUNCHED();
+    GemmArgs a{};
+    a.A = s.col;
+    a.sam = l.K;
+    a.sak = 1;
+    a.B = s.wb + l.woff;  // weights [co][K]: B(k, n) = W[n*K + k]
+    a.sbk = 1;
+    a.sbn = l.K;
+    a.M = (int)M;
+    a.N = l.g.co;
+    a.K = (int)l.K;
+    a.bias = s.w + l.boff;
+    a.relu = l.relu;
+    if (i == nl - 1)
+      a.Cf = s.out;
+    else
+      a.Cb = s.act[i + 1];
+    a.scm = l.g.co;
+    a.scn = 1;
+    STRY(gemm(s.st, a, s.ws));
+    if (l.up) {
+      k_up2<<<grid_for((long long)layer_out_elems(l, B) * 4), 256, 0, s.st>>>(s.act[i + 1], s.upa[i], B, l.g.hout,
+                                                                               l.g.wout, l.g.co);
+      CU_LAUNCHED();
+    }
+  }
+  return IRLCU_OK;
+}
+
+// backward from s.dout (dLoss / d output); parameter gradients into s.g
+static int sur_backward(irlcu_sur &s, int B) {
+  const int nl = (int)s.L.size();
+  float *gcur = s.gf, *gnext = s.gf2;  // dLoss / d(layer output after ReLU)
+  CU_TRY(cudaMemcpyAsync(gcur, s.dout, sizeof(float) * (size_t)B * 128 * 128, cudaMemcpyDeviceToDevice, s.st));
+  for (int i = nl - 1; i >= 0; --i) {
+    Layer l = s.L[i];
+    l.g.b = B;
+    const long long M = (long long)B * l.g.dout * l.g.hout * l.g.wout;
+    const long long nout = M * l.g.co;
+    const bf16 *yact = (i == nl - 1) ? nullptr : s.act[i + 1];
+    k_relu_grad<<<grid_for(nout), 256, 0, s.st>>>(gcur, yact, s.gb, nout, (yact && l.relu) ? 1 : 0);
+    CU_LAUNCHED();
+    k_im2col<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
+    CU_LAUNCHED();
+    // dW[n][k] = sum_m col[m][k] g[m][n]
+    GemmArgs a{};
+    a.A = s.col;  // A'(k, m) = col[m*K + k]
+    a.sam = 1;
+    a.sak = l.K;
+    a.B = s.gb;   // B'(m, n) = g[m*co + n]
+    a.sbk = l.g.co;
+    a.sbn = 1;
+    a.M = (int)l.K;
+    a.N = l.g.co;
+    a.K = (int)M;
+    a.Cf = s.g + l.woff;  // dW[n*K + k]
+    a.scm = 1;
+    a.scn = l.K;
+    STRY(gemm(s.st, a, s.ws));
+    k_bias_grad<<<l.g.co, 256, 0, s.st>>>(s.gb, M, l.g.co, s.g + l.boff);
+    CU_LAUNCHED();
+    if (i == 0) break;  // no gradient for the input
+    // dcol[m][k] = sum_n g[m][n] W[n][k]
+    GemmArgs d{};
+    d.A = s.gb;
+    d.sam = l.g.co;
+    d.sak = 1;
+    d.B = s.wb + l.woff;  // B(n, k) = W[n*K + k]
+    d.sbk = l.K;
+    d.sbn = 1;
+    d.M = (int)M;
+    d.N = (int)l.K;
+    d.K = l.g.co;
+    d.Cf = s.dcol;
+    d.scm = l.K;
+    d.scn = 1;
+    STRY(gemm(s.st, d, s.ws));
+    const long long nin = (long long)layer_in_elems(l, B);
+    k_col2im<<<grid_for(nin), 256, 0, s.st>>>(l.g, s.dcol, gnext);
+    CU_LAUNCHED();
+    // gnext = dLoss / d(layer i input): map it to layer i-1's output
+    if (i == 3) {
+      const Layer &p = s.L[2];
+      k_unfold_f<<<grid_for(nin), 256, 0, s.st>>>(gnext, gcur, B, p.g.dout, p.g.hout, p.g.wout, p.g.co);
+      CU_LAUNCHED();
+    } else if (i > 3 && s.L[i - 1].up) {
+      const Layer &p = s.L[i - 1];
+      k_up2_grad<<<grid_for((long long)layer_out_elems(p, B)), 256, 0, s.st>>>(gnext, gcur, B, p.g.hout, p.g.wout,
+                                                                              p.g.co);
+      CU_LAUNCHED();
+    } else {
+      std::swap(gcur, gnext);
+    }
+  }
+  return IRLCU_OK;
+}
+
+static int sur_loss(irlcu_sur &s, int B, const float *t, float *loss) {
+  const int P = 128 * 128;
+  k_mse<<<B, 256, 0, s.st>>>(s.out, t, s.dout, s.loss_part, P, 1.f / ((float)B * P));
+  CU_LAUNCHED();
+  if (loss) {
+    std::vector<float> part(B);
+    CU_TRY(cudaMemcpyAsync(part.data(), s.loss_part, sizeof(float) * B, cudaMemcpyDeviceToHost, s.st));
+    CU_TRY(cudaStreamSynchronize(s.st));
+    double sum = 0.0;
+    for (float p : part) sum += p;
+    *loss = (float)(sum / ((double)B * P));
+  }
+  return IRLCU_OK;
+}
+
+static int sur_check_batch(const irlcu_sur *s, int B) {
+  if (!s) return set_error(IRLCU_EARG, "surrogate: null network");
+  if (B < 1 || B > s->max_batch) return set_error(IRLCU_EARG, "surrogate: batch %d outside 1..%d", B, s->max_batch);
+  return IRLCU_OK;
+}
+
+// ------------------------------------------- use inside the projector
+
+int sur_max_batch(const irlcu_sur *s) { return s ? s->max_batch : 0; }
+void *sur_input(irlcu_sur *s) { return s->act[0]; }
+
+// forward of the B samples already in sur_input(s), on stream st; FP32
+// output [B][128*128] in *y (the network's buffer, valid until its next use)
+int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y) {
+  STRY(sur_check_batch(s, B));
+  s->st = st;
+  const int rc = sur_forward(*s, B);
+  s->st = s->own;
+  *y = s->out;
+  return rc;
+}
+
+// pooled network inputs of nv rotated volumes (act, stride act_stride) with
+// the per-view mu and depth tables; the activity means go to scale
+int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
+                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out) {
+  k_view_mean<<<nv, 256, 0, st>>>(act, act_stride, vox, scale);
+  CU_LAUNCHED();
+  const long long P3 = (long long)(n / 4) * (n / 4) * (n / 4);
+  dim3 grid((unsigned)std::min<long long>((P3 + 255) / 256, 1024), nv);
+  k_pool_inputs<<<grid, 256, 0, st>>>(act, act_stride, mu, S, dviews, vox, n, scale, static_cast<bf16 *>(out));
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size_t n) {
+  k_sub<<<grid_for((long long)n), 256, 0, st>>>(a, b, out, n);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_scale_views(cudaStream_t st, const float *x, const float *s, float *y, int P, int nb, int accumulate) {
+  k_scale_views<<<grid_for((long long)P * nb), 256, 0, st>>>(x, s, y, P, nb, accumulate);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_div_views(cudaStream_t st, const float *a, const float *s, float *out, int P, int nb) {
+  k_div_views<<<grid_for((long long)P * nb), 256, 0, st>>>(a, s, out, P, nb);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+}  // namespace irlcu
+
+using namespace irlcu;
+
+extern "C" {
+
+int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
+  *out = nullptr;
+  if (max_batch < 1 || max_batch > 256) return set_error(IRLCU_EARG, "surrogate: batch %d outside 1..256", max_batch);
+  irlcu_sur *s = new irlcu_sur;
+  s->max_batch = max_batch;
+  build_layers(*s);
+  int rc = IRLCU_OK;
+  auto fail = [&](int r) {
+    sur_free(s);
+    return r;
+  };
+  if (cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(set_error(IRLCU_ECUDA, "surrogate: stream creation failed"));
+  s->st = s->own;
+  const size_t P = s->nparams;
+  if ((rc = dmalloc(&s->w, P)) || (rc = dmalloc(&s->g, P)) || (rc = dmalloc(&s->m, P)) || (rc = dmalloc(&s->v, P)) ||
+      (rc = dmalloc(&s->wb, P)))
+    return fail(rc);
+  const int B = max_batch;
+  size_t colmax = 0, actmax = 0;
+  s->act.assign(s->L.size() + 1, nullptr);
+  s->upa.assign(s->L.size(), nullptr);
+  for (size_t i = 0; i < s->L.size(); ++i) {
+    const Layer &l = s->L[i];
+    const size_t M = (size_t)B * l.g.dout * l.g.hout * l.g.wout;
+    colmax = std::max(colmax, M * (size_t)l.K);
+    actmax = std::max(actmax, std::max(layer_in_elems(l, B), layer_out_elems(l, B)));
+    if (i == 0 && (rc = dmalloc(&s->act[0], layer_in_elems(l, B)))) return fail(rc);
+    if ((rc = dmalloc(&s->act[i + 1], layer_out_elems(l, B)))) return fail(rc);
+    if (l.up) {
+      if ((rc = dmalloc(&s->upa[i], layer_out_elems(l, B) * 4))) return fail(rc);
+      actmax = std::max(actmax, layer_out_elems(l, B) * 4);
+    }
+  }
+  if ((rc = dmalloc(&s->fold, layer_out_elems(s->L[2], B))) || (rc = dmalloc(&s->col, colmax)) ||
+      (rc = dmalloc(&s->dcol, colmax)) || (rc = dmalloc(&s->gf, actmax)) || (rc = dmalloc(&s->gf2, actmax)) ||
+      (rc = dmalloc(&s->gb, actmax)) || (rc = dmalloc(&s->out, (size_t)B * 128 * 128)) ||
+      (rc = dmalloc(&s->dout, (size_t)B * 128 * 128)) || (rc = dmalloc(&s->loss_part, (size_t)B)) ||
+      (rc = dmalloc(&s->ws, GEMM_WS_ELEMS)))
+    return fail(rc);
+  std::vector<float> w;
+  init_weights(*s, seed, w);
+  if (cudaMemcpy(s->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(s->m, 0, sizeof(float) * P) != cudaSuccess || cudaMemset(s->v, 0, sizeof(float) * P) != cudaSuccess)
+    return fail(set_error(IRLCU_ECUDA, "surrogate: initial upload failed"));
+  k_to_bf16<<<grid_for((long long)P), 256, 0, s->st>>>(s->w, s->wb, (long long)P);
+  ++g_launch_count;
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s->st) != cudaSuccess)
+    return fail(set_error(IRLCU_ECUDA, "surrogate: initialisation failed"));
+  *out = s;
+  return IRLCU_OK;
+}
+
+void irlcu_sur_destroy(irlcu_sur *s) {
+  if (s) cudaStreamSynchronize(s->own);
+  sur_free(s);
+}
+
+size_t irlcu_sur_nparams(const irlcu_sur *s) { return s ? s->nparams : 0; }
+
+int irlcu_sur_get_weights(irlcu_sur *s, float *host, size_t n) {
+  if (!s || n != s->nparams) return set_error(IRLCU_EARG, "surrogate: expected %zu parameters", s ? s->nparams : 0);
+  CU_TRY(cudaStreamSynchronize(s->st));
+  CU_TRY(cudaMemcpy(host, s->w, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return IRLCU_OK;
+}
+
+int irlcu_sur_set_weights(irlcu_sur *s, const float *host, size_t n) {
+  if (!s || n != s->nparams) return set_error(IRLCU_EARG, "surrogate: expected %zu parameters", s ? s->nparams : 0);
+  CU_TRY(cudaStreamSynchronize(s->st));
+  CU_TRY(cudaMemcpy(s->w, host, sizeof(float) * n, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemset(s->m, 0, sizeof(float) * n));
+  CU_TRY(cudaMemset(s->v, 0, sizeof(float) * n));
+  s->step = 0;
+  k_to_bf16<<<grid_for((long long)n), 256, 0, s->st>>>(s->w, s->wb, (long long)n);
+  CU_LAUNCHED();
+  CU_TRY(cudaStreamSynchronize(s->st));
+  return IRLCU_OK;
+}
+
+int irlcu_sur_forward(irlcu_sur *s, int B, const void *x, float *y) {
+  STRY(sur_check_batch(s, B));
+  CU_TRY(cudaMemcpyAsync(s->act[0], x, sizeof(bf16) * layer_in_elems(s->L[0], B), cudaMemcpyDeviceToDevice, s->st));
+  STRY(sur_forward(*s, B));
+  CU_TRY(cudaMemcpyAsync(y, s->out, sizeof(float) * (size_t)B * 128 * 128, cudaMemcpyDeviceToDevice, s->st));
+  CU_TRY(cudaStreamSynchronize(s->st));
+  return IRLCU_OK;
+}
+
+int irlcu_sur_gradient(irlcu_sur *s, int B, const void *x, const float *t, float *loss, float *grad_host) {
+  STRY(sur_check_batch(s, B));
+  CU_TRY(cudaMemcpyAsync(s->act[0], x, sizeof(bf16) * layer_in_elems(s->L[0], B), cudaMemcpyDeviceToDevice, s->st));
+  STRY(sur_forward(*s, B));
+  STRY(sur_loss(*s, B, t, loss));
+  STRY(sur_backward(*s, B));
+  CU_TRY(cudaStreamSynchronize(s->st));
+  if (grad_host) CU_TRY(cudaMemcpy(grad_host, s->g, sizeof(float) * s->nparams, cudaMemcpyDeviceToHost));
+  return IRLCU_OK;
+}
+
+int irlcu_sur_train_step(irlcu_sur *s, int B, const void *x, const float *t, float lr, float *loss) {
+  STRY(irlcu_sur_gradient(s, B, x, t, loss, nullptr));
+  s->step += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = (float)(1.0 / (1.0 - std::pow((double)b1, (double)s->step)));
+  const float c2 = (float)(1.0 / (1.0 - std::pow((double)b2, (double)s->step)));
+  k_adam<<<grid_for((long long)s->nparams), 256, 0, s->st>>>(s->w, s->g, s->m, s->v, s->wb, (long long)s->nparams, lr,
+                                                             b1, b2, c1, c2, 1e-8f);
+  CU_LAUNCHED();
+  CU_TRY(cudaStreamSynchronize(s->st));
+  return IRLCU_OK;
+}
+
+}  // extern "C"

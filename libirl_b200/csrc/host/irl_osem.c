@@ -78,12 +78,24 @@ typedef struct {
 	sOsemData hd;            /* hook data (osemhooks.h:18-27) */
 	int hook_norm;           /* subset whose norm the hooks see, or -1 */
 	size_t vox, prjn;
+	irlcu_sur *sur;          /* learned scatter surrogate, or NULL */
+	float *sur_nrmse;        /* per view, after the first scatter iteration */
+	int sur_pending;         /* NRMSE check still to run */
 } osem_session;
+
+/* learned scatter surrogate for the next sessions (IrlSetScatterSurrogate) */
+static char *g_sur_fname = NULL;
+static float g_sur_fallback = 0.02f;
 
 static osem_session S;
 
 static void session_close(void)
 {
+	if (S.sur != NULL) {
+		irlcu_set_surrogate(NULL, NULL);
+		irlcu_sur_destroy(S.sur);
+	}
+	free(S.sur_nrmse);
 	irlcu_shutdown();
 	irl_free_run_tables();
 	free(S.views);
@@ -273,6 +285,85 @@ static void compute_norms(void)
 	irl_msg(5, "Done Computing Norm Matrix (%.3f s)\n", now_s() - t0);
 }
 
+/* the surrogate network of this session from g_sur_fname: "IRLSUR01",
+   uint32 parameter count, float32 parameters (little-endian) */
+static void sur_load(void)
+{
+	char magic[8];
+	unsigned int n = 0;
+	float *w;
+	size_t want;
+	FILE *fp = fopen(g_sur_fname, "rb");
+	if (fp == NULL)
+		irl_fatal(IRL_E_IO, "ScatterSurrogate", "cannot open %s", g_sur_fname);
+	if (fread(magic, 1, 8, fp) != 8 || memcmp(magic, "IRLSUR01", 8) != 0 || fread(&n, 4, 1, fp) != 1) {
+		fclose(fp);
+		irl_fatal(IRL_E_IO, "ScatterSurrogate", "%s is not a surrogate weights file", g_sur_fname);
+	}
+	irl_cu(irlcu_sur_create(S.max_batch, 1, &S.sur), "ScatterSurrogate");
+	want = irlcu_sur_nparams(S.sur);
+	if (n != want) {
+		fclose(fp);
+		irl_fatal(IRL_E_VALUE, "ScatterSurrogate", "%s holds %u parameters, the network has %zu", g_sur_fname, n,
+			want);
+	}
+	w = (float *)irl_malloc(sizeof(float) * want, "surrogate weights");
+	if (fread(w, sizeof(float), want, fp) != want) {
+		free(w);
+		fclose(fp);
+		irl_fatal(IRL_E_IO, "ScatterSurrogate", "%s is truncated", g_sur_fname);
+	}
+	fclose(fp);
+	irl_cu(irlcu_sur_set_weights(S.sur, w, want), "ScatterSurrogate");
+	free(w);
+	S.sur_nrmse = (float *)irl_calloc(sizeof(float) * S.p.nviews, "surrogate NRMSE");
+	S.sur_pending = 1;
+}
+
+/* after the first scatter iteration (ESSE on every view): per-view NRMSE of
+   the surrogate against ESSE on the current estimate; views above the
+   fallback threshold keep ESSE, the others use the network from now on */
+static void sur_check(int model)
+{
+	unsigned char *flags;
+	int *all;
+	int v, nflag = 0;
+	all = (int *)irl_malloc(sizeof(int) * S.p.nviews, "surrogate views");
+	for (v = 0; v < S.p.nviews; ++v)
+		all[v] = v;
+	irl_cu(irlcu_sur_check(S.sur, S.p.nviews, all, model, S.sur_nrmse), "ScatterSurrogate");
+	free(all);
+	flags = (unsigned char *)irl_calloc(S.p.nviews, "surrogate flags");
+	for (v = 0; v < S.p.nviews; ++v)
+		if (!(S.sur_nrmse[v] <= g_sur_fallback)) {
+			flags[v] = 1;
+			++nflag;
+		}
+	irl_cu(irlcu_set_surrogate(S.sur, flags), "ScatterSurrogate");
+	free(flags);
+	S.sur_pending = 0;
+	irl_msg(4, "scatter surrogate: %d of %d views above NRMSE %.3f keep ESSE\n", nflag, S.p.nviews,
+		g_sur_fallback);
+}
+
+int IrlSetScatterSurrogate(const char *pchWeightsFname, float fFallbackNrmse)
+{
+	free(g_sur_fname);
+	g_sur_fname = pchWeightsFname != NULL ? irl_strdup(pchWeightsFname) : NULL;
+	g_sur_fallback = fFallbackNrmse > 0 ? fFallbackNrmse : 0.02f;
+	return 0;
+}
+
+int IrlGetScatterSurrogateNrmse(float *pfNrmse, int iNumViews)
+{
+	int v;
+	if (!S.open || S.sur == NULL || S.sur_pending || pfNrmse == NULL || iNumViews != S.p.nviews)
+		return IRL_E_VALUE;
+	for (v = 0; v < iNumViews; ++v)
+		pfNrmse[v] = S.sur_nrmse[v];
+	return 0;
+}
+
 int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
 	void (*cb)(int, float *), float *scatest, float *atn, float *prj, float *recon, char *logname, char *msgname)
 {
@@ -363,6 +454,8 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		irl_cu(irlcu_set_subsets(S.ns, S.per, S.ang, all), "OsemRecon");
 		free(all);
 	}
+	if (g_sur_fname != NULL && (S.p.prj_model & MODEL_SRF) && S.p.srf_iters > 0)
+		sur_load();
 	for (m = 0; m < 6; ++m)
 		if (g_irl_hooks[m] != NULL && S.norm_host == NULL) {
 			S.norm_host = (float *)irl_calloc(sizeof(float) * S.vox, "norm mirror");
@@ -436,6 +529,8 @@ static void one_iteration(void)
 		hook_call(HOOK_POST_SUBSET);
 	}
 	hook_call(HOOK_POST_ITER);
+	if (S.sur != NULL && S.sur_pending && S.this_srf)
+		sur_check(model);
 	/* bCheckIfSaveIteration is true for every iteration with libirl's
 	   SaveInterval of 1 (IrlSetup.c:87-88, osemrecon.c:513-555) */
 	if (S.cb != NULL) {

@@ -1,0 +1,174 @@
+"""Train the learned scatter surrogate on the GPU.
+
+    python -m libirl_b200.surrogate.train --phantoms 200 --val 16 --steps 6000 \
+        --out libirl_b200/surrogate/sur128.bin --summary sur128.json
+
+Training pairs come from the library's GPU ESSE path (irlcu_sur_pairs): for
+every seeded full128 phantom (the 128^3 config-2 generator of
+libirl_b200.workloads, a different seed per phantom) and each of its 120
+views, the pooled rotated activity / attenuation / depth and the ESSE
+scatter projection (projection with the scatter model minus without),
+divided by the view's mean activity.  The network is trained with the
+library's own forward, backward and Adam kernels (irlcu_sur_train_step);
+torch only holds the device arrays and draws the batches.  Held-out
+phantoms give the per-view NRMSE = ||y - t|| / ||t||.
+
+Phantoms are generated on the host in a pool of processes started with
+"spawn" while the GPU turns earlier ones into pairs.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import multiprocessing as mp
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from libirl_b200 import api, workloads as W  # noqa: E402
+from libirl_b200 import surrogate as SU  # noqa: E402
+
+_libc = C.CDLL(None)
+_libc.strdup.restype = C.c_void_p
+_libc.strdup.argtypes = [C.c_char_p]
+
+
+def _dup(s):
+    return C.cast(_libc.strdup(s.encode()), C.c_char_p)
+
+
+def _phantom(seed):
+    return W.full128(seed=seed)
+
+
+def generate(lib, seeds, workers=8, batch=15):
+    """Network inputs X, normalised targets T and scales S of every view of
+    every phantom, on the device."""
+    import torch
+    nv = 120
+    N = len(seeds) * nv
+    X = torch.empty((N,) + SU.INPUT_SHAPE, dtype=torch.bfloat16, device="cuda")
+    T = torch.empty((N, SU.OUTPUT_SIZE), dtype=torch.float32, device="cuda")
+    S = torch.empty((N,), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    tmp = tempfile.mkdtemp(prefix="irlsur_")
+    k = 0
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        for case in pool.imap(_phantom, seeds):
+            assert case.nviews == nv and case.n == 128
+            files = case.write_tables(tmp)
+            p, o, v = case.parms(), case.options(), case.views()
+            o.bReconIsInitEst = 1  # the phantom is the estimate
+            rec, atn = case.act.copy(), case.atn.copy()
+            prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+            rc = lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(),
+                                  None, api.fptr(atn), api.fptr(prj), api.fptr(rec), None, None)
+            if rc:
+                raise RuntimeError(lib.pchIrlErrorString().decode())
+            try:
+                for v0 in range(0, nv, batch):
+                    nb = min(batch, nv - v0)
+                    views = (C.c_int * nb)(*range(v0, v0 + nb))
+                    rc = lib.irlcu_sur_pairs(nb, views, SU.MODEL_SRF, X[k].data_ptr(), T[k].data_ptr(),
+                                             S[k].data_ptr())
+                    if rc:
+                        raise RuntimeError(lib.irlcu_error_string().decode())
+                    k += nb
+            finally:
+                lib.IrlOsemEnd(None)
+    return X, T, S
+
+
+def nrmse(net, X, T, idx, batch):
+    """Per-view ||y - t|| / ||t|| of the network on the views idx."""
+    import torch
+    out = []
+    y = torch.empty((batch, SU.OUTPUT_SIZE), dtype=torch.float32, device="cuda")
+    for i0 in range(0, len(idx), batch):
+        sel = idx[i0:i0 + batch]
+        xb = X.index_select(0, sel).contiguous()
+        tb = T.index_select(0, sel)
+        torch.cuda.synchronize()
+        net.forward(len(sel), xb.data_ptr(), y.data_ptr())
+        d = (y[:len(sel)] - tb).norm(dim=1) / tb.norm(dim=1).clamp_min(1e-30)
+        out.append(d.cpu().numpy())
+    return np.concatenate(out)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--phantoms", type=int, default=200, help="training phantoms")
+    ap.add_argument("--val", type=int, default=16, help="held-out phantoms")
+    ap.add_argument("--seed0", type=int, default=40000)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--init", default=None, help="start from this weights file")
+    ap.add_argument("--out", default=SU.DEFAULT_WEIGHTS)
+    ap.add_argument("--summary", default=None)
+    args = ap.parse_args(argv)
+
+    import torch
+    import libirl_b200 as L
+    lib = L.load()
+    t0 = time.time()
+    seeds = [args.seed0 + i for i in range(args.phantoms + args.val)]
+    X, T, _ = generate(lib, seeds, workers=args.workers)
+    t_gen = time.time() - t0
+    ntrain = args.phantoms * 120
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234)
+    net = SU.Network(lib, args.batch, seed=17)
+    if args.init:
+        net.set_weights(SU.load_weights(args.init))
+    curve = []
+    t1 = time.time()
+    for step in range(args.steps):
+        # linear warm-up over 200 steps, then cosine decay to 2% of lr
+        warm = min(1.0, (step + 1) / 200.0)
+        lr = args.lr * warm * (0.02 + 0.98 * 0.5 * (1.0 + math.cos(math.pi * step / args.steps)))
+        idx = torch.randint(0, ntrain, (args.batch,), device="cuda", generator=g)
+        xb = X.index_select(0, idx).contiguous()
+        tb = T.index_select(0, idx).contiguous()
+        torch.cuda.synchronize()
+        loss = net.train_step(args.batch, xb.data_ptr(), tb.data_ptr(), lr)
+        if step % 100 == 0 or step == args.steps - 1:
+            curve.append((step, loss))
+            print(f"step {step} loss {loss:.4e} lr {lr:.2e} ({time.time() - t1:.0f} s)", flush=True)
+    t_train = time.time() - t1
+    val_idx = torch.arange(ntrain, X.shape[0], device="cuda")
+    e = nrmse(net, X, T, val_idx, args.batch)
+    tr_idx = torch.arange(0, min(ntrain, 16 * 120), device="cuda")
+    etr = nrmse(net, X, T, tr_idx, args.batch)
+    SU.save_weights(args.out, net.get_weights())
+    summ = {
+        "phantoms": args.phantoms, "val_phantoms": args.val, "views": int(X.shape[0]), "steps": args.steps,
+        "batch": args.batch, "lr": args.lr, "generate_s": round(t_gen, 1), "train_s": round(t_train, 1),
+        "ms_per_step": round(1000 * t_train / max(1, args.steps), 2),
+        "loss_curve": [(s, float(f"{l_:.4e}")) for s, l_ in curve],
+        "val_nrmse": {"mean": float(e.mean()), "median": float(np.median(e)), "p90": float(np.percentile(e, 90)),
+                      "max": float(e.max()), "frac_le_1pct": float((e <= 0.01).mean()),
+                      "frac_le_2pct": float((e <= 0.02).mean())},
+        "train_nrmse_mean": float(etr.mean()),
+        "weights": os.path.relpath(args.out, ROOT) if args.out.startswith(ROOT) else args.out,
+    }
+    print(json.dumps(summ))
+    if args.summary:
+        with open(args.summary, "w") as f:
+            json.dump(summ, f, indent=1)
+    net.close()
+
+
+if __name__ == "__main__":
+    main()

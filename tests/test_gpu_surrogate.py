@@ -1,0 +1,162 @@
+"""The learned scatter surrogate on the GPU (irlcu_sur_* and the projector
+integration), checked against a CPU reference of the same network.
+
+The CPU reference runs the network in float64 with torch on the CPU, with
+BF16 rounding at the points where the kernels store BF16: weights, layer
+outputs after the ReLU, and the gradients of each layer's pre-activation.
+What remains is FP32 against FP64 accumulation, so outputs and gradients
+agree to about 1e-3.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import dup
+from libirl_b200 import api, workloads as W
+from libirl_b200 import surrogate as SU
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    return pytest.importorskip("torch")
+
+
+def cpu_network(w, x, t):
+    """Loss, output and parameter gradients of the network on the CPU."""
+    torch = _torch()
+    F = torch.nn.functional
+
+    def bf(v):  # BF16 value, identity gradient
+        return v + (v.to(torch.bfloat16).to(torch.float64) - v).detach()
+
+    def round_grad(v):
+        v.register_hook(lambda g: g.to(torch.bfloat16).to(torch.float64))
+
+    params = []
+    h = torch.from_numpy(x.astype(np.float64)).permute(0, 4, 1, 2, 3)  # [B, c, y, z, x]
+    B = h.shape[0]
+    for li, ((wt, b), (ci, co, kd, s, relu, up)) in enumerate(zip(SU.split_params(w), SU.layer_specs())):
+        W_ = torch.from_numpy(wt.astype(np.float64)).requires_grad_(True)
+        b_ = torch.from_numpy(b.astype(np.float64)).requires_grad_(True)
+        params.append((W_, b_))
+        if li == 3:  # fold depth into channels: channel = y * 64 + c
+            h = h.permute(0, 2, 1, 3, 4).reshape(B, -1, h.shape[3], h.shape[4])
+        if kd == 3:
+            z = F.conv3d(h, bf(W_).permute(0, 4, 1, 2, 3), padding=1, stride=s)
+            z = z + b_.view(1, -1, 1, 1, 1)
+        else:
+            z = F.conv2d(h, bf(W_)[:, 0].permute(0, 3, 1, 2), padding=1)
+            z = z + b_.view(1, -1, 1, 1)
+        round_grad(z)
+        if li == len(SU.layer_specs()) - 1:
+            h = z
+            break
+        h = bf(torch.relu(z) if relu else z)
+        if up:
+            h = F.interpolate(h, scale_factor=2, mode="nearest")
+    y = h.reshape(B, -1)
+    tt = torch.from_numpy(t.astype(np.float64))
+    loss = ((y - tt) ** 2).mean()
+    loss.backward()
+    grads = []
+    for W_, b_ in params:
+        grads += [W_.grad.numpy().ravel(), b_.grad.numpy().ravel()]
+    return float(loss.detach()), y.detach().numpy(), np.concatenate(grads)
+
+
+def _inputs(rng, B):
+    torch = _torch()
+    x = rng.random((B,) + SU.INPUT_SHAPE, dtype=np.float32)
+    xt = torch.from_numpy(x).to(torch.bfloat16)
+    return xt.to(torch.float32).numpy(), xt.cuda()
+
+
+def test_forward_and_gradients_match_cpu_reference(product):
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    net = SU.Network(product, 2, seed=7)
+    try:
+        w = net.get_weights()
+        x, xd = _inputs(rng, 2)
+        y = torch.zeros((2, SU.OUTPUT_SIZE), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        net.forward(2, xd.data_ptr(), y.data_ptr())
+        t = (rng.standard_normal((2, SU.OUTPUT_SIZE)) * float(y.abs().mean().item())).astype(np.float32)
+        td = torch.from_numpy(t).cuda()
+        torch.cuda.synchronize()
+        loss, g = net.gradient(2, xd.data_ptr(), td.data_ptr())
+        lref, yref, gref = cpu_network(w, x, t)
+        yg = y.cpu().numpy()
+        assert np.linalg.norm(yg - yref) <= 5e-3 * np.linalg.norm(yref)
+        assert abs(loss - lref) <= 5e-3 * lref
+        off = 0
+        for (wt, b), spec in zip(SU.split_params(w), SU.layer_specs()):
+            for part in (wt, b):
+                a, r = g[off:off + part.size], gref[off:off + part.size]
+                off += part.size
+                assert np.linalg.norm(a - r) <= 2e-2 * np.linalg.norm(r) + 1e-30, (spec, part.shape)
+    finally:
+        net.close()
+
+
+def test_training_steps_reduce_the_loss(product):
+    torch = _torch()
+    rng = np.random.default_rng(6)
+    net = SU.Network(product, 4, seed=8)
+    try:
+        _, xd = _inputs(rng, 4)
+        zz, xx = np.meshgrid(np.linspace(-1, 1, 128), np.linspace(-1, 1, 128), indexing="ij")
+        t = np.stack([np.exp(-((zz - 0.2 * k) ** 2 + xx ** 2) * 3).ravel() for k in range(4)]).astype(np.float32)
+        td = torch.from_numpy(t).cuda()
+        torch.cuda.synchronize()
+        losses = [net.train_step(4, xd.data_ptr(), td.data_ptr(), 1e-3) for _ in range(40)]
+        assert losses[-1] < 0.3 * losses[0], losses[::8]
+    finally:
+        net.close()
+
+
+def _osem(product, case, files, meas, iterations):
+    p, o, v = case.parms(), case.options(), case.views()
+    p.NumIterations = iterations
+    atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+    rc = product.IrlOsem(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), api.ITER_CB(), None,
+                         api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+    assert rc == 0, product.pchIrlErrorString()
+    return rec
+
+
+def test_osem_surrogate_fallback(product, tmp_path):
+    """Every view above the NRMSE threshold keeps ESSE: a threshold no view
+    meets gives exactly the ESSE reconstruction; a threshold every view
+    meets runs the network and reports each view's NRMSE."""
+    case = W.full128(seed=5100, n=128, nviews=8, subsets=2, iterations=2)
+    files = case.write_tables(str(tmp_path))
+    meas = W.poisson_counts(np.ones((case.nviews, case.nz, case.n), np.float32), 2e5, 3)
+    net = SU.Network(product, 4, seed=9)
+    wfile = str(tmp_path / "w.bin")
+    SU.save_weights(wfile, net.get_weights())
+    net.close()
+    try:
+        product.IrlSetScatterSurrogate(None, 0.0)
+        plain = _osem(product, case, files, meas, 2)
+        product.IrlSetScatterSurrogate(wfile.encode(), 1e-9)
+        flagged = _osem(product, case, files, meas, 2)
+        assert np.array_equal(flagged, plain)
+        product.IrlSetScatterSurrogate(wfile.encode(), 1e9)
+        p, o, v = case.parms(), case.options(), case.views()
+        atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+        assert product.IrlOsemBegin(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), api.ITER_CB(),
+                                    None, api.fptr(atn), api.fptr(m), api.fptr(rec), None, None) == 0
+        try:
+            assert product.IrlOsemIterate(2) == 0, product.pchIrlErrorString()
+            nrmse = np.zeros(case.nviews, np.float32)
+            assert product.IrlGetScatterSurrogateNrmse(api.fptr(nrmse), case.nviews) == 0
+        finally:
+            assert product.IrlOsemEnd(api.fptr(rec)) == 0
+        assert np.all(np.isfinite(rec)) and np.all(nrmse > 0)
+        assert not np.array_equal(rec, plain)
+    finally:
+        product.IrlSetScatterSurrogate(None, 0.0)
