@@ -233,6 +233,10 @@ def run_b200(args):
                            "host<->device copies from pageable memory, per-iteration callback",
                "phases_s": phases}
 
+    learned = None
+    if not args.no_surrogate and case.n == 128:
+        learned = measure_learned_scatter(lib, case, files, meas, K, Wm, ms_step, torch)
+
     clocks = clk.summary()
     roofline = make_roofline(prof, case, list(grids))
     stages = {L.STAGES[i]: {"ms": round(prof.ms[i], 3), "launches": int(prof.launches[i]),
@@ -260,8 +264,80 @@ def run_b200(args):
                    "drf_autotune_ms": {"direct": round(tune[0], 3), "fourier": round(tune[1], 3)}},
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "stages_ms_per_iteration": {k: {**s, "ms": round(s["ms"] / P, 3)} for k, s in stages.items()},
+        "learned_scatter": learned,
     }
     print(json.dumps(line))
+
+
+def _osem_image(lib, case, files, meas, iterations, srf_iters=None):
+    from libirl_b200 import api
+    p, o, v = case.parms(), case.options(), case.views()
+    p.NumIterations = iterations
+    if srf_iters is not None:
+        p.iNumSrfIterations = srf_iters
+    atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+    rc = lib.IrlOsem(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(), None,
+                     api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    return rec
+
+
+def measure_learned_scatter(lib, case, files, meas, K, Wm, esse_ms, torch):
+    """The same OSEM iteration with the learned scatter surrogate in place of
+    ESSE (IrlSetScatterSurrogate with the committed weights): device time per
+    iteration after the first iteration (ESSE on every view + the per-view
+    NRMSE check), the per-view NRMSE against ESSE, and the image NRMSE of a
+    10-iteration reconstruction against the ESSE one; the ablation is the
+    reconstruction without scatter modelling."""
+    from libirl_b200 import api
+    from libirl_b200 import surrogate as SU
+    wfile = SU.DEFAULT_WEIGHTS
+    if not os.path.exists(wfile):
+        return {"unavailable": "no trained weights (libirl_b200/surrogate/sur128.bin)"}
+    lib.IrlSetScatterSurrogate(wfile.encode(), 0.02)
+    try:
+        p, o, v = case.parms(), case.options(), case.views()
+        p.NumIterations = 1 + Wm + K
+        p.iNumSrfIterations = p.NumIterations
+        atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+        rc = lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(),
+                              None, api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+        if rc:
+            raise RuntimeError(lib.pchIrlErrorString().decode())
+        try:
+            lib.IrlOsemIterate(1 + Wm)
+            nr = np.zeros(case.nviews, np.float32)
+            lib.IrlGetScatterSurrogateNrmse(api.fptr(nr), case.nviews)
+            stream = torch.cuda.ExternalStream(lib.irlcu_stream())
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.IrlOsemIterate(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rc:
+                raise RuntimeError(lib.pchIrlErrorString().decode())
+            ms = e0.elapsed_time(e1) / K
+        finally:
+            lib.IrlOsemEnd(None)
+        sur_img = _osem_image(lib, case, files, meas, 10)
+    finally:
+        lib.IrlSetScatterSurrogate(None, 0.0)
+    esse_img = _osem_image(lib, case, files, meas, 10)
+    none_img = _osem_image(lib, case, files, meas, 10, srf_iters=0)
+    ref = np.linalg.norm(esse_img)
+    return {
+        "ms_per_iteration": round(ms, 3), "esse_ms_per_iteration": round(esse_ms, 3),
+        "speedup_vs_esse": round(esse_ms / ms, 3) if ms > 0 else None,
+        "image_nrmse_vs_esse": round(float(np.linalg.norm(sur_img - esse_img) / ref), 5),
+        "image_nrmse_no_scatter_vs_esse": round(float(np.linalg.norm(none_img - esse_img) / ref), 5),
+        "views_on_esse": int((nr > 0.02).sum()),
+        "view_nrmse": {"mean": round(float(nr.mean()), 5), "median": round(float(np.median(nr)), 5),
+                       "max": round(float(nr.max()), 5)},
+        "nrmse": "||x - x_ESSE|| / ||x_ESSE||; per view on the scatter projection after iteration 1",
+        "reconstruction": "config-2 data, 10 iterations, scatter model in all of them",
+    }
 
 
 def _message_phases(path):
@@ -460,6 +536,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
     # reduced variants for profiling captures (the bench line uses the defaults)
     ap.add_argument("--nviews", type=int, default=120)
     ap.add_argument("--subsets", type=int, default=8)

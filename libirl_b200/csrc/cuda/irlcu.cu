@@ -129,6 +129,7 @@ static void free_ctx(Ctx *c) {
   cudaStreamSynchronize(c->st);
   graphs_clear(*c);
   dfree(c->sur_scale);
+  dfree(c->sur_work);
   dfree(c->dviews_all);
   dfree(c->dvp_all);
   dfree(c->rot.hdr);
@@ -575,7 +576,7 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
       CU_TRY(cudaMemcpyAsync(out_nosrf, out, sizeof(float) * c.pln * nv, cudaMemcpyDeviceToDevice, c.st));
     Stage s(IRLCU_ST_ESSE, c.st);
     TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, c.sur_scale,
-                          sur_input(c.sur)));
+                          sur_input(c.sur), c.sur_work));
     const float *y = nullptr;
     TRY(sur_infer(c.sur, c.st, nv, &y));
     return launch_scale_views(c.st, y, c.sur_scale, out, (int)c.pln, nv, 1);
@@ -778,6 +779,13 @@ int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mod
 
 // ------------------------------------------------ learned scatter surrogate
 
+// pooling work buffer of max_batch views
+static int sur_work_ensure(Ctx &c) {
+  if (c.sur_work) return IRLCU_OK;
+  const size_t P = (size_t)(c.n / 4) * (c.n / 4) * (c.n / 4);
+  return dalloc(&c.sur_work, (size_t)c.g.max_batch * (P + SUR_POOL_PARTS));
+}
+
 static int sur_geometry(const Ctx &c, irlcu_sur *net, int model) {
   if (!net) return set_error(IRLCU_EARG, "surrogate: null network");
   if (c.n != 128 || c.nz != 128)
@@ -808,7 +816,8 @@ int irlcu_sur_pairs(int nv, const int *views, int model, void *x_out, float *t_o
     return set_error(IRLCU_ESTATE, "surrogate pairs: ESSE is not set up");
   TRY(upload_views(views, nv, nullptr));
   TRY(esse_scatter(c, nv, views, model, c.wprj));
-  TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, scale_out, x_out));
+  TRY(sur_work_ensure(c));
+  TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, scale_out, x_out, c.sur_work));
   TRY(launch_div_views(c.st, c.wprj, scale_out, t_out, (int)c.pln, nv));
   CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
@@ -819,6 +828,7 @@ int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *
   Ctx &c = *g_ctx;
   TRY(sur_geometry(c, net, model));
   const int B = std::min(sur_max_batch(net), c.g.max_batch);
+  TRY(sur_work_ensure(c));
   float *scale = nullptr;
   TRY(dalloc(&scale, (size_t)B));
   std::vector<float> y(c.pln * B), t(c.pln * B);
@@ -827,7 +837,8 @@ int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *
     const int nb = std::min(B, nv - v0);
     if ((rc = upload_views(views + v0, nb, nullptr))) break;
     if ((rc = esse_scatter(c, nb, views + v0, model, c.wprj))) break;
-    if ((rc = launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nb, c.n, c.vox, scale, sur_input(net))))
+    if ((rc = launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nb, c.n, c.vox, scale, sur_input(net),
+                                c.sur_work)))
       break;
     const float *yd = nullptr;
     if ((rc = sur_infer(net, c.st, nb, &yd))) break;
@@ -866,6 +877,7 @@ int irlcu_set_surrogate(irlcu_sur *net, const unsigned char *flags) {
     return set_error(IRLCU_EARG, "surrogate: network batch %d below the context's %d", sur_max_batch(net),
                      c.g.max_batch);
   if (!c.sur_scale) TRY(dalloc(&c.sur_scale, (size_t)c.g.max_batch));
+  TRY(sur_work_ensure(c));
   c.sur = net;
   if (flags)
     c.sur_flags.assign(flags, flags + c.nv);

@@ -143,6 +143,7 @@ struct Ctx {
   irlcu_sur *sur = nullptr;
   std::vector<unsigned char> sur_flags;   // per view: 1 = ESSE for that view
   float *sur_scale = nullptr;             // max_batch activity means
+  float *sur_work = nullptr;              // pooling work of max_batch views
   // three-shear intermediate for slices beyond shared memory, grown on use
   mutable float *xscratch = nullptr;
   mutable size_t xscratch_elems = 0;
@@ -221,8 +222,10 @@ int launch_norm_planes(const Ctx &c, const int *dviews, const float *vt_dev, int
 int sur_max_batch(const irlcu_sur *s);
 void *sur_input(irlcu_sur *s);
 int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y);
+// work: nv * ((n/4)^3 + SUR_POOL_PARTS) floats
+constexpr int SUR_POOL_PARTS = 128;
 int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
-                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out);
+                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out, float *work);
 int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size_t n);
 int launch_scale_views(cudaStream_t st, const float *x, const float *s, float *y, int P, int nb, int accumulate);
 int launch_div_views(cudaStream_t st, const float *a, const float *s, float *out, int P, int nb);

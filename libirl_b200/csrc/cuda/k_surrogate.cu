@@ -17,11 +17,13 @@
 //   D3 conv2d 128->64  k3 + ReLU, x2                    [64][64][64]
 //   D4 conv2d 64->32   k3 + ReLU, x2                    [128][128][32]
 //   D5 conv2d 32->1    k3 (linear)                      [128][128]
-// 1,653,153 parameters.  Every convolution is an explicit im2col followed by
-// a BF16 tensor-core GEMM (mma.sync m16n8k16, FP32 accumulate) with the bias
-// and ReLU in its epilogue; backward uses the same GEMM for the weight and
-// input gradients (split over K where the reduction is long, summed in a
-// fixed order) and a gather-form col2im, so results are deterministic.
+// 1,653,153 parameters.  Every convolution is a BF16 tensor-core GEMM
+// (mma.sync m16n8k16, FP32 accumulate) with the bias and ReLU in its
+// epilogue: forward as an implicit GEMM that reads the channels-last input
+// directly; backward on explicit im2col columns for the weight gradient and
+// the input-gradient columns, folded back by a gather-form col2im.  Long
+// reductions are split over K and summed in a fixed order, so results are
+// deterministic.
 // Training: Adam on FP32 master weights, BF16 copies for the GEMMs.
 #include <algorithm>
 #include <cmath>
@@ -37,6 +39,22 @@
 namespace irlcu {
 
 typedef __nv_bfloat16 bf16;
+
+// activations are channels-last: [b][d][h][w][c]; 2D layers use d = 1.
+struct ConvGeom {
+  int b, di, hi, wi, ci;   // input (hi, wi: after the optional upsampling)
+  int kd, kh, kw, s;       // kernel (odd sides, "same" padding k/2), stride
+  int dout, hout, wout, co;
+  int up;                  // 1: the input is the x2 nearest upsampling of a
+                           // stored [b][di][hi/2][wi/2][ci] tensor
+};
+
+// element offset of input (b, id, ih, iw, c), upsampling folded in
+__device__ __forceinline__ size_t in_off(const ConvGeom &g, int b, int id, int ih, int iw, int c) {
+  const int ph = g.up ? ih >> 1 : ih, pw = g.up ? iw >> 1 : iw;
+  const int H = g.up ? g.hi >> 1 : g.hi, Wd = g.up ? g.wi >> 1 : g.wi;
+  return ((((size_t)b * g.di + id) * H + ph) * Wd + pw) * g.ci + c;
+}
 
 // ------------------------------------------------------------------ GEMM
 // C(m, n) = sum_k A(m, k) B(k, n) over BF16 operands with FP32
@@ -164,6 +182,124 @@ __global__ void __launch_bounds__(GNT) k_gemm_bf16(GemmArgs a) {
       }
 }
 
+// Convolution as an implicit GEMM (forward): C(m, n) = sum_k A(m, k) W[n][k]
+// with A(m, k) read straight from the channels-last input, m = output
+// position (b, od, oh, ow), k = tap*ci + c.  The CTA's 64 output positions
+// are decoded once into shared memory; with ci a multiple of 8 every
+// 8-wide k chunk is one tap's contiguous channels (a 16-byte load).
+template <bool VEC>
+__global__ void __launch_bounds__(GNT) k_conv_gemm(GemmArgs a, ConvGeom g, const bf16 *__restrict__ X) {
+  __shared__ __align__(16) bf16 As[GBM][GBK + GPAD];
+  __shared__ __align__(16) bf16 Bs[GBN][GBK + GPAD];
+  __shared__ int rb[GBM], rd[GBM], rh[GBM], rw[GBM];
+  const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int gq = lane >> 2, t = lane & 3;
+  if (threadIdx.x < GBM) {
+    const int m = m0 + threadIdx.x;
+    if (m < a.M) {
+      int r = m;
+      const int ow = r % g.wout; r /= g.wout;
+      const int oh = r % g.hout; r /= g.hout;
+      const int od = r % g.dout;
+      rb[threadIdx.x] = r / g.dout;
+      rd[threadIdx.x] = od * g.s - g.kd / 2;
+      rh[threadIdx.x] = oh * g.s - g.kh / 2;
+      rw[threadIdx.x] = ow * g.s - g.kw / 2;
+    } else {
+      rb[threadIdx.x] = -1;
+    }
+  }
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+  const int kb = a.splits > 1 ? blockIdx.z * a.kper : 0;
+  const int ke = a.splits > 1 ? min(a.K, kb + a.kper) : a.K;
+  const int khw = g.kh * g.kw;
+  for (int k0 = kb; k0 < ke; k0 += GBK) {
+    __syncthreads();
+    if (VEC) {
+      for (int e = threadIdx.x; e < GBM * (GBK / 8); e += GNT) {
+        const int r = e / (GBK / 8), kk = (e % (GBK / 8)) * 8, k = k0 + kk;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        const int b = rb[r];
+        if (b >= 0 && k < ke) {
+          const int tap = k / g.ci, c = k - tap * g.ci;
+          const int td = tap / khw, th = (tap - td * khw) / g.kw, tw = tap - td * khw - th * g.kw;
+          const int id = rd[r] + td, ih = rh[r] + th, iw = rw[r] + tw;
+          if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
+            v = *reinterpret_cast<const uint4 *>(X + in_off(g, b, id, ih, iw, c));
+        }
+        *reinterpret_cast<uint4 *>(&As[r][kk]) = v;
+      }
+    } else {
+      const bf16 zero = __float2bfloat16(0.f);
+      for (int e = threadIdx.x; e < GBM * GBK; e += GNT) {
+        const int r = e / GBK, kk = e % GBK, k = k0 + kk;
+        bf16 v = zero;
+        const int b = rb[r];
+        if (b >= 0 && k < ke) {
+          const int tap = k / g.ci, c = k - tap * g.ci;
+          const int td = tap / khw, th = (tap - td * khw) / g.kw, tw = tap - td * khw - th * g.kw;
+          const int id = rd[r] + td, ih = rh[r] + th, iw = rw[r] + tw;
+          if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
+            v = X[in_off(g, b, id, ih, iw, c)];
+        }
+        As[r][kk] = v;
+      }
+    }
+    load_tile(Bs, a.B, a.sbn, a.sbk, n0, k0, a.N, ke);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 16) {
+      uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + gq;
+        af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t]);
+        af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t]);
+        af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * t + 8]);
+        af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = wn + j * 8 + gq;
+        bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][kk + 2 * t]);
+        bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm + i * 16 + gq + (q >= 2 ? 8 : 0);
+        const int n = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if (m >= a.M || n >= a.N) continue;
+        float v = acc[i][j][q];
+        if (a.splits > 1) {
+          a.ws[((size_t)blockIdx.z * a.M + m) * a.N + n] = v;
+          continue;
+        }
+        if (a.bias) v += a.bias[n];
+        if (a.relu) v = fmaxf(v, 0.f);
+        const long long o = (long long)m * a.scm + (long long)n * a.scn;
+        if (a.Cf) a.Cf[o] = v;
+        if (a.Cb) a.Cb[o] = __float2bfloat16(v);
+      }
+}
+
 __global__ void k_splitk_reduce(GemmArgs a) {
   const size_t tot = (size_t)a.M * a.N;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
@@ -181,7 +317,7 @@ __global__ void k_splitk_reduce(GemmArgs a) {
 // split-K workspace of a network (FP32 elements)
 constexpr size_t GEMM_WS_ELEMS = (size_t)16 << 20;
 
-static int gemm(cudaStream_t st, GemmArgs a, float *ws) {
+static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = nullptr, const bf16 *X = nullptr) {
   if (a.M <= 0 || a.N <= 0 || a.K <= 0) return IRLCU_OK;
   const int tiles_m = (a.M + GBM - 1) / GBM, tiles_n = (a.N + GBN - 1) / GBN;
   if (tiles_m > 65535) return set_error(IRLCU_EARG, "GEMM with M = %d too large", a.M);
@@ -198,7 +334,14 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws) {
     a.ws = ws;
   }
   const dim3 grid(tiles_n, tiles_m, a.splits);
-  k_gemm_bf16<<<grid, GNT, 0, st>>>(a);
+  if (conv) {
+    if (conv->ci % 8 == 0 && ((uintptr_t)X & 15) == 0)
+      k_conv_gemm<true><<<grid, GNT, 0, st>>>(a, *conv, X);
+    else
+      k_conv_gemm<false><<<grid, GNT, 0, st>>>(a, *conv, X);
+  } else {
+    k_gemm_bf16<<<grid, GNT, 0, st>>>(a);
+  }
   CU_LAUNCHED();
   if (a.splits > 1) {
     const size_t tot = (size_t)a.M * a.N;
@@ -209,12 +352,6 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws) {
 }
 
 // ---------------------------------------------------------- conv helpers
-// activations are channels-last: [b][d][h][w][c]; 2D layers use d = 1.
-struct ConvGeom {
-  int b, di, hi, wi, ci;   // input
-  int kd, kh, kw, s;       // kernel (odd sides, "same" padding k/2), stride
-  int dout, hout, wout, co;
-};
 
 __host__ __device__ inline int conv_out(int in, int k, int s) { return (in + 2 * (k / 2) - k) / s + 1; }
 
@@ -239,7 +376,7 @@ __global__ void k_im2col(ConvGeom g, const bf16 *__restrict__ x, bf16 *__restric
     const int id = od * g.s + td - g.kd / 2, ih = oh * g.s + th - g.kh / 2, iw = ow * g.s + tw - g.kw / 2;
     bf16 v = zero;
     if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
-      v = x[((((long long)b * g.di + id) * g.hi + ih) * g.wi + iw) * g.ci + c];
+      v = x[in_off(g, b, id, ih, iw, c)];
     col[e] = v;
   }
 }
@@ -281,6 +418,84 @@ __global__ void k_col2im(ConvGeom g, const float *__restrict__ dcol, float *__re
     }
     dx[e] = s;
   }
+}
+
+// First layer (3 input channels) as a direct convolution: one thread per
+// output position, all 32 output channels in registers, FP32 products of the
+// BF16 weights and inputs; + bias, ReLU, BF16 store
+constexpr int FIRST_CI = 3, FIRST_CO = 32, FIRST_TAPS = 27;
+__global__ void __launch_bounds__(128) k_conv_first(ConvGeom g, const bf16 *__restrict__ x,
+                                                    const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                    bf16 *__restrict__ y) {
+  __shared__ float ws[FIRST_TAPS * FIRST_CI][FIRST_CO];
+  __shared__ float bs[FIRST_CO];
+  for (int e = threadIdx.x; e < FIRST_TAPS * FIRST_CI * FIRST_CO; e += blockDim.x) {
+    const int co = e / (FIRST_TAPS * FIRST_CI), k = e % (FIRST_TAPS * FIRST_CI);
+    ws[k][co] = __bfloat162float(w[e]);
+  }
+  if (threadIdx.x < FIRST_CO) bs[threadIdx.x] = bias[threadIdx.x];
+  __syncthreads();
+  const long long M = (long long)g.b * g.dout * g.hout * g.wout;
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  long long r = m;
+  const int ow = (int)(r % g.wout); r /= g.wout;
+  const int oh = (int)(r % g.hout); r /= g.hout;
+  const int od = (int)(r % g.dout);
+  const int b = (int)(r / g.dout);
+  float acc[FIRST_CO];
+#pragma unroll
+  for (int co = 0; co < FIRST_CO; ++co) acc[co] = bs[co];
+  for (int tap = 0; tap < FIRST_TAPS; ++tap) {
+    const int td = tap / 9, th = (tap / 3) % 3, tw = tap % 3;
+    const int id = od * g.s + td - 1, ih = oh * g.s + th - 1, iw = ow * g.s + tw - 1;
+    if (id < 0 || id >= g.di || ih < 0 || ih >= g.hi || iw < 0 || iw >= g.wi) continue;
+    const bf16 *px = x + in_off(g, b, id, ih, iw, 0);
+#pragma unroll
+    for (int c = 0; c < FIRST_CI; ++c) {
+      const float v = __bfloat162float(px[c]);
+      const float *wr = ws[tap * FIRST_CI + c];
+#pragma unroll
+      for (int co = 0; co < FIRST_CO; ++co) acc[co] = fmaf(wr[co], v, acc[co]);
+    }
+  }
+  uint4 *o = reinterpret_cast<uint4 *>(y + m * FIRST_CO);
+#pragma unroll
+  for (int q = 0; q < FIRST_CO / 8; ++q) {
+    __align__(16) bf16 h[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) h[j] = __float2bfloat16(fmaxf(acc[q * 8 + j], 0.f));
+    o[q] = *reinterpret_cast<const uint4 *>(h);
+  }
+}
+
+// Last layer (one output channel, 2D, input 32 channels) as a direct
+// convolution: one thread per output pixel, FP32 output
+constexpr int LAST_CI = 32;
+__global__ void __launch_bounds__(256) k_conv_last(ConvGeom g, const bf16 *__restrict__ x,
+                                                   const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                   float *__restrict__ y) {
+  __shared__ float ws[9 * LAST_CI];
+  for (int e = threadIdx.x; e < 9 * LAST_CI; e += blockDim.x) ws[e] = __bfloat162float(w[e]);
+  __syncthreads();
+  const long long M = (long long)g.b * g.hout * g.wout;
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  const int ow = (int)(m % g.wout), oh = (int)((m / g.wout) % g.hout), b = (int)(m / ((long long)g.wout * g.hout));
+  float acc = bias[0];
+  for (int tap = 0; tap < 9; ++tap) {
+    const int ih = oh + tap / 3 - 1, iw = ow + tap % 3 - 1;
+    if (ih < 0 || ih >= g.hi || iw < 0 || iw >= g.wi) continue;
+    const uint4 *px = reinterpret_cast<const uint4 *>(x + in_off(g, b, 0, ih, iw, 0));
+#pragma unroll
+    for (int q = 0; q < LAST_CI / 8; ++q) {
+      const uint4 u = px[q];
+      const bf16 *h = reinterpret_cast<const bf16 *>(&u);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc = fmaf(ws[tap * LAST_CI + q * 8 + j], __bfloat162float(h[j]), acc);
+    }
+  }
+  y[m] = acc;
 }
 
 // gradient through ReLU: g = dy * (y > 0), to BF16 for the next GEMMs
@@ -409,52 +624,67 @@ __global__ void k_to_bf16(const float *__restrict__ x, bf16 *__restrict__ y, lon
     y[e] = __float2bfloat16(x[e]);
 }
 
-// network input from the rotated volumes of a batch: 4x4x4 means of the
-// activity / s, mu * 10 (per pixel -> order 1) and exp(-S), channels last;
-// s = scale[b], the view's mean activity
-__global__ void k_pool_inputs(const float *__restrict__ act, size_t act_stride, const float *__restrict__ mu,
-                              const float *__restrict__ S, const int *__restrict__ views, size_t vox, int n,
-                              const float *__restrict__ scale, bf16 *__restrict__ out) {
+// Network input from the rotated volumes of a batch, channels last: 4x4x4
+// means of the activity / s, of mu * 10 (per pixel -> order 1) and of
+// exp(-S); s = the view's mean activity.  Pass 1 writes the mu and depth
+// channels, the pooled activity means (pa) and one partial sum of them per
+// CTA; pass 2 forms s from the partial sums (fixed order) and writes the
+// normalised activity channel.
+constexpr int POOL_NT = 256;
+__global__ void __launch_bounds__(POOL_NT) k_pool_inputs(const float *__restrict__ act, size_t act_stride,
+                                                         const float *__restrict__ mu, const float *__restrict__ S,
+                                                         const int *__restrict__ views, size_t vox, int n,
+                                                         float *__restrict__ pa, float *__restrict__ part,
+                                                         bf16 *__restrict__ out) {
   const int P = n / 4;
-  const long long tot = (long long)P * P * P;
+  const int tot = P * P * P;
   const int b = blockIdx.y;
   const int view = views[b];
-  const float inv_s = scale[b] > 0.f ? 1.f / scale[b] : 0.f;
   const float *a = act + (size_t)b * act_stride;
   const float *m = mu + (size_t)view * vox;
   const float *sd = S + (size_t)view * vox;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int px = (int)(e % P), pz = (int)((e / P) % P), py = (int)(e / ((long long)P * P));
+  __shared__ float red[POOL_NT];
+  float psum = 0.f;
+  for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
+    const int px = e % P, pz = (e / P) % P, py = e / (P * P);
     float sa = 0.f, sm = 0.f, se = 0.f;
     for (int dy = 0; dy < 4; ++dy)
-      for (int dz = 0; dz < 4; ++dz)
-        for (int dx = 0; dx < 4; ++dx) {
-          const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px + dx;
-          sa += a[i];
-          sm += m[i];
-          se += __expf(-sd[i]);
-        }
+      for (int dz = 0; dz < 4; ++dz) {
+        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
+        const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
+        const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
+        const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
+        sa += (va.x + va.y) + (va.z + va.w);
+        sm += (vm.x + vm.y) + (vm.z + vm.w);
+        se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
+      }
+    const float mean_a = sa * (1.f / 64.f);
+    pa[(size_t)b * tot + e] = mean_a;
+    psum += mean_a;
     bf16 *o = out + ((size_t)b * tot + e) * 3;
-    o[0] = __float2bfloat16(sa * (1.f / 64.f) * inv_s);
     o[1] = __float2bfloat16(sm * (10.f / 64.f));
     o[2] = __float2bfloat16(se * (1.f / 64.f));
   }
-}
-
-// mean of each view's rotated activity (the input / target normalisation)
-__global__ void k_view_mean(const float *__restrict__ act, size_t stride, size_t vox, float *__restrict__ mean) {
-  const int b = blockIdx.x;
-  __shared__ double red[256];
-  double s = 0.0;
-  for (size_t i = threadIdx.x; i < vox; i += blockDim.x) s += act[(size_t)b * stride + i];
-  red[threadIdx.x] = s;
+  red[threadIdx.x] = psum;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (int w = POOL_NT / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) mean[b] = (float)(red[0] / (double)vox);
+  if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(POOL_NT) k_pool_normalise(const float *__restrict__ pa,
+                                                            const float *__restrict__ part, int nparts, int tot,
+                                                            float *__restrict__ scale, bf16 *__restrict__ out) {
+  const int b = blockIdx.y;
+  float s = 0.f;
+  for (int j = 0; j < nparts; ++j) s += part[(size_t)b * nparts + j];
+  s /= (float)tot;
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[b] = s;
+  const float inv = s > 0.f ? 1.f / s : 0.f;
+  for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT)
+    out[((size_t)b * tot + e) * 3] = __float2bfloat16(pa[(size_t)b * tot + e] * inv);
 }
 
 // out = a - c, elementwise
@@ -504,9 +734,9 @@ struct irlcu_sur {
   float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // FP32 master, gradient, Adam moments
   irlcu::bf16 *wb = nullptr;                                     // BF16 weights
   long long step = 0;
-  // act[0] = input, act[i+1] = output of layer i after ReLU (before any
-  // upsampling); upa[i] its upsampled copy; fold = E3 output, depth folded
-  std::vector<irlcu::bf16 *> act, upa;
+  // act[0] = input, act[i+1] = output of layer i after ReLU (the next layer
+  // reads it upsampled where it is); fold = E3 output, depth folded
+  std::vector<irlcu::bf16 *> act;
   irlcu::bf16 *fold = nullptr;
   irlcu::bf16 *col = nullptr;     // im2col buffer (largest layer)
   float *dcol = nullptr;          // input-gradient columns
@@ -550,6 +780,7 @@ static void build_layers(irlcu_sur &s) {
     l.g.co = p.co;
     l.relu = p.relu;
     l.up = p.up;
+    l.g.up = (!s.L.empty() && s.L.back().up) ? 1 : 0;
     l.K = (long long)l.g.kd * 9 * p.ci;
     l.woff = off;
     off += (size_t)l.K * p.co;
@@ -601,7 +832,6 @@ static void sur_free(irlcu_sur *s) {
   cudaFree(s->v);
   cudaFree(s->wb);
   for (auto p : s->act) cudaFree(p);
-  for (auto p : s->upa) cudaFree(p);
   cudaFree(s->fold);
   cudaFree(s->col);
   cudaFree(s->dcol);
@@ -625,8 +855,7 @@ static void sur_free(irlcu_sur *s) {
 // input of layer i as im2col sees it
 static const bf16 *layer_input(const irlcu_sur &s, int i) {
   if (i == 3) return s.fold;
-  if (i > 3 && s.L[i - 1].up) return s.upa[i - 1];
-  return s.act[i];
+  return s.act[i];  // layers after an upsampling read it through ConvGeom::up
 }
 
 // forward over the B samples in act[0]; FP32 output [B][128*128] in s.out
@@ -642,12 +871,19 @@ static int sur_forward(irlcu_sur &s, int B) {
       CU_LAUNCHED();
     }
     const long long M = (long long)B * l.g.dout * l.g.hout * l.g.wout;
-    k_im2col<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
-    CU_LAUNCHED();
-    GemmArgs a{};
-    a.A = s.col;
-    a.sam = l.K;
-    a.sak = 1;
+    if (i == 0 && l.g.ci == FIRST_CI && l.g.co == FIRST_CO && l.g.kd == 3) {
+      k_conv_first<<<(unsigned)((M + 127) / 128), 128, 0, s.st>>>(l.g, s.act[0], s.wb + l.woff, s.w + l.boff,
+                                                                 s.act[1]);
+      CU_LAUNCHED();
+      continue;
+    }
+    if (i == nl - 1 && l.g.co == 1 && l.g.ci == LAST_CI && l.g.kd == 1) {
+      k_conv_last<<<(unsigned)((M + 255) / 256), 256, 0, s.st>>>(l.g, layer_input(s, i), s.wb + l.woff,
+                                                                 s.w + l.boff, s.out);
+      CU_LAUNCHED();
+      continue;
+    }
+    GemmArgs a{};  // A read straight from the layer input (implicit im2col)
     a.B = s.wb + l.woff;  // weights [co][K]: B(k, n) = W[n*K + k]
     a.sbk = 1;
     a.sbn = l.K;
@@ -662,12 +898,7 @@ static int sur_forward(irlcu_sur &s, int B) {
       a.Cb = s.act[i + 1];
     a.scm = l.g.co;
     a.scn = 1;
-    STRY(gemm(s.st, a, s.ws));
-    if (l.up) {
-      k_up2<<<grid_for((long long)layer_out_elems(l, B) * 4), 256, 0, s.st>>>(s.act[i + 1], s.upa[i], B, l.g.hout,
-                                                                               l.g.wout, l.g.co);
-      CU_LAUNCHED();
-    }
+    STRY(gemm(s.st, a, s.ws, &l.g, layer_input(s, i)));
   }
   return IRLCU_OK;
 }
@@ -780,12 +1011,14 @@ int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y) {
 // pooled network inputs of nv rotated volumes (act, stride act_stride) with
 // the per-view mu and depth tables; the activity means go to scale
 int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
-                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out) {
-  k_view_mean<<<nv, 256, 0, st>>>(act, act_stride, vox, scale);
+                      const int *dviews, int nv, int n, size_t vox, float *scale, void *out, float *work) {
+  const int P = n / 4, tot = P * P * P;
+  const int nparts = SUR_POOL_PARTS;
+  float *pa = work, *part = work + (size_t)nv * tot;
+  dim3 grid(nparts, nv);
+  k_pool_inputs<<<grid, POOL_NT, 0, st>>>(act, act_stride, mu, S, dviews, vox, n, pa, part, static_cast<bf16 *>(out));
   CU_LAUNCHED();
-  const long long P3 = (long long)(n / 4) * (n / 4) * (n / 4);
-  dim3 grid((unsigned)std::min<long long>((P3 + 255) / 256, 1024), nv);
-  k_pool_inputs<<<grid, 256, 0, st>>>(act, act_stride, mu, S, dviews, vox, n, scale, static_cast<bf16 *>(out));
+  k_pool_normalise<<<grid, POOL_NT, 0, st>>>(pa, part, nparts, tot, scale, static_cast<bf16 *>(out));
   CU_LAUNCHED();
   return IRLCU_OK;
 }
@@ -835,7 +1068,6 @@ int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
   const int B = max_batch;
   size_t colmax = 0, actmax = 0;
   s->act.assign(s->L.size() + 1, nullptr);
-  s->upa.assign(s->L.size(), nullptr);
   for (size_t i = 0; i < s->L.size(); ++i) {
     const Layer &l = s->L[i];
     const size_t M = (size_t)B * l.g.dout * l.g.hout * l.g.wout;
@@ -843,10 +1075,7 @@ int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
     actmax = std::max(actmax, std::max(layer_in_elems(l, B), layer_out_elems(l, B)));
     if (i == 0 && (rc = dmalloc(&s->act[0], layer_in_elems(l, B)))) return fail(rc);
     if ((rc = dmalloc(&s->act[i + 1], layer_out_elems(l, B)))) return fail(rc);
-    if (l.up) {
-      if ((rc = dmalloc(&s->upa[i], layer_out_elems(l, B) * 4))) return fail(rc);
-      actmax = std::max(actmax, layer_out_elems(l, B) * 4);
-    }
+    if (l.up) actmax = std::max(actmax, layer_out_elems(l, B) * 4);
   }
   if ((rc = dmalloc(&s->fold, layer_out_elems(s->L[2], B))) || (rc = dmalloc(&s->col, colmax)) ||
       (rc = dmalloc(&s->dcol, colmax)) || (rc = dmalloc(&s->gf, actmax)) || (rc = dmalloc(&s->gf2, actmax)) ||
