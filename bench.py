@@ -528,6 +528,144 @@ def run_reference(args):
     }))
 
 
+# ------------------------------------------------- further workloads (manual)
+
+def _genprj(lib, case, files, primary=1.0, fft=False):
+    from libirl_b200 import api
+    p, o, v = case.parms(), case.options(), case.views()
+    if fft:
+        o.bFFTConvolve = 1
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    rc = lib.IrlGenprj(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), None, None,
+                       api.fptr(act), api.fptr(atn), api.fptr(prj), primary, None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    return prj
+
+
+def run_batch32(args):
+    """Config 3: 32 seeded problems of uneven size (N 64..128, 60..120
+    views, 4..12 subsets, DRF + ESSE), 5 iterations each: IrlOsemBatch
+    against the same 32 IrlOsem calls one after another, wall time, after
+    one untimed batch pass (table autotuning and module loading)."""
+    import torch  # noqa: F401  (CUDA context for the library)
+    import libirl_b200 as L
+    from libirl_b200 import api, workloads as W
+    lib = L.load()
+    tmp = tempfile.mkdtemp(prefix="irlbatch_")
+    cases = W.batch32(iterations=5)
+    data = []
+    for j, case in enumerate(cases):
+        files = case.write_tables(os.path.join(tmp, f"c{j}"))
+        meas = W.poisson_counts(_genprj(lib, case, files), case.counts, 3000 + j)
+        data.append((case, files, meas))
+
+    def batch(iters=None):
+        probs = (api.OsemProblem * len(data))()
+        keep = []
+        for q, (case, files, meas) in zip(probs, data):
+            p, o, v = case.parms(), case.options(), case.views()
+            if iters is not None:
+                p.NumIterations = iters
+            atn, prj, rec = case.atn.copy(), meas.copy(), np.zeros_like(case.act)
+            keep.append((p, o, v, atn, prj, rec))
+            q.psIrlParms, q.psOptions = C.pointer(p), C.pointer(o)
+            q.psViews = C.cast(v, C.POINTER(api.PrjView))
+            q.pchDrfTabFname = C.cast(_dup(files["drf"]), C.c_void_p)
+            q.pchScatKrnlFname = C.cast(_dup(files["krnl"]), C.c_void_p)
+            q.pfAtnMap, q.pfPrjImage, q.pfReconImage = api.fptr(atn), api.fptr(prj), api.fptr(rec)
+        t0 = time.perf_counter()
+        rc = lib.IrlOsemBatch(len(data), probs)
+        wall = time.perf_counter() - t0
+        if rc:
+            raise RuntimeError(lib.pchIrlErrorString().decode())
+        return wall, [k[5] for k in keep]
+
+    def sequential(iters=None):
+        out = []
+        t0 = time.perf_counter()
+        for case, files, meas in data:
+            out.append(_osem_image(lib, case, files, meas, iters or case.iterations))
+        return time.perf_counter() - t0, out
+
+    batch()
+    seq_s, seq_imgs = sequential()
+    bat_s, bat_imgs = batch()
+    same = all(np.array_equal(a, b) for a, b in zip(seq_imgs, bat_imgs))
+    iters = sum(c.iterations for c, _, _ in data)
+    # the iteration phase alone: 5 iterations minus 1 (set-up and the first
+    # iteration cancel)
+    seq1, _ = sequential(1)
+    bat1, _ = batch(1)
+    it_seq, it_bat = seq_s - seq1, bat_s - bat1
+    print(json.dumps({
+        "metric": "wall s for 32 uneven OSEM reconstructions (5 iterations each), 1 B200", "value": round(bat_s, 3),
+        "unit": "s", "n_gpus": 1, "higher_is_better": False, "impl": "b200 IrlOsemBatch",
+        "sequential_s": round(seq_s, 3), "speedup_vs_sequential": round(seq_s / bat_s, 3),
+        "ms_per_problem_iteration": round(1000 * bat_s / iters, 3), "identical_to_sequential": bool(same),
+        "iterations_2_to_5_s": {"batched": round(it_bat, 3), "sequential": round(it_seq, 3),
+                                "speedup": round(it_seq / it_bat, 3) if it_bat > 0 else None},
+        "config": {"workload": "batch32: " + ", ".join(f"{c.n}^3/{c.nviews}v/{c.subsets}s" for c, _, _ in data),
+                   "includes": "set-up (tables, norm images) and result copies of every problem"},
+        "data": "synthetic (seeded phantoms, Poisson data)"}))
+
+
+def run_large256(args):
+    """Config 5: 256^3, 128 views, 16 subsets, 65 x 65 DRF on libirl's FFT
+    convolution path, ESSE; IrlGenprj of the photopeak and the lower
+    (scatter-only, fPrimaryFac = 0) window, and OSEM iterations of the
+    photopeak window timed with CUDA events on the library stream."""
+    import torch
+    import libirl_b200 as L
+    from libirl_b200 import api, workloads as W
+    lib = L.load()
+    tmp = tempfile.mkdtemp(prefix="irl256_")
+    pp, lw = W.large256(window="photopeak"), W.large256(window="lower")
+    fpp, flw = pp.write_tables(os.path.join(tmp, "pp")), lw.write_tables(os.path.join(tmp, "lw"))
+    t0 = time.perf_counter()
+    prj = _genprj(lib, pp, fpp, 1.0, fft=True)
+    g_pp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _genprj(lib, lw, flw, 0.0, fft=True)
+    g_lw = time.perf_counter() - t0
+    meas = W.poisson_counts(prj, pp.counts, 5000)
+    K, Wm = max(1, min(args.steps, 5)), 1
+    p, o, v = pp.parms(), pp.options(), pp.views()
+    o.bFFTConvolve = 1
+    p.NumIterations = Wm + K
+    p.iNumSrfIterations = p.NumIterations
+    atn, rec, m = pp.atn.copy(), np.zeros_like(pp.act), meas.copy()
+    rc = lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(fpp["drf"]), _dup(fpp["krnl"]), api.ITER_CB(), None,
+                          api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    try:
+        grids = (C.c_int * 5)()
+        lib.irlcu_grids(grids)
+        lib.IrlOsemIterate(Wm)
+        stream = torch.cuda.ExternalStream(lib.irlcu_stream())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.IrlOsemIterate(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc:
+            raise RuntimeError(lib.pchIrlErrorString().decode())
+        ms = e0.elapsed_time(e1) / K
+    finally:
+        lib.IrlOsemEnd(api.fptr(rec))
+    print(json.dumps({
+        "metric": "ms per OSEM iteration, 256^3/128 views/16 subsets, 65x65 FFT DRF + ESSE, 1 B200",
+        "value": round(ms, 2), "unit": "ms", "n_gpus": 1, "steps": K, "warmup": Wm, "higher_is_better": False,
+        "genprj_s": {"photopeak": round(g_pp, 3), "lower_window": round(g_lw, 3)},
+        "image_finite": bool(np.all(np.isfinite(rec))),
+        "config": {"workload": "large256: 0.2 cm voxels, 28 cm circular orbit, 2e7 counts, collapse 2",
+                   "drf_grid": [grids[0], grids[1]], "esse_grid": [grids[2], grids[3], grids[4]]},
+        "data": "synthetic (seeded phantom, Poisson data)"}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -541,7 +679,13 @@ def main():
     ap.add_argument("--nviews", type=int, default=120)
     ap.add_argument("--subsets", type=int, default=8)
     ap.add_argument("--cpu-views", type=int, default=2)
+    ap.add_argument("--workload", default="full128", choices=["full128", "batch32", "large256"],
+                    help="full128 is the bench line; the others are measured by hand")
     args = ap.parse_args()
+    if args.workload == "batch32":
+        return run_batch32(args)
+    if args.workload == "large256":
+        return run_large256(args)
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":

@@ -253,14 +253,20 @@ def plain64(seed=1000, n=64, nviews=60, subsets=4, iterations=5):
 
 
 def full128(seed=2000, n=128, nz=None, nviews=120, subsets=8, iterations=10, collapse=2,
-            drf_max_offs=17, with_srf=True):
-    """The full-physics case (DRF + ESSE); n/nz/nviews may be reduced for tests."""
+            drf_max_offs=17, with_srf=True, pix=None, body_scale=None, orbit_radius=None, counts=5e6,
+            krnl_lens=(0.9, 4.0), name="full128"):
+    """The full-physics case (DRF + ESSE); n/nz/nviews may be reduced for tests.
+
+    Defaults give config 2: 0.3125 cm voxels at 128, the body scaled to a
+    40 cm field of view, the 22 x 18 cm elliptical orbit.  pix, body_scale
+    (cm per body unit), orbit_radius (a circular orbit) and krnl_lens (the
+    two scatter-kernel decay lengths) override them."""
     rng = np.random.default_rng(seed)
-    pix = 0.3125 * 128 / n
+    pix = 0.3125 * 128 / n if pix is None else pix
     nz = n if nz is None else nz
     X, Y, Z = _grid(n, nz, pix)
     fov = n * pix
-    s = fov / 40.0
+    s = fov / 40.0 if body_scale is None else body_scale
     body = _ellipsoid(X, Y, Z, (0, 0, 0), (17 * s, 12.5 * s, 0.6 * fov))
     act = np.zeros(X.shape, np.float32)
     act[body] = 0.5
@@ -281,7 +287,10 @@ def full128(seed=2000, n=128, nz=None, nviews=120, subsets=8, iterations=10, col
         atn[_ellipsoid(X, Y, Z, (sx * 6.5 * s, -1.0 * s, 0.0), (4.0 * s, 6.0 * s, 0.45 * fov)) & body] = 0.04
     atn[((X - 0.0) ** 2 + (Y - 8.0 * s) ** 2 <= (1.8 * s) ** 2) & body] = 0.25
     angles = 2 * np.pi * np.arange(nviews) / nviews
-    cfcr = np.sqrt((22 * s * np.cos(angles)) ** 2 + (18 * s * np.sin(angles)) ** 2)
+    if orbit_radius is None:
+        cfcr = np.sqrt((22 * s * np.cos(angles)) ** 2 + (18 * s * np.sin(angles)) ** 2)
+    else:
+        cfcr = np.full(nviews, float(orbit_radius))
     # distance range as libirl's psDrfSetup computes it (IrlSetup.c:538-540)
     dmin = float(cfcr.min()) - n // 2 * pix + pix / 2
     if dmin < 0:
@@ -294,11 +303,40 @@ def full128(seed=2000, n=128, nz=None, nviews=120, subsets=8, iterations=10, col
         kpix = pix * collapse
         noffs = max(8, int(round(10.0 / kpix)))
         ndists = 2 * noffs
-        k, kmu = esse_kernel(noffs, ndists, kpix)
+        k, kmu = esse_kernel(noffs, ndists, kpix, lens=krnl_lens)
         krnl = (k, kmu, 0.15, kpix)
-    return Case("full128", n, nz, pix, nviews, subsets, iterations, 5e6, act, atn,
+    return Case(name, n, nz, pix, nviews, subsets, iterations, counts, act, atn,
                 angles.astype(np.float32), cfcr.astype(np.float32), pix,
                 psfs, dmin, pix, krnl, collapse, iterations if with_srf else 0)
+
+
+def large256(seed=5000, window="photopeak", n=256, nviews=128, subsets=16, iterations=8):
+    """Config 5: 256^3 at 0.2 cm (51.2 cm field of view), 128 views on a
+    28 cm circular orbit, a 65 x 65 DRF (the FFT convolution path), ESSE
+    with c = 2, 2e7 counts.  window: "photopeak", or "lower" (a scatter
+    window with a broader kernel, projected with fPrimaryFac = 0)."""
+    lens = (0.9, 4.0) if window == "photopeak" else (1.6, 7.0)
+    return full128(seed=seed, n=n, nviews=nviews, subsets=subsets, iterations=iterations, collapse=2,
+                   drf_max_offs=33, pix=0.2, body_scale=1.0, orbit_radius=28.0, counts=2e7, krnl_lens=lens,
+                   name="large256_" + window)
+
+
+def batch32(seed0=3000, count=32, iterations=5):
+    """Config 3: independent problems of uneven size, each drawn from its own
+    seed: N in {64, 80, 96, 112, 128}, views in {60, 72, 90, 96, 120}, an
+    even number of subsets (4..12) that divides the views, DRF and ESSE on.
+    N is restricted to sides whose ESSE grid (N at c = 2) has factors 2, 3,
+    5, 7 only."""
+    rng = np.random.default_rng(seed0)
+    cases = []
+    for j in range(count):
+        n = int(rng.choice([64, 80, 96, 112, 128]))
+        nv = int(rng.choice([60, 72, 90, 96, 120]))
+        subs = [k for k in (4, 6, 8, 10, 12) if nv % k == 0]
+        ns = int(rng.choice(subs))
+        cases.append(full128(seed=seed0 + 1 + j, n=n, nviews=nv, subsets=ns, iterations=iterations,
+                             name=f"batch{j}"))
+    return cases
 
 
 def poisson_counts(prj, counts, seed):
