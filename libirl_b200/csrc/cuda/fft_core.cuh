@@ -132,23 +132,25 @@ template <>
 __device__ __forceinline__ void dft_r<7>(float2 *v, float s) { dft_odd<7>(v, s); }
 
 // one Stockham pass of radix R over W lines of length L held in shared
-// memory (element (w, i) at base[w*lstride + i])
-template <int L, int R>
-__device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int W, int lstride, int Ns,
-                                              const float2 *tw, float s) {
+// memory (element (w, i) at base[w*lstride + i]); NS, the length of the
+// sub-transforms already done, is a compile-time constant so that every
+// index division is by a constant
+template <int L, int R, int NS>
+__device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int W, int lstride, const float2 *tw,
+                                              float s) {
   constexpr int J = L / R;
+  constexpr int STEP = L / (NS * R);  // twiddle index stride; r*k*STEP < L
   const int jobs = W * J;
-  const int step = L / (Ns * R);  // twiddle index stride; r*k*step < L
   for (int q = threadIdx.x; q < jobs; q += blockDim.x) {
     const int w = q / J, j = q - w * J;
     const float2 *src = in + w * lstride;
     float2 v[R];
-    const int k = j % Ns;
+    const int k = j % NS;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       float2 x = src[j + r * J];
       if (r > 0 && k > 0) {
-        float2 t = tw[r * k * step];
+        float2 t = tw[r * k * STEP];
         t.y *= s;  // conjugate for the inverse
         x = cmul(x, t);
       }
@@ -156,44 +158,40 @@ __device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int
     }
     dft_r<R>(v, s);
     float2 *dst = out + w * lstride;
-    const int idxD = (j / Ns) * Ns * R + k;
+    const int idxD = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[idxD + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) dst[idxD + r * NS] = v[r];
   }
 }
+
+// radix of the next pass when rem = L / NS points remain: the largest
+// power-of-two radix first, then 5, 3, 7
+__host__ __device__ constexpr int next_radix(int rem) {
+  return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 5 == 0 ? 5 : rem % 3 == 0 ? 3 : 7;
+}
+
+template <int L, int NS>
+struct FftPlan {
+  static __device__ __forceinline__ void run(float2 *&in, float2 *&out, int W, int lstride, const float2 *tw,
+                                             float s) {
+    if constexpr (NS < L) {
+      constexpr int R = next_radix(L / NS);
+      stockham_pass<L, R, NS>(in, out, W, lstride, tw, s);
+      __syncthreads();
+      float2 *t = in;
+      in = out;
+      out = t;
+      FftPlan<L, NS * R>::run(in, out, W, lstride, tw, s);
+    }
+  }
+};
 
 // full transform of W lines; returns the buffer holding the result (a or b).
 // Ends with a barrier.
 template <int L>
 __device__ float2 *fft_lines(float2 *a, float2 *b, int W, int lstride, const float2 *tw, float s) {
-  int Ns = 1;
   float2 *in = a, *out = b;
-  while (Ns < L) {
-    const int rem = L / Ns;
-    if (rem % 8 == 0) {
-      stockham_pass<L, 8>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 8;
-    } else if (rem % 4 == 0) {
-      stockham_pass<L, 4>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 4;
-    } else if (rem % 2 == 0) {
-      stockham_pass<L, 2>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 2;
-    } else if (rem % 5 == 0) {
-      stockham_pass<L, 5>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 5;
-    } else if (rem % 3 == 0) {
-      stockham_pass<L, 3>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 3;
-    } else {
-      stockham_pass<L, 7>(in, out, W, lstride, Ns, tw, s);
-      Ns *= 7;
-    }
-    __syncthreads();
-    float2 *t = in;
-    in = out;
-    out = t;
-  }
+  FftPlan<L, 1>::run(in, out, W, lstride, tw, s);
   return in;
 }
 

@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_rows_fwd(RowSrc a, const float2 
   } else if (y < a.ndist) {
     psf = a.psf + (size_t)y * (2 * a.h + 1) * a.pstride;
   }
+#pragma unroll 4
   for (int e = threadIdx.x; e < PR * L; e += FT_NT) {
     const int w = e / L, x = e - w * L;
     float v[2] = {0.f, 0.f};
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_rows_fwd(RowSrc a, const float2 
   // two real rows from one complex line: A = (Z[k] + conj Z[L-k]) / 2,
   // B = (Z[k] - conj Z[L-k]) / 2i
   const int Mxh = a.Mxh;
+#pragma unroll 4
   for (int e = threadIdx.x; e < PR * Mxh; e += FT_NT) {
     const int w = e / Mxh, k = e - w * Mxh;
     const int g = g0 + 2 * w;
@@ -185,6 +187,7 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_rows_inv(RowInv a, const float2 
   const int Mxh = a.Mxh, nz = a.nz;
   const size_t rbase = ((size_t)b * a.np + p) * a.rs + a.r0;
   // Z = A + iB from the half spectra of rows z (A) and z+1 (B)
+#pragma unroll 4
   for (int e = threadIdx.x; e < PR * Mxh; e += FT_NT) {
     const int w = e / Mxh, k = e - w * Mxh;
     const int z = z0 + 2 * w;
@@ -213,6 +216,7 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_rows_inv(RowInv a, const float2 
 template <int L>
 __device__ __forceinline__ void load_cols(float2 *s, const float2 *src, int k0, int Mxh, int valid) {
   constexpr int CK = col_chunk<L>(), LS = L + 1;
+#pragma unroll 4
   for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
     const int c = e % CK, g = e / CK, k = k0 + c;
     s[c * LS + g] = (g < valid && k < Mxh) ? src[(size_t)g * Mxh + k] : make_float2(0.f, 0.f);
@@ -253,13 +257,15 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_cols(ColArgsD a, int mode, const
   __syncthreads();
   float2 *res = fft_lines<L>(s0, s1, CK, LS, tw, 1.f);
   if (mode == COL_H) {
-    for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
+  #pragma unroll 4
+  for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
       const int c = e % CK, g = e / CK, k = k0 + c;
       if (k < Mxh) a.out[(plane + g) * Mxh + k] = cscale(res[c * LS + g], a.hscale);
     }
     return;
   }
   const float2 *Hd = a.H + (size_t)spectrum_of(a, b, y) * L * Mxh;
+#pragma unroll 4
   for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
     const int c = e % CK, g = e / CK, k = k0 + c;
     if (k < Mxh) res[c * LS + g] = cmul(res[c * LS + g], __ldg(Hd + (size_t)g * Mxh + k));
@@ -325,6 +331,7 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_fwd_finish(ColArgsD a, const flo
   for (int i = threadIdx.x; i < L; i += FT_NT) tw[i] = twg[i];
   const int k0 = blockIdx.x * CK, b = blockIdx.y;
   const int Mxh = a.Mxh;
+#pragma unroll 4
   for (int e = threadIdx.x; e < CK * L; e += FT_NT) {
     const int c = e % CK, g = e / CK, k = k0 + c;
     float2 v = make_float2(0.f, 0.f);

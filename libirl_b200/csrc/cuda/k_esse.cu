@@ -236,14 +236,14 @@ constexpr int YZ_CH = 16;    // z lines per inverse-y chunk
 // base[w*ls + i*es]; every thread stages its butterflies in registers, so
 // reads complete (barrier) before any write.  WFAST: consecutive threads
 // take consecutive lines (use when ls == 1) instead of consecutive points.
-template <int L, int R, int MAXW, bool WFAST>
-__device__ __forceinline__ void ip_pass(float2 *base, int W, int ls, int es, int Ns, const float2 *tw, float s) {
+template <int L, int R, int MAXW, bool WFAST, int Ns>
+__device__ __forceinline__ void ip_pass(float2 *base, int W, int ls, int es, const float2 *tw, float s) {
   constexpr int JPL = L / R;
   constexpr int MAXJ = (MAXW * JPL + YZ_NT - 1) / YZ_NT;
   const int jobs = W * JPL;
   float2 v[MAXJ][R];
   int dst[MAXJ];
-  const int step = L / (Ns * R);
+  constexpr int step = L / (Ns * R);
 #pragma unroll
   for (int jj = 0; jj < MAXJ; ++jj) {
     const int q = threadIdx.x + jj * YZ_NT;
@@ -284,6 +284,21 @@ __device__ __forceinline__ void ip_pass(float2 *base, int W, int ls, int es, int
   __syncthreads();
 }
 
+// radix 8 while possible, 4 x 4 instead of 8 x 2 (fewer staged jobs);
+// the pass sequence is unrolled at compile time
+__host__ __device__ constexpr int ip_radix(int rem) { return (rem >= 8 && rem != 16) ? 8 : (rem == 4 || rem == 16) ? 4 : 2; }
+
+template <int L, int MAXW, bool WFAST, int Ns>
+struct IpPlan {
+  static __device__ __forceinline__ void run(float2 *base, int W, int ls, int es, const float2 *tw, float s) {
+    if constexpr (Ns < L) {
+      constexpr int R = ip_radix(L / Ns);
+      ip_pass<L, R, MAXW, WFAST, Ns>(base, W, ls, es, tw, s);
+      IpPlan<L, MAXW, WFAST, Ns * R>::run(base, W, ls, es, tw, s);
+    }
+  }
+};
+
 // transforms W lines in chunks of at most MAXW lines (bounds the registers
 // that stage one pass of a chunk)
 template <int L, int MAXW, bool WFAST>
@@ -291,21 +306,7 @@ __device__ void fft_ip(float2 *base_all, int W, int ls, int es, const float2 *tw
   for (int w0 = 0; w0 < W; w0 += MAXW) {
     float2 *base = base_all + (size_t)w0 * ls;
     const int Wc = min(MAXW, W - w0);
-    int Ns = 1;
-    while (Ns < L) {
-      const int rem = L / Ns;
-      // radix 8 while possible, 4 x 4 instead of 8 x 2 (fewer staged jobs)
-      if (rem >= 8 && rem != 16) {
-        ip_pass<L, 8, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
-        Ns *= 8;
-      } else if (rem == 4 || rem == 16) {
-        ip_pass<L, 4, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
-        Ns *= 4;
-      } else {
-        ip_pass<L, 2, MAXW, WFAST>(base, Wc, ls, es, Ns, tw, s);
-        Ns *= 2;
-      }
-    }
+    IpPlan<L, MAXW, WFAST, 1>::run(base, Wc, ls, es, tw, s);
   }
 }
 
@@ -524,6 +525,19 @@ struct CombineArgs {
   float primary;
 };
 
+// one voxel of the combination (krnlprj3d.c:833-946) and the projector
+// source (prjbck.c:170-173), rounded like libirl's float code
+__device__ __forceinline__ float combine_one(const CombineArgs &a, float T0, float T1, float S, float act, float mu) {
+  const float d = __fmul_rn(S, a.cnv);
+  float eff = T0;
+  if (a.nt > 1) eff = __fsub_rn(eff, __fmul_rn(d, T1));
+  eff = (float)((double)eff * exp((double)__fmul_rn(d, a.fmu)));
+  if (a.cntr > 0.f) eff = __fadd_rn(eff, __fmul_rn(act, a.cntr));
+  eff = __fmul_rn(eff, __fmul_rn(mu, a.cnv_pix));
+  if (eff < 0.f) eff = 0.f;
+  return __fadd_rn(__fmul_rn(act, a.primary), eff);
+}
+
 // CTA of 32 x CX_TY threads per (b, y, block of XZB z rows); rows are staged
 // with an odd stride so that one thread per row can walk x without bank
 // conflicts.
@@ -539,11 +553,25 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
   const int rows = min(XZB, nz - z0);
   const size_t pln = (size_t)nz * n, vox = pln * n;
   const size_t base = (size_t)b * vox + (size_t)y * pln + (size_t)z0 * n;
+  const bool vec = (n & 3) == 0;  // rows of whole float4s (16-byte aligned)
+  const int n4 = n >> 2;
   for (int t = 0; t < a.nt; ++t) {
     const float *src = (t == 0 ? a.t0 : a.t1) + base;
     float *dst = smx + (size_t)t * XZB * ld;
-    for (int rr = ty; rr < rows; rr += CX_TY)
-      for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * n + xx];
+    if (vec) {
+      for (int e = tid; e < rows * n4; e += 32 * CX_TY) {
+        const int rr = e / n4, x = (e - rr * n4) * 4;
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(src + (size_t)rr * n + x));
+        float *d = dst + rr * ld + x;
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+      }
+    } else {
+      for (int rr = ty; rr < rows; rr += CX_TY)
+        for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * n + xx];
+    }
   }
   __syncthreads();
   if (H > 0 && tid < a.nt * XZB && (tid % XZB) < rows) {
@@ -559,20 +587,32 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
   __syncthreads();
   const int view = a.views[b];
   const size_t tb = (size_t)view * vox + (size_t)y * pln + (size_t)z0 * n;
+  if (vec) {
+    for (int e = tid; e < rows * n4; e += 32 * CX_TY) {
+      const int rr = e / n4, x = (e - rr * n4) * 4;
+      const size_t g = (size_t)rr * n + x;
+      const float4 S4 = __ldg(reinterpret_cast<const float4 *>(a.S + tb + g));
+      const float4 A4 = __ldg(reinterpret_cast<const float4 *>(a.rot + base + g));
+      const float4 M4 = __ldg(reinterpret_cast<const float4 *>(a.mu + tb + g));
+      const float Sv[4] = {S4.x, S4.y, S4.z, S4.w}, Av[4] = {A4.x, A4.y, A4.z, A4.w};
+      const float Mv[4] = {M4.x, M4.y, M4.z, M4.w};
+      float out[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float T0 = smx[rr * ld + x + q];
+        const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + x + q] : 0.f;
+        out[q] = combine_one(a, T0, T1, Sv[q], Av[q], Mv[q]);
+      }
+      *reinterpret_cast<float4 *>(a.src + base + g) = make_float4(out[0], out[1], out[2], out[3]);
+    }
+    return;
+  }
   for (int rr = ty; rr < rows; rr += CX_TY) {
     for (int xx = tx; xx < n; xx += 32) {
       const size_t e = (size_t)rr * n + xx;
       const float T0 = smx[rr * ld + xx];
       const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + xx] : 0.f;
-      const float d = __fmul_rn(__ldg(a.S + tb + e), a.cnv);
-      float eff = T0;
-      if (a.nt > 1) eff = __fsub_rn(eff, __fmul_rn(d, T1));
-      eff = (float)((double)eff * exp((double)__fmul_rn(d, a.fmu)));
-      const float act = __ldg(a.rot + base + e);
-      if (a.cntr > 0.f) eff = __fadd_rn(eff, __fmul_rn(act, a.cntr));
-      eff = __fmul_rn(eff, __fmul_rn(__ldg(a.mu + tb + e), a.cnv_pix));
-      if (eff < 0.f) eff = 0.f;
-      a.src[base + e] = __fadd_rn(__fmul_rn(act, a.primary), eff);
+      a.src[base + e] = combine_one(a, T0, T1, __ldg(a.S + tb + e), __ldg(a.rot + base + e), __ldg(a.mu + tb + e));
     }
   }
 }

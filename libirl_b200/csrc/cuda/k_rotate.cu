@@ -16,6 +16,7 @@
 //
 // Volume layout [y][z][x]; a slice k is the set of rows y*nz*n + k*n.
 #include <cstdio>
+#include <cstdlib>
 
 #include "irlcu_internal.cuh"
 #include "../host/irl_geom.h"
@@ -124,6 +125,9 @@ __device__ __forceinline__ RotHdr load_hdr(const RotTabs &T, int r) {
 // grid (nz, nv).
 constexpr int SH_TX = 32, SH_TY = 16;
 
+// STAGE = false: pass 1 reads the source slice from global memory (L1 /
+// L2) instead of staging it, which halves the shared memory per CTA
+template <bool STAGE>
 __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__restrict__ src, size_t src_stride,
                                                              float *__restrict__ dst, size_t dst_stride,
                                                              const int *__restrict__ views, int rot_base,
@@ -132,8 +136,8 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
                                                              int xld) {
   extern __shared__ float sm[];
   const int ld = n + 1;
-  float *s_slice = sm;                          // n * ld
-  float *s_x = s_slice + (size_t)n * ld;        // n * xld
+  float *s_slice = sm;                                   // n * ld (STAGE)
+  float *s_x = STAGE ? s_slice + (size_t)n * ld : sm;    // n * xld
   int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xld);
   int *t_st = t_rsh + n, *t_en = t_st + n;
   float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
@@ -158,7 +162,8 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
     t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
     t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
   }
-  if ((n & 3) == 0) {
+  if (!STAGE) {
+  } else if ((n & 3) == 0) {
     const int n4 = n >> 2;
 #pragma unroll 4
     for (int y = ty; y < n; y += SH_TY)
@@ -175,6 +180,11 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
       for (int x = tx; x < n; x += SH_TX) s_slice[y * ld + x] = __ldg(s + (size_t)y * rs + x);
   }
   __syncthreads();
+  // source slice element (row y, column x)
+  auto SL = [&](int yy, int xx) -> float {
+    if (STAGE) return s_slice[yy * ld + xx];
+    return __ldg(s + (size_t)yy * rs + xx);
+  };
   // pass 1 (x shear): X row j from source row j (or column, when flipped)
   for (int j = ty; j < n; j += SH_TY) {
     const int sh = t_rsh[j], st = t_st[j], en = t_en[j];
@@ -187,15 +197,15 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
         if (h.b180 == 0) {
           const int t = i + sh - h.iadd;
           if (h.b90 == 0)
-            val = lerp2(f1, s_slice[j * ld + t], f2, s_slice[j * ld + t + 1]);
+            val = lerp2(f1, SL(j, t), f2, SL(j, t + 1));
           else
-            val = lerp2(f1, s_slice[t * ld + (n - j - 1)], f2, s_slice[(t + 1) * ld + (n - j - 1)]);
+            val = lerp2(f1, SL(t, n - j - 1), f2, SL(t + 1, n - j - 1));
         } else {
           const int t = n - i - (sh - h.iadd + 1);
           if (h.b90 == 0)
-            val = lerp2(f1, s_slice[(n - j - 1) * ld + t], f2, s_slice[(n - j - 1) * ld + t - 1]);
+            val = lerp2(f1, SL(n - j - 1, t), f2, SL(n - j - 1, t - 1));
           else
-            val = lerp2(f1, s_slice[t * ld + j], f2, s_slice[(t - 1) * ld + j]);
+            val = lerp2(f1, SL(t, j), f2, SL(t - 1, j));
         }
       }
       xr[i] = val;
@@ -235,8 +245,8 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
   }
 }
 
-static size_t shear_smem_bytes(int n, int xld) {
-  return sizeof(float) * ((size_t)n * (n + 1) + (size_t)n * xld + 5 * (size_t)n + 3 * (size_t)xld);
+static size_t shear_smem_bytes(int n, int xld, bool stage) {
+  return sizeof(float) * ((stage ? (size_t)n * (n + 1) : 0) + (size_t)n * xld + 5 * (size_t)n + 3 * (size_t)xld);
 }
 
 // Path B, for slices too large for shared memory: pass 1 into a global
@@ -362,19 +372,36 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   }
   // widest intermediate image over the rotations in use (mdim < 2n)
   const int xld = c.max_mdim > 0 ? c.max_mdim : 2 * n;
-  const size_t smem = shear_smem_bytes(n, xld);
-  int dev = 0, maxsm = 0;
+  int dev = 0, maxsm = 0, smsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  // stage the slice only while two CTAs still fit an SM; otherwise pass 1
+  // reads the slice through L1 and the CTA keeps only X
+  // (IRLCU_SHEAR_STAGE = 1 / 0 forces either form)
+  const size_t sm_stage = shear_smem_bytes(n, xld, true), sm_glob = shear_smem_bytes(n, xld, false);
+  const char *env = getenv("IRLCU_SHEAR_STAGE");
+  bool stage = 2 * sm_stage + 2048 <= (size_t)smsm;
+  if (env && env[0] == '1') stage = true;
+  if (env && env[0] == '0') stage = false;
+  if (stage && sm_stage > (size_t)maxsm) stage = false;
+  const size_t smem = stage ? sm_stage : sm_glob;
   dim3 grid(nz, nv);
   if (smem <= (size_t)maxsm) {
-    static size_t s_configured = 0;
-    if (smem > s_configured) {
-      CU_TRY(cudaFuncSetAttribute(k_shear_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      s_configured = smem;
+    static size_t s_conf[2] = {0, 0};
+    if (smem > s_conf[stage]) {
+      if (stage)
+        CU_TRY(cudaFuncSetAttribute(k_shear_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      else
+        CU_TRY(cudaFuncSetAttribute(k_shear_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      s_conf[stage] = smem;
     }
-    k_shear_smem<<<grid, dim3(SH_TX, SH_TY), smem, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base,
-                                                          c.rot, c.sup_start, c.sup_end, n, nz, xld);
+    if (stage)
+      k_shear_smem<true><<<grid, dim3(SH_TX, SH_TY), smem, c.st>>>(src, src_stride, dst, dst_stride, dviews,
+                                                                  rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xld);
+    else
+      k_shear_smem<false><<<grid, dim3(SH_TX, SH_TY), smem, c.st>>>(src, src_stride, dst, dst_stride, dviews,
+                                                                   rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xld);
     CU_LAUNCHED();
     return IRLCU_OK;
   }
