@@ -55,10 +55,11 @@ typedef struct {
 } IrlOsemProblem_t;
 
 /* Runs nprob independent OSEM reconstructions, each exactly as IrlOsem
-   would run it alone (same results), resident together on the device:
-   every problem has its own device context and stream, and the host
-   enqueues their iterations round-robin so that small problems overlap on
-   the GPU.  Not allowed with hooks, or with iSetupExtraPrjViewData /
+   would run it alone (same results).  Every problem has its own device
+   context and stream; they run pipelined: while the device iterates one
+   problem (all its iterations enqueued at once), the host sets up the next
+   and finishes the one before, so at most two are resident at a time.
+   Not allowed with hooks, or with iSetupExtraPrjViewData /
    iSetupDetectors data pending (those are per-call state of IrlOsem).
    Returns 0, or the first non-zero iStatus. */
 int IrlOsemBatch(int nprob, IrlOsemProblem_t *psProblems);

@@ -205,6 +205,6 @@ inline bool fft_len_ok(int L) {
 }
 
 // host: twiddle table exp(-2 pi i m / L), m < L, in device memory
-int upload_twiddle_table(float2 **d, int L);
+int upload_twiddle_table(cudaStream_t st, float2 **d, int L);
 
 }  // namespace irlcu

@@ -18,6 +18,8 @@ namespace irlcu {
 Ctx *g_ctx = nullptr;
 long long g_launch_count = 0;
 static char g_err[1024] = "";
+// stream of the context being built or torn down before it is current
+static cudaStream_t g_init_stream = nullptr;
 
 // ------------------------------------------------------- stage profiling
 struct ProfRec {
@@ -99,21 +101,45 @@ size_t forward_partial_elems(int n, int nz, int max_batch);
 void free_rotate_scratch(Ctx &c);
 void esse_free(Ctx &c);
 
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t st) {
+  static bool ready[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && !ready[dev]) {
+    cudaMemPool_t pool;
+    if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    ready[dev] = true;
+  }
+  if ((e = cudaMallocAsync(p, bytes, st)) != cudaSuccess) return e;
+  return cudaStreamSynchronize(st);
+}
+
+void dev_free(void *p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
+// allocations of the current context (its stream orders them)
+static cudaStream_t alloc_stream() { return g_ctx ? g_ctx->st : g_init_stream; }
+
 template <class T>
 static int dalloc(T **p, size_t count) {
   *p = nullptr;
   if (count == 0) return IRLCU_OK;
-  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  cudaError_t e = dev_alloc_t(p, count, alloc_stream());
   if (e != cudaSuccess) {
     *p = nullptr;
-    return set_error(IRLCU_ENOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return set_error(IRLCU_ENOMEM, "device allocation of %zu bytes failed: %s", count * sizeof(T),
+                     cudaGetErrorString(e));
   }
   return IRLCU_OK;
 }
 
 template <class T>
 static void dfree(T *&p) {
-  if (p) cudaFree(p);
+  dev_free(p, alloc_stream());
   p = nullptr;
 }
 
@@ -126,6 +152,8 @@ static void graphs_clear(Ctx &c) {
 
 static void free_ctx(Ctx *c) {
   if (!c) return;
+  Ctx *const cur = g_ctx;
+  g_ctx = c;  // dfree orders the frees on this context's stream
   cudaStreamSynchronize(c->st);
   graphs_clear(*c);
   dfree(c->sur_scale);
@@ -166,7 +194,7 @@ static void free_ctx(Ctx *c) {
     dfree(c->drf[w].psf);
     dfree(c->drf[w].pad_rows);
     dfree(c->drf[w].row_idist);
-    drf_fft_free(c->drf[w]);
+    drf_fft_free(*c, c->drf[w]);
   }
   drf_fft_work_free(*c);
   esse_free(*c);
@@ -174,6 +202,7 @@ static void free_ctx(Ctx *c) {
   for (auto &e : c->ev) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
+  g_ctx = cur == c ? nullptr : cur;
 }
 
 #define TRY(x)                 \
@@ -372,7 +401,7 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
   dfree(D.psf);
   dfree(D.pad_rows);
   dfree(D.row_idist);
-  drf_fft_free(D);
+  drf_fft_free(c, D);
   D = DrfDev{};
   if (!d) return IRLCU_OK;
   // engine: the direct kernels take half-widths up to 32, the Fourier-domain
@@ -417,7 +446,7 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
     if (mode == ENGINE_TUNE) {
       bool fft = true;
       TRY(drf_autotune(c, D, max_pad, &fft));
-      if (!fft) drf_fft_free(D);
+      if (!fft) drf_fft_free(c, D);
     }
   }
   return IRLCU_OK;

@@ -151,6 +151,18 @@ struct Ctx {
 
 extern Ctx *g_ctx;
 
+// Device memory of a context: stream-ordered allocations from the device's
+// default pool, whose release threshold is raised so that freed memory stays
+// cached for the next context (set-up reuses it without reaching the driver
+// and teardown never synchronises the device).  dev_alloc waits for its
+// stream, so the memory can be used at once by any stream or copy.
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t st);
+void dev_free(void *p, cudaStream_t st);
+template <class T>
+inline cudaError_t dev_alloc_t(T **p, size_t count, cudaStream_t st) {
+  return dev_alloc(reinterpret_cast<void **>(p), count * sizeof(T), st);
+}
+
 // error helpers
 int set_error(int code, const char *fmt, ...);
 #define CU_TRY(x)                                                         \
@@ -194,7 +206,7 @@ int launch_backproject(const Ctx &c, const float *planes, const int *dviews, int
 
 // Fourier-domain DRF engine (k_drf_fft.cu); max_pad: the largest axial pad
 int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad);
-void drf_fft_free(DrfDev &D);
+void drf_fft_free(Ctx &c, DrfDev &D);
 void drf_fft_work_free(Ctx &c);
 int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
                        float scale, float *out);

@@ -395,27 +395,27 @@ static int set_col_attrs() {
 
 
 
-static int grow(float2 **p, size_t *have, size_t need) {
+static int grow(cudaStream_t st, float2 **p, size_t *have, size_t need) {
   if (need <= *have) return IRLCU_OK;
-  if (*p) cudaFree(*p);
+  dev_free(*p, st);
   *p = nullptr;
   *have = 0;
-  CU_TRY(cudaMalloc(p, need * sizeof(float2)));
+  CU_TRY(dev_alloc_t(p, need, st));
   *have = need;
   return IRLCU_OK;
 }
 
-void drf_fft_free(DrfDev &D) {
-  if (D.fft.H) cudaFree(D.fft.H);
-  if (D.fft.twx) cudaFree(D.fft.twx);
-  if (D.fft.twz) cudaFree(D.fft.twz);
+void drf_fft_free(Ctx &c, DrfDev &D) {
+  dev_free(D.fft.H, c.st);
+  dev_free(D.fft.twx, c.st);
+  dev_free(D.fft.twz, c.st);
   D.fft = DrfFft{};
 }
 
 void drf_fft_work_free(Ctx &c) {
-  if (c.dw.S) cudaFree(c.dw.S);
-  if (c.dw.part) cudaFree(c.dw.part);
-  if (c.dw.Y) cudaFree(c.dw.Y);
+  dev_free(c.dw.S, c.st);
+  dev_free(c.dw.part, c.st);
+  dev_free(c.dw.Y, c.st);
   c.dw = DfftWork{};
 }
 
@@ -423,7 +423,7 @@ void drf_fft_work_free(Ctx &c) {
 static int fwd_groups(int nplanes) { return nplanes < 16 ? nplanes : 16; }
 
 int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
-  drf_fft_free(D);
+  drf_fft_free(c, D);
   const int n = c.n, nz = c.nz, h = D.halo;
   const int Mx = grid_len(n + h), Mz = grid_len(nz + max_pad + h);
   if (Mx < 0 || Mz < 0 || Mx < 2 * h + 1 || Mz < 2 * h + 1)
@@ -435,15 +435,15 @@ int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
   F.P = max_pad;
   F.G = nz + 2 * max_pad;
   if (F.G > Mz) F.G = Mz;
-  TRY_RC(upload_twiddle_table(&F.twx, Mx));
-  TRY_RC(upload_twiddle_table(&F.twz, Mz));
+  TRY_RC(upload_twiddle_table(c.st, &F.twx, Mx));
+  TRY_RC(upload_twiddle_table(c.st, &F.twz, Mz));
   const int nspec = D.ndist + 1;
-  CU_TRY(cudaMalloc(&F.H, sizeof(float2) * (size_t)nspec * Mz * F.Mxh));
+  CU_TRY(dev_alloc_t(&F.H, (size_t)nspec * Mz * F.Mxh, c.st));
   // work: row spectra for max_batch views (also holds the PSF rows here)
   const int B = c.g.max_batch;
-  TRY_RC(grow(&c.dw.S, &c.dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
-  TRY_RC(grow(&c.dw.part, &c.dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
-  TRY_RC(grow(&c.dw.Y, &c.dw.y_elems, (size_t)B * nz * F.Mxh));
+  TRY_RC(grow(c.st, &c.dw.S, &c.dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
+  TRY_RC(grow(c.st, &c.dw.part, &c.dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
+  TRY_RC(grow(c.st, &c.dw.Y, &c.dw.y_elems, (size_t)B * nz * F.Mxh));
   // spectra of the quadrant-swapped PSFs (and the identity), 1/(Mz Mx)
   RowSrc r{};
   r.mode = MODE_PSF;

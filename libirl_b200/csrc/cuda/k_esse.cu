@@ -627,18 +627,18 @@ __global__ void k_scale_copy(const float *__restrict__ in, float *__restrict__ o
 
 
 
-int upload_twiddle_table(float2 **d, int L) {
+int upload_twiddle_table(cudaStream_t st, float2 **d, int L) {
   std::vector<float2> h(L);
   for (int m = 0; m < L; ++m) {
     const double a = -2.0 * M_PI * (double)m / (double)L;
     h[m] = make_float2((float)cos(a), (float)sin(a));
   }
-  CU_TRY(cudaMalloc(d, sizeof(float2) * L));
+  CU_TRY(dev_alloc_t(d, (size_t)L, st));
   CU_TRY(cudaMemcpy(*d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
   return IRLCU_OK;
 }
 
-static int upload_twiddles(float2 **d, int L) { return upload_twiddle_table(d, L); }
+static int upload_twiddles(float2 **d, int L) { return upload_twiddle_table(g_ctx->st, d, L); }
 
 // ESSE grid sides with instantiated kernels: products of 2, 3, 5, 7 that
 // ceil(2 N / c) takes for the usual volume sizes and collapse factors
@@ -770,23 +770,23 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
 
 void esse_free(Ctx &c) {
   for (int t = 0; t < 3; ++t) {
-    if (c.esse.kft[t]) cudaFree(c.esse.kft[t]), c.esse.kft[t] = nullptr;
-    if (c.esse.kftT[t]) cudaFree(c.esse.kftT[t]), c.esse.kftT[t] = nullptr;
+    dev_free(c.esse.kft[t], c.st), c.esse.kft[t] = nullptr;
+    dev_free(c.esse.kftT[t], c.st), c.esse.kftT[t] = nullptr;
   }
   c.esse.on = false;
   c.esse.zero = false;
   c.esse.fused = false;
   EsseWork &w = c.ew;
-  cudaFree(w.twx);
-  cudaFree(w.twy);
-  cudaFree(w.twz);
-  cudaFree(w.A);
-  cudaFree(w.Bf);
+  dev_free(w.twx, c.st);
+  dev_free(w.twy, c.st);
+  dev_free(w.twz, c.st);
+  dev_free(w.A, c.st);
+  dev_free(w.Bf, c.st);
   for (int t = 0; t < 2; ++t) {
-    cudaFree(w.C2[t]);
-    cudaFree(w.D[t]);
-    cudaFree(w.g[t]);
-    cudaFree(w.T[t]);
+    dev_free(w.C2[t], c.st);
+    dev_free(w.D[t], c.st);
+    dev_free(w.g[t], c.st);
+    dev_free(w.T[t], c.st);
   }
   c.ew = EsseWork{};
 }
@@ -832,34 +832,34 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
   const int B = c.g.max_batch;
   w.batch = B;
   const size_t spec = (size_t)E.ky * E.kz * E.kxh;
-  CU_TRY(cudaMalloc(&w.A, sizeof(float2) * (size_t)B * w.nyv * E.kz * E.kxh));
-  CU_TRY(cudaMalloc(&w.Bf, sizeof(float2) * (size_t)B * spec));
+  CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.A), sizeof(float2) * (size_t)B * w.nyv * E.kz * E.kxh, c.st));
+  CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.Bf), sizeof(float2) * (size_t)B * spec, c.st));
   for (int t = 0; t < 2; ++t) {
-    CU_TRY(cudaMalloc(&w.C2[t], sizeof(float2) * (size_t)B * w.nyv * E.kz * E.kxh));
-    CU_TRY(cudaMalloc(&w.D[t], sizeof(float2) * (size_t)B * w.nyv * w.nzv * E.kxh));
-    CU_TRY(cudaMalloc(&w.g[t], sizeof(float) * (size_t)B * w.nyv * w.nzv * w.nxv));
-    CU_TRY(cudaMalloc(&w.T[t], sizeof(float) * (size_t)B * c.vox));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.C2[t]), sizeof(float2) * (size_t)B * w.nyv * E.kz * E.kxh, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.D[t]), sizeof(float2) * (size_t)B * w.nyv * w.nzv * E.kxh, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.g[t]), sizeof(float) * (size_t)B * w.nyv * w.nzv * w.nxv, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.T[t]), sizeof(float) * (size_t)B * c.vox, c.st));
   }
   // kernel spectra: forward transform of the full real grids
   const float *hk[3] = {e->krnl, e->kmu, e->kmu2};
   float *dgrid = nullptr;
-  CU_TRY(cudaMalloc(&dgrid, sizeof(float) * (size_t)E.kx * E.ky * E.kz));
+  CU_TRY(dev_alloc(reinterpret_cast<void **>(&dgrid), sizeof(float) * (size_t)E.kx * E.ky * E.kz, c.st));
   for (int t = 0; t < E.nterms; ++t) {
-    CU_TRY(cudaMalloc(&E.kft[t], sizeof(float2) * spec));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kft[t]), sizeof(float2) * spec, c.st));
     CU_TRY(cudaMemcpy(dgrid, hk[t], sizeof(float) * (size_t)E.kx * E.ky * E.kz, cudaMemcpyHostToDevice));
     float2 *ta = nullptr, *tb = nullptr;
-    CU_TRY(cudaMalloc(&ta, sizeof(float2) * spec));
-    CU_TRY(cudaMalloc(&tb, sizeof(float2) * spec));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&ta), sizeof(float2) * spec, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&tb), sizeof(float2) * spec, c.st));
     int rc = fft3_forward(c.st, E, nullptr, dgrid, c.n, c.nz, 1, E.ky, E.kz, E.kx, 1, ta, tb, E.kft[t]);
     CU_TRY(cudaStreamSynchronize(c.st));
-    cudaFree(ta);
-    cudaFree(tb);
+    dev_free(ta, c.st);
+    dev_free(tb, c.st);
     if (rc) {
-      cudaFree(dgrid);
+      dev_free(dgrid, c.st);
       return rc;
     }
   }
-  cudaFree(dgrid);
+  dev_free(dgrid, c.st);
   // fused y-z kernel when the plane fits in shared memory
   {
     int dev = 0, maxsm = 0;
@@ -869,7 +869,7 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     const size_t sm = yz_smem(L, w.nyv);
     if (E.ky == E.kz && (L == 32 || L == 64 || L == 128) && sm <= (size_t)maxsm) {
       for (int t = 0; t < E.nterms; ++t) {
-        CU_TRY(cudaMalloc(&E.kftT[t], sizeof(float2) * spec));
+        CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kftT[t]), sizeof(float2) * spec, c.st));
         k_spec_kmajor<<<592, 256, 0, c.st>>>(E.kft[t], E.kftT[t], E.ky, E.kz, E.kxh);
         CU_LAUNCHED();
       }

@@ -407,10 +407,10 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   }
   const size_t need = (size_t)nv * nz * n * xld;
   if (need > c.xscratch_elems) {
-    if (c.xscratch) cudaFree(c.xscratch);
+    dev_free(c.xscratch, c.st);
     c.xscratch = nullptr;
     c.xscratch_elems = 0;
-    CU_TRY(cudaMalloc(&c.xscratch, need * sizeof(float)));
+    CU_TRY(dev_alloc_t(&c.xscratch, need, c.st));
     c.xscratch_elems = need;
   }
   k_shear_pass1_glob<<<grid, 512, 0, c.st>>>(src, src_stride, c.xscratch, dviews, rot_base, c.rot,
@@ -423,7 +423,7 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
 }
 
 void free_rotate_scratch(Ctx &c) {
-  if (c.xscratch) cudaFree(c.xscratch);
+  dev_free(c.xscratch, c.st);
   c.xscratch = nullptr;
   c.xscratch_elems = 0;
 }

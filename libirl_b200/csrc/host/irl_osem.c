@@ -612,11 +612,25 @@ static void session_unpark(parked_session *h)
 	free(h);
 }
 
+/* ends parked problem p (result copy unless a problem failed) */
+static int batch_end(parked_session **h, IrlOsemProblem_t *pp, int p, int err)
+{
+	int e;
+	if (h[p] == NULL)
+		return 0;
+	session_unpark(h[p]);
+	h[p] = NULL;
+	e = IrlOsemEnd(err ? NULL : pp[p].pfReconImage);
+	if (!pp[p].iStatus)
+		pp[p].iStatus = e;
+	return e;
+}
+
 int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 {
 	jmp_buf env;
 	parked_session **h = NULL;
-	int p, m, err = 0, left;
+	int p, m, err = 0;
 	if ((err = setjmp(env)) != 0) {
 		irl_untrap();
 		return err;
@@ -634,43 +648,34 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 		irl_fatal(IRL_E_VALUE, "IrlOsemBatch", "an IrlOsemBegin session is open");
 	h = (parked_session **)irl_calloc(sizeof(parked_session *) * nprob, "batch sessions");
 	irl_untrap();
+	/* pipelined: problem p is set up and all its iterations are enqueued
+	   (asynchronous device work on its own stream); the host then sets up
+	   p + 1 while the device runs p, and ends p - 1 */
 	for (p = 0; p < nprob && !err; ++p) {
 		IrlOsemProblem_t *q = pp + p;
 		q->iStatus = IrlOsemBegin(q->psIrlParms, q->psOptions, q->psViews, q->pchDrfTabFname,
 			q->pchScatKrnlFname, NULL, q->pfScatterEstimate, q->pfAtnMap, q->pfPrjImage, q->pfReconImage,
 			NULL, NULL);
-		if (q->iStatus)
+		if (q->iStatus) {
 			err = q->iStatus;
-		else
-			h[p] = session_park();
-	}
-	/* iterations round-robin: each call only enqueues device work */
-	do {
-		left = 0;
-		for (p = 0; p < nprob && !err; ++p) {
-			if (h[p] == NULL)
-				continue;
-			session_unpark(h[p]);
-			h[p] = NULL;
-			if (S.it < S.p.iterations) {
-				const int e = IrlOsemIterate(1);
-				if (e) {  /* IrlOsemIterate closed the session */
-					pp[p].iStatus = err = e;
-					continue;
-				}
-			}
-			left |= S.it < S.p.iterations;
-			h[p] = session_park();
+			break;
 		}
-	} while (left && !err);
+		{
+			const int e = IrlOsemIterate(S.p.iterations);
+			if (e) {  /* IrlOsemIterate closed the session */
+				q->iStatus = err = e;
+				break;
+			}
+		}
+		h[p] = session_park();
+		if (p > 0 && h[p - 1] != NULL) {
+			const int e = batch_end(h, pp, p - 1, err);
+			if (!err)
+				err = e;
+		}
+	}
 	for (p = 0; p < nprob; ++p) {
-		int e;
-		if (h[p] == NULL)
-			continue;
-		session_unpark(h[p]);
-		e = IrlOsemEnd(err ? NULL : pp[p].pfReconImage);
-		if (!pp[p].iStatus)
-			pp[p].iStatus = e;
+		const int e = batch_end(h, pp, p, err);
 		if (!err)
 			err = e;
 	}
