@@ -35,6 +35,7 @@ struct DrfFft {
   int P = 0, G = 0;             // row offset; rows that can be nonzero
   float2 *H = nullptr;          // [ndist + 1][Mz][Mxh]
   float2 *twx = nullptr, *twz = nullptr;
+  bool fused = false;           // square grid (Mz == Mx), one CTA per plane
 };
 
 struct DrfDev {

@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "drf_plane.cuh"
 #include "fft_core.cuh"
 #include "irlcu_internal.cuh"
 
@@ -84,23 +85,6 @@ struct RowSrc {
   int Mxh, nplanes;
 };
 constexpr int MODE_PLANE = 0, MODE_PSF = 1;
-
-__device__ __forceinline__ float plane_in(const float *a, const float *e, int i) {
-  const float v = __ldg(a + i);
-  return e ? __fmul_rn(v, __ldg(e + i)) : v;
-}
-
-// value of the attenuated, axially padded plane at (z, x), x < n
-__device__ __forceinline__ float plane_pad_val(const float *a, const float *e, int z, int x, int n, int nz,
-                                               int pady, int avgy) {
-  if (z >= 0 && z < nz) return plane_in(a, e, z * n + x);
-  if (pady <= 0 || avgy <= 0 || z < -pady || z >= nz + pady) return 0.f;
-  // pfAvgRows (pad2d.c:92-122): row sum in order, divided when > 1 row
-  const int r0 = z < 0 ? 0 : nz - avgy;
-  float s = 0.f;
-  for (int r = 0; r < avgy; ++r) s = __fadd_rn(s, plane_in(a, e, (r0 + r) * n + x));
-  return avgy > 1 ? __fdiv_rn(s, (float)avgy) : s;
-}
 
 // index of grid offset g in a centred (2h+1) table, or -1
 __device__ __forceinline__ int centred(int g, int M, int h) {
@@ -347,6 +331,164 @@ __global__ void __launch_bounds__(FT_NT) k_dfft_fwd_finish(ColArgsD a, const flo
   }
 }
 
+// ------------------------------------------------- one CTA per plane
+// Square grids L x L (L = Mz = Mx) whose half spectrum fits shared memory:
+// the row transforms, column transforms, PSF product and inverses of a
+// plane run in one CTA (drf_plane.cuh), so the row spectra never travel
+// through global memory.
+//   backward: one CTA per (plane y, view b) -> bck[b][y][z][x];
+//   forward:  one CTA per (plane group pg, view b) accumulates
+//             sum_y H[d(y)] * FFT2(plane y) in registers -> part[pg][b];
+//             the finish CTA of view b adds the groups in order, inverts
+//             and writes out[b][z][x].
+
+struct PlaneArgs {
+  const float *a;       // plane (b, y) at a + b*a_bs + y*a_ys, [z][x]
+  size_t a_bs, a_ys;
+  const float *E;       // attenuation factors [view][y][z][x] or null
+  const int *views, *row_idist, *pad_rows;
+  int avgy, ndist;
+  const float2 *H;      // [ndist + 1][L][L/2 + 1]
+  int n, nz, P, G, nplanes;
+  float scale;
+  float *out;           // backward [b][y][z][x]; forward [b][z][x]
+  float2 *part;         // forward partial sums [pg][b][L][L/2 + 1]
+  int npg, nb;
+};
+
+// source of plane (b, y) and its PSF spectrum (the identity for rows
+// without DRF, prjbck.c:233)
+template <int L>
+__device__ __forceinline__ const float2 *dp_plane_src(const PlaneArgs &a, int b, int y, PlaneSrc &p) {
+  const int view = a.views[b];
+  const size_t pln = (size_t)a.nz * a.n;
+  p.a = a.a + (size_t)b * a.a_bs + (size_t)y * a.a_ys;
+  p.e = a.E ? a.E + ((size_t)view * a.nplanes + y) * pln : nullptr;
+  const int d = a.row_idist ? a.row_idist[(size_t)view * a.nplanes + y] : -1;
+  p.pady = (d >= 0 && a.pad_rows) ? a.pad_rows[d] : 0;
+  p.n = a.n;
+  p.nz = a.nz;
+  p.P = a.P;
+  p.avgy = a.avgy;
+  return a.H + (size_t)(d >= 0 ? d : a.ndist) * L * DPlane<L>::H;
+}
+
+// grid rows 0 .. G-1 of the plane -> half spectra S[g][kx].  Ends with a barrier.
+template <int L>
+__device__ __forceinline__ void dp_rows_forward(int tid, const PlaneSrc &p, int G, float2 *S, float2 *X,
+                                                const float2 *twr) {
+  using D = DPlane<L>;
+  const int nl = (G + 1) / 2;
+  const int src = dp_partner<L>(tid) & 31;
+  for (int w0 = 0; w0 < nl; w0 += D::LINES) {
+    dp_rows_fwd_a<L>(tid, w0, p, G, X, twr);
+    __syncthreads();
+    float2 u[D::N2], q[D::N2];
+    dp_rows_b<L, false>(tid, X, u);
+#pragma unroll
+    for (int t = 0; t < D::N2; ++t) {
+      q[t].x = __shfl_sync(0xffffffffu, u[t].x, src);
+      q[t].y = __shfl_sync(0xffffffffu, u[t].y, src);
+    }
+    dp_rows_fwd_store<L>(tid, w0, G, u, q, S);
+    __syncthreads();
+  }
+}
+
+// spectrum rows r0 .. r0+nz-1 -> output rows [z][x], x < n, times scale
+template <int L, bool PERM>
+__device__ __forceinline__ void dp_rows_inverse(int tid, const float2 *S, float2 *X, const float2 *twr, int r0,
+                                                int nz, int n, float *out, float scale) {
+  using D = DPlane<L>;
+  const int nl = (nz + 1) / 2;
+  for (int w0 = 0; w0 < nl; w0 += D::LINES) {
+    dp_rows_inv_a<L, PERM>(tid, w0, S, X, twr, r0, nz);
+    __syncthreads();
+    float2 u[D::N2];
+    dp_rows_b<L, true>(tid, X, u);
+    dp_rows_inv_store<L>(tid, w0, u, out, n, nz, scale);
+    __syncthreads();
+  }
+}
+
+// persistent: CTA i takes planes i, i + gridDim.x, ... (plane p = view
+// p / nplanes, row p mod nplanes) and prefetches its next plane into L2
+template <int L>
+__global__ void __launch_bounds__(DP_NT, 1) k_dplane_bck(PlaneArgs a, const float2 *__restrict__ twg) {
+  using D = DPlane<L>;
+  extern __shared__ __align__(16) float2 dsm[];
+  float2 *S = dsm, *X = S + D::S_ELEMS, *tw = X + D::X_ELEMS, *twr = tw + L;
+  const int tid = threadIdx.x, total = a.nb * a.nplanes;
+  dp_twiddles<L>(tid, tw, twr, twg);
+  for (int pl = blockIdx.x; pl < total; pl += gridDim.x) {
+    const int b = pl / a.nplanes, y = pl - b * a.nplanes;
+    PlaneSrc p;
+    const float2 *Hd = dp_plane_src<L>(a, b, y, p);
+    if (pl + (int)gridDim.x < total) {
+      const int nx = pl + gridDim.x, bn = nx / a.nplanes;
+      PlaneSrc pn;
+      dp_plane_src<L>(a, bn, nx - bn * a.nplanes, pn);
+      dp_prefetch_plane(tid, pn);
+    }
+    __syncthreads();
+    dp_rows_forward<L>(tid, p, a.G, S, X, twr);
+    dp_cols_a<L>(tid, S, tw, a.G);
+    __syncthreads();
+    dp_cols_b_bck<L>(tid, S, tw, Hd);
+    __syncthreads();
+    dp_cols_c<L>(tid, S, a.P, a.P + a.nz);
+    __syncthreads();
+    dp_rows_inverse<L, false>(tid, S, X, twr, a.P, a.nz, a.n, a.out + ((size_t)b * a.nplanes + y) * a.nz * a.n,
+                              a.scale);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(DP_NT, 1) k_dplane_fwd(PlaneArgs a, const float2 *__restrict__ twg) {
+  using D = DPlane<L>;
+  extern __shared__ __align__(16) float2 dsm[];
+  float2 *S = dsm, *X = S + D::S_ELEMS, *tw = X + D::X_ELEMS, *twr = tw + L;
+  const int tid = threadIdx.x, pg = blockIdx.x, b = blockIdx.y;
+  const int y0 = pg * a.nplanes / a.npg, y1 = (pg + 1) * a.nplanes / a.npg;
+  dp_twiddles<L>(tid, tw, twr, twg);
+  float2 acc[D::NRB][D::N2];
+#pragma unroll
+  for (int r = 0; r < D::NRB; ++r)
+#pragma unroll
+    for (int k = 0; k < D::N2; ++k) acc[r][k] = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int y = y0; y < y1; ++y) {
+    PlaneSrc p;
+    const float2 *Hd = dp_plane_src<L>(a, b, y, p);
+    if (y + 1 < y1) {
+      PlaneSrc pn;
+      dp_plane_src<L>(a, b, y + 1, pn);
+      dp_prefetch_plane(tid, pn);
+    }
+    dp_rows_forward<L>(tid, p, a.G, S, X, twr);
+    dp_cols_a<L>(tid, S, tw, a.G);
+    __syncthreads();
+    dp_cols_b_acc<L>(tid, S, Hd, acc);
+    __syncthreads();
+  }
+  dp_store_acc<L>(tid, a.part + ((size_t)pg * a.nb + b) * L * D::H, acc);
+}
+
+template <int L>
+__global__ void __launch_bounds__(DP_NT, 1) k_dplane_fwd_finish(PlaneArgs a, const float2 *__restrict__ twg) {
+  using D = DPlane<L>;
+  extern __shared__ __align__(16) float2 dsm[];
+  float2 *S = dsm, *X = S + D::S_ELEMS, *tw = X + D::X_ELEMS, *twr = tw + L;
+  const int tid = threadIdx.x, b = blockIdx.x;
+  dp_twiddles<L>(tid, tw, twr, twg);
+  __syncthreads();
+  dp_fin_b<L>(tid, S, tw, a.part + (size_t)b * L * D::H, (size_t)a.nb * L * D::H, a.npg);
+  __syncthreads();
+  dp_fin_c<L>(tid, S);
+  __syncthreads();
+  dp_rows_inverse<L, true>(tid, S, X, twr, a.P, a.nz, a.n, a.out + (size_t)b * a.nz * a.n, a.scale);
+}
+
 // -------------------------------------------------------------- host side
 
 // grid lengths with instantiated kernels
@@ -380,6 +522,81 @@ static int grid_len(int need) {
     case 1024: { constexpr int LL = 1024; __VA_ARGS__; } break;                   \
     default: return set_error(IRLCU_EARG, "DRF FFT length %d not supported", L);   \
   }
+
+// square grid lengths of the one-CTA-per-plane kernels
+static const int kPlaneLens[] = {32, 40, 48, 64, 80, 96, 128, 160, 192};
+
+#define DPLANE_DISPATCH(L, ...)                                                    \
+  switch (L) {                                                                    \
+    case 32: { constexpr int LL = 32; __VA_ARGS__; } break;                      \
+    case 40: { constexpr int LL = 40; __VA_ARGS__; } break;                      \
+    case 48: { constexpr int LL = 48; __VA_ARGS__; } break;                      \
+    case 64: { constexpr int LL = 64; __VA_ARGS__; } break;                      \
+    case 80: { constexpr int LL = 80; __VA_ARGS__; } break;                      \
+    case 96: { constexpr int LL = 96; __VA_ARGS__; } break;                      \
+    case 128: { constexpr int LL = 128; __VA_ARGS__; } break;                    \
+    case 160: { constexpr int LL = 160; __VA_ARGS__; } break;                    \
+    case 192: { constexpr int LL = 192; __VA_ARGS__; } break;                    \
+    default: return set_error(IRLCU_EARG, "DRF plane length %d not supported", L); \
+  }
+
+static size_t dplane_smem(int L) {
+  size_t sm = 0;
+  switch (L) {
+#define DPLANE_SMEM_CASE(X) case X: sm = DPlane<X>::SMEM; break;
+    DPLANE_SMEM_CASE(32) DPLANE_SMEM_CASE(40) DPLANE_SMEM_CASE(48) DPLANE_SMEM_CASE(64) DPLANE_SMEM_CASE(80)
+    DPLANE_SMEM_CASE(96) DPLANE_SMEM_CASE(128) DPLANE_SMEM_CASE(160) DPLANE_SMEM_CASE(192)
+#undef DPLANE_SMEM_CASE
+    default: break;
+  }
+  return sm;
+}
+
+// the one-CTA-per-plane form for an L x L grid: instantiated length, shared
+// memory within the device limit, not switched off (IRLCU_DRF_PLANE=0)
+static bool dplane_usable(int L) {
+  const char *env = getenv("IRLCU_DRF_PLANE");
+  if (env && env[0] == '0') return false;
+  bool len = false;
+  for (int l : kPlaneLens) len = len || l == L;
+  if (!len) return false;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return dplane_smem(L) <= (size_t)maxsm;
+}
+
+template <int L>
+static int dplane_attrs() {
+  static bool done = false;
+  if (done) return IRLCU_OK;
+  const int sm = (int)DPlane<L>::SMEM;
+  CU_TRY(cudaFuncSetAttribute(k_dplane_bck<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_dplane_fwd<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_dplane_fwd_finish<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  done = true;
+  return IRLCU_OK;
+}
+
+static int sm_count() {
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 1;
+  }
+  return nsm;
+}
+
+// plane groups of the forward pass: one CTA per SM over the batch
+static int dplane_groups(int nv, int nplanes) {
+  const int g = sm_count() / std::max(nv, 1);
+  return std::max(1, std::min(g, std::min(16, nplanes)));
+}
+
+// CTAs of the persistent backward pass: one per SM
+static int dplane_ctas(int planes) { return std::max(1, std::min(planes, sm_count())); }
 
 template <int L>
 static int set_col_attrs() {
@@ -425,10 +642,14 @@ static int fwd_groups(int nplanes) { return nplanes < 16 ? nplanes : 16; }
 int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
   drf_fft_free(c, D);
   const int n = c.n, nz = c.nz, h = D.halo;
-  const int Mx = grid_len(n + h), Mz = grid_len(nz + max_pad + h);
+  int Mx = grid_len(n + h), Mz = grid_len(nz + max_pad + h);
   if (Mx < 0 || Mz < 0 || Mx < 2 * h + 1 || Mz < 2 * h + 1)
     return set_error(IRLCU_EARG, "DRF FFT grid for n=%d nz=%d h=%d pad=%d exceeds %d", n, nz, h, max_pad, 1024);
   DrfFft &F = D.fft;
+  // one CTA per plane on a square grid when it fits shared memory (a larger
+  // grid than needed along one axis leaves the linear convolution unchanged)
+  F.fused = dplane_usable(std::max(Mx, Mz));
+  if (F.fused) Mx = Mz = std::max(Mx, Mz);
   F.Mx = Mx;
   F.Mz = Mz;
   F.Mxh = Mx / 2 + 1;
@@ -441,9 +662,11 @@ int drf_fft_setup(Ctx &c, DrfDev &D, int max_pad) {
   CU_TRY(dev_alloc_t(&F.H, (size_t)nspec * Mz * F.Mxh, c.st));
   // work: row spectra for max_batch views (also holds the PSF rows here)
   const int B = c.g.max_batch;
-  TRY_RC(grow(c.st, &c.dw.S, &c.dw.s_elems, std::max((size_t)B * n * F.G * F.Mxh, (size_t)nspec * Mz * F.Mxh)));
+  // (the plane form needs only the partial sums; S holds the PSF rows here)
+  const size_t s_need = (size_t)nspec * Mz * F.Mxh;
+  TRY_RC(grow(c.st, &c.dw.S, &c.dw.s_elems, F.fused ? s_need : std::max((size_t)B * n * F.G * F.Mxh, s_need)));
   TRY_RC(grow(c.st, &c.dw.part, &c.dw.part_elems, (size_t)fwd_groups(n) * B * Mz * F.Mxh));
-  TRY_RC(grow(c.st, &c.dw.Y, &c.dw.y_elems, (size_t)B * nz * F.Mxh));
+  if (!F.fused) TRY_RC(grow(c.st, &c.dw.Y, &c.dw.y_elems, (size_t)B * nz * F.Mxh));
   // spectra of the quadrant-swapped PSFs (and the identity), 1/(Mz Mx)
   RowSrc r{};
   r.mode = MODE_PSF;
@@ -522,9 +745,52 @@ static ColArgsD col_args(const Ctx &c, const DrfDev &D, const int *dviews, int n
   return a;
 }
 
+static PlaneArgs plane_args(const Ctx &c, const DrfDev &D, const float *a, size_t a_bs, size_t a_ys, const float *E,
+                            const int *dviews, float scale, float *out) {
+  PlaneArgs p{};
+  p.a = a;
+  p.a_bs = a_bs;
+  p.a_ys = a_ys;
+  p.E = E;
+  p.views = dviews;
+  p.row_idist = D.row_idist;
+  p.pad_rows = D.pad_rows;
+  p.avgy = D.avg_rows;
+  p.ndist = D.ndist;
+  p.H = D.fft.H;
+  p.n = c.n;
+  p.nz = c.nz;
+  p.P = D.fft.P;
+  p.G = D.fft.G;
+  p.nplanes = c.n;
+  p.scale = scale;
+  p.out = out;
+  return p;
+}
+
+static int launch_project_plane(const Ctx &c, const float *src, const int *dviews, int nv, const float *E,
+                                const DrfDev &D, float scale, float *out) {
+  const DrfFft &F = D.fft;
+  PlaneArgs a = plane_args(c, D, src, c.vox, c.pln, E, dviews, scale, out);
+  a.part = c.dw.part;
+  a.nb = nv;
+  a.npg = dplane_groups(nv, c.n);
+  if ((size_t)a.npg * nv * F.Mz * F.Mxh > c.dw.part_elems)
+    return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
+  DPLANE_DISPATCH(F.Mx, {
+    TRY_RC(dplane_attrs<LL>());
+    k_dplane_fwd<LL><<<dim3(a.npg, nv), DP_NT, DPlane<LL>::SMEM, c.st>>>(a, F.twx);
+    CU_LAUNCHED();
+    k_dplane_fwd_finish<LL><<<nv, DP_NT, DPlane<LL>::SMEM, c.st>>>(a, F.twx);
+    CU_LAUNCHED();
+  });
+  return IRLCU_OK;
+}
+
 int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv, const float *E, const DrfDev &D,
                        float scale, float *out) {
   const DrfFft &F = D.fft;
+  if (F.fused) return launch_project_plane(c, src, dviews, nv, E, D, scale, out);
   if ((size_t)nv * c.n * F.G * F.Mxh > c.dw.s_elems || (size_t)nv * c.nz * F.Mxh > c.dw.y_elems ||
       (size_t)fwd_groups(c.n) * nv * F.Mz * F.Mxh > c.dw.part_elems)
     return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
@@ -565,6 +831,16 @@ int launch_project_fft(const Ctx &c, const float *src, const int *dviews, int nv
 int launch_backproject_fft(const Ctx &c, const float *planes, const int *dviews, int nv, const float *E,
                            const DrfDev &D, float scale, float *bck) {
   const DrfFft &F = D.fft;
+  if (F.fused) {
+    PlaneArgs a = plane_args(c, D, planes, c.pln, 0, E, dviews, scale, bck);
+    a.nb = nv;
+    DPLANE_DISPATCH(F.Mx, {
+      TRY_RC(dplane_attrs<LL>());
+      k_dplane_bck<LL><<<dplane_ctas(nv * c.n), DP_NT, DPlane<LL>::SMEM, c.st>>>(a, F.twx);
+      CU_LAUNCHED();
+    });
+    return IRLCU_OK;
+  }
   if ((size_t)nv * c.n * F.G * F.Mxh > c.dw.s_elems)
     return set_error(IRLCU_EARG, "DRF FFT batch of %d views exceeds the work buffers", nv);
   const RowSrc r = plane_rows(c, D, planes, c.pln, 0, E, dviews);

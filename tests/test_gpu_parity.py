@@ -113,11 +113,13 @@ def test_genprj_per_view(product, orc, tmp_path, variant):
         assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (variant, vi, rel_l2(got[vi], want[vi]))
 
 
-@pytest.mark.parametrize("engine", ["direct", "fft"])
+@pytest.mark.parametrize("engine", ["direct", "fft", "fft_lines"])
 def test_genprj_drf_engines(product, orc, tmp_path, monkeypatch, engine):
-    """Both DRF engines (direct convolution kernels and the Fourier-domain
-    engine) against the oracle on a 33 x 33 DRF with axial padding."""
-    monkeypatch.setenv("IRLCU_DRF_ENGINE", engine)
+    """The DRF engines (direct convolution kernels; the Fourier-domain
+    engine with one CTA per plane, and in its row/column-pass form) against
+    the oracle on a 33 x 33 DRF with axial padding."""
+    monkeypatch.setenv("IRLCU_DRF_ENGINE", "fft" if engine.startswith("fft") else engine)
+    monkeypatch.setenv("IRLCU_DRF_PLANE", "0" if engine == "fft_lines" else "1")
     case = W.full128(seed=2150, n=48, nviews=6, subsets=2, iterations=1, drf_max_offs=17, with_srf=False)
     files = case.write_tables(str(tmp_path))
     opts = {"iAxialPadLength": 4, "iAxialAvgLength": 3}
@@ -314,9 +316,12 @@ def test_osem_norm_files_and_errors(product, tmp_path):
 
 # --------------------------------------------------------- full-size checks
 
-def test_full_size_views_against_oracle(product, orc, tmp_path):
+@pytest.mark.parametrize("engine", ["direct", "fft"])
+def test_full_size_views_against_oracle(product, orc, tmp_path, monkeypatch, engine):
     """Two views of the full-physics 128^3 case (DRF 33x33 + ESSE c=2)
-    against the oracle."""
+    against the oracle, with each DRF engine (the Fourier-domain one on its
+    160 x 160 one-CTA-per-plane grid)."""
+    monkeypatch.setenv("IRLCU_DRF_ENGINE", engine)
     full = W.full128(seed=2000)
     sel = [0, 37]
     case = W.Case(full.name, full.n, full.nz, full.pix, len(sel), 1, 1, full.counts, full.act, full.atn,
