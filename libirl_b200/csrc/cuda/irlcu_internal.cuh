@@ -58,6 +58,7 @@ struct EsseDev {
   float2 *kft[3] = {nullptr, nullptr, nullptr};  // kernel spectra [ky][kz][kxh]
   float2 *kftT[3] = {nullptr, nullptr, nullptr}; // kx-major copies [kxh][ky][kz]
   bool fused = false;         // y-z transforms in one shared-memory kernel
+  bool yz_reg = false;        // ... with register transforms (kftT in position order)
 };
 
 // ESSE work buffers of one context (k_esse.cu)

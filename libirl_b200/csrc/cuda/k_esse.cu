@@ -24,8 +24,10 @@
 // of two from 8 to 1024.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
+#include "esse_yz.cuh"
 #include "fft_core.cuh"
 #include "irlcu_internal.cuh"
 
@@ -358,6 +360,54 @@ __global__ void __launch_bounds__(YZ_NT, 1) k_esse_yz(YzArgs a, const float2 *__
       D[e] = G[y * L + z];
     }
     __syncthreads();
+  }
+}
+
+// y-z plane with register transforms (esse_yz.cuh): one CTA per (kx, view),
+// every transform in place in the plane; both terms from one forward
+// spectrum.  Needs nyv <= L / 2 (the terms' cropped rows share the plane).
+template <int L>
+__global__ void __launch_bounds__(EY_NT, 1) k_esse_yz_reg(YzArgs a, const float2 *__restrict__ twg) {
+  using D = EYz<L>;
+  extern __shared__ __align__(16) float2 eys[];
+  float2 *F = eys, *C = F + D::F_ELEMS, *tw = C + 2 * D::C_ELEMS;
+  const int kx = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+  const int nyv = a.nyv, nzv = a.nzv, nt = a.nt;
+  for (int i = tid; i < L; i += EY_NT) tw[i] = twg[i];
+  const size_t plane = ((size_t)b * a.kxh + kx) * nyv * nzv;
+  ey_load<L>(tid, F, a.A + plane, nyv, nzv);
+  __syncthreads();
+  ey_z_fwd_a<L>(tid, F, tw, nyv, nzv);
+  __syncthreads();
+  ey_z_fwd_b<L>(tid, F, nyv);
+  __syncthreads();
+  ey_y_fwd_a<L>(tid, F, tw, nyv);
+  __syncthreads();
+  const float2 *K0 = a.K[0] + (size_t)kx * L * L;
+  const float2 *K1 = nt > 1 ? a.K[1] + (size_t)kx * L * L : K0;
+  for (int z0 = 0; z0 < L; z0 += EY_ZC) {
+    ey_y_mid<L>(tid, F, C, tw, K0, K1, nt, z0);
+    __syncthreads();
+    ey_y_inv_c<L>(tid, F, C, nt, nyv, z0);
+    __syncthreads();
+  }
+  ey_z_inv_b<L>(tid, F, tw, nt * nyv);
+  __syncthreads();
+  ey_z_inv_c<L>(tid, F, nt * nyv, nzv);
+  __syncthreads();
+  ey_store<L>(tid, F, a.D[0] + plane, nt > 1 ? a.D[1] + plane : nullptr, nt, nyv, nzv);
+}
+
+// [ky][kz][kxh] -> [kxh][ky][p], p the position of kz after the forward z
+// transform of k_esse_yz_reg (kz = (p mod N2) N1 + p / N2)
+__global__ void k_spec_kpos(const float2 *__restrict__ in, float2 *__restrict__ out, int L, int kxh, int N1, int N2) {
+  const size_t tot = (size_t)L * L * kxh;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e % L);
+    const size_t r = e / L;
+    const int ky = (int)(r % L), kx = (int)(r / L);
+    const int kz = (p % N2) * N1 + p / N2;
+    out[e] = in[((size_t)ky * L + kz) * kxh + kx];
   }
 }
 
@@ -776,6 +826,7 @@ void esse_free(Ctx &c) {
   c.esse.on = false;
   c.esse.zero = false;
   c.esse.fused = false;
+  c.esse.yz_reg = false;
   EsseWork &w = c.ew;
   dev_free(w.twx, c.st);
   dev_free(w.twy, c.st);
@@ -860,14 +911,40 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     }
   }
   dev_free(dgrid, c.st);
-  // fused y-z kernel when the plane fits in shared memory
+  // fused y-z kernel when the plane fits in shared memory: the register
+  // form when the cropped rows of both terms fit the plane (nyv <= L/2),
+  // else the pass form (IRLCU_ESSE_YZ=pass forces the latter)
   {
     int dev = 0, maxsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const int L = E.ky;
+    const char *yzenv = getenv("IRLCU_ESSE_YZ");
+    size_t rsm = 0;
+    switch (L) {
+      case 32: rsm = EYz<32>::SMEM; break;
+      case 64: rsm = EYz<64>::SMEM; break;
+      case 128: rsm = EYz<128>::SMEM; break;
+      default: break;
+    }
+    if (E.ky == E.kz && rsm && 2 * w.nyv <= L && rsm <= (size_t)maxsm && !(yzenv && !strcmp(yzenv, "pass"))) {
+      const int N1 = L % 16 == 0 ? 16 : 8;
+      for (int t = 0; t < E.nterms; ++t) {
+        CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kftT[t]), sizeof(float2) * spec, c.st));
+        k_spec_kpos<<<592, 256, 0, c.st>>>(E.kft[t], E.kftT[t], L, E.kxh, N1, L / N1);
+        CU_LAUNCHED();
+      }
+      switch (L) {
+        case 32: CU_TRY(cudaFuncSetAttribute(k_esse_yz_reg<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm)); break;
+        case 64: CU_TRY(cudaFuncSetAttribute(k_esse_yz_reg<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm)); break;
+        default: CU_TRY(cudaFuncSetAttribute(k_esse_yz_reg<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm)); break;
+      }
+      CU_TRY(cudaStreamSynchronize(c.st));
+      E.fused = true;
+      E.yz_reg = true;
+    }
     const size_t sm = yz_smem(L, w.nyv);
-    if (E.ky == E.kz && (L == 32 || L == 64 || L == 128) && sm <= (size_t)maxsm) {
+    if (!E.fused && E.ky == E.kz && (L == 32 || L == 64 || L == 128) && sm <= (size_t)maxsm) {
       for (int t = 0; t < E.nterms; ++t) {
         CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kftT[t]), sizeof(float2) * spec, c.st));
         k_spec_kmajor<<<592, 256, 0, c.st>>>(E.kft[t], E.kftT[t], E.ky, E.kz, E.kxh);
@@ -931,7 +1008,15 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     ya.nyv = nyv;
     ya.nzv = nzv;
     ya.nt = E.nterms;
-    {
+    if (E.yz_reg) {
+      dim3 grid_(kxh, nv);
+      switch (E.ky) {
+        case 32: k_esse_yz_reg<32><<<grid_, EY_NT, EYz<32>::SMEM, c.st>>>(ya, w.twy); break;
+        case 64: k_esse_yz_reg<64><<<grid_, EY_NT, EYz<64>::SMEM, c.st>>>(ya, w.twy); break;
+        default: k_esse_yz_reg<128><<<grid_, EY_NT, EYz<128>::SMEM, c.st>>>(ya, w.twy); break;
+      }
+      CU_LAUNCHED();
+    } else {
       dim3 grid_(kxh, nv);
       const size_t sm = yz_smem(E.ky, nyv);
       switch (E.ky) {

@@ -148,6 +148,19 @@ def test_drf_half_width_beyond_direct_limit(product, orc, tmp_path, monkeypatch)
         assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (vi, rel_l2(got[vi], want[vi]))
 
 
+@pytest.mark.parametrize("form", ["reg", "pass"])
+def test_genprj_esse_yz_forms(product, orc, tmp_path, monkeypatch, form):
+    """The y-z part of ESSE in its register-transform form and its
+    Stockham-pass form, on a 64^3 grid with both Taylor terms."""
+    monkeypatch.setenv("IRLCU_ESSE_YZ", form)
+    case = W.full128(seed=2180, n=64, nviews=6, subsets=2, iterations=1, collapse=2, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    got = gpu_genprj(product, case, files)
+    want = orc.Problem(case).genprj()
+    for vi in range(case.nviews):
+        assert rel_l2(got[vi], want[vi]) <= VIEW_TOL, (form, vi, rel_l2(got[vi], want[vi]))
+
+
 @pytest.mark.parametrize("n,collapse", [(40, 2), (48, 2), (24, 1)])
 def test_genprj_esse_mixed_radix_grid(product, orc, tmp_path, n, collapse):
     """ESSE grids of ceil(2 N / c) that are not powers of two (40 = 8*5,
