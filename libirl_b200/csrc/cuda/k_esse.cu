@@ -27,11 +27,18 @@
 #include <cstring>
 #include <vector>
 
+#include "esse_rows.cuh"
 #include "esse_yz.cuh"
 #include "fft_core.cuh"
 #include "irlcu_internal.cuh"
 
 namespace irlcu {
+
+#define TRY_ESSE(x)      \
+  do {                 \
+    int rc_ = (x);     \
+    if (rc_) return rc_; \
+  } while (0)
 
 // ----------------------------------------------------------- pass kernels
 
@@ -172,6 +179,76 @@ __global__ void k_fft_row_inv(RowInvArgs a, const float2 *__restrict__ twg) {
     }
   }
 }
+
+// x transforms with register transforms (esse_rows.cuh), kx-major layout:
+// one CTA per ER_LW row pairs of a view (and term)
+template <int L>
+__global__ void __launch_bounds__(ER_NT, 2) k_esse_row_fwd_reg(RowFwdArgs a, const float2 *__restrict__ twg) {
+  using D = ERow<L>;
+  extern __shared__ __align__(16) float2 ers[];
+  float2 *X = ers, *tw = X + D::X_ELEMS;
+  const int tid = threadIdx.x, b = blockIdx.y, w0 = blockIdx.x * ER_LW;
+  const int nrows = a.nyv * a.nzv;
+  for (int i = tid; i < L; i += ER_NT) tw[i] = twg[i];
+  __syncthreads();
+  er_fwd_a<L>(tid, w0, X, tw, a.rot + (size_t)b * a.vox, a.n, a.nz, a.c, a.nzv, a.nxv, nrows);
+  __syncthreads();
+  constexpr int NB = (ER_LW * D::N1 + ER_NT - 1) / ER_NT;
+  float2 u[NB][D::N2];
+#pragma unroll
+  for (int r = 0; r < NB; ++r) {
+    const int it = tid + r * ER_NT;
+    if (it < ER_LW * D::N1) er_b<L, false>(it, X, u[r]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NB; ++r) {
+    const int it = tid + r * ER_NT;
+    if (it < ER_LW * D::N1) er_fwd_b_store<L>(it, u[r], X);
+  }
+  __syncthreads();
+  er_fwd_unpack<L>(tid, w0, X, a.out + (size_t)b * a.kxh * nrows, nrows);
+}
+
+// grid (row-pair blocks, view, term)
+template <int L>
+__global__ void __launch_bounds__(ER_NT, 2) k_esse_row_inv_reg(RowInvArgs a, const float2 *__restrict__ twg) {
+  using D = ERow<L>;
+  extern __shared__ __align__(16) float2 ers[];
+  float2 *X = ers, *tw = X + D::X_ELEMS;
+  const int tid = threadIdx.x, b = blockIdx.y, t = blockIdx.z, w0 = blockIdx.x * ER_LW;
+  const int nrows = a.nyv * a.nzv;
+  for (int i = tid; i < L; i += ER_NT) tw[i] = twg[i];
+  __syncthreads();
+  er_inv_a<L>(tid, w0, X, tw, (t ? a.in[1] : a.in[0]) + (size_t)b * a.kxh * nrows, nrows);
+  __syncthreads();
+  float *out = (t ? a.out[1] : a.out[0]) + (size_t)b * nrows * a.nxv;
+  for (int it = tid; it < ER_LW * D::N1; it += ER_NT) {
+    float2 u[D::N2];
+    er_b<L, true>(it, X, u);
+    er_inv_b_store<L>(it, w0, u, out, nrows, a.nxv, a.scale);
+  }
+}
+
+static bool er_len_ok(int L) { return L == 32 || L == 64 || L == 128 || L == 256; }
+
+static int er_attrs(int L) {
+  static bool done = false;
+  if (done) return IRLCU_OK;
+  CU_TRY(cudaFuncSetAttribute(k_esse_row_fwd_reg<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
+  CU_TRY(cudaFuncSetAttribute(k_esse_row_inv_reg<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
+  (void)L;
+  done = true;
+  return IRLCU_OK;
+}
+
+#define ER_DISPATCH(L, ...)                                  \
+  switch (L) {                                               \
+    case 32: { constexpr int LL = 32; __VA_ARGS__; } break;  \
+    case 64: { constexpr int LL = 64; __VA_ARGS__; } break;  \
+    case 128: { constexpr int LL = 128; __VA_ARGS__; } break; \
+    default: { constexpr int LL = 256; __VA_ARGS__; } break; \
+  }
 
 // Column pass (z or y axis): lines are (outer, kx); 16 consecutive kx per
 // CTA for coalescing.  Input point p of line (b, o, kx) at
@@ -993,7 +1070,16 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     ra.zext = nzv;
     ra.kxh = kxh;
     ra.kmajor = 1;
-    {
+    // x transforms: register form unless IRLCU_ESSE_YZ=pass selects the
+    // pass forms of all three transforms
+    const bool reg_rows = er_len_ok(E.kx) && E.yz_reg;
+    const int lines = (nyv * nzv + 1) / 2;
+    if (reg_rows) {
+      TRY_ESSE(er_attrs(E.kx));
+      dim3 grid_((lines + ER_LW - 1) / ER_LW, nv);
+      ER_DISPATCH(E.kx, k_esse_row_fwd_reg<LL><<<grid_, ER_NT, ERow<LL>::SMEM, c.st>>>(ra, w.twx));
+      CU_LAUNCHED();
+    } else {
       dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
       LDISPATCH(E.kx, k_fft_row_fwd, grid_, 256, 0, c.st, ra, w.twx);
       CU_LAUNCHED();
@@ -1038,7 +1124,11 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     ri.kxh = kxh;
     ri.scale = (float)(1.0 / ((double)E.kx * E.ky * E.kz));
     ri.kmajor = 1;
-    {
+    if (reg_rows) {
+      dim3 grid_((lines + ER_LW - 1) / ER_LW, nv, E.nterms);
+      ER_DISPATCH(E.kx, k_esse_row_inv_reg<LL><<<grid_, ER_NT, ERow<LL>::SMEM, c.st>>>(ri, w.twx));
+      CU_LAUNCHED();
+    } else {
       dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
       LDISPATCH(E.kx, k_fft_row_inv, grid_, 256, 0, c.st, ri, w.twx);
       CU_LAUNCHED();

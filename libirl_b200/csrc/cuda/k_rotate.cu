@@ -97,11 +97,13 @@ struct SmemX {
   int ld;
   __device__ float operator()(int r, int c) const { return p[r * ld + c]; }
 };
-struct GlobSlice {  // rows y*nz*n + k*n of a volume
+struct GlobSlice {  // rows y*nz*n + k*n of a volume; outside the slice: 0
   const float *__restrict__ p;
   int n;
   size_t rs;
-  __device__ float operator()(int y, int x) const { return __ldg(p + (size_t)y * rs + x); }
+  __device__ float operator()(int y, int x) const {
+    return (y < 0 || y >= n || x < 0 || x >= n) ? 0.f : __ldg(p + (size_t)y * rs + x);
+  }
 };
 struct GlobX {
   const float *__restrict__ p;
@@ -181,7 +183,9 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
   }
   __syncthreads();
   // source slice element (row y, column x)
+  // taps outside the slice read as 0 (weight 0: see shear_tap)
   auto SL = [&](int yy, int xx) -> float {
+    if (yy < 0 || yy >= n || xx < 0 || xx >= n) return 0.f;
     if (STAGE) return s_slice[yy * ld + xx];
     return __ldg(s + (size_t)yy * rs + xx);
   };
@@ -241,6 +245,168 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
         out = lerp2(f1, y2[0], f2, y2[1]);
       }
       orow[x] = out;
+    }
+  }
+}
+
+// Column-walk form: one CTA of 32 x 16 threads per (slice, view), only X in
+// shared memory (two CTAs per SM).
+//   pass 1: X[j][i] from the source slice through L1; the thread index runs
+//           along the source row that the rotation reads contiguously (i
+//           for the unflipped cases, j for the 90-degree-flipped ones);
+//   pass 2: the y shear in place: each column c of X is shifted by its own
+//           csh[c] with weights cf1[c], cf2[c], one thread per column walking
+//           the rows away from the rows it still has to read (ascending
+//           for csh >= 0, descending otherwise), so every intermediate value
+//           is computed once;
+//   pass 3: the second x shear, two reads of the y-sheared row per output.
+// Every product and sum is rounded as in the fused form above, so the
+// output is the same bit for bit.
+// Pass 1 reads source taps p(i) and p(i+1) of one source line (taps
+// outside [0, n) read as 0: for odd n the middle row's last second tap is
+// one past the line, with weight f2 = 0 exactly), where
+//   b180 = 0: p(i) = i + sh - iadd,            line = row j (col n-j-1 if b90)
+//   b180 = 1: p(i) = n - i - (sh - iadd + 1),  line = row n-j-1 (col j if b90)
+// so the second tap of i is the first tap of i + 1.
+//   unflipped (rows): a warp per row j, lanes along i; the second tap comes
+//     from the next lane;
+//   flipped (columns): a lane per j (consecutive columns of the source),
+//     walking a quarter of the i range with the tap carried along.
+__device__ __forceinline__ int shear_tap(const RotHdr &h, int n, int sh, int i) {
+  return h.b180 ? n - i - (sh - h.iadd + 1) : i + sh - h.iadd;
+}
+
+__device__ __forceinline__ void shear_pass1_rows(const float *__restrict__ s, int rs, float *s_x, int xld, int n,
+                                                 const RotHdr &h, const int *t_rsh, const float *t_rf1,
+                                                 const float *t_rf2, const int *t_st, const int *t_en, int warp,
+                                                 int lane) {
+  for (int j = warp; j < n; j += SH_TY) {
+    const int sh = t_rsh[j];
+    const int lo = t_st[j] - sh + h.iadd, hi = t_en[j] - sh - 1 + h.iadd;
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float *line = s + (h.b180 ? n - j - 1 : j) * rs;
+    float *xr = s_x + j * xld;
+    // taps read: i in [lo, min(hi, mdim)] (the second tap of i is tap i + 1)
+    const int hl = min(hi, h.mdim);
+    for (int i0 = 0; i0 < h.mdim; i0 += SH_TX) {
+      const int i = i0 + lane;
+      const int p = shear_tap(h, n, sh, i), pn = shear_tap(h, n, sh, i + 1);
+      const float v = (i >= lo && i <= hl && p >= 0 && p < n) ? __ldg(line + p) : 0.f;
+      float vn = __shfl_down_sync(0xffffffffu, v, 1);
+      if (lane == SH_TX - 1) vn = (i + 1 >= lo && i + 1 <= hl && pn >= 0 && pn < n) ? __ldg(line + pn) : 0.f;
+      if (i < h.mdim) xr[i] = (i >= lo && i < hi) ? lerp2(f1, v, f2, vn) : 0.f;
+    }
+  }
+}
+
+__device__ __forceinline__ void shear_pass1_cols(const float *__restrict__ s, int rs, float *s_x, int xld, int n,
+                                                 const RotHdr &h, const int *t_rsh, const float *t_rf1,
+                                                 const float *t_rf2, const int *t_st, const int *t_en, int tid) {
+  constexpr int NCH = 4;  // i chunks per j
+  const int nt = SH_TX * SH_TY;
+  const int per = (h.mdim + NCH - 1) / NCH;
+  for (int e = tid; e < n * NCH; e += nt) {
+    const int ch = e / n, j = e - ch * n;
+    const int sh = t_rsh[j];
+    const int lo = t_st[j] - sh + h.iadd, hi = t_en[j] - sh - 1 + h.iadd;
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float *col = s + (h.b180 ? j : n - j - 1);
+    float *xc = s_x + j * xld;
+    const int i0 = ch * per, i1 = min(h.mdim, i0 + per);
+    const int p0 = shear_tap(h, n, sh, i0);
+    float v = (i0 >= lo && i0 <= hi && p0 >= 0 && p0 < n) ? __ldg(col + p0 * rs) : 0.f;
+    for (int i = i0; i < i1; ++i) {
+      const int pn = shear_tap(h, n, sh, i + 1);
+      const float vn = (i + 1 >= lo && i + 1 <= hi && pn >= 0 && pn < n) ? __ldg(col + pn * rs) : 0.f;
+      xc[i] = (i >= lo && i < hi) ? lerp2(f1, v, f2, vn) : 0.f;
+      v = vn;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__restrict__ src, size_t src_stride,
+                                                             float *__restrict__ dst, size_t dst_stride,
+                                                             const int *__restrict__ views, int rot_base,
+                                                             RotTabs T, const int *__restrict__ sup_st,
+                                                             const int *__restrict__ sup_en, int n, int nz,
+                                                             int xld) {
+  extern __shared__ float sm[];
+  float *s_x = sm;  // n * xld
+  int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xld);
+  int *t_st = t_rsh + n, *t_en = t_st + n;
+  float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
+  int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
+  float *t_cf1 = reinterpret_cast<float *>(t_csh + xld), *t_cf2 = t_cf1 + xld;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH_TY;
+  const int k = blockIdx.x, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  const float *s = src + (size_t)v * src_stride + (size_t)k * n;
+  float *d = dst + (size_t)v * dst_stride + (size_t)k * n;
+  const int rs = nz * n;
+  for (int i = tid; i < n; i += nt) {
+    t_rsh[i] = T.row_sh[(size_t)r * n + i];
+    t_rf1[i] = T.row_f1[(size_t)r * n + i];
+    t_rf2[i] = T.row_f2[(size_t)r * n + i];
+    t_st[i] = sup_st[i];
+    t_en[i] = sup_en[i];
+  }
+  for (int i = tid; i < h.mdim; i += nt) {
+    t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
+    t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
+    t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
+  }
+  __syncthreads();
+  if (h.b90)
+    shear_pass1_cols(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, tid);
+  else
+    shear_pass1_rows(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, ty, tx);
+  __syncthreads();
+  // pass 2: Y[j][c] = lerp(X[j+jt][c], X[j+jt+1][c]) for jj = j + iadd in
+  // [max(0, -jt), min(mdim, mdim - jt - 1)), else 0; X rows outside [0, n)
+  // are 0
+  for (int c = tid; c < h.mdim; c += nt) {
+    const int jt = t_csh[c];
+    const float w1 = t_cf1[c], w2 = t_cf2[c];
+    const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
+    float *col = s_x + c;
+    if (jt >= 0) {
+      // rows read (j + jt, j + jt + 1) are never below the row written
+      float x0 = jt < n ? col[jt * xld] : 0.f;
+#pragma unroll 4
+      for (int j = 0; j < n; ++j) {
+        const int r1 = j + jt + 1;
+        const float x1 = r1 < n ? col[r1 * xld] : 0.f;
+        col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        x0 = x1;
+      }
+    } else {
+      // rows read are below the row written: walk downwards
+      float x1 = (n + jt >= 0 && n + jt < n) ? col[(n + jt) * xld] : 0.f;
+#pragma unroll 4
+      for (int j = n - 1; j >= 0; --j) {
+        const int r0 = j + jt;
+        const float x0 = r0 >= 0 ? col[r0 * xld] : 0.f;
+        col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        x1 = x0;
+      }
+    }
+  }
+  __syncthreads();
+  // pass 3: output (j, x) = lerp(Y[j][a], Y[j][a+1]), a = x + sh + iadd; a
+  // warp per row, the second tap from the next lane
+  for (int j = ty; j < n; j += SH_TY) {
+    const int sh = t_rsh[j], st = t_st[j], en = t_en[j];
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float *yr = s_x + j * xld;
+    float *orow = d + (size_t)j * rs;
+    const int off = sh + h.iadd;
+    for (int x0 = 0; x0 < n; x0 += SH_TX) {
+      const int x = x0 + tx, a = x + off;
+      const float y0 = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
+      float y1 = __shfl_down_sync(0xffffffffu, y0, 1);
+      if (tx == SH_TX - 1) y1 = (a + 1 >= 0 && a + 1 < h.mdim) ? yr[a + 1] : 0.f;
+      if (x < n) orow[x] = (x >= st + 1 && x < en - 1) ? lerp2(f1, y0, f2, y1) : 0.f;
     }
   }
 }
@@ -381,6 +547,21 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   // (IRLCU_SHEAR_STAGE = 1 / 0 forces either form)
   const size_t sm_stage = shear_smem_bytes(n, xld, true), sm_glob = shear_smem_bytes(n, xld, false);
   const char *env = getenv("IRLCU_SHEAR_STAGE");
+  // column-walk form unless IRLCU_SHEAR_STAGE selects the fused one; its
+  // X rows get an odd stride (bank-conflict-free column walks)
+  const int xo = xld | 1;
+  const size_t smc = shear_smem_bytes(n, xo, false);
+  if (!env && smc <= (size_t)maxsm) {
+    static size_t s_cw = 0;
+    if (smc > s_cw) {
+      CU_TRY(cudaFuncSetAttribute(k_shear_cw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
+      s_cw = smc;
+    }
+    k_shear_cw<<<dim3(nz, nv), dim3(SH_TX, SH_TY), smc, c.st>>>(src, src_stride, dst, dst_stride, dviews, rot_base,
+                                                                c.rot, c.sup_start, c.sup_end, n, nz, xo);
+    CU_LAUNCHED();
+    return IRLCU_OK;
+  }
   bool stage = 2 * sm_stage + 2048 <= (size_t)smsm;
   if (env && env[0] == '1') stage = true;
   if (env && env[0] == '0') stage = false;

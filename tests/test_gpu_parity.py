@@ -68,9 +68,14 @@ def gpu_osem(lib, case, files, meas, iterations=None, opts=None, parms=None, krn
 # ------------------------------------------------------------- rotations
 
 @pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (200, 1)])
-@pytest.mark.parametrize("fast", [1, 0])
-def test_rotation_bit_exact(product, orc, n, nz, fast):
+@pytest.mark.parametrize("fast", [1, 0, "fused"])
+def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
+    """Both rotators bit for bit against the oracle; the three-shear one in
+    its column-walk form (default) and its fused-pass form."""
     import libirl_b200 as L
+    if fast == "fused":
+        monkeypatch.setenv("IRLCU_SHEAR_STAGE", "0")
+        fast = 1
     rng = np.random.default_rng(n * 7 + nz)
     vol = rng.random((n, nz, n), dtype=np.float32)
     g = L.IrlcuGeom(n, nz, 1, fast, 1)
