@@ -25,6 +25,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -377,47 +378,62 @@ def _hbm_peak():
 
 
 def make_roofline(prof, case, grids):
-    """Roofline of the dominant stage of an OSEM iteration.  Both candidate
-    stages are FFT work that the per-unit figures bound by HBM traffic:
+    """Roofline of the stage with the largest device time in an OSEM
+    iteration, with the other stages beside it.  Algorithmic bytes per view
+    follow the per-unit figures of the hot-path scope table (b = 4 bytes,
+    V = N^2 Nz voxels, P = N Nz bins):
 
-      DRF (Fourier-domain engine, projector + backprojector): per plane one
-        2D transform forward and two backward, each 2 passes (rows, columns)
-        of >= 2 x 4 bytes x Mz*Mx (the transform grid);
-      ESSE: per view three 3D transforms (one forward, two inverse) of
-        3 passes each of >= 2 x 4 bytes x Kx*Ky*Kz, plus 3 x 4 bytes x voxels
-        for the depth / density combination.
+      ESSE: 3 3D transforms x 3 passes of >= 2 b G (G = Kx Ky Kz), plus
+        3 b V for the depth/density combination;
+      DRF, Fourier domain (projector + backprojector): per plane 3 2D
+        transforms (one forward, forward + inverse backward) x 2 passes of
+        >= 2 b Mz Mx; also 5 n log2 n FP32 FLOP per complex transform of
+        n = Mz Mx points, against the nominal FP32 peak (the one-CTA-per-
+        plane kernels keep the passes in shared memory, so their DRAM
+        traffic is far below those bytes);
+      rotate: 2 b V per view;
+      unrotate + accumulate: 2 b V per view (unrotation) + b V per view
+        (accumulation read) + 2 b V per subset (accumulator).
 
     achieved = those bytes per subset / the stage's device time per subset
     (CUDA events around the stage on the library stream); peak = the
-    measured HBM copy bandwidth."""
+    measured HBM copy bandwidth.  `traffic` = ncu DRAM read + write bytes
+    per subset from profiles/osem_subset_full128_traffic.md."""
     peak, src = _hbm_peak()
     n, nz = case.n, case.nz
     vox = n * nz * n
     mz, mx, kx, ky, kz = grids
-    per_view = {}
-    if mz and mx:
-        per_view["drf"] = n * 3 * 2 * (2 * 4 * mz * mx)
-    if kx:
-        per_view["esse"] = 3 * 3 * (2 * 4 * kx * ky * kz) + 3 * 4 * vox
-    idx = {"drf": (2, 4), "esse": (1,)}
-    names = {"drf": "k_dfft_rows_fwd / k_dfft_cols_fwd / k_dfft_cols / k_dfft_rows_inv (Fourier-domain DRF)",
-             "esse": "k_fft_row_fwd / k_esse_yz / k_fft_row_inv / k_expand_y / k_smooth_z / k_smooth_x_combine (ESSE)"}
-    traffic_keys = {"drf": ("drf_fft_full128.md", "traffic_bytes_per_subset"),
-                    "esse": ("esse_full128.md", "traffic_bytes_per_subset")}
     subsets = case.subsets
     per = case.nviews // subsets
+    b = 4
+    stages = []
+    if kx:
+        stages.append(("esse", (1,), per * (3 * 3 * (2 * b * kx * ky * kz) + 3 * b * vox),
+                       "k_esse_row_fwd_reg / k_esse_yz_reg / k_esse_row_inv_reg / k_expand_y / k_smooth_z / "
+                       "k_smooth_x_combine (ESSE)"))
+    if mz and mx:
+        stages.append(("drf", (2, 4), per * n * 3 * 2 * (2 * b * mz * mx),
+                       "k_dplane_fwd / k_dplane_fwd_finish / k_dplane_bck (Fourier-domain DRF, one CTA per plane)"))
+    stages.append(("rotate", (0,), per * 2 * b * vox, "k_shear_cw (three-shear rotation)"))
+    stages.append(("unrotate", (5,), per * 3 * b * vox + 2 * b * vox, "k_shear_cw + k_accumulate"))
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal SIMT FP32 TFLOP/s (not measured)
     out = []
-    for k, bytes_view in per_view.items():
-        ms = sum(prof.ms[i] for i in idx[k]) / subsets
+    for k, idx, bytes_subset, kern in stages:
+        ms = sum(prof.ms[i] for i in idx) / subsets
         if ms <= 0:
             continue
-        b = bytes_view * per
-        gbs = b / (ms * 1e-3) / 1e9
-        tr = _traffic_from_profiles(*traffic_keys[k])
-        out.append({"stage": k, "kernel": names[k], "bound": "hbm", "achieved": round(gbs, 1), "peak": peak,
-                    "unit": "GB/s", "frac": round(gbs / peak, 3), "peak_source": src,
-                    "traffic": tr, "algorithmic_bytes_per_launch": int(b), "launch_ms": round(ms, 4),
-                    "launch": f"one subset ({per} views)"})
+        gbs = bytes_subset / (ms * 1e-3) / 1e9
+        tr = _traffic_from_profiles("osem_subset_full128_traffic.md", "traffic_bytes_per_subset_" + k)
+        r = {"stage": k, "kernel": kern, "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+             "frac": round(gbs / peak, 3), "peak_source": src, "traffic": tr,
+             "algorithmic_bytes_per_launch": int(bytes_subset), "launch_ms": round(ms, 4),
+             "launch": f"one subset ({per} views)"}
+        if k == "drf":
+            flop = per * n * 3 * 5 * (mz * mx) * math.log2(mz * mx)
+            tf = flop / (ms * 1e-3) / 1e12
+            r["fp32"] = {"achieved_tflops": round(tf, 2), "peak_tflops": round(fp32_peak, 1),
+                         "frac": round(tf / fp32_peak, 3), "peak_source": "nominal (148 SMs x 128 lanes x 2 x 1.965 GHz)"}
+        out.append(r)
     if not out:
         return None
     out.sort(key=lambda r: -r["launch_ms"])
