@@ -568,6 +568,9 @@ constexpr int WALK_PF = 8;
 
 // expansion along y with the y smoothing: thread per (b, z, x) line of the
 // fine grid; g = cropped coarse result [B][nyv][nzv][nxv]; C = collapse
+// (n = C nyv).  The walk goes coarse row by coarse row: each coarse value
+// is loaded and scaled once and feeds the C fine steps whose look-ahead
+// input (fine row y + H) it is; loads run WALK_PF coarse rows ahead.
 template <int C>
 __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1,
                                                   float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
@@ -579,25 +582,39 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
   const int b = (int)(e / pln);
   const int i = (int)(e - (size_t)b * pln);
   const int z = i / n, x = i - z * n;
-  const size_t gs = (size_t)nzv * nxv;
+  const int gs = nzv * nxv;
   for (int t = 0; t < nt; ++t) {
-    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (size_t)(z / C) * nxv + x / C;
+    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (z / C) * nxv + x / C;
     float *o = (t == 0 ? t0 : t1) + (size_t)b * pln * n + i;
     LineSmoother<H> L;
+    float cv[WALK_PF];
 #pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = expand_scale<C>(__ldg(g + (size_t)(q / C) * gs));
-    for (int y0 = 0; y0 < n; y0 += WALK_PF) {
+    for (int q = 0; q < WALK_PF; ++q) cv[q] = expand_scale<C>(__ldg(g + min(q, nyv - 1) * gs));
+    // fine rows q < H look ahead into coarse row 0
+#pragma unroll
+    for (int q = 0; q < H; ++q) L.in[q] = cv[0];
+    for (int yc0 = 0; yc0 < nyv; yc0 += WALK_PF) {
       float nx[WALK_PF];
 #pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(g + (size_t)(min(y0 + q + H, n - 1) / C) * gs);
+      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(g + min(yc0 + WALK_PF + q, nyv - 1) * gs);
+      const float cnext = expand_scale<C>(nx[0]);
 #pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) {
-        const int y = y0 + q;
-        if (y < n) {
-          L.in[H] = expand_scale<C>(nx[q]);
-          o[(size_t)y * pln] = L.step(y, n);
+      for (int r = 0; r < WALK_PF; ++r) {
+        const int yc = yc0 + r;
+        if (yc < nyv) {
+          // coarse row yc and the next one (the last row repeats: fine
+          // look-ahead rows past the end read the last row, as min(y+H, n-1))
+          const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : cnext;
+#pragma unroll
+          for (int q = 0; q < C; ++q) {
+            const int y = yc * C + q;
+            L.in[H] = ((q + H) / C == 0) ? ca : cb;
+            o[(size_t)y * pln] = L.step(y, n);
+          }
         }
       }
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) cv[q] = expand_scale<C>(nx[q]);
     }
   }
 }
@@ -944,6 +961,11 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
   E.pix = e->pix;
   E.cntr = e->cntr_pix_fac;
   EsseWork &w = c.ew;
+  // CollapseByFac (krnlprj3d.c:559-562) requires the factor to divide the
+  // image dimensions
+  if (E.collapse < 1 || c.n % E.collapse != 0 || c.nz % E.collapse != 0)
+    return set_error(IRLCU_EARG, "ESSE collapse factor %d does not evenly divide the image dimensions %d, %d",
+                     E.collapse, c.n, c.nz);
   w.nxv = c.n / E.collapse;
   w.nyv = c.n / E.collapse;
   w.nzv = c.nz / E.collapse;

@@ -276,25 +276,46 @@ __device__ __forceinline__ int shear_tap(const RotHdr &h, int n, int sh, int i) 
   return h.b180 ? n - i - (sh - h.iadd + 1) : i + sh - h.iadd;
 }
 
+// per row j of pass 1: tap(i) = c0 + dir i; taps are read for i in
+// [la, lb] (the valid interval [lo, min(hi, mdim)] clipped to taps inside
+// [0, n)); values for i in [lo, vb)
+struct ShearRow {
+  int dir, c0, lo, vb, la, lb;
+  float f1, f2;
+};
+
+__device__ __forceinline__ ShearRow shear_row(const RotHdr &h, int n, int j, const int *t_rsh, const float *t_rf1,
+                                              const float *t_rf2, const int *t_st, const int *t_en) {
+  ShearRow r;
+  const int sh = t_rsh[j];
+  r.lo = t_st[j] - sh + h.iadd;
+  const int hi = t_en[j] - sh - 1 + h.iadd;
+  r.vb = min(hi, h.mdim);
+  r.dir = h.b180 ? -1 : 1;
+  r.c0 = h.b180 ? n - sh + h.iadd - 1 : sh - h.iadd;
+  r.la = max(r.lo, h.b180 ? r.c0 - n + 1 : -r.c0);
+  r.lb = min(r.vb, h.b180 ? r.c0 : n - 1 - r.c0);
+  r.f1 = t_rf1[j];
+  r.f2 = t_rf2[j];
+  return r;
+}
+
 __device__ __forceinline__ void shear_pass1_rows(const float *__restrict__ s, int rs, float *s_x, int xld, int n,
                                                  const RotHdr &h, const int *t_rsh, const float *t_rf1,
                                                  const float *t_rf2, const int *t_st, const int *t_en, int warp,
                                                  int lane) {
   for (int j = warp; j < n; j += SH_TY) {
-    const int sh = t_rsh[j];
-    const int lo = t_st[j] - sh + h.iadd, hi = t_en[j] - sh - 1 + h.iadd;
-    const float f1 = t_rf1[j], f2 = t_rf2[j];
-    const float *line = s + (h.b180 ? n - j - 1 : j) * rs;
+    const ShearRow r = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+    const float *line = s + (h.b180 ? n - j - 1 : j) * rs + r.c0;  // tap(i) at line[dir i]
     float *xr = s_x + j * xld;
-    // taps read: i in [lo, min(hi, mdim)] (the second tap of i is tap i + 1)
-    const int hl = min(hi, h.mdim);
+    float v = (lane >= r.la && lane <= r.lb) ? __ldg(line + r.dir * lane) : 0.f;
     for (int i0 = 0; i0 < h.mdim; i0 += SH_TX) {
-      const int i = i0 + lane;
-      const int p = shear_tap(h, n, sh, i), pn = shear_tap(h, n, sh, i + 1);
-      const float v = (i >= lo && i <= hl && p >= 0 && p < n) ? __ldg(line + p) : 0.f;
-      float vn = __shfl_down_sync(0xffffffffu, v, 1);
-      if (lane == SH_TX - 1) vn = (i + 1 >= lo && i + 1 <= hl && pn >= 0 && pn < n) ? __ldg(line + pn) : 0.f;
-      if (i < h.mdim) xr[i] = (i >= lo && i < hi) ? lerp2(f1, v, f2, vn) : 0.f;
+      const int i = i0 + lane, inx = i + SH_TX;
+      const float vn = (inx >= r.la && inx <= r.lb) ? __ldg(line + r.dir * inx) : 0.f;
+      // second tap of i = tap(i + 1): the next lane's, lane 0's next chunk for lane 31
+      const float sec = __shfl_sync(0xffffffffu, lane == 0 ? vn : v, (lane + 1) & (SH_TX - 1));
+      if (i < h.mdim) xr[i] = (i >= r.lo && i < r.vb) ? lerp2(r.f1, v, r.f2, sec) : 0.f;
+      v = vn;
     }
   }
 }
@@ -307,18 +328,16 @@ __device__ __forceinline__ void shear_pass1_cols(const float *__restrict__ s, in
   const int per = (h.mdim + NCH - 1) / NCH;
   for (int e = tid; e < n * NCH; e += nt) {
     const int ch = e / n, j = e - ch * n;
-    const int sh = t_rsh[j];
-    const int lo = t_st[j] - sh + h.iadd, hi = t_en[j] - sh - 1 + h.iadd;
-    const float f1 = t_rf1[j], f2 = t_rf2[j];
-    const float *col = s + (h.b180 ? j : n - j - 1);
+    const ShearRow r = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+    const int step = r.dir * rs;
+    const float *col = s + (h.b180 ? j : n - j - 1) + r.c0 * rs;  // tap(i) at col[i step]
     float *xc = s_x + j * xld;
     const int i0 = ch * per, i1 = min(h.mdim, i0 + per);
-    const int p0 = shear_tap(h, n, sh, i0);
-    float v = (i0 >= lo && i0 <= hi && p0 >= 0 && p0 < n) ? __ldg(col + p0 * rs) : 0.f;
-    for (int i = i0; i < i1; ++i) {
-      const int pn = shear_tap(h, n, sh, i + 1);
-      const float vn = (i + 1 >= lo && i + 1 <= hi && pn >= 0 && pn < n) ? __ldg(col + pn * rs) : 0.f;
-      xc[i] = (i >= lo && i < hi) ? lerp2(f1, v, f2, vn) : 0.f;
+    float v = (i0 >= r.la && i0 <= r.lb) ? __ldg(col + i0 * step) : 0.f;
+    const float *pn = col + (i0 + 1) * step;
+    for (int i = i0; i < i1; ++i, pn += step) {
+      const float vn = (i + 1 >= r.la && i + 1 <= r.lb) ? __ldg(pn) : 0.f;
+      xc[i] = (i >= r.lo && i < r.vb) ? lerp2(r.f1, v, r.f2, vn) : 0.f;
       v = vn;
     }
   }
@@ -364,49 +383,66 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
   __syncthreads();
   // pass 2: Y[j][c] = lerp(X[j+jt][c], X[j+jt+1][c]) for jj = j + iadd in
   // [max(0, -jt), min(mdim, mdim - jt - 1)), else 0; X rows outside [0, n)
-  // are 0
+  // are 0.  Each group of 4 rows loads its inputs before storing: the rows
+  // read are on the far side of the rows written (below them for jt < 0,
+  // at or above them for jt >= 0), so the loads see X.
+  constexpr int G = 4;
   for (int c = tid; c < h.mdim; c += nt) {
     const int jt = t_csh[c];
     const float w1 = t_cf1[c], w2 = t_cf2[c];
     const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
     float *col = s_x + c;
     if (jt >= 0) {
-      // rows read (j + jt, j + jt + 1) are never below the row written
       float x0 = jt < n ? col[jt * xld] : 0.f;
-#pragma unroll 4
-      for (int j = 0; j < n; ++j) {
-        const int r1 = j + jt + 1;
-        const float x1 = r1 < n ? col[r1 * xld] : 0.f;
-        col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
-        x0 = x1;
+      for (int j0 = 0; j0 < n; j0 += G) {
+        float xs[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          const int r1 = j0 + q + jt + 1;
+          xs[q] = r1 < n ? col[r1 * xld] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          const int j = j0 + q;
+          if (j < n) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, xs[q]) : 0.f;
+          x0 = xs[q];
+        }
       }
     } else {
-      // rows read are below the row written: walk downwards
-      float x1 = (n + jt >= 0 && n + jt < n) ? col[(n + jt) * xld] : 0.f;
-#pragma unroll 4
-      for (int j = n - 1; j >= 0; --j) {
-        const int r0 = j + jt;
-        const float x0 = r0 >= 0 ? col[r0 * xld] : 0.f;
-        col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
-        x1 = x0;
+      float x1 = (n + jt >= 0) ? col[(n + jt) * xld] : 0.f;
+      for (int j0 = n - 1; j0 >= 0; j0 -= G) {
+        float xs[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          const int r0 = j0 - q + jt;
+          xs[q] = r0 >= 0 ? col[r0 * xld] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          const int j = j0 - q;
+          if (j >= 0) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, xs[q], w2, x1) : 0.f;
+          x1 = xs[q];
+        }
       }
     }
   }
   __syncthreads();
-  // pass 3: output (j, x) = lerp(Y[j][a], Y[j][a+1]), a = x + sh + iadd; a
-  // warp per row, the second tap from the next lane
+  // pass 3: output (j, x) = lerp(Y[j][a], Y[j][a+1]), a = x + sh + iadd, for
+  // x in [st + 1, en - 1); a warp per row, the second tap from the next lane
   for (int j = ty; j < n; j += SH_TY) {
-    const int sh = t_rsh[j], st = t_st[j], en = t_en[j];
+    const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
     const float f1 = t_rf1[j], f2 = t_rf2[j];
     const float *yr = s_x + j * xld;
     float *orow = d + (size_t)j * rs;
-    const int off = sh + h.iadd;
+    int a = tx + off;
+    float y = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
     for (int x0 = 0; x0 < n; x0 += SH_TX) {
-      const int x = x0 + tx, a = x + off;
-      const float y0 = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
-      float y1 = __shfl_down_sync(0xffffffffu, y0, 1);
-      if (tx == SH_TX - 1) y1 = (a + 1 >= 0 && a + 1 < h.mdim) ? yr[a + 1] : 0.f;
-      if (x < n) orow[x] = (x >= st + 1 && x < en - 1) ? lerp2(f1, y0, f2, y1) : 0.f;
+      const int x = x0 + tx;
+      a += SH_TX;
+      const float yn = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
+      const float sec = __shfl_sync(0xffffffffu, tx == 0 ? yn : y, (tx + 1) & (SH_TX - 1));
+      if (x < n) orow[x] = (x >= xa && x < xb) ? lerp2(f1, y, f2, sec) : 0.f;
+      y = yn;
     }
   }
 }
