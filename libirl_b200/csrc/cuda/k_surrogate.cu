@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -300,6 +301,241 @@ __global__ void __launch_bounds__(GNT) k_conv_gemm(GemmArgs a, ConvGeom g, const
       }
 }
 
+// ------------------------------------------------ tcgen05 implicit GEMM
+// Forward convolution on the 5th-generation tensor cores: one CTA of 128
+// threads per 128 output positions (rows) x all N = co output channels.
+//   * operands: the CTA gathers A (the implicit im2col of the channels-last
+//     input, 16-byte chunks of 8 channels of one tap) and B (the weights
+//     [co][K], K contiguous) for a k tile of TC_BK into shared memory in
+//     the K-major, no-swizzle canonical layout: core matrices of 8 rows x
+//     16 bytes, row r of k chunk q at byte q * (R * 16) + r * 16, so the
+//     descriptor's stride byte offset (between 8-row groups) is 128 and its
+//     leading byte offset (between the two k chunks of one MMA) is R * 16;
+//   * one elected thread issues tcgen05.mma (M 128, N, K 16, BF16 x BF16 ->
+//     FP32) into a TMEM accumulator of N columns and commits to the
+//     stage's mbarrier; two stages, so the gather of tile t + 1 overlaps
+//     the MMAs of tile t;
+//   * epilogue: warp w reads TMEM lanes 32w .. 32w+31 (its rows) with
+//     tcgen05.ld, adds the bias, applies ReLU and stores 8 channels per
+//     16-byte vector, or writes raw split-K partial sums.
+// Every mbarrier wait is bounded; on a timeout the CTA records the error in
+// g_tc_error, waits (bounded) for its last commit and frees its TMEM.
+constexpr int TC_BM = 128, TC_BK = 64, TC_NT = 128, TC_S = 4;
+constexpr int TC_MAXCH = 640;  // k chunks (of 8) of one CTA's k range: K / 8 <= 576 here
+constexpr unsigned TC_WAIT_LIMIT = 1u << 22;
+
+__device__ int g_tc_error;
+
+template <int N>
+struct TcCfg {
+  static constexpr int A_BYTES = TC_BM * TC_BK * 2;
+  static constexpr int B_BYTES = N * TC_BK * 2;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int TMEM_COLS = N < 32 ? 32 : N;
+  // stages, the k-chunk tap table, barriers, alignment slack
+  static constexpr size_t SMEM = TC_S * (size_t)STAGE + TC_MAXCH * 8 + 256 + 128;
+  // kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major,
+  // N >> 3 at bit 17, M >> 4 at bit 24
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+                                    ((uint32_t)(TC_BM >> 4) << 24);
+  static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N a multiple of 16 up to 256");
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start, leading and stride byte offsets
+// (16-byte units), version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned it = 0; it < TC_WAIT_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16-byte asynchronous copy global -> shared; ok = false fills zeros
+__device__ __forceinline__ void cp16(uint32_t dst, const void *src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0) : "memory");
+}
+
+template <int N>
+__global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const bf16 *__restrict__ X) {
+  using Cfg = TcCfg<N>;
+  extern __shared__ __align__(128) unsigned char tcs[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)tcs + 127) & ~(uintptr_t)127);
+  int2 *ktab = reinterpret_cast<int2 *>(base + TC_S * Cfg::STAGE);     // per k chunk: packed tap, channel
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ktab + TC_MAXCH);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + TC_S);
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * TC_BM;
+  const int kb = a.splits > 1 ? blockIdx.z * a.kper : 0;
+  const int ke = a.splits > 1 ? min(a.K, kb + a.kper) : a.K;
+  const int nk = (ke - kb + TC_BK - 1) / TC_BK;
+  // this thread's A row: output position decoded once
+  int rb = -1, rd = 0, rh = 0, rw = 0;
+  {
+    const int m = m0 + tid;
+    if (m < a.M) {
+      int r = m;
+      const int ow = r % g.wout;
+      r /= g.wout;
+      const int oh = r % g.hout;
+      r /= g.hout;
+      const int od = r % g.dout;
+      rb = r / g.dout;
+      rd = od * g.s - g.kd / 2;
+      rh = oh * g.s - g.kh / 2;
+      rw = ow * g.s - g.kw / 2;
+    }
+  }
+  // tap offsets of the k chunks of [kb, kb + nk TC_BK) (c = -1 past ke)
+  const int nch = nk * (TC_BK / 8);
+  const int khw = g.kh * g.kw;
+  for (int q = tid; q < nch; q += TC_NT) {
+    const int k = kb + q * 8;
+    int2 t = make_int2(0, -1);
+    if (k < ke) {
+      const int tap = k / g.ci, c = k - tap * g.ci;
+      const int td = tap / khw, th = (tap - td * khw) / g.kw, tw = tap - td * khw - th * g.kw;
+      t = make_int2(td | (th << 8) | (tw << 16), c);
+    }
+    ktab[q] = t;
+  }
+  if (tid == 0) {
+    for (int i = 0; i < TC_S; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[i])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    abort_flag = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(Cfg::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t sbase = smem_addr(base);
+  // issue the copies of k tile t into stage t % TC_S
+  auto load_tile = [&](int t) {
+    const uint32_t As = sbase + (t % TC_S) * Cfg::STAGE, Bs = As + Cfg::A_BYTES;
+    const int k0 = kb + t * TC_BK;
+#pragma unroll
+    for (int q = 0; q < TC_BK / 8; ++q) {
+      const int2 e = ktab[t * (TC_BK / 8) + q];
+      const int id = rd + (e.x & 0xff), ih = rh + ((e.x >> 8) & 0xff), iw = rw + (e.x >> 16);
+      const bool ok = rb >= 0 && e.y >= 0 && id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi;
+      cp16(As + q * (TC_BM * 16) + tid * 16, ok ? (const void *)(X + in_off(g, rb, id, ih, iw, e.y)) : (const void *)X,
+           ok);
+    }
+    // B: 8 consecutive threads read one weight row's 8 chunks (128 bytes)
+    for (int e = tid; e < N * (TC_BK / 8); e += TC_NT) {
+      const int n = e >> 3, q = e & 7, k = k0 + q * 8;
+      const bool ok = n < a.N && k < ke;
+      cp16(Bs + q * (N * 16) + n * 16, ok ? (const void *)(a.B + (size_t)n * a.sbn + k) : (const void *)a.B, ok);
+    }
+  };
+#pragma unroll
+  for (int p = 0; p < TC_S - 1; ++p) {
+    if (p < nk) load_tile(p);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  int last_it = -1;  // last tile whose MMAs were committed
+  for (int it = 0; it < nk; ++it) {
+    const int st = it % TC_S;
+    asm volatile("cp.async.wait_group %0;" ::"n"(TC_S - 2) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = sbase + st * Cfg::STAGE, b0 = a0 + Cfg::A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 16; ++kk) {
+        const uint64_t ad = umma_desc(a0 + kk * 2 * (TC_BM * 16), TC_BM * 16, 128);
+        const uint64_t bd = umma_desc(b0 + kk * 2 * (N * 16), N * 16, 128);
+        const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(Cfg::IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&bars[st]))
+                   : "memory");
+    }
+    last_it = it;
+    // refill the stage of tile it - 1 with tile it + TC_S - 1 once the MMAs
+    // of tile it - 1 have read it
+    const int nt = it + TC_S - 1;
+    if (nt < nk) {
+      if (it >= 1) {
+        const int pt = it - 1;
+        if (!mbar_wait(smem_addr(&bars[pt % TC_S]), (pt / TC_S) & 1)) {
+          if (tid == 0) atomicExch(&g_tc_error, 1);
+          abort_flag = 1;
+        }
+      }
+      load_tile(nt);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  // all MMAs done: the last commit tracks every earlier one
+  if (last_it >= 0 && !mbar_wait(smem_addr(&bars[last_it % TC_S]), (last_it / TC_S) & 1)) {
+    if (tid == 0) atomicExch(&g_tc_error, 1);
+    abort_flag = 1;
+  }
+  __syncthreads();
+  const bool ok = !abort_flag;  // uniform: the TMEM loads below are warp-collective
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (ok && last_it >= 0) {
+    const int row = warp * 32 + lane, m = m0 + row;
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      uint32_t v[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < a.M) {
+        float f[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] = __uint_as_float(v[q]);
+        if (a.splits > 1) {
+          float *w = a.ws + ((size_t)blockIdx.z * a.M + m) * a.N + c0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) w[q] = f[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            if (a.bias) f[q] += a.bias[c0 + q];
+            if (a.relu) f[q] = fmaxf(f[q], 0.f);
+          }
+          __align__(16) bf16 h[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(f[q]);
+          *reinterpret_cast<uint4 *>(a.Cb + (long long)m * a.scm + c0) = *reinterpret_cast<const uint4 *>(h);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
+}
+
 __global__ void k_splitk_reduce(GemmArgs a) {
   const size_t tot = (size_t)a.M * a.N;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
@@ -317,6 +553,38 @@ __global__ void k_splitk_reduce(GemmArgs a) {
 // split-K workspace of a network (FP32 elements)
 constexpr size_t GEMM_WS_ELEMS = (size_t)16 << 20;
 
+// the tcgen05 convolution takes 16-byte channel chunks (ci a multiple of
+// 8, aligned input and weights), N = co in {32, 64, 128, 256} and a
+// channels-last output; IRLCU_SUR_TC=0 keeps the mma.sync kernel
+static bool tc_usable(const GemmArgs &a, const ConvGeom &g, const bf16 *X) {
+  static int env = -1;
+  if (env < 0) {
+    const char *e = getenv("IRLCU_SUR_TC");
+    env = (e && e[0] == '0') ? 0 : 1;
+  }
+  if (!env) return false;
+  const bool n_ok = a.N == 32 || a.N == 64 || a.N == 128 || a.N == 256;
+  const int kspan = a.splits > 1 ? a.kper : a.K;  // one CTA's k range, in chunks of 8 for the tap table
+  return n_ok && g.ci % 8 == 0 && a.K % 8 == 0 && a.sbk == 1 && a.sbn == a.K && ((uintptr_t)X & 15) == 0 &&
+         ((uintptr_t)a.B & 15) == 0 && a.scn == 1 && a.scm == a.N && !a.Cf && a.Cb &&
+         (kspan + TC_BK - 1) / TC_BK * (TC_BK / 8) <= TC_MAXCH && g.kd < 256 && g.kh < 256 && g.kw < 256;
+}
+
+#define TC_TRY(x)          \
+  do {                     \
+    const int rc_ = (x);   \
+    if (rc_) return rc_;   \
+  } while (0)
+
+template <int N>
+static int tc_attr() {
+  static bool done = false;
+  if (done) return IRLCU_OK;
+  CU_TRY(cudaFuncSetAttribute(k_conv_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<N>::SMEM));
+  done = true;
+  return IRLCU_OK;
+}
+
 static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = nullptr, const bf16 *X = nullptr) {
   if (a.M <= 0 || a.N <= 0 || a.K <= 0) return IRLCU_OK;
   const int tiles_m = (a.M + GBM - 1) / GBM, tiles_n = (a.N + GBN - 1) / GBN;
@@ -333,6 +601,16 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = n
     a.splits = (a.K + a.kper - 1) / a.kper;  // slices actually populated
     a.ws = ws;
   }
+  if (conv && tc_usable(a, *conv, X)) {
+    const dim3 tgrid((a.M + TC_BM - 1) / TC_BM, 1, a.splits);
+    switch (a.N) {
+      case 32: TC_TRY(tc_attr<32>()); k_conv_tc<32><<<tgrid, TC_NT, TcCfg<32>::SMEM, st>>>(a, *conv, X); break;
+      case 64: TC_TRY(tc_attr<64>()); k_conv_tc<64><<<tgrid, TC_NT, TcCfg<64>::SMEM, st>>>(a, *conv, X); break;
+      case 128: TC_TRY(tc_attr<128>()); k_conv_tc<128><<<tgrid, TC_NT, TcCfg<128>::SMEM, st>>>(a, *conv, X); break;
+      default: TC_TRY(tc_attr<256>()); k_conv_tc<256><<<tgrid, TC_NT, TcCfg<256>::SMEM, st>>>(a, *conv, X); break;
+    }
+    CU_LAUNCHED();
+  } else {
   const dim3 grid(tiles_n, tiles_m, a.splits);
   if (conv) {
     if (conv->ci % 8 == 0 && ((uintptr_t)X & 15) == 0)
@@ -343,6 +621,7 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = n
     k_gemm_bf16<<<grid, GNT, 0, st>>>(a);
   }
   CU_LAUNCHED();
+  }
   if (a.splits > 1) {
     const size_t tot = (size_t)a.M * a.N;
     k_splitk_reduce<<<(unsigned)std::min<size_t>((tot + 255) / 256, 148 * 32), 256, 0, st>>>(a);
