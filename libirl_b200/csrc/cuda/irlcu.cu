@@ -158,6 +158,7 @@ static void free_ctx(Ctx *c) {
   graphs_clear(*c);
   dfree(c->sur_scale);
   dfree(c->sur_work);
+  dfree(c->sur_static);
   dfree(c->dviews_all);
   dfree(c->dvp_all);
   dfree(c->rot.hdr);
@@ -550,10 +551,22 @@ static int upload_views(const int *views, int nv, const irlcu_view_parm *vp) {
   return IRLCU_OK;
 }
 
+// the surrogate's iteration-invariant input channels of every view, from
+// the current per-view mu and S tables (not inside a graph capture)
+static int sur_static_ensure(Ctx &c) {
+  if (c.sur_static_ok || !c.tMu || !c.tS || (c.n & 3) || c.n != c.nz) return IRLCU_OK;
+  const size_t P = (size_t)(c.n / 4) * (c.n / 4) * (c.n / 4);
+  if (!c.sur_static) TRY(dalloc(&c.sur_static, (size_t)c.nv * P));  // one BF16 pair per float
+  TRY(launch_sur_static(c.st, c.tMu, c.tS, c.nv, c.n, c.vox, c.sur_static));
+  c.sur_static_ok = true;
+  return IRLCU_OK;
+}
+
 int irlcu_prepare_attenuation(int need_srf) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
   if (!c.atn) return set_error(IRLCU_ESTATE, "attenuation map not uploaded");
+  c.sur_static_ok = false;
   if (!c.tE) TRY(dalloc(&c.tE, c.vox * c.nv));
   if (need_srf) {
     if (!c.tS) TRY(dalloc(&c.tS, c.vox * c.nv));
@@ -569,6 +582,7 @@ int irlcu_prepare_attenuation(int need_srf) {
     TRY(launch_rotate(c, c.atn, 0, rmu, c.vox, c.dviews, nb, 0));
     TRY(launch_atn_tables(c, rmu, c.tE + (size_t)v0 * c.vox, need_srf ? c.tS + (size_t)v0 * c.vox : nullptr, nb));
   }
+  if (need_srf && c.sur) TRY(sur_static_ensure(c));
   CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
 }
@@ -604,8 +618,12 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
     if (out_nosrf)
       CU_TRY(cudaMemcpyAsync(out_nosrf, out, sizeof(float) * c.pln * nv, cudaMemcpyDeviceToDevice, c.st));
     Stage s(IRLCU_ST_ESSE, c.st);
-    TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, c.sur_scale,
-                          sur_input(c.sur), c.sur_work));
+    if (c.sur_static_ok)
+      TRY(launch_sur_inputs_static(c.st, c.wrot, c.vox, c.sur_static, c.dviews, nv, c.n, c.sur_scale,
+                                   sur_input(c.sur), c.sur_work));
+    else
+      TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, c.sur_scale,
+                            sur_input(c.sur), c.sur_work));
     const float *y = nullptr;
     TRY(sur_infer(c.sur, c.st, nv, &y));
     return launch_scale_views(c.st, y, c.sur_scale, out, (int)c.pln, nv, 1);
@@ -908,6 +926,7 @@ int irlcu_set_surrogate(irlcu_sur *net, const unsigned char *flags) {
   if (!c.sur_scale) TRY(dalloc(&c.sur_scale, (size_t)c.g.max_batch));
   TRY(sur_work_ensure(c));
   c.sur = net;
+  TRY(sur_static_ensure(c));
   if (flags)
     c.sur_flags.assign(flags, flags + c.nv);
   else

@@ -146,6 +146,8 @@ struct Ctx {
   std::vector<unsigned char> sur_flags;   // per view: 1 = ESSE for that view
   float *sur_scale = nullptr;             // max_batch activity means
   float *sur_work = nullptr;              // pooling work of max_batch views
+  float *sur_static = nullptr;            // pooled mu and exp(-S) channels of every view (BF16 pairs)
+  bool sur_static_ok = false;             // ... computed from the current attenuation tables
   // three-shear intermediate for slices beyond shared memory, grown on use
   mutable float *xscratch = nullptr;
   mutable size_t xscratch_elems = 0;
@@ -238,6 +240,9 @@ void *sur_input(irlcu_sur *s);
 int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y);
 // work: nv * ((n/4)^3 + SUR_POOL_PARTS) floats
 constexpr int SUR_POOL_PARTS = 128;
+int launch_sur_static(cudaStream_t st, const float *mu, const float *S, int nviews, int n, size_t vox, void *stat);
+int launch_sur_inputs_static(cudaStream_t st, const float *act, size_t act_stride, const void *stat,
+                             const int *dviews, int nv, int n, float *scale, void *out, float *work);
 int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
                       const int *dviews, int nv, int n, size_t vox, float *scale, void *out, float *work);
 int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size_t n);

@@ -706,7 +706,7 @@ constexpr int FIRST_CI = 3, FIRST_CO = 32, FIRST_TAPS = 27;
 __global__ void __launch_bounds__(128) k_conv_first(ConvGeom g, const bf16 *__restrict__ x,
                                                     const bf16 *__restrict__ w, const float *__restrict__ bias,
                                                     bf16 *__restrict__ y) {
-  __shared__ float ws[FIRST_TAPS * FIRST_CI][FIRST_CO];
+  __shared__ __align__(16) float ws[FIRST_TAPS * FIRST_CI][FIRST_CO];
   __shared__ float bs[FIRST_CO];
   for (int e = threadIdx.x; e < FIRST_TAPS * FIRST_CI * FIRST_CO; e += blockDim.x) {
     const int co = e / (FIRST_TAPS * FIRST_CI), k = e % (FIRST_TAPS * FIRST_CI);
@@ -733,9 +733,16 @@ __global__ void __launch_bounds__(128) k_conv_first(ConvGeom g, const bf16 *__re
 #pragma unroll
     for (int c = 0; c < FIRST_CI; ++c) {
       const float v = __bfloat162float(px[c]);
-      const float *wr = ws[tap * FIRST_CI + c];
+      // one 16-byte (broadcast) shared load per 4 output channels
+      const float4 *wr = reinterpret_cast<const float4 *>(ws[tap * FIRST_CI + c]);
 #pragma unroll
-      for (int co = 0; co < FIRST_CO; ++co) acc[co] = fmaf(wr[co], v, acc[co]);
+      for (int q = 0; q < FIRST_CO / 4; ++q) {
+        const float4 w4 = wr[q];
+        acc[4 * q] = fmaf(w4.x, v, acc[4 * q]);
+        acc[4 * q + 1] = fmaf(w4.y, v, acc[4 * q + 1]);
+        acc[4 * q + 2] = fmaf(w4.z, v, acc[4 * q + 2]);
+        acc[4 * q + 3] = fmaf(w4.w, v, acc[4 * q + 3]);
+      }
     }
   }
   uint4 *o = reinterpret_cast<uint4 *>(y + m * FIRST_CO);
@@ -951,6 +958,84 @@ __global__ void __launch_bounds__(POOL_NT) k_pool_inputs(const float *__restrict
     __syncthreads();
   }
   if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = red[0];
+}
+
+// the iteration-invariant channels (mu * 10 and exp(-S), 4^3 means) of
+// every view, [view][P^3][2], pooled once per reconstruction
+__global__ void __launch_bounds__(POOL_NT) k_pool_static(const float *__restrict__ mu, const float *__restrict__ S,
+                                                         size_t vox, int n, bf16 *__restrict__ stat) {
+  const int P = n / 4;
+  const int tot = P * P * P;
+  const int view = blockIdx.y;
+  const float *m = mu + (size_t)view * vox;
+  const float *sd = S + (size_t)view * vox;
+  for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
+    const int px = e % P, pz = (e / P) % P, py = e / (P * P);
+    float sm = 0.f, se = 0.f;
+    for (int dy = 0; dy < 4; ++dy)
+      for (int dz = 0; dz < 4; ++dz) {
+        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
+        const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
+        const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
+        sm += (vm.x + vm.y) + (vm.z + vm.w);
+        se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
+      }
+    bf16 *o = stat + ((size_t)view * tot + e) * 2;
+    o[0] = __float2bfloat16(sm * (10.f / 64.f));
+    o[1] = __float2bfloat16(se * (1.f / 64.f));
+  }
+}
+
+// activity channel only: 4^3 means and their partial sums
+__global__ void __launch_bounds__(POOL_NT) k_pool_act(const float *__restrict__ act, size_t act_stride, int n,
+                                                      float *__restrict__ pa, float *__restrict__ part) {
+  const int P = n / 4;
+  const int tot = P * P * P;
+  const int b = blockIdx.y;
+  const float *a = act + (size_t)b * act_stride;
+  __shared__ float red[POOL_NT];
+  float psum = 0.f;
+  for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
+    const int px = e % P, pz = (e / P) % P, py = e / (P * P);
+    float sa = 0.f;
+    for (int dy = 0; dy < 4; ++dy)
+      for (int dz = 0; dz < 4; ++dz) {
+        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
+        const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
+        sa += (va.x + va.y) + (va.z + va.w);
+      }
+    const float mean_a = sa * (1.f / 64.f);
+    pa[(size_t)b * tot + e] = mean_a;
+    psum += mean_a;
+  }
+  red[threadIdx.x] = psum;
+  __syncthreads();
+  for (int w = POOL_NT / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = red[0];
+}
+
+// channel 0 = activity / its mean; channels 1, 2 from the per-view cache
+__global__ void __launch_bounds__(POOL_NT) k_pool_normalise_static(const float *__restrict__ pa,
+                                                                   const float *__restrict__ part, int nparts,
+                                                                   int tot, const int *__restrict__ views,
+                                                                   const bf16 *__restrict__ stat,
+                                                                   float *__restrict__ scale, bf16 *__restrict__ out) {
+  const int b = blockIdx.y;
+  float s = 0.f;
+  for (int j = 0; j < nparts; ++j) s += part[(size_t)b * nparts + j];
+  s /= (float)tot;
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[b] = s;
+  const float inv = s > 0.f ? 1.f / s : 0.f;
+  const bf16 *st = stat + (size_t)views[b] * tot * 2;
+  for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
+    bf16 *o = out + ((size_t)b * tot + e) * 3;
+    o[0] = __float2bfloat16(pa[(size_t)b * tot + e] * inv);
+    o[1] = st[2 * e];
+    o[2] = st[2 * e + 1];
+  }
 }
 
 __global__ void __launch_bounds__(POOL_NT) k_pool_normalise(const float *__restrict__ pa,
@@ -1289,6 +1374,26 @@ int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y) {
 
 // pooled network inputs of nv rotated volumes (act, stride act_stride) with
 // the per-view mu and depth tables; the activity means go to scale
+int launch_sur_static(cudaStream_t st, const float *mu, const float *S, int nviews, int n, size_t vox, void *stat) {
+  k_pool_static<<<dim3(SUR_POOL_PARTS, nviews), POOL_NT, 0, st>>>(mu, S, vox, n, static_cast<bf16 *>(stat));
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_sur_inputs_static(cudaStream_t st, const float *act, size_t act_stride, const void *stat,
+                             const int *dviews, int nv, int n, float *scale, void *out, float *work) {
+  const int P = n / 4, tot = P * P * P;
+  const int nparts = SUR_POOL_PARTS;
+  float *pa = work, *part = work + (size_t)nv * tot;
+  dim3 grid(nparts, nv);
+  k_pool_act<<<grid, POOL_NT, 0, st>>>(act, act_stride, n, pa, part);
+  CU_LAUNCHED();
+  k_pool_normalise_static<<<grid, POOL_NT, 0, st>>>(pa, part, nparts, tot, dviews,
+                                                    static_cast<const bf16 *>(stat), scale, static_cast<bf16 *>(out));
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
 int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
                       const int *dviews, int nv, int n, size_t vox, float *scale, void *out, float *work) {
   const int P = n / 4, tot = P * P * P;
