@@ -121,7 +121,10 @@ void dev_free(void *p, cudaStream_t st) {
   if (p) cudaFreeAsync(p, st);
 }
 
-// allocations of the current context (its stream orders them)
+// allocations, uploads and memsets of the current context go on its stream:
+// the context's kernels run on a non-blocking stream, which is not ordered
+// after legacy-stream copies or memsets (a pageable cudaMemcpy may return
+// before its DMA lands, a cudaMemset before it runs)
 static cudaStream_t alloc_stream() { return g_ctx ? g_ctx->st : g_init_stream; }
 
 template <class T>
@@ -270,8 +273,8 @@ int irlcu_init(const irlcu_geom *g) {
   {
     std::vector<int> st(n), en(n);
     irl_shear_support(n, st.data(), en.data());
-    CU_TRY(cudaMemcpy(c->sup_start, st.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CU_TRY(cudaMemcpy(c->sup_end, en.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpyAsync(c->sup_start, st.data(), n * sizeof(int), cudaMemcpyHostToDevice, alloc_stream()));
+    CU_TRY(cudaMemcpyAsync(c->sup_end, en.data(), n * sizeof(int), cudaMemcpyHostToDevice, alloc_stream()));
   }
   const int B = c->g.max_batch;
   TRY(dalloc(&c->est, c->vox));
@@ -286,10 +289,10 @@ int irlcu_init(const irlcu_geom *g) {
   TRY(dalloc(&c->wpart, c->wpart_elems));
   TRY(dalloc(&c->dviews, (size_t)c->nv));
   TRY(dalloc(&c->dvp, (size_t)c->nv));
-  CU_TRY(cudaMemset(c->prj, 0, c->pln * c->nv * sizeof(float)));
-  CU_TRY(cudaMemset(c->upd, 0, c->vox * sizeof(float)));
+  CU_TRY(cudaMemsetAsync(c->prj, 0, c->pln * c->nv * sizeof(float), alloc_stream()));
+  CU_TRY(cudaMemsetAsync(c->upd, 0, c->vox * sizeof(float), alloc_stream()));
   std::vector<unsigned char> ones((size_t)c->nv * n, 3);
-  CU_TRY(cudaMemcpy(c->colmask, ones.data(), ones.size(), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(c->colmask, ones.data(), ones.size(), cudaMemcpyHostToDevice, alloc_stream()));
   return IRLCU_OK;
 }
 
@@ -327,15 +330,15 @@ int irlcu_set_angles(const float *angles) {
     const float ang3 = r < c.nv ? (float)(0.5 * M_PI + a) : (float)(-a - 0.5 * M_PI);
     irl_rot3dpar_sincos(ang3, &sn[r], &cs[r]);
   }
-  CU_TRY(cudaMemcpy(c.rot.hdr, hdr.data(), hdr.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_sh, rsh.data(), rsh.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_f1, rf1.data(), rf1.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_f2, rf2.data(), rf2.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_sh, csh.data(), csh.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_f1, cf1.data(), cf1.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(c.rot.hdr, hdr.data(), hdr.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_sh, rsh.data(), rsh.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_f1, rf1.data(), rf1.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_f2, rf2.data(), rf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_sh, csh.data(), csh.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_f1, cf1.data(), cf1.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   return IRLCU_OK;
 }
 
@@ -427,11 +430,11 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
         pad[(size_t)i * PW * PLD + (size_t)(yy + H - d->halo) * PLD + (xx + H - d->halo)] =
             d->psf[(size_t)i * w * w + (size_t)yy * w + xx];
   TRY(dalloc(&D.psf, pad.size()));
-  CU_TRY(cudaMemcpy(D.psf, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(D.psf, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   TRY(dalloc(&D.pad_rows, (size_t)d->ndist));
-  CU_TRY(cudaMemcpy(D.pad_rows, d->pad_rows, d->ndist * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(D.pad_rows, d->pad_rows, d->ndist * 4, cudaMemcpyHostToDevice, alloc_stream()));
   TRY(dalloc(&D.row_idist, (size_t)c.nv * c.n));
-  CU_TRY(cudaMemcpy(D.row_idist, d->row_idist, (size_t)c.nv * c.n * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(D.row_idist, d->row_idist, (size_t)c.nv * c.n * 4, cudaMemcpyHostToDevice, alloc_stream()));
   D.ndist = d->ndist;
   D.halo = H;
   D.pstride = PLD;
@@ -456,7 +459,7 @@ int irlcu_set_drf(int which, const irlcu_drf *d) {
 int irlcu_set_column_mask(const unsigned char *mask) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
-  CU_TRY(cudaMemcpy(c.colmask, mask, (size_t)c.nv * c.n, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(c.colmask, mask, (size_t)c.nv * c.n, cudaMemcpyHostToDevice, alloc_stream()));
   return IRLCU_OK;
 }
 
@@ -475,7 +478,7 @@ static int buf_ptr(int buf, int index, float **p, size_t *count, bool alloc) {
     case IRLCU_BUF_PRJSCAT:
       if (!c.prjscat && alloc) {
         TRY(dalloc(&c.prjscat, c.pln * c.nv));
-        CU_TRY(cudaMemset(c.prjscat, 0, c.pln * c.nv * 4));
+        CU_TRY(cudaMemsetAsync(c.prjscat, 0, c.pln * c.nv * 4, alloc_stream()));
       }
       *p = c.prjscat; *count = c.pln * c.nv; return IRLCU_OK;
     case IRLCU_BUF_NORM:
@@ -742,8 +745,8 @@ int irlcu_set_subsets(int nsub, int per, const int *views, const irlcu_view_parm
   c.h_vp_all.assign(vp, vp + tot);
   for (auto &q : c.h_vp_all) q.scat_mode = 0;
   c.vp_scat_mode = 0;
-  CU_TRY(cudaMemcpy(c.dviews_all, views, tot * sizeof(int), cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.dvp_all, c.h_vp_all.data(), tot * sizeof(irlcu_view_parm), cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(c.dviews_all, views, tot * sizeof(int), cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.dvp_all, c.h_vp_all.data(), tot * sizeof(irlcu_view_parm), cudaMemcpyHostToDevice, alloc_stream()));
   c.nsub_all = nsub;
   c.per_all = per;
   return IRLCU_OK;
@@ -993,15 +996,15 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   // the last unrotation slot (index 2*nv-1) is borrowed and restored by the
   // caller through irlcu_set_angles when needed
   const int r = 2 * c.nv - 1;
-  CU_TRY(cudaMemcpy(c.rot.hdr + 4 * r, hdr.data(), 16, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_sh + (size_t)r * n, rsh.data(), n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_f1 + (size_t)r * n, rf1.data(), n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.row_f2 + (size_t)r * n, rf2.data(), n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_sh + (size_t)r * 2 * n, csh.data(), 2 * n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_f1 + (size_t)r * 2 * n, cf1.data(), 2 * n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.col_f2 + (size_t)r * 2 * n, cf2.data(), 2 * n * 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.sn + r, &sn, 4, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemcpy(c.rot.cs + r, &cs, 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(c.rot.hdr + 4 * r, hdr.data(), 16, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_sh + (size_t)r * n, rsh.data(), n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_f1 + (size_t)r * n, rf1.data(), n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.row_f2 + (size_t)r * n, rf2.data(), n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_sh + (size_t)r * 2 * n, csh.data(), 2 * n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_f1 + (size_t)r * 2 * n, cf1.data(), 2 * n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.col_f2 + (size_t)r * 2 * n, cf2.data(), 2 * n * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.sn + r, &sn, 4, cudaMemcpyHostToDevice, alloc_stream()));
+  CU_TRY(cudaMemcpyAsync(c.rot.cs + r, &cs, 4, cudaMemcpyHostToDevice, alloc_stream()));
   int zero = 0;
   TRY(upload_views(&zero, 1, nullptr));
   const float *s = src;

@@ -778,7 +778,7 @@ int upload_twiddle_table(cudaStream_t st, float2 **d, int L) {
     h[m] = make_float2((float)cos(a), (float)sin(a));
   }
   CU_TRY(dev_alloc_t(d, (size_t)L, st));
-  CU_TRY(cudaMemcpy(*d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpyAsync(*d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice, st));
   return IRLCU_OK;
 }
 
@@ -996,7 +996,7 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
   CU_TRY(dev_alloc(reinterpret_cast<void **>(&dgrid), sizeof(float) * (size_t)E.kx * E.ky * E.kz, c.st));
   for (int t = 0; t < E.nterms; ++t) {
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kft[t]), sizeof(float2) * spec, c.st));
-    CU_TRY(cudaMemcpy(dgrid, hk[t], sizeof(float) * (size_t)E.kx * E.ky * E.kz, cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpyAsync(dgrid, hk[t], sizeof(float) * (size_t)E.kx * E.ky * E.kz, cudaMemcpyHostToDevice, c.st));
     float2 *ta = nullptr, *tb = nullptr;
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&ta), sizeof(float2) * spec, c.st));
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&tb), sizeof(float2) * spec, c.st));

@@ -1469,8 +1469,9 @@ int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
     return fail(rc);
   std::vector<float> w;
   init_weights(*s, seed, w);
-  if (cudaMemcpy(s->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemset(s->m, 0, sizeof(float) * P) != cudaSuccess || cudaMemset(s->v, 0, sizeof(float) * P) != cudaSuccess)
+  if (cudaMemcpyAsync(s->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice, s->st) != cudaSuccess ||
+      cudaMemsetAsync(s->m, 0, sizeof(float) * P, s->st) != cudaSuccess ||
+      cudaMemsetAsync(s->v, 0, sizeof(float) * P, s->st) != cudaSuccess)
     return fail(set_error(IRLCU_ECUDA, "surrogate: initial upload failed"));
   k_to_bf16<<<grid_for((long long)P), 256, 0, s->st>>>(s->w, s->wb, (long long)P);
   ++g_launch_count;
@@ -1490,16 +1491,17 @@ size_t irlcu_sur_nparams(const irlcu_sur *s) { return s ? s->nparams : 0; }
 int irlcu_sur_get_weights(irlcu_sur *s, float *host, size_t n) {
   if (!s || n != s->nparams) return set_error(IRLCU_EARG, "surrogate: expected %zu parameters", s ? s->nparams : 0);
   CU_TRY(cudaStreamSynchronize(s->st));
-  CU_TRY(cudaMemcpy(host, s->w, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpyAsync(host, s->w, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st));
+  CU_TRY(cudaStreamSynchronize(s->st));
   return IRLCU_OK;
 }
 
 int irlcu_sur_set_weights(irlcu_sur *s, const float *host, size_t n) {
   if (!s || n != s->nparams) return set_error(IRLCU_EARG, "surrogate: expected %zu parameters", s ? s->nparams : 0);
   CU_TRY(cudaStreamSynchronize(s->st));
-  CU_TRY(cudaMemcpy(s->w, host, sizeof(float) * n, cudaMemcpyHostToDevice));
-  CU_TRY(cudaMemset(s->m, 0, sizeof(float) * n));
-  CU_TRY(cudaMemset(s->v, 0, sizeof(float) * n));
+  CU_TRY(cudaMemcpyAsync(s->w, host, sizeof(float) * n, cudaMemcpyHostToDevice, s->st));
+  CU_TRY(cudaMemsetAsync(s->m, 0, sizeof(float) * n, s->st));
+  CU_TRY(cudaMemsetAsync(s->v, 0, sizeof(float) * n, s->st));
   s->step = 0;
   k_to_bf16<<<grid_for((long long)n), 256, 0, s->st>>>(s->w, s->wb, (long long)n);
   CU_LAUNCHED();
@@ -1523,7 +1525,10 @@ int irlcu_sur_gradient(irlcu_sur *s, int B, const void *x, const float *t, float
   STRY(sur_loss(*s, B, t, loss));
   STRY(sur_backward(*s, B));
   CU_TRY(cudaStreamSynchronize(s->st));
-  if (grad_host) CU_TRY(cudaMemcpy(grad_host, s->g, sizeof(float) * s->nparams, cudaMemcpyDeviceToHost));
+  if (grad_host) {
+    CU_TRY(cudaMemcpyAsync(grad_host, s->g, sizeof(float) * s->nparams, cudaMemcpyDeviceToHost, s->st));
+    CU_TRY(cudaStreamSynchronize(s->st));
+  }
   return IRLCU_OK;
 }
 

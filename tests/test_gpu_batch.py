@@ -34,17 +34,13 @@ def _meas(case):
                             1e5, case.n)
 
 
-def test_batch_equals_separate_calls(product, tmp_path):
-    cases = _cases()
-    files = [c.write_tables(str(tmp_path / f"c{i}")) for i, c in enumerate(cases)]
-    meas = [_meas(c) for c in cases]
-    alone = [gpu_osem(product, c, f, m) for c, f, m in zip(cases, files, meas)]
+def _batch(product, cases, files, meas):
     keep = []
     probs = (api.OsemProblem * len(cases))()
     for i, (c, f, m) in enumerate(zip(cases, files, meas)):
         p, o, v = c.parms(), c.options(), c.views()
         atn, prj, rec = c.atn.copy(), m.copy(), np.zeros_like(c.act)
-        keep += [p, o, v, atn, prj, rec]
+        keep.append((p, o, v, atn, prj, rec))
         q = probs[i]
         q.psIrlParms, q.psOptions = C.pointer(p), C.pointer(o)
         q.psViews = C.cast(v, C.POINTER(api.PrjView))
@@ -55,8 +51,30 @@ def test_batch_equals_separate_calls(product, tmp_path):
     assert rc == 0, product.pchIrlErrorString()
     for i in range(len(cases)):
         assert probs[i].iStatus == 0
-        rec = keep[6 * i + 5]
-        assert np.array_equal(rec, alone[i]), f"problem {i}: {int((rec != alone[i]).sum())} voxels differ"
+    return [k[5] for k in keep]
+
+
+def _check_batch(product, cases, tmp_path):
+    files = [c.write_tables(str(tmp_path / f"c{i}")) for i, c in enumerate(cases)]
+    meas = [_meas(c) for c in cases]
+    alone = [gpu_osem(product, c, f, m) for c, f, m in zip(cases, files, meas)]
+    got = _batch(product, cases, files, meas)
+    for i, (rec, ref) in enumerate(zip(got, alone)):
+        assert np.array_equal(rec, ref), f"problem {i}: {int((rec != ref).sum())} voxels differ"
+
+
+def test_batch_equals_separate_calls(product, tmp_path):
+    _check_batch(product, _cases(), tmp_path)
+
+
+def test_batch_small_problems_behind_a_large_one(product, tmp_path):
+    # 64^3 problems are set up while the 112^3 problem before them still
+    # runs: their set-up copies and memsets must be ordered on their own
+    # streams, or their first kernels read buffers not yet written
+    cases = [W.full128(seed=3700, n=112, nviews=60, subsets=12, iterations=3)]
+    cases += [W.full128(seed=3710 + k, n=64, nviews=nv, subsets=ns, iterations=3)
+              for k, (nv, ns) in enumerate([(90, 6), (120, 8), (60, 12)])]
+    _check_batch(product, cases, tmp_path)
 
 
 def test_graph_replay_equals_eager(product, tmp_path, monkeypatch):
