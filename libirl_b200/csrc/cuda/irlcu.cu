@@ -508,6 +508,7 @@ int irlcu_download(int buf, int index, float *host, size_t count) {
   if (count > cap) return set_error(IRLCU_EARG, "download of %zu floats exceeds buffer %d", count, buf);
   CU_TRY(cudaMemcpyAsync(host, p, count * 4, cudaMemcpyDeviceToHost, g_ctx->st));
   CU_TRY(cudaStreamSynchronize(g_ctx->st));
+  if (g_ctx->sur) TRY(sur_tc_status(g_ctx->st));
   return IRLCU_OK;
 }
 
@@ -531,6 +532,7 @@ int irlcu_download_external(int buf, float *host) {
   CU_LAUNCHED();
   CU_TRY(cudaMemcpyAsync(host, c.wbck, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
   CU_TRY(cudaStreamSynchronize(c.st));
+  if (c.sur) TRY(sur_tc_status(c.st));
   return IRLCU_OK;
 }
 
@@ -899,6 +901,7 @@ int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *
       rc = set_error(IRLCU_ECUDA, "surrogate check: copy failed");
       break;
     }
+    if ((rc = sur_tc_status(c.st))) break;
     for (int b = 0; b < nb; ++b) {
       double e2 = 0.0, t2 = 0.0;
       for (size_t i = 0; i < c.pln; ++i) {

@@ -236,6 +236,7 @@ int launch_norm_planes(const Ctx &c, const int *dviews, const float *vt_dev, int
 
 // learned scatter surrogate (k_surrogate.cu)
 int sur_max_batch(const irlcu_sur *s);
+int sur_tc_status(cudaStream_t st);
 void *sur_input(irlcu_sur *s);
 int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y);
 // work: nv * ((n/4)^3 + SUR_POOL_PARTS) floats

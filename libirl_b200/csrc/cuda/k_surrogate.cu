@@ -1358,6 +1358,20 @@ static int sur_check_batch(const irlcu_sur *s, int B) {
 
 // ------------------------------------------- use inside the projector
 
+// a tcgen05 pipeline wait that ran out leaves g_tc_error set (the kernel
+// freed its TMEM and returned); the host reads and clears the flag after it
+// has synchronised with st and reports it as an error
+int sur_tc_status(cudaStream_t st) {
+  int v = 0;
+  CU_TRY(cudaMemcpyFromSymbolAsync(&v, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  if (!v) return IRLCU_OK;
+  const int zero = 0;
+  CU_TRY(cudaMemcpyToSymbolAsync(g_tc_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  return set_error(IRLCU_ECUDA, "surrogate: a tensor-core pipeline wait timed out");
+}
+
 int sur_max_batch(const irlcu_sur *s) { return s ? s->max_batch : 0; }
 void *sur_input(irlcu_sur *s) { return s->act[0]; }
 
@@ -1514,8 +1528,7 @@ int irlcu_sur_forward(irlcu_sur *s, int B, const void *x, float *y) {
   CU_TRY(cudaMemcpyAsync(s->act[0], x, sizeof(bf16) * layer_in_elems(s->L[0], B), cudaMemcpyDeviceToDevice, s->st));
   STRY(sur_forward(*s, B));
   CU_TRY(cudaMemcpyAsync(y, s->out, sizeof(float) * (size_t)B * 128 * 128, cudaMemcpyDeviceToDevice, s->st));
-  CU_TRY(cudaStreamSynchronize(s->st));
-  return IRLCU_OK;
+  return sur_tc_status(s->st);
 }
 
 int irlcu_sur_gradient(irlcu_sur *s, int B, const void *x, const float *t, float *loss, float *grad_host) {
@@ -1524,7 +1537,7 @@ int irlcu_sur_gradient(irlcu_sur *s, int B, const void *x, const float *t, float
   STRY(sur_forward(*s, B));
   STRY(sur_loss(*s, B, t, loss));
   STRY(sur_backward(*s, B));
-  CU_TRY(cudaStreamSynchronize(s->st));
+  STRY(sur_tc_status(s->st));
   if (grad_host) {
     CU_TRY(cudaMemcpyAsync(grad_host, s->g, sizeof(float) * s->nparams, cudaMemcpyDeviceToHost, s->st));
     CU_TRY(cudaStreamSynchronize(s->st));
