@@ -255,10 +255,10 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
 //           along the source row that the rotation reads contiguously (i
 //           for the unflipped cases, j for the 90-degree-flipped ones);
 //   pass 2: the y shear in place: each column c of X is shifted by its own
-//           csh[c] with weights cf1[c], cf2[c], one thread per column walking
-//           the rows away from the rows it still has to read (ascending
-//           for csh >= 0, descending otherwise), so every intermediate value
-//           is computed once;
+//           csh[c] with weights cf1[c], cf2[c], a warp per column stepping
+//           32 rows at a time away from the rows it still has to read
+//           (ascending for csh >= 0, descending otherwise), so every
+//           intermediate value is computed once and every warp has work;
 //   pass 3: the second x shear, two reads of the y-sheared row per output.
 // Every product and sum is rounded as in the fused form above, so the
 // output is the same bit for bit.
@@ -383,48 +383,34 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
   __syncthreads();
   // pass 2: Y[j][c] = lerp(X[j+jt][c], X[j+jt+1][c]) for jj = j + iadd in
   // [max(0, -jt), min(mdim, mdim - jt - 1)), else 0; X rows outside [0, n)
-  // are 0.  Each group of 4 rows loads its inputs before storing: the rows
-  // read are on the far side of the rows written (below them for jt < 0,
-  // at or above them for jt >= 0), so the loads see X.
-  constexpr int G = 4;
-  for (int c = tid; c < h.mdim; c += nt) {
+  // are 0.  A warp per column c, in place, 32 rows per step: all lanes
+  // load before any stores, and the rows read lie on the far side of the
+  // rows already written (at or past the step's first row for jt >= 0,
+  // walking down; at or before its last row for jt < 0, walking up), so
+  // every load sees X.
+  for (int c = ty; c < h.mdim; c += SH_TY) {
     const int jt = t_csh[c];
     const float w1 = t_cf1[c], w2 = t_cf2[c];
     const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
     float *col = s_x + c;
     if (jt >= 0) {
-      float x0 = jt < n ? col[jt * xld] : 0.f;
-      for (int j0 = 0; j0 < n; j0 += G) {
-        float xs[G];
-#pragma unroll
-        for (int q = 0; q < G; ++q) {
-          const int r1 = j0 + q + jt + 1;
-          xs[q] = r1 < n ? col[r1 * xld] : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < G; ++q) {
-          const int j = j0 + q;
-          if (j < n) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, xs[q]) : 0.f;
-          x0 = xs[q];
-        }
+      for (int j0 = 0; j0 < n; j0 += SH_TX) {
+        const int j = j0 + tx, r0 = j + jt;
+        const float x0 = (j < n && r0 < n) ? col[r0 * xld] : 0.f;
+        const float x1 = (j < n && r0 + 1 < n) ? col[(r0 + 1) * xld] : 0.f;
+        __syncwarp();
+        if (j < n) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
       }
     } else {
-      float x1 = (n + jt >= 0) ? col[(n + jt) * xld] : 0.f;
-      for (int j0 = n - 1; j0 >= 0; j0 -= G) {
-        float xs[G];
-#pragma unroll
-        for (int q = 0; q < G; ++q) {
-          const int r0 = j0 - q + jt;
-          xs[q] = r0 >= 0 ? col[r0 * xld] : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < G; ++q) {
-          const int j = j0 - q;
-          if (j >= 0) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, xs[q], w2, x1) : 0.f;
-          x1 = xs[q];
-        }
+      for (int j0 = n - 1; j0 >= 0; j0 -= SH_TX) {
+        const int j = j0 - tx, r0 = j + jt;
+        const float x0 = (j >= 0 && r0 >= 0) ? col[r0 * xld] : 0.f;
+        const float x1 = (j >= 0 && r0 + 1 >= 0) ? col[(r0 + 1) * xld] : 0.f;
+        __syncwarp();
+        if (j >= 0) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
       }
     }
+    __syncwarp();
   }
   __syncthreads();
   // pass 3: output (j, x) = lerp(Y[j][a], Y[j][a+1]), a = x + sh + iadd, for
