@@ -12,13 +12,15 @@ terms), Poisson data at 5e6 counts.  One step = one OSEM iteration (all
   e2e        the public call IrlOsem (host buffers in, result out, set-up,
              normalisation images and a per-iteration callback included),
              wall time / iterations
-  roofline   the dominant stage (the DRF convolution) against its bound
+  roofline   the stage with the largest device time (ESSE) against its bound,
+             the other stages beside it
   cpu_baseline  the reference C (compiled here) on a bounded sample
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-For N > 1 (torchrun) every rank runs an independent replica (the path does
-not shard) and rank 0 prints the job line.
+For N > 1 (torchrun) every rank runs an independent replica (a reconstruction
+is one device's work: its subsets depend on one another) and rank 0 prints
+the job line.
 """
 from __future__ import annotations
 
@@ -639,6 +641,10 @@ def run_large256(args):
     tmp = tempfile.mkdtemp(prefix="irl256_")
     pp, lw = W.large256(window="photopeak"), W.large256(window="lower")
     fpp, flw = pp.write_tables(os.path.join(tmp, "pp")), lw.write_tables(os.path.join(tmp, "lw"))
+    # the process's first device work (context creation, module loading) in
+    # a small untimed IrlGenprj, so that the timed calls measure projection
+    warm = W.full128(seed=1, n=32, nviews=8, subsets=2, iterations=1, drf_max_offs=6, name="warm")
+    _genprj(lib, warm, warm.write_tables(os.path.join(tmp, "warm")), 1.0)
     t0 = time.perf_counter()
     prj = _genprj(lib, pp, fpp, 1.0, fft=True)
     g_pp = time.perf_counter() - t0
