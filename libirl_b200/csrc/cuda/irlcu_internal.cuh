@@ -66,7 +66,8 @@ struct EsseWork {
   float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;
   float2 *A = nullptr, *Bf = nullptr, *C2[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
   float *g[2] = {nullptr, nullptr};
-  float *T[2] = {nullptr, nullptr};
+  float *T[2] = {nullptr, nullptr};   // smoothed terms (coarse in x after the z pass)
+  float *Tc[2] = {nullptr, nullptr};  // terms after the y pass, coarse in z and x
   int batch = 0;
   int nxv = 0, nyv = 0, nzv = 0;
 };

@@ -11,7 +11,9 @@
 //      keeping only the cropped output region), i.e. the circular
 //      convolution of krnlprj3d.c:783-790, 815-817;
 //   4. expand by c with libirl's recursive (in place) (c+1)-point smoothing
-//      along y, then z, then x (ExpandByFac, krnlprj3d.c:595-673);
+//      along y, then z, then x (ExpandByFac, krnlprj3d.c:595-673); lines
+//      that receive the same inputs are smoothed once (coarse z and x after
+//      the y pass, coarse x after the z pass);
 //   5. combine with the depth and density terms: eff = T0 - d*T1,
 //      eff *= exp(d*(mu0-mu_avg)), eff += act*CntrPixFac, eff *= mu/(mu0*pix),
 //      clamp at 0 (krnlprj3d.c:833-946), and form the projector source
@@ -566,31 +568,36 @@ __device__ __forceinline__ float expand_scale(float v) {
 // loads issued ahead of the dependent walk along a line
 constexpr int WALK_PF = 8;
 
-// expansion along y with the y smoothing: thread per (b, z, x) line of the
-// fine grid; g = cropped coarse result [B][nyv][nzv][nxv]; C = collapse
-// (n = C nyv).  The walk goes coarse row by coarse row: each coarse value
-// is loaded and scaled once and feeds the C fine steps whose look-ahead
-// input (fine row y + H) it is; loads run WALK_PF coarse rows ahead.
+// The expansion replicates each coarse value over a c x c x c block, so a
+// fine (z, x) line's inputs along y depend only on (z / c, x / c): after the
+// y smoothing every c x c group of lines holds the same values, and after
+// the z smoothing every group of c lines along x does.  The terms are
+// therefore kept at coarse z and x after the y pass, and at coarse x after
+// the z pass; the x pass expands x as it stages its rows.
+
+// expansion along y with the y smoothing: thread per (b, zc, xc) coarse
+// line; g = cropped coarse result [B][nyv][nzv][nxv]; output
+// t[b][y][zc][xc] (y fine).  The walk goes coarse row by coarse row: each
+// coarse value is loaded and scaled once and feeds the C fine steps whose
+// look-ahead input (fine row y + H) it is; loads run WALK_PF coarse rows
+// ahead.
 template <int C>
 __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1,
-                                                  float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
-                                                  int nz, int nyv, int nzv, int nxv, int nb) {
+                                                   float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
+                                                   int nyv, int nzv, int nxv, int nb) {
   constexpr int H = C / 2;
-  const size_t pln = (size_t)nz * n;
+  const size_t gs = (size_t)nzv * nxv;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)nb * pln) return;
-  const int b = (int)(e / pln);
-  const int i = (int)(e - (size_t)b * pln);
-  const int z = i / n, x = i - z * n;
-  const int gs = nzv * nxv;
+  if (e >= (size_t)nb * gs) return;
+  const int b = (int)(e / gs);
+  const size_t i = e - (size_t)b * gs;  // zc * nxv + xc
   for (int t = 0; t < nt; ++t) {
-    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + (z / C) * nxv + x / C;
-    float *o = (t == 0 ? t0 : t1) + (size_t)b * pln * n + i;
+    const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + i;
+    float *o = (t == 0 ? t0 : t1) + (size_t)b * n * gs + i;
     LineSmoother<H> L;
     float cv[WALK_PF];
 #pragma unroll
     for (int q = 0; q < WALK_PF; ++q) cv[q] = expand_scale<C>(__ldg(g + min(q, nyv - 1) * gs));
-    // fine rows q < H look ahead into coarse row 0
 #pragma unroll
     for (int q = 0; q < H; ++q) L.in[q] = cv[0];
     for (int yc0 = 0; yc0 < nyv; yc0 += WALK_PF) {
@@ -602,14 +609,12 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
       for (int r = 0; r < WALK_PF; ++r) {
         const int yc = yc0 + r;
         if (yc < nyv) {
-          // coarse row yc and the next one (the last row repeats: fine
-          // look-ahead rows past the end read the last row, as min(y+H, n-1))
           const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : cnext;
 #pragma unroll
           for (int q = 0; q < C; ++q) {
             const int y = yc * C + q;
             L.in[H] = ((q + H) / C == 0) ? ca : cb;
-            o[(size_t)y * pln] = L.step(y, n);
+            o[(size_t)y * gs] = L.step(y, n);
           }
         }
       }
@@ -619,34 +624,36 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
   }
 }
 
-// recursive smoothing along z in place: thread per (b, y, x).  A batch of
-// inputs is loaded before the batch's outputs are stored; the loads are at
-// z + H and beyond, which no earlier batch has overwritten.
-template <int H>
-__global__ void __launch_bounds__(256) k_smooth_z(float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
-                                                  int nz, int nb) {
+// z expansion with the z smoothing: thread per (b, y, xc); input
+// tc[b][y][zc][xc], output u[b][y][z][xc] with every entry written (entries
+// z < h and z >= nz - h keep their input value, as the in-place pass leaves
+// them).  Each coarse value feeds the C fine rows z with z / C = zc.
+template <int C>
+__global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0, const float *__restrict__ tc1,
+                                                   float *__restrict__ u0, float *__restrict__ u1, int nt, int n,
+                                                   int nz, int nzv, int nxv, int nb) {
+  constexpr int H = C / 2;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t lines = (size_t)nb * n * n;
+  const size_t lines = (size_t)nb * n * nxv;
   if (e >= lines) return;
-  const int b = (int)(e / ((size_t)n * n));
-  const int r = (int)(e - (size_t)b * n * n);
-  const int y = r / n, x = r - y * n;
+  const size_t by = e / nxv;  // b * n + y
+  const int xc = (int)(e - by * nxv);
   for (int t = 0; t < nt; ++t) {
-    float *o = (t == 0 ? t0 : t1) + (size_t)b * n * nz * n + (size_t)y * nz * n + x;
+    const float *in = (t == 0 ? tc0 : tc1) + by * nzv * nxv + xc;
+    float *o = (t == 0 ? u0 : u1) + by * nz * nxv + xc;
     LineSmoother<H> L;
 #pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = o[(size_t)q * n];
+    for (int q = 0; q < H; ++q) L.in[q] = __ldg(in + (size_t)(q / C) * nxv);
     for (int z0 = 0; z0 < nz; z0 += WALK_PF) {
       float nx[WALK_PF];
 #pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) nx[q] = o[(size_t)min(z0 + q + H, nz - 1) * n];
+      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(in + (size_t)(min(z0 + q + H, nz - 1) / C) * nxv);
 #pragma unroll
       for (int q = 0; q < WALK_PF; ++q) {
         const int z = z0 + q;
         if (z < nz) {
           L.in[H] = nx[q];
-          const float v = L.step(z, nz);
-          if (z >= H && z < nz - H) o[(size_t)z * n] = v;
+          o[(size_t)z * nxv] = L.step(z, nz);
         }
       }
     }
@@ -656,12 +663,13 @@ __global__ void __launch_bounds__(256) k_smooth_z(float *__restrict__ t0, float 
 // recursive smoothing along x (rows staged in shared memory) fused with the
 // depth/density combination and the projector source.
 struct CombineArgs {
-  const float *t0, *t1;   // expanded terms [B][n][nz][n]
+  const float *t0, *t1;   // smoothed terms [B][n][nz][n / xc]: fine x = xc * coarse x + k
   const float *rot;       // rotated activity [B][n][nz][n]
   const float *S, *mu;    // per-view tables [view][n][nz][n]
   const int *views;
   float *src;             // output [B][n][nz][n]
   int n, nz, c, nt;
+  int xc;                 // x replication of the term rows (1: full resolution)
   float cnv;              // (float)(1.0/mu0)
   float fmu;              // mu0 - mu_avg
   float cntr;             // CntrPixFac
@@ -699,22 +707,27 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
   const size_t base = (size_t)b * vox + (size_t)y * pln + (size_t)z0 * n;
   const bool vec = (n & 3) == 0;  // rows of whole float4s (16-byte aligned)
   const int n4 = n >> 2;
+  // term rows of tn = n / xc values, each replicated xc times along x
+  const int xc = a.xc, tn = n / xc;
+  const size_t tbase = ((size_t)b * n + y) * nz * tn + (size_t)z0 * tn;
+  const bool tvec = (tn & 3) == 0;
+  const int tn4 = tn >> 2;
   for (int t = 0; t < a.nt; ++t) {
-    const float *src = (t == 0 ? a.t0 : a.t1) + base;
+    const float *src = (t == 0 ? a.t0 : a.t1) + tbase;
     float *dst = smx + (size_t)t * XZB * ld;
-    if (vec) {
-      for (int e = tid; e < rows * n4; e += 32 * CX_TY) {
-        const int rr = e / n4, x = (e - rr * n4) * 4;
-        const float4 v = __ldg(reinterpret_cast<const float4 *>(src + (size_t)rr * n + x));
-        float *d = dst + rr * ld + x;
-        d[0] = v.x;
-        d[1] = v.y;
-        d[2] = v.z;
-        d[3] = v.w;
+    if (tvec) {
+      for (int e = tid; e < rows * tn4; e += 32 * CX_TY) {
+        const int rr = e / tn4, q4 = (e - rr * tn4) * 4;
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(src + (size_t)rr * tn + q4));
+        float *d = dst + rr * ld + q4 * xc;
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          for (int k = 0; k < xc; ++k) d[j * xc + k] = vv[j];
       }
     } else {
       for (int rr = ty; rr < rows; rr += CX_TY)
-        for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * n + xx];
+        for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * tn + xx / xc];
     }
   }
   __syncthreads();
@@ -932,6 +945,7 @@ void esse_free(Ctx &c) {
     dev_free(w.D[t], c.st);
     dev_free(w.g[t], c.st);
     dev_free(w.T[t], c.st);
+    dev_free(w.Tc[t], c.st);
   }
   c.ew = EsseWork{};
 }
@@ -988,7 +1002,8 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.C2[t]), sizeof(float2) * (size_t)B * w.nyv * E.kz * E.kxh, c.st));
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.D[t]), sizeof(float2) * (size_t)B * w.nyv * w.nzv * E.kxh, c.st));
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.g[t]), sizeof(float) * (size_t)B * w.nyv * w.nzv * w.nxv, c.st));
-    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.T[t]), sizeof(float) * (size_t)B * c.vox, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.T[t]), sizeof(float) * (size_t)B * c.n * c.nz * w.nxv, c.st));
+    CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.Tc[t]), sizeof(float) * (size_t)B * c.n * w.nzv * w.nxv, c.st));
   }
   // kernel spectra: forward transform of the full real grids
   const float *hk[3] = {e->krnl, e->kmu, e->kmu2};
@@ -1231,21 +1246,18 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
   EsseWork &w = c.ew;
   const int nyv = w.nyv, nzv = w.nzv, nxv = w.nxv;
   const int cf = E.collapse;
-  if (cf == 1) {
-    // no collapse: the cropped grid is the full-resolution term
-    for (int t = 0; t < E.nterms; ++t)
-      CU_TRY(cudaMemcpyAsync(w.T[t], w.g[t], sizeof(float) * (size_t)nv * c.vox, cudaMemcpyDeviceToDevice, c.st));
-  } else {
-    const size_t lines = (size_t)nv * c.pln;
-    const unsigned gy = (unsigned)((lines + 255) / 256);
-    const size_t zl = (size_t)nv * c.n * c.n;
-    const unsigned gz = (unsigned)((zl + 255) / 256);
-#define EXPAND_Z(C)                                                                                          \
-  case C:                                                                                                    \
-    k_expand_y<C><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, nyv, nzv, nxv, nv); \
-    CU_LAUNCHED();                                                                                           \
-    k_smooth_z<C / 2><<<gz, 256, 0, c.st>>>(w.T[0], w.T[1], E.nterms, c.n, c.nz, nv);                        \
-    CU_LAUNCHED();                                                                                           \
+  // c = 1: the cropped grid is the full-resolution term and needs no
+  // smoothing; otherwise y expansion and smoothing (coarse z and x), then z
+  // expansion and smoothing (coarse x)
+  if (cf > 1) {
+    const unsigned gy = (unsigned)(((size_t)nv * nzv * nxv + 255) / 256);
+    const unsigned gz = (unsigned)(((size_t)nv * c.n * nxv + 255) / 256);
+#define EXPAND_Z(C)                                                                                            \
+  case C:                                                                                                      \
+    k_expand_y<C><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.Tc[0], w.Tc[1], E.nterms, c.n, nyv, nzv, nxv, nv);    \
+    CU_LAUNCHED();                                                                                             \
+    k_smooth_z<C><<<gz, 256, 0, c.st>>>(w.Tc[0], w.Tc[1], w.T[0], w.T[1], E.nterms, c.n, c.nz, nzv, nxv, nv);   \
+    CU_LAUNCHED();                                                                                             \
     break;
     switch (cf) {
       EXPAND_Z(2)
@@ -1260,8 +1272,8 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
 #undef EXPAND_Z
   }
   CombineArgs ca{};
-  ca.t0 = w.T[0];
-  ca.t1 = w.T[1];
+  ca.t0 = cf > 1 ? w.T[0] : w.g[0];
+  ca.t1 = cf > 1 ? w.T[1] : w.g[1];
   ca.rot = rot;
   ca.S = c.tS;
   ca.mu = c.tMu;
@@ -1270,6 +1282,7 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
   ca.n = c.n;
   ca.nz = c.nz;
   ca.c = cf;
+  ca.xc = cf;
   ca.nt = E.nterms;
   ca.cnv = (float)(1.0 / (double)E.mu0);
   ca.fmu = E.mu0 - E.mu_avg;

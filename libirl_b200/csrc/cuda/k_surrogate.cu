@@ -319,7 +319,8 @@ __global__ void __launch_bounds__(GNT) k_conv_gemm(GemmArgs a, ConvGeom g, const
 //     tcgen05.ld, adds the bias, applies ReLU and stores 8 channels per
 //     16-byte vector, or writes raw split-K partial sums.
 // Every mbarrier wait is bounded; on a timeout the CTA records the error in
-// g_tc_error, waits (bounded) for its last commit and frees its TMEM.
+// g_tc_error, issues no further copies or MMAs, waits for its copies in
+// flight and (bounded) for its last commit, and frees its TMEM.
 constexpr int TC_BM = 128, TC_BK = 64, TC_NT = 128, TC_S = 4;
 constexpr int TC_MAXCH = 640;  // k chunks (of 8) of one CTA's k range: K / 8 <= 576 here
 constexpr unsigned TC_WAIT_LIMIT = 1u << 22;
@@ -457,6 +458,7 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
     asm volatile("cp.async.wait_group %0;" ::"n"(TC_S - 2) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
+    if (abort_flag) break;  // a wait ran out (flag set before the barrier): issue nothing more
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t a0 = sbase + st * Cfg::STAGE, b0 = a0 + Cfg::A_BYTES;
