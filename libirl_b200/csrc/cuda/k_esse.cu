@@ -663,13 +663,12 @@ __global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0,
 // recursive smoothing along x (rows staged in shared memory) fused with the
 // depth/density combination and the projector source.
 struct CombineArgs {
-  const float *t0, *t1;   // smoothed terms [B][n][nz][n / xc]: fine x = xc * coarse x + k
+  const float *t0, *t1;   // terms after the z pass [B][n][nz][n / c] (coarse x)
   const float *rot;       // rotated activity [B][n][nz][n]
   const float *S, *mu;    // per-view tables [view][n][nz][n]
   const int *views;
   float *src;             // output [B][n][nz][n]
   int n, nz, c, nt;
-  int xc;                 // x replication of the term rows (1: full resolution)
   float cnv;              // (float)(1.0/mu0)
   float fmu;              // mu0 - mu_avg
   float cntr;             // CntrPixFac
@@ -690,61 +689,74 @@ __device__ __forceinline__ float combine_one(const CombineArgs &a, float T0, flo
   return __fadd_rn(__fmul_rn(act, a.primary), eff);
 }
 
-// CTA of 32 x CX_TY threads per (b, y, block of XZB z rows); rows are staged
-// with an odd stride so that one thread per row can walk x without bank
-// conflicts.
+// CTA of 32 x CX_TY threads per (b, y, block of XZB z rows).  The terms'
+// rows arrive coarse in x (n / C values, each standing for C fine ones) and
+// are staged as they are; one thread per (term, row) walks the fine x
+// positions, reading its inputs from the coarse row (never overwritten, so
+// every read sees an input as libirl's in-place walk does) and writing the
+// smoothed fine row.  Rows have odd strides, so the row walks are free of
+// bank conflicts.  C = 1 (no smoothing): the combination reads the staged
+// rows.
 constexpr int XZB = 32;
 constexpr int CX_TY = 8;
 
-template <int H>
+static size_t smooth_x_smem(int n, int c) { return sizeof(float) * 2 * XZB * ((size_t)(n + 1) + (n / c + 1)); }
+
+template <int C>
 __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) {
-  extern __shared__ float smx[];  // [nt][XZB][n + 1]
-  const int n = a.n, nz = a.nz, ld = n + 1;
+  constexpr int H = C / 2;
+  extern __shared__ float smx[];  // fine rows [2][XZB][n + 1], coarse rows [2][XZB][n / C + 1]
+  const int n = a.n, nz = a.nz, ld = n + 1, tn = n / C, lq = tn + 1;
+  float *F = smx, *Q = smx + (size_t)2 * XZB * ld;
   const int y = blockIdx.x, z0 = blockIdx.y * XZB, b = blockIdx.z;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int rows = min(XZB, nz - z0);
   const size_t pln = (size_t)nz * n, vox = pln * n;
   const size_t base = (size_t)b * vox + (size_t)y * pln + (size_t)z0 * n;
-  const bool vec = (n & 3) == 0;  // rows of whole float4s (16-byte aligned)
-  const int n4 = n >> 2;
-  // term rows of tn = n / xc values, each replicated xc times along x
-  const int xc = a.xc, tn = n / xc;
   const size_t tbase = ((size_t)b * n + y) * nz * tn + (size_t)z0 * tn;
-  const bool tvec = (tn & 3) == 0;
+  const bool tvec = (tn & 3) == 0;  // coarse rows of whole float4s (16-byte aligned)
   const int tn4 = tn >> 2;
   for (int t = 0; t < a.nt; ++t) {
     const float *src = (t == 0 ? a.t0 : a.t1) + tbase;
-    float *dst = smx + (size_t)t * XZB * ld;
+    float *dst = Q + (size_t)t * XZB * lq;
     if (tvec) {
       for (int e = tid; e < rows * tn4; e += 32 * CX_TY) {
         const int rr = e / tn4, q4 = (e - rr * tn4) * 4;
         const float4 v = __ldg(reinterpret_cast<const float4 *>(src + (size_t)rr * tn + q4));
-        float *d = dst + rr * ld + q4 * xc;
-        const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          for (int k = 0; k < xc; ++k) d[j * xc + k] = vv[j];
+        float *d = dst + rr * lq + q4;
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
       }
     } else {
       for (int rr = ty; rr < rows; rr += CX_TY)
-        for (int xx = tx; xx < n; xx += 32) dst[rr * ld + xx] = src[(size_t)rr * tn + xx / xc];
+        for (int xx = tx; xx < tn; xx += 32) dst[rr * lq + xx] = src[(size_t)rr * tn + xx];
     }
   }
   __syncthreads();
-  if (H > 0 && tid < a.nt * XZB && (tid % XZB) < rows) {
-    float *row = smx + (size_t)tid * ld;  // (term, row) = (tid / XZB, tid % XZB)
-    LineSmoother<H> L;
+  const float *R = Q;  // rows the combination reads, stride lr
+  int lr = lq;
+  if (H > 0) {
+    if (tid < a.nt * XZB && (tid % XZB) < rows) {
+      const float *qrow = Q + (size_t)tid * lq;  // (term, row) = (tid / XZB, tid % XZB)
+      float *frow = F + (size_t)tid * ld;
+      LineSmoother<H> L;
 #pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = row[q];
-    for (int x = 0; x < n; ++x) {
-      L.in[H] = row[min(x + H, n - 1)];
-      row[x] = L.step(x, n);
+      for (int q = 0; q < H; ++q) L.in[q] = qrow[q / C];
+      for (int x = 0; x < n; ++x) {
+        L.in[H] = qrow[min(x + H, n - 1) / C];
+        frow[x] = L.step(x, n);
+      }
     }
+    __syncthreads();
+    R = F;
+    lr = ld;
   }
-  __syncthreads();
   const int view = a.views[b];
   const size_t tb = (size_t)view * vox + (size_t)y * pln + (size_t)z0 * n;
-  if (vec) {
+  if ((n & 3) == 0) {
+    const int n4 = n >> 2;
     for (int e = tid; e < rows * n4; e += 32 * CX_TY) {
       const int rr = e / n4, x = (e - rr * n4) * 4;
       const size_t g = (size_t)rr * n + x;
@@ -756,8 +768,8 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
       float out[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float T0 = smx[rr * ld + x + q];
-        const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + x + q] : 0.f;
+        const float T0 = R[rr * lr + x + q];
+        const float T1 = a.nt > 1 ? R[(XZB + rr) * lr + x + q] : 0.f;
         out[q] = combine_one(a, T0, T1, Sv[q], Av[q], Mv[q]);
       }
       *reinterpret_cast<float4 *>(a.src + base + g) = make_float4(out[0], out[1], out[2], out[3]);
@@ -767,8 +779,8 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
   for (int rr = ty; rr < rows; rr += CX_TY) {
     for (int xx = tx; xx < n; xx += 32) {
       const size_t e = (size_t)rr * n + xx;
-      const float T0 = smx[rr * ld + xx];
-      const float T1 = a.nt > 1 ? smx[(XZB + rr) * ld + xx] : 0.f;
+      const float T0 = R[rr * lr + xx];
+      const float T1 = a.nt > 1 ? R[(XZB + rr) * lr + xx] : 0.f;
       a.src[base + e] = combine_one(a, T0, T1, __ldg(a.S + tb + e), __ldg(a.rot + base + e), __ldg(a.mu + tb + e));
     }
   }
@@ -1282,7 +1294,6 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
   ca.n = c.n;
   ca.nz = c.nz;
   ca.c = cf;
-  ca.xc = cf;
   ca.nt = E.nterms;
   ca.cnv = (float)(1.0 / (double)E.mu0);
   ca.fmu = E.mu0 - E.mu_avg;
@@ -1291,21 +1302,24 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
   ca.primary = primary;
   {
     dim3 grid_(c.n, (c.nz + XZB - 1) / XZB, nv);
-    const size_t sm = sizeof(float) * 2 * XZB * (size_t)(c.n + 1);
-    static size_t configured = 0;
-    if (sm > 48 * 1024 && sm > configured) {
-      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      configured = sm;
+    const size_t sm = smooth_x_smem(c.n, cf);
+    static size_t configured[8] = {};
+    if (cf < 1 || cf > 7) return set_error(IRLCU_EARG, "ESSE collapse factor %d not supported (1..7)", cf);
+    if (sm > 48 * 1024 && sm > configured[cf]) {
+      switch (cf) {
+#define SXC_ATTR(C) \
+  case C: CU_TRY(cudaFuncSetAttribute(k_smooth_x_combine<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); break;
+        SXC_ATTR(1) SXC_ATTR(2) SXC_ATTR(3) SXC_ATTR(4) SXC_ATTR(5) SXC_ATTR(6) SXC_ATTR(7)
+#undef SXC_ATTR
+      }
+      configured[cf] = sm;
     }
     const dim3 blk(32, CX_TY);
-    switch (cf / 2) {
-      case 0: k_smooth_x_combine<0><<<grid_, blk, sm, c.st>>>(ca); break;
-      case 1: k_smooth_x_combine<1><<<grid_, blk, sm, c.st>>>(ca); break;
-      case 2: k_smooth_x_combine<2><<<grid_, blk, sm, c.st>>>(ca); break;
-      default: k_smooth_x_combine<3><<<grid_, blk, sm, c.st>>>(ca); break;
+    switch (cf) {
+#define SXC_LAUNCH(C) \
+  case C: k_smooth_x_combine<C><<<grid_, blk, sm, c.st>>>(ca); break;
+      SXC_LAUNCH(1) SXC_LAUNCH(2) SXC_LAUNCH(3) SXC_LAUNCH(4) SXC_LAUNCH(5) SXC_LAUNCH(6) SXC_LAUNCH(7)
+#undef SXC_LAUNCH
     }
     CU_LAUNCHED();
   }
