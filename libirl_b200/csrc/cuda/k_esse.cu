@@ -575,8 +575,8 @@ constexpr int WALK_PF = 8;
 // therefore kept at coarse z and x after the y pass, and at coarse x after
 // the z pass; the x pass expands x as it stages its rows.
 
-// expansion along y with the y smoothing: thread per (b, zc, xc) coarse
-// line; g = cropped coarse result [B][nyv][nzv][nxv]; output
+// expansion along y with the y smoothing: thread per (term, b, zc, xc)
+// coarse line; g = cropped coarse result [B][nyv][nzv][nxv]; output
 // t[b][y][zc][xc] (y fine).  The walk goes coarse row by coarse row: each
 // coarse value is loaded and scaled once and feeds the C fine steps whose
 // look-ahead input (fine row y + H) it is; loads run WALK_PF coarse rows
@@ -586,12 +586,13 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
                                                    float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
                                                    int nyv, int nzv, int nxv, int nb) {
   constexpr int H = C / 2;
-  const size_t gs = (size_t)nzv * nxv;
+  const size_t gs = (size_t)nzv * nxv, per = (size_t)nb * gs;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)nb * gs) return;
-  const int b = (int)(e / gs);
-  const size_t i = e - (size_t)b * gs;  // zc * nxv + xc
-  for (int t = 0; t < nt; ++t) {
+  if (e >= (size_t)nt * per) return;
+  const int t = (int)(e / per);
+  const int b = (int)((e - t * per) / gs);
+  const size_t i = e - t * per - (size_t)b * gs;  // zc * nxv + xc
+  {
     const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + i;
     float *o = (t == 0 ? t0 : t1) + (size_t)b * n * gs + i;
     LineSmoother<H> L;
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
   }
 }
 
-// z expansion with the z smoothing: thread per (b, y, xc); input
+// z expansion with the z smoothing: thread per (term, b, y, xc); input
 // tc[b][y][zc][xc], output u[b][y][z][xc] with every entry written (entries
 // z < h and z >= nz - h keep their input value, as the in-place pass leaves
 // them).  Each coarse value feeds the C fine rows z with z / C = zc.
@@ -635,10 +636,11 @@ __global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0,
   constexpr int H = C / 2;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t lines = (size_t)nb * n * nxv;
-  if (e >= lines) return;
-  const size_t by = e / nxv;  // b * n + y
-  const int xc = (int)(e - by * nxv);
-  for (int t = 0; t < nt; ++t) {
+  if (e >= (size_t)nt * lines) return;
+  const int t = (int)(e / lines);
+  const size_t by = (e - t * lines) / nxv;  // b * n + y
+  const int xc = (int)(e - t * lines - by * nxv);
+  {
     const float *in = (t == 0 ? tc0 : tc1) + by * nzv * nxv + xc;
     float *o = (t == 0 ? u0 : u1) + by * nz * nxv + xc;
     LineSmoother<H> L;
@@ -1262,8 +1264,8 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
   // smoothing; otherwise y expansion and smoothing (coarse z and x), then z
   // expansion and smoothing (coarse x)
   if (cf > 1) {
-    const unsigned gy = (unsigned)(((size_t)nv * nzv * nxv + 255) / 256);
-    const unsigned gz = (unsigned)(((size_t)nv * c.n * nxv + 255) / 256);
+    const unsigned gy = (unsigned)(((size_t)E.nterms * nv * nzv * nxv + 255) / 256);
+    const unsigned gz = (unsigned)(((size_t)E.nterms * nv * c.n * nxv + 255) / 256);
 #define EXPAND_Z(C)                                                                                            \
   case C:                                                                                                      \
     k_expand_y<C><<<gy, 256, 0, c.st>>>(w.g[0], w.g[1], w.Tc[0], w.Tc[1], E.nterms, c.n, nyv, nzv, nxv, nv);    \
