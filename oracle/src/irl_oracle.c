@@ -43,6 +43,12 @@ void or_shears_rotate(float fAngle, const float *in, float *out, int n, int nz)
 	int b90 = 0, b180 = 0, i, j, k, iAdd, mDim, iT, jT, *st, *en;
 	float c, tc, yd, xd, fd, f1, f2, *X, *Y;
 #define IN(x, y, s) in[(size_t)(y) * nz * n + (size_t)(s) * n + (x)]
+	/* a pass-1 tap outside the slice (x or y outside [0, n)) reads 0: for odd
+	   n the middle row's last second tap lies one past the row
+	   (fastrotate.c:400-488 reads that memory, and for the last row of the
+	   last slice memory past the volume) with weight f2 = 0 exactly, so the
+	   reference's result equals this one whenever that memory is finite */
+#define TAP(x, y, s) (((x) < 0 || (x) >= n || (y) < 0 || (y) >= n) ? 0.f : IN(x, y, s))
 	while (fAngle > 0.75 * M_PI) {
 		fAngle -= M_PI;
 		b180 = !b180;
@@ -89,20 +95,20 @@ void or_shears_rotate(float fAngle, const float *in, float *out, int n, int nz)
 				if (!b180) {
 					int t = i + iT - iAdd;
 					if (!b90) {
-						a = IN(t, j, k);
-						b = IN(t + 1, j, k);
+						a = TAP(t, j, k);
+						b = TAP(t + 1, j, k);
 					} else {
-						a = IN(jj, t, k);
-						b = IN(jj, t + 1, k);
+						a = TAP(jj, t, k);
+						b = TAP(jj, t + 1, k);
 					}
 				} else {
 					int t = n - i - (iT - iAdd + 1);
 					if (!b90) {
-						a = IN(t, jj, k);
-						b = IN(t - 1, jj, k);
+						a = TAP(t, jj, k);
+						b = TAP(t - 1, jj, k);
 					} else {
-						a = IN(j, t, k);
-						b = IN(j, t - 1, k);
+						a = TAP(j, t, k);
+						b = TAP(j, t - 1, k);
 					}
 				}
 				X[i + (size_t)mDim * (j + iAdd)] = f1 * a + f2 * b;
@@ -134,6 +140,7 @@ void or_shears_rotate(float fAngle, const float *in, float *out, int n, int nz)
 					f1 * Y[i + iT + (size_t)mDim * (j + iAdd)] + f2 * Y[i + iT + 1 + (size_t)mDim * (j + iAdd)];
 		}
 	}
+#undef TAP
 #undef IN
 	free(X);
 	free(Y);
