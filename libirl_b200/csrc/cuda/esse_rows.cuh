@@ -74,10 +74,12 @@ __device__ __forceinline__ int er_xi(int wl, int n2) {
   return INV ? n2 * ER_LW + wl : wl * ERow<L>::N2 + n2;
 }
 
-// forward step A, round of lines w0 .. w0 + ER_LW - 1 (item: n2 fastest)
-template <int L>
+// forward step A, round of lines w0 .. w0 + ER_LW - 1 (item: n2 fastest);
+// the collapsed values come from pre (rows [nrows][nxv], already collapsed
+// by k_esse_collapse) when PRE, else from rot
+template <int L, bool PRE = false>
 __device__ __forceinline__ void er_fwd_a(int tid, int w0, float2 *X, const float2 *tw, const float *rot, int n,
-                                         int nz, int c, int nzv, int nxv, int nrows) {
+                                         int nz, int c, int nzv, int nxv, int nrows, const float *pre = nullptr) {
   using D = ERow<L>;
   for (int it = tid; it < ER_LW * D::N2; it += ER_NT) {
     const int wl = it / D::N2, n2 = it - wl * D::N2;
@@ -90,8 +92,13 @@ __device__ __forceinline__ void er_fwd_a(int tid, int w0, float2 *X, const float
       const int x = n2 + D::N2 * n1;
       float re = 0.f, im = 0.f;
       if (x < nxv) {
-        if (h0) re = er_collapse(rot, n, nz, c, y0, z0, x);
-        if (h1) im = er_collapse(rot, n, nz, c, y1, z1, x);
+        if constexpr (PRE) {
+          if (h0) re = er_ld(pre + (size_t)r0 * nxv + x);
+          if (h1) im = er_ld(pre + (size_t)(r0 + 1) * nxv + x);
+        } else {
+          if (h0) re = er_collapse(rot, n, nz, c, y0, z0, x);
+          if (h1) im = er_collapse(rot, n, nz, c, y1, z1, x);
+        }
       }
       v[n1] = make_float2(re, im);
     }

@@ -57,6 +57,7 @@ struct RowFwdArgs {
   float2 *out;          // [B][nyv][zext][kxh] with zext >= nzv, or kx-major
   int zext, kxh;
   int kmajor;           // 1: out is [B][kxh][nyv][nzv] (planes of fixed kx)
+  const float *pre;     // register form: B collapsed volumes [nyv][nzv][nxv], or null
 };
 
 // rows per CTA of the x passes (host: row_wr)
@@ -184,7 +185,23 @@ __global__ void k_fft_row_inv(RowInvArgs a, const float2 *__restrict__ twg) {
 
 // x transforms with register transforms (esse_rows.cuh), kx-major layout:
 // one CTA per ER_LW row pairs of a view (and term)
-template <int L>
+// CollapseByFac of nb rotated volumes into [b][y'][z'][x'], a thread per
+// collapsed value (consecutive x' in consecutive threads), summed as in
+// er_collapse
+__global__ void __launch_bounds__(256) k_esse_collapse(const float *__restrict__ rot, size_t vox, int n, int nz, int c,
+                                                       int nyv, int nzv, int nxv, int nb, float *__restrict__ out) {
+  const size_t per = (size_t)nyv * nzv * nxv;
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)nb * per) return;
+  const int b = (int)(e / per);
+  const size_t i = e - (size_t)b * per;
+  const int x = (int)(i % nxv);
+  const size_t r = i / nxv;
+  const int y = (int)(r / nzv), z = (int)(r - (size_t)y * nzv);
+  out[e] = er_collapse(rot + (size_t)b * vox, n, nz, c, y, z, x);
+}
+
+template <int L, bool PRE>
 __global__ void __launch_bounds__(ER_NT, 2) k_esse_row_fwd_reg(RowFwdArgs a, const float2 *__restrict__ twg) {
   using D = ERow<L>;
   extern __shared__ __align__(16) float2 ers[];
@@ -193,7 +210,8 @@ __global__ void __launch_bounds__(ER_NT, 2) k_esse_row_fwd_reg(RowFwdArgs a, con
   const int nrows = a.nyv * a.nzv;
   for (int i = tid; i < L; i += ER_NT) tw[i] = twg[i];
   __syncthreads();
-  er_fwd_a<L>(tid, w0, X, tw, a.rot + (size_t)b * a.vox, a.n, a.nz, a.c, a.nzv, a.nxv, nrows);
+  er_fwd_a<L, PRE>(tid, w0, X, tw, a.rot + (size_t)b * a.vox, a.n, a.nz, a.c, a.nzv, a.nxv, nrows,
+                   PRE ? a.pre + (size_t)b * nrows * a.nxv : nullptr);
   __syncthreads();
   constexpr int NB = (ER_LW * D::N1 + ER_NT - 1) / ER_NT;
   float2 u[NB][D::N2];
@@ -237,7 +255,8 @@ static bool er_len_ok(int L) { return L == 32 || L == 64 || L == 128 || L == 256
 static int er_attrs(int L) {
   static bool done = false;
   if (done) return IRLCU_OK;
-  CU_TRY(cudaFuncSetAttribute(k_esse_row_fwd_reg<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
+  CU_TRY(cudaFuncSetAttribute(k_esse_row_fwd_reg<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
+  CU_TRY(cudaFuncSetAttribute(k_esse_row_fwd_reg<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
   CU_TRY(cudaFuncSetAttribute(k_esse_row_inv_reg<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ERow<256>::SMEM));
   (void)L;
   done = true;
@@ -1127,8 +1146,21 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     const int lines = (nyv * nzv + 1) / 2;
     if (reg_rows) {
       TRY_ESSE(er_attrs(E.kx));
+      if (E.collapse > 1) {
+        // the collapse as its own streaming pass into g[0] (free until the
+        // x inverse writes it)
+        const size_t tot = (size_t)nv * nyv * nzv * nxv;
+        k_esse_collapse<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(rot, c.vox, c.n, c.nz, E.collapse, nyv, nzv,
+                                                                         nxv, nv, w.g[0]);
+        CU_LAUNCHED();
+        ra.pre = w.g[0];
+      }
       dim3 grid_((lines + ER_LW - 1) / ER_LW, nv);
-      ER_DISPATCH(E.kx, k_esse_row_fwd_reg<LL><<<grid_, ER_NT, ERow<LL>::SMEM, c.st>>>(ra, w.twx));
+      if (ra.pre) {
+        ER_DISPATCH(E.kx, k_esse_row_fwd_reg<LL, true><<<grid_, ER_NT, ERow<LL>::SMEM, c.st>>>(ra, w.twx));
+      } else {
+        ER_DISPATCH(E.kx, k_esse_row_fwd_reg<LL, false><<<grid_, ER_NT, ERow<LL>::SMEM, c.st>>>(ra, w.twx));
+      }
       CU_LAUNCHED();
     } else {
       dim3 grid_((nyv * nzv + row_wr(E.kx) - 1) / row_wr(E.kx), nv);
