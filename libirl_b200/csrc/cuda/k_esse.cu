@@ -662,21 +662,33 @@ __global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0,
   {
     const float *in = (t == 0 ? tc0 : tc1) + by * nzv * nxv + xc;
     float *o = (t == 0 ? u0 : u1) + by * nz * nxv + xc;
+    // coarse row by coarse row, as in k_expand_y: the look-ahead input of
+    // fine row z is coarse row min(z + H, nz - 1) / C
     LineSmoother<H> L;
+    float cv[WALK_PF];
 #pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = __ldg(in + (size_t)(q / C) * nxv);
-    for (int z0 = 0; z0 < nz; z0 += WALK_PF) {
+    for (int q = 0; q < WALK_PF; ++q) cv[q] = __ldg(in + (size_t)min(q, nzv - 1) * nxv);
+#pragma unroll
+    for (int q = 0; q < H; ++q) L.in[q] = cv[0];
+    for (int zc0 = 0; zc0 < nzv; zc0 += WALK_PF) {
       float nx[WALK_PF];
 #pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(in + (size_t)(min(z0 + q + H, nz - 1) / C) * nxv);
+      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(in + (size_t)min(zc0 + WALK_PF + q, nzv - 1) * nxv);
 #pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) {
-        const int z = z0 + q;
-        if (z < nz) {
-          L.in[H] = nx[q];
-          o[(size_t)z * nxv] = L.step(z, nz);
+      for (int r = 0; r < WALK_PF; ++r) {
+        const int zc = zc0 + r;
+        if (zc < nzv) {
+          const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : nx[0];
+#pragma unroll
+          for (int q = 0; q < C; ++q) {
+            const int z = zc * C + q;
+            L.in[H] = ((q + H) / C == 0) ? ca : cb;
+            o[(size_t)z * nxv] = L.step(z, nz);
+          }
         }
       }
+#pragma unroll
+      for (int q = 0; q < WALK_PF; ++q) cv[q] = nx[q];
     }
   }
 }
