@@ -774,12 +774,33 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
     if (tid < a.nt * XZB && (tid % XZB) < rows) {
       const float *qrow = Q + (size_t)tid * lq;  // (term, row) = (tid / XZB, tid % XZB)
       float *frow = F + (size_t)tid * ld;
+      // coarse value by coarse value (the look-ahead input of fine x is
+      // coarse min(x + H, n - 1) / C), loaded WALK_PF ahead
       LineSmoother<H> L;
+      float cv[WALK_PF];
 #pragma unroll
-      for (int q = 0; q < H; ++q) L.in[q] = qrow[q / C];
-      for (int x = 0; x < n; ++x) {
-        L.in[H] = qrow[min(x + H, n - 1) / C];
-        frow[x] = L.step(x, n);
+      for (int q = 0; q < WALK_PF; ++q) cv[q] = qrow[min(q, tn - 1)];
+#pragma unroll
+      for (int q = 0; q < H; ++q) L.in[q] = cv[0];
+      for (int xc0 = 0; xc0 < tn; xc0 += WALK_PF) {
+        float nx[WALK_PF];
+#pragma unroll
+        for (int q = 0; q < WALK_PF; ++q) nx[q] = qrow[min(xc0 + WALK_PF + q, tn - 1)];
+#pragma unroll
+        for (int r = 0; r < WALK_PF; ++r) {
+          const int xc = xc0 + r;
+          if (xc < tn) {
+            const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : nx[0];
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+              const int x = xc * C + q;
+              L.in[H] = ((q + H) / C == 0) ? ca : cb;
+              frow[x] = L.step(x, n);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < WALK_PF; ++q) cv[q] = nx[q];
       }
     }
     __syncthreads();
