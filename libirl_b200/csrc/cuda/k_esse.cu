@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "esse_rows.cuh"
+#include "esse_walk.cuh"
 #include "esse_yz.cuh"
 #include "fft_core.cuh"
 #include "irlcu_internal.cuh"
@@ -523,70 +524,6 @@ __global__ void k_spec_kmajor(const float2 *__restrict__ in, float2 *__restrict_
 
 // ------------------------------------------------- expansion / smoothing
 
-// x / D for the odd window lengths D = 2h+1 of the smoothing and for odd
-// collapse factors: q0 = x * RN(1/D), then one correction with the exact
-// residual r = x - q0*D (Markstein, IBM J. Res. Dev. 34(1), 1990).  For
-// D = 3, 5, 7 this equals the correctly rounded x / D for every finite x
-// except -0 (checked over all float inputs; tests/test_const_division.py
-// repeats it over the binades where under- and overflow could matter).
-// The sums divided here start from +0, so they are never -0.
-template <int D>
-__device__ __forceinline__ float div_const(float x) {
-  if constexpr (D == 1) {
-    return x;
-  } else if constexpr (D == 3 || D == 5 || D == 7) {
-    const float y = __int_as_float(D == 3 ? 0x3eaaaaab : (D == 5 ? 0x3e4ccccd : 0x3e124925));
-    const float q0 = __fmul_rn(x, y);
-    const float r = __fmaf_rn(-q0, (float)D, x);
-    return __fmaf_rn(r, y, q0);
-  } else if constexpr ((D & (D - 1)) == 0) {
-    return __fmul_rn(x, 1.0f / (float)D);  // exact for powers of two
-  } else {
-    return __fdiv_rn(x, (float)D);
-  }
-}
-
-// ExpandByFac's smoothing (krnlprj3d.c:636-670) walks each line once in
-// increasing order and overwrites it in place, so every output is
-//   out[k] = (out[k-h] + .. + out[k-1] + in[k] + .. + in[k+h]) / (2h+1)
-// summed left to right from 0, for h <= k < len-h (other entries keep
-// their input value), h = c/2.  The line walkers below keep the last h
-// outputs and the next h+1 inputs in registers.
-template <int H>
-struct LineSmoother {
-  float outp[H > 0 ? H : 1];   // out[k-H..k-1]
-  float in[H + 1];             // in[k..k+H]
-  // push in[k+H] after in[k..k+H-1] are loaded, return out[k]
-  __device__ __forceinline__ float step(int k, int len) {
-    float v;
-    if (k < H || k >= len - H) {
-      v = in[0];
-    } else {
-      float s = 0.f;
-#pragma unroll
-      for (int q = 0; q < H; ++q) s = __fadd_rn(s, outp[q]);
-#pragma unroll
-      for (int q = 0; q <= H; ++q) s = __fadd_rn(s, in[q]);
-      v = div_const<2 * H + 1>(s);
-    }
-#pragma unroll
-    for (int q = 0; q + 1 < H; ++q) outp[q] = outp[q + 1];
-    if (H > 0) outp[H - 1] = v;
-#pragma unroll
-    for (int q = 0; q < H; ++q) in[q] = in[q + 1];
-    return v;
-  }
-};
-
-// fine value of the expansion: coarse / c / c / c in libirl's order
-template <int C>
-__device__ __forceinline__ float expand_scale(float v) {
-  return div_const<C>(div_const<C>(div_const<C>(v)));
-}
-
-// loads issued ahead of the dependent walk along a line
-constexpr int WALK_PF = 8;
-
 // The expansion replicates each coarse value over a c x c x c block, so a
 // fine (z, x) line's inputs along y depend only on (z / c, x / c): after the
 // y smoothing every c x c group of lines holds the same values, and after
@@ -596,15 +533,11 @@ constexpr int WALK_PF = 8;
 
 // expansion along y with the y smoothing: thread per (term, b, zc, xc)
 // coarse line; g = cropped coarse result [B][nyv][nzv][nxv]; output
-// t[b][y][zc][xc] (y fine).  The walk goes coarse row by coarse row: each
-// coarse value is loaded and scaled once and feeds the C fine steps whose
-// look-ahead input (fine row y + H) it is; loads run WALK_PF coarse rows
-// ahead.
+// t[b][y][zc][xc] (y fine)
 template <int C>
 __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, const float *__restrict__ g1,
                                                    float *__restrict__ t0, float *__restrict__ t1, int nt, int n,
                                                    int nyv, int nzv, int nxv, int nb) {
-  constexpr int H = C / 2;
   const size_t gs = (size_t)nzv * nxv, per = (size_t)nb * gs;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (size_t)nt * per) return;
@@ -614,45 +547,18 @@ __global__ void __launch_bounds__(256) k_expand_y(const float *__restrict__ g0, 
   {
     const float *g = (t == 0 ? g0 : g1) + (size_t)b * nyv * gs + i;
     float *o = (t == 0 ? t0 : t1) + (size_t)b * n * gs + i;
-    LineSmoother<H> L;
-    float cv[WALK_PF];
-#pragma unroll
-    for (int q = 0; q < WALK_PF; ++q) cv[q] = expand_scale<C>(__ldg(g + min(q, nyv - 1) * gs));
-#pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = cv[0];
-    for (int yc0 = 0; yc0 < nyv; yc0 += WALK_PF) {
-      float nx[WALK_PF];
-#pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(g + min(yc0 + WALK_PF + q, nyv - 1) * gs);
-      const float cnext = expand_scale<C>(nx[0]);
-#pragma unroll
-      for (int r = 0; r < WALK_PF; ++r) {
-        const int yc = yc0 + r;
-        if (yc < nyv) {
-          const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : cnext;
-#pragma unroll
-          for (int q = 0; q < C; ++q) {
-            const int y = yc * C + q;
-            L.in[H] = ((q + H) / C == 0) ? ca : cb;
-            o[(size_t)y * gs] = L.step(y, n);
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) cv[q] = expand_scale<C>(nx[q]);
-    }
+    coarse_walk<C, true, true>(g, gs, nyv, o, gs);
   }
 }
 
 // z expansion with the z smoothing: thread per (term, b, y, xc); input
 // tc[b][y][zc][xc], output u[b][y][z][xc] with every entry written (entries
 // z < h and z >= nz - h keep their input value, as the in-place pass leaves
-// them).  Each coarse value feeds the C fine rows z with z / C = zc.
+// them)
 template <int C>
 __global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0, const float *__restrict__ tc1,
                                                    float *__restrict__ u0, float *__restrict__ u1, int nt, int n,
                                                    int nz, int nzv, int nxv, int nb) {
-  constexpr int H = C / 2;
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t lines = (size_t)nb * n * nxv;
   if (e >= (size_t)nt * lines) return;
@@ -662,34 +568,7 @@ __global__ void __launch_bounds__(256) k_smooth_z(const float *__restrict__ tc0,
   {
     const float *in = (t == 0 ? tc0 : tc1) + by * nzv * nxv + xc;
     float *o = (t == 0 ? u0 : u1) + by * nz * nxv + xc;
-    // coarse row by coarse row, as in k_expand_y: the look-ahead input of
-    // fine row z is coarse row min(z + H, nz - 1) / C
-    LineSmoother<H> L;
-    float cv[WALK_PF];
-#pragma unroll
-    for (int q = 0; q < WALK_PF; ++q) cv[q] = __ldg(in + (size_t)min(q, nzv - 1) * nxv);
-#pragma unroll
-    for (int q = 0; q < H; ++q) L.in[q] = cv[0];
-    for (int zc0 = 0; zc0 < nzv; zc0 += WALK_PF) {
-      float nx[WALK_PF];
-#pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) nx[q] = __ldg(in + (size_t)min(zc0 + WALK_PF + q, nzv - 1) * nxv);
-#pragma unroll
-      for (int r = 0; r < WALK_PF; ++r) {
-        const int zc = zc0 + r;
-        if (zc < nzv) {
-          const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : nx[0];
-#pragma unroll
-          for (int q = 0; q < C; ++q) {
-            const int z = zc * C + q;
-            L.in[H] = ((q + H) / C == 0) ? ca : cb;
-            o[(size_t)z * nxv] = L.step(z, nz);
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) cv[q] = nx[q];
-    }
+    coarse_walk<C, false, true>(in, nxv, nzv, o, nxv);
   }
 }
 
@@ -774,34 +653,7 @@ __global__ void __launch_bounds__(32 * CX_TY) k_smooth_x_combine(CombineArgs a) 
     if (tid < a.nt * XZB && (tid % XZB) < rows) {
       const float *qrow = Q + (size_t)tid * lq;  // (term, row) = (tid / XZB, tid % XZB)
       float *frow = F + (size_t)tid * ld;
-      // coarse value by coarse value (the look-ahead input of fine x is
-      // coarse min(x + H, n - 1) / C), loaded WALK_PF ahead
-      LineSmoother<H> L;
-      float cv[WALK_PF];
-#pragma unroll
-      for (int q = 0; q < WALK_PF; ++q) cv[q] = qrow[min(q, tn - 1)];
-#pragma unroll
-      for (int q = 0; q < H; ++q) L.in[q] = cv[0];
-      for (int xc0 = 0; xc0 < tn; xc0 += WALK_PF) {
-        float nx[WALK_PF];
-#pragma unroll
-        for (int q = 0; q < WALK_PF; ++q) nx[q] = qrow[min(xc0 + WALK_PF + q, tn - 1)];
-#pragma unroll
-        for (int r = 0; r < WALK_PF; ++r) {
-          const int xc = xc0 + r;
-          if (xc < tn) {
-            const float ca = cv[r], cb = r + 1 < WALK_PF ? cv[r + 1] : nx[0];
-#pragma unroll
-            for (int q = 0; q < C; ++q) {
-              const int x = xc * C + q;
-              L.in[H] = ((q + H) / C == 0) ? ca : cb;
-              frow[x] = L.step(x, n);
-            }
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < WALK_PF; ++q) cv[q] = nx[q];
-      }
+      coarse_walk<C, false, false>(qrow, 1, tn, frow, 1);
     }
     __syncthreads();
     R = F;

@@ -2,11 +2,14 @@
 
 Each phase of the one-CTA-per-plane DRF kernels (drf_plane.cuh) and of the
 ESSE x and y-z kernels (esse_rows.cuh, esse_yz.cuh) is a function of the
-thread index.  The C++ programs under tests/emulation run every phase for
+thread index, and the ESSE expansion's line walk (esse_walk.cuh) a function
+of one line.  The C++ programs under tests/emulation run every phase for
 all threads of a CTA, once in increasing and once in decreasing thread order
 (a phase that read another thread's result of the same phase would differ),
 under AddressSanitizer (any index outside the shared-memory buffers or the
-global arrays aborts), and compare with direct transforms in double.
+global arrays aborts), and compare with direct transforms in double; the
+line walk at coarse resolution is compared bit for bit with the
+full-resolution expansion and in-place smoothing.
 """
 import os
 import shutil
@@ -35,7 +38,7 @@ def _build_and_run(name, tmp_path):
     return run.stdout
 
 
-@pytest.mark.parametrize("name", ["dplane_host_test", "esse_yz_host_test", "esse_rows_host_test"])
+@pytest.mark.parametrize("name", ["dplane_host_test", "esse_yz_host_test", "esse_rows_host_test", "esse_walk_host_test"])
 def test_kernel_phases_match_direct_transforms(name, tmp_path):
     out = _build_and_run(name, tmp_path)
     assert "worst" in out
