@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(ER_NT, 2) k_esse_row_fwd_reg(RowFwdArgs a, con
 
 // grid (row-pair blocks, view, term)
 template <int L>
-__global__ void __launch_bounds__(ER_NT, 2) k_esse_row_inv_reg(RowInvArgs a, const float2 *__restrict__ twg) {
+__global__ void __launch_bounds__(ER_NT, 3) k_esse_row_inv_reg(RowInvArgs a, const float2 *__restrict__ twg) {
   using D = ERow<L>;
   extern __shared__ __align__(16) float2 ers[];
   float2 *X = ers, *tw = X + D::X_ELEMS;
