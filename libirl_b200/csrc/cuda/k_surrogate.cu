@@ -757,6 +757,81 @@ __global__ void __launch_bounds__(128) k_conv_first(ConvGeom g, const bf16 *__re
   }
 }
 
+// The first layer for an even output width: two adjacent output positions
+// (ow, ow + 1) per thread, so that every shared-memory weight load feeds
+// both.  Each output accumulates its products in the order k_conv_first does
+// (taps, then channels), and a tap outside the input is skipped for that
+// output alone, so the results are the same bit for bit.
+__global__ void __launch_bounds__(128) k_conv_first2(ConvGeom g, const bf16 *__restrict__ x,
+                                                     const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                     bf16 *__restrict__ y) {
+  __shared__ __align__(16) float ws[FIRST_TAPS * FIRST_CI][FIRST_CO];
+  __shared__ float bs[FIRST_CO];
+  for (int e = threadIdx.x; e < FIRST_TAPS * FIRST_CI * FIRST_CO; e += blockDim.x) {
+    const int co = e / (FIRST_TAPS * FIRST_CI), k = e % (FIRST_TAPS * FIRST_CI);
+    ws[k][co] = __bfloat162float(w[e]);
+  }
+  if (threadIdx.x < FIRST_CO) bs[threadIdx.x] = bias[threadIdx.x];
+  __syncthreads();
+  const int wh = g.wout >> 1;
+  const long long M2 = (long long)g.b * g.dout * g.hout * wh;
+  const long long m2 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m2 >= M2) return;
+  long long r = m2;
+  const int ow = (int)(r % wh) * 2;
+  r /= wh;
+  const int oh = (int)(r % g.hout);
+  r /= g.hout;
+  const int od = (int)(r % g.dout);
+  const int b = (int)(r / g.dout);
+  float a0[FIRST_CO], a1[FIRST_CO];
+#pragma unroll
+  for (int co = 0; co < FIRST_CO; ++co) a0[co] = a1[co] = bs[co];
+  for (int tap = 0; tap < FIRST_TAPS; ++tap) {
+    const int td = tap / 9, th = (tap / 3) % 3, tw = tap % 3;
+    const int id = od * g.s + td - 1, ih = oh * g.s + th - 1, iw0 = ow * g.s + tw - 1, iw1 = iw0 + g.s;
+    const bool dh = id >= 0 && id < g.di && ih >= 0 && ih < g.hi;
+    const bool v0 = dh && iw0 >= 0 && iw0 < g.wi, v1 = dh && iw1 >= 0 && iw1 < g.wi;
+    if (!v0 && !v1) continue;
+    const bf16 *p0 = v0 ? x + in_off(g, b, id, ih, iw0, 0) : x;
+    const bf16 *p1 = v1 ? x + in_off(g, b, id, ih, iw1, 0) : x;
+#pragma unroll
+    for (int c = 0; c < FIRST_CI; ++c) {
+      const float x0 = v0 ? __bfloat162float(p0[c]) : 0.f, x1 = v1 ? __bfloat162float(p1[c]) : 0.f;
+      const float4 *wr = reinterpret_cast<const float4 *>(ws[tap * FIRST_CI + c]);
+#pragma unroll
+      for (int q = 0; q < FIRST_CO / 4; ++q) {
+        const float4 w4 = wr[q];
+        if (v0) {
+          a0[4 * q] = fmaf(w4.x, x0, a0[4 * q]);
+          a0[4 * q + 1] = fmaf(w4.y, x0, a0[4 * q + 1]);
+          a0[4 * q + 2] = fmaf(w4.z, x0, a0[4 * q + 2]);
+          a0[4 * q + 3] = fmaf(w4.w, x0, a0[4 * q + 3]);
+        }
+        if (v1) {
+          a1[4 * q] = fmaf(w4.x, x1, a1[4 * q]);
+          a1[4 * q + 1] = fmaf(w4.y, x1, a1[4 * q + 1]);
+          a1[4 * q + 2] = fmaf(w4.z, x1, a1[4 * q + 2]);
+          a1[4 * q + 3] = fmaf(w4.w, x1, a1[4 * q + 3]);
+        }
+      }
+    }
+  }
+  const long long m = (((long long)b * g.dout + od) * g.hout + oh) * g.wout + ow;
+  uint4 *o = reinterpret_cast<uint4 *>(y + m * FIRST_CO);
+#pragma unroll
+  for (int q = 0; q < FIRST_CO / 8; ++q) {
+    __align__(16) bf16 h0[8], h1[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      h0[j] = __float2bfloat16(fmaxf(a0[q * 8 + j], 0.f));
+      h1[j] = __float2bfloat16(fmaxf(a1[q * 8 + j], 0.f));
+    }
+    o[q] = *reinterpret_cast<const uint4 *>(h0);
+    o[FIRST_CO / 8 + q] = *reinterpret_cast<const uint4 *>(h1);
+  }
+}
+
 // Last layer (one output channel, 2D, input 32 channels) as a direct
 // convolution: one thread per output pixel, FP32 output
 constexpr int LAST_CI = 32;
@@ -1238,8 +1313,12 @@ static int sur_forward(irlcu_sur &s, int B) {
     }
     const long long M = (long long)B * l.g.dout * l.g.hout * l.g.wout;
     if (i == 0 && l.g.ci == FIRST_CI && l.g.co == FIRST_CO && l.g.kd == 3) {
-      k_conv_first<<<(unsigned)((M + 127) / 128), 128, 0, s.st>>>(l.g, s.act[0], s.wb + l.woff, s.w + l.boff,
-                                                                 s.act[1]);
+      if ((l.g.wout & 1) == 0)
+        k_conv_first2<<<(unsigned)((M / 2 + 127) / 128), 128, 0, s.st>>>(l.g, s.act[0], s.wb + l.woff,
+                                                                        s.w + l.boff, s.act[1]);
+      else
+        k_conv_first<<<(unsigned)((M + 127) / 128), 128, 0, s.st>>>(l.g, s.act[0], s.wb + l.woff, s.w + l.boff,
+                                                                   s.act[1]);
       CU_LAUNCHED();
       continue;
     }
