@@ -56,3 +56,18 @@ def test_no_cpu_fallback_without_a_device(product):
                          api.fptr(atn), api.fptr(meas), api.fptr(rec), None, None)
     assert rc != 0
     assert b"CUDA" in product.pchIrlErrorString()
+
+
+def test_device_copies_and_memsets_are_stream_ordered():
+    """Every copy and memset of the CUDA sources is issued on a stream
+    (the *Async forms). A context's kernels run on a non-blocking stream,
+    which legacy-stream copies and memsets do not order against. A batch of
+    reconstructions, set up while the previous one still ran, raced on
+    exactly that."""
+    legacy = re.compile(r"\bcudaMem(?:cpy|set|cpy2D|cpy3D|cpyToSymbol|cpyFromSymbol)\s*\(")
+    bad = []
+    for f in sorted(glob.glob(os.path.join(ROOT, "libirl_b200", "csrc", "**", "*.cu*"), recursive=True)):
+        for i, line in enumerate(open(f), 1):
+            if legacy.search(line):
+                bad.append(f"{os.path.relpath(f, ROOT)}:{i}: {line.strip()}")
+    assert not bad, "\n".join(bad)
