@@ -108,6 +108,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ------------------------------------------------------------ ranks
+
+def max_over_ranks(value, dist, failed=False):
+    """(the maximum of value over all ranks, whether any rank failed).
+    Every rank calls this at the same point, failed or not, so that the
+    ranks' collectives match; without a process group it returns its
+    arguments."""
+    if not dist:
+        return value, failed
+    import torch
+    dist.barrier()
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value), 1.0 if failed else 0.0], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0].item()), bool(t[1].item() > 0.0)
+
+
 # --------------------------------------------------------------- workload
 
 def make_workload(lib, tmpdir, nviews=120, subsets=8):
@@ -176,15 +193,12 @@ def run_b200(args):
         rc = lib.IrlOsemIterate(K)
         ev1.record(stream)
         torch.cuda.synchronize()
+    launches = lib.irlcu_launch_count() - l0
+    ms_total, failed = max_over_ranks(ev0.elapsed_time(ev1), dist, failed=bool(rc))
     if rc:
         raise RuntimeError(lib.pchIrlErrorString().decode())
-    launches = lib.irlcu_launch_count() - l0
-    ms_total = ev0.elapsed_time(ev1)
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    if failed:
+        raise RuntimeError("another rank's timed iterations failed")
     ms_step = ms_total / K
 
     # --- stage profile over one more iteration (separate from the timing)
