@@ -3,8 +3,10 @@
 //
 // Per view of a batch (all in the view's rotated frame, layout [y][z][x]):
 //   1. collapse the rotated activity by c (sum pooling, CollapseByFac) and
-//      zero-pad it into the Ky x Kz x Kx FFT grid -- fused into the first
-//      FFT pass, which only visits the rows that hold data;
+//      zero-pad it into the Ky x Kz x Kx FFT grid: a streaming pass
+//      (k_esse_collapse) ahead of the register x transform, or fused into
+//      the first FFT pass of the pass form; only the rows that hold data
+//      are transformed;
 //   2. forward 3D DFT (x, z, y passes; z and y skip the known-zero lines);
 //   3. for the zeroth and first Taylor terms: multiply by the kernel spectra
 //      K^ and (K (mu - mu_avg))^, inverse 3D DFT (y, z, x passes, each
