@@ -29,6 +29,24 @@ def test_rotations_match_golden_bit_for_bit(orc):
         assert np.array_equal(_rot(orc, "or_rot3dpar", a, vol), d["rot3dpar"][i])
 
 
+def test_shear_rotation_reads_nothing_past_the_volume(orc):
+    """For odd n the middle row's last second tap lies one past the row, with
+    weight 0 (for the last row of the last slice: past the volume). The
+    oracle reads 0 there, so NaN in the memory after the volume (and before
+    it, for the flipped taps) must not reach the output."""
+    rng = np.random.default_rng(9)
+    for n, nz in [(33, 2), (17, 3), (65, 1)]:
+        pad = n * nz * n
+        buf = np.full(3 * pad, np.nan, np.float32)
+        vol = buf[pad:2 * pad].reshape(n, nz, n)  # NaN on both sides of the volume
+        vol[...] = rng.random((n, nz, n), dtype=np.float32)
+        angles = np.concatenate([rng.uniform(-7, 7, 24), np.pi / 2 * np.arange(-4, 5)]).astype(np.float32)
+        for a in angles:
+            out = np.zeros_like(vol)
+            orc.orc().or_shears_rotate(float(a), api.fptr(vol), api.fptr(out), n, nz)
+            assert np.isfinite(out).all(), (n, nz, float(a))
+
+
 def test_conv2d_ypad_matches_golden_bit_for_bit(orc):
     d = np.load(os.path.join(GOLDEN, "conv2d_ypad.npz"))
     plane, psf = d["plane"], d["psf"]
