@@ -528,34 +528,69 @@ def cpu_baseline(case, files, views=2):
             "threads_available": os.cpu_count()}
 
 
+_REF_ONE = None  # per reference worker process: view -> seconds
+
+
+def _ref_worker_init(seed, files):
+    global _REF_ONE
+    import libirl_b200.workloads as W
+    _REF_ONE = _ref_view_timer(W.full128(seed=seed), files)
+
+
+def _ref_worker_view(view):
+    one, _ = _REF_ONE
+    return one(view)
+
+
 def run_reference(args):
-    """Reference arm: the reference's own CPU implementation, one view per
-    step, reported as ms per OSEM iteration (x120 views)."""
+    """Reference arm: the reference's own CPU implementation on all the
+    host's cores. libirl keeps global state and has no threads, so every
+    core gets its own process (spawned). A step runs one view of an OSEM
+    iteration (projection with ESSE + DRF + attenuation, backprojection) in
+    every process at once, and its wall time is scaled to ms per iteration
+    (x views / processes). Under torchrun rank 0 alone runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import multiprocessing as mp
     import libirl_b200.workloads as W
-    case = W.full128(seed=2000)
+    seed = 2000
+    case = W.full128(seed=seed)
     tmp = tempfile.mkdtemp(prefix="irlbench_ref_")
     files = case.write_tables(tmp)
     try:
-        one, kind = _ref_view_timer(case, files)
+        procs = len(os.sched_getaffinity(0))
+    except AttributeError:
+        procs = os.cpu_count() or 1
+    procs = max(1, min(procs, case.nviews))
+    try:
+        _, kind = _ref_view_timer(case, files)  # fails here, not in the pool, when the path is missing
+        pool = mp.get_context("spawn").Pool(procs, initializer=_ref_worker_init, initargs=(seed, files))
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {e}"[:300]}))
         return
-    for i in range(args.warmup):
-        one(i % case.nviews)
-    secs = [one((7 * (i + 1)) % case.nviews) for i in range(args.steps)]
-    per_view = statistics.median(secs)
-    val = round(1000.0 * per_view * case.nviews, 1)
+    walls = []
+    try:
+        for i in range(args.warmup + args.steps):
+            views = [(7 * (i * procs + j + 1)) % case.nviews for j in range(procs)]
+            t0 = time.perf_counter()
+            pool.map(_ref_worker_view, views, chunksize=1)
+            if i >= args.warmup:
+                walls.append(time.perf_counter() - t0)
+    finally:
+        pool.close()
+        pool.join()
+    wall = statistics.median(walls)
+    val = round(1000.0 * wall * case.nviews / procs, 1)
     print(json.dumps({
         "metric": METRIC, "value": val, "unit": "ms", "n_gpus": _WORLD, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson data)",
-        "config": {"workload": WORKLOAD, "parallelism": "single"}, "impl": "reference",
-        "cpu_baseline": {"value": val, "unit": "ms", "cores": 1, "kind": kind,
-                         "sample": f"each step one of {case.nviews} views of an OSEM iteration (projection with ESSE + "
-                                   f"DRF + attenuation, backprojection), median {per_view:.2f} s/view, x{case.nviews}"},
+        "config": {"workload": WORKLOAD, "parallelism": f"{procs} host processes"}, "impl": "reference",
+        "cpu_baseline": {"value": val, "unit": "ms", "cores": procs, "kind": kind,
+                         "sample": f"each step {procs} of {case.nviews} views of an OSEM iteration (projection with "
+                                   f"ESSE + DRF + attenuation, backprojection) at once, one per process; median step "
+                                   f"{wall:.2f} s, x{case.nviews}/{procs}"},
         "e2e": {"value": val, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
