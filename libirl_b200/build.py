@@ -29,7 +29,7 @@ CC = os.environ.get("CC", "gcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-ffp-contract=off", f"-I{INCLUDE}"]
-CC_FLAGS = ["-O2", "-std=gnu99", "-fPIC", "-ffp-contract=off", "-Wall",
+CC_FLAGS = ["-O2", "-std=gnu99", "-fPIC", "-pthread", "-ffp-contract=off", "-Wall",
             "-Wno-unused-function", f"-I{INCLUDE}"]
 
 
@@ -74,7 +74,7 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
         with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
             list(ex.map(_compile, todo))
     if todo or not os.path.exists(SO) or any(os.path.getmtime(o) > os.path.getmtime(SO) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", SO] + objs + ["-lm"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", SO] + objs + ["-lm", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

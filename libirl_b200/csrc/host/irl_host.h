@@ -90,6 +90,12 @@ int irl_compute_subsets(int nangles, int per_subset, int **angles);
 /* external [z][y][x] <-> internal [y][z][x] */
 void irl_reorder(int d0, int d1, int d2, const float *in, float *out);
 
+/* fn(lo, hi, ctx) over [0, n) in chunks of at least grain elements, on up
+   to 16 host threads (irl_par.c); for element-wise work only */
+typedef void (*irl_range_fn)(size_t lo, size_t hi, void *ctx);
+void irl_parallel_for(size_t n, size_t grain, irl_range_fn fn, void *ctx);
+#define IRL_PAR_GRAIN ((size_t)1 << 18)
+
 /* uploads the DRF tables of every view to the device (slot 0 projector,
    slot 1 backprojector when any detector has a separate GRF table) */
 void irl_upload_drf(const irl_parms *p, irl_view *views, int ndet, irl_detector *dets);

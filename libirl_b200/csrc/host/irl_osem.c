@@ -187,19 +187,38 @@ static void open_logs(const char *logname, const char *msgname, int level, FILE 
 	}
 }
 
-static void zero_neg(float *p, size_t n)
+typedef struct {
+	float *p;
+	float s;
+} fspan;
+
+static void zero_neg_range(size_t lo, size_t hi, void *c)
 {
+	float *p = ((fspan *)c)->p;
 	size_t i;
-	for (i = 0; i < n; ++i)
+	for (i = lo; i < hi; ++i)
 		if (p[i] < 0.0f)
 			p[i] = 0.0f;
 }
 
+static void scale_range(size_t lo, size_t hi, void *c)
+{
+	float *p = ((fspan *)c)->p, s = ((fspan *)c)->s;
+	size_t i;
+	for (i = lo; i < hi; ++i)
+		p[i] *= s;
+}
+
+static void zero_neg(float *p, size_t n)
+{
+	fspan c = {p, 0.0f};
+	irl_parallel_for(n, IRL_PAR_GRAIN, zero_neg_range, &c);
+}
+
 static void scale_f(float *p, size_t n, float s)
 {
-	size_t i;
-	for (i = 0; i < n; ++i)
-		p[i] *= s;
+	fspan c = {p, s};
+	irl_parallel_for(n, IRL_PAR_GRAIN, scale_range, &c);
 }
 
 /* shared device set-up of IrlOsem and IrlGenprj */

@@ -722,6 +722,30 @@ static void zero_behind(int nd, float fSin, float fCos, float fRadius, float *pi
 	}
 }
 
+typedef struct {
+	float *init;
+	float v;
+	const float *atn;
+	float thresh;
+} fill_ctx;
+
+static void fill_range(size_t lo, size_t hi, void *c)
+{
+	const fill_ctx *f = (const fill_ctx *)c;
+	size_t i;
+	for (i = lo; i < hi; ++i)
+		f->init[i] = f->v;
+}
+
+static void mask_range(size_t lo, size_t hi, void *c)
+{
+	const fill_ctx *f = (const fill_ctx *)c;
+	size_t i;
+	for (i = lo; i < hi; ++i)
+		if (f->atn[i] < f->thresh)
+			f->init[i] = 0.0;
+}
+
 /* pfComputeInitialEstimate, initial_est.c:29-158 (internal layout) */
 float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const irl_view *views, const float *prj,
 	const float *atn, float *init)
@@ -743,8 +767,8 @@ float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const
 			use_map = fMapThresh > 0.0;
 	}
 	if (!contour) {
-		for (i = 0; i < (size_t)n * nz * n; ++i)
-			init[i] = fAvg;
+		fill_ctx fc = {init, fAvg, NULL, 0.0f};
+		irl_parallel_for((size_t)n * nz * n, IRL_PAR_GRAIN, fill_range, &fc);
 	} else {
 		float *img = (float *)irl_malloc(sizeof(float) * n * n, "contour image");
 		for (i = 0; i < (size_t)n * n; ++i)
@@ -759,10 +783,10 @@ float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const
 					init[(size_t)r * nz * n + (size_t)s * n + c2] = img[c2 + r * n];
 		free(img);
 	}
-	if (use_map)
-		for (i = 0; i < (size_t)n * nz * n; ++i)
-			if (atn[i] < fMapThresh)
-				init[i] = 0.0;
+	if (use_map) {
+		fill_ctx mc = {init, 0.0f, atn, fMapThresh};
+		irl_parallel_for((size_t)n * nz * n, IRL_PAR_GRAIN, mask_range, &mc);
+	}
 	{
 		float fRadius = (float)n * 0.5, fX, fY, fCent = fRadius;
 		for (r = 0; r < n; ++r) {
@@ -807,11 +831,26 @@ int irl_compute_subsets(int na, int per, int **angles)
 	return ns;
 }
 
+typedef struct {
+	int d0, d1, d2;
+	const float *in;
+	float *out;
+} reorder_ctx;
+
+static void reorder_range(size_t lo, size_t hi, void *c)
+{
+	const reorder_ctx *r = (const reorder_ctx *)c;
+	size_t j;
+	int i, k;
+	for (j = lo; j < hi; ++j)
+		for (k = 0; k < r->d0; ++k)
+			for (i = 0; i < r->d2; ++i)
+				r->out[(j * r->d0 + k) * r->d2 + i] = r->in[((size_t)k * r->d1 + j) * r->d2 + i];
+}
+
 void irl_reorder(int d0, int d1, int d2, const float *in, float *out)
 {
-	int i, j, k;
-	for (j = 0; j < d1; ++j)
-		for (k = 0; k < d0; ++k)
-			for (i = 0; i < d2; ++i)
-				out[((size_t)j * d0 + k) * d2 + i] = in[((size_t)k * d1 + j) * d2 + i];
+	reorder_ctx c = {d0, d1, d2, in, out};
+	const size_t row = (size_t)d0 * d2;
+	irl_parallel_for((size_t)d1, row ? (IRL_PAR_GRAIN + row - 1) / row : 1, reorder_range, &c);
 }
