@@ -171,15 +171,18 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
    intermediate side for this angle (n = nz = 128: at most 4.2 M floats).
    Larger sizes return IRLCU_EARG before any device access.
 
-   src and dst are device pointers of n*nz*n floats ([y][z][x]), distinct.
-   Requires irlcu_init (the call runs on the library stream and synchronises
-   it before returning).  The results are bit-identical to
+   src and dst are device pointers of n*nz*n floats ([y][z][x]), distinct,
+   on the device that was current at irlcu_init; that device must be the
+   current one (otherwise IRLCU_EARG).  The results are bit-identical to
    irlcu_rotate_volume with a fast-rotation context.
 
-   Set-up: the first call on a device looks up the array's address with
-   cudaGetSymbolAddress (which may load the module); make that first call
-   before any stream capture.  There is one scratch array per device, so
-   overlapping calls (from several host threads) race. */
+   The call is synchronous: it copies its tables from a static host buffer
+   to the array on the library stream, launches the two shear kernels and
+   synchronises the stream before returning.  So it must not be made while
+   the library stream is being captured into a CUDA graph.  The first call
+   on a device looks up the array's address with cudaGetSymbolAddress (which
+   may load the module).  There is one scratch array per device and one host
+   staging buffer, so overlapping calls (from several host threads) race. */
 #define IRLCU_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define IRLCU_NOALLOC_TAB_BYTES (64u << 10)
 #define IRLCU_NOALLOC_X_FLOATS ((IRLCU_NOALLOC_SCRATCH_BYTES - IRLCU_NOALLOC_TAB_BYTES) / 4u)

@@ -256,6 +256,7 @@ int irlcu_init(const irlcu_geom *g) {
   c->pln = (size_t)c->nz * c->n;
   c->vox = c->pln * c->n;
   g_ctx = c;
+  CU_TRY(cudaGetDevice(&c->dev));
   CU_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   for (auto &e : c->ev) CU_TRY(cudaEventCreate(&e));
   const int n = c->n, R = 2 * c->nv;
@@ -1030,7 +1031,14 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
 int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
-  TRY(launch_rotate_noalloc(c.st, angle, src, dst, n, nz));
+  int cur = -1;
+  CU_TRY(cudaGetDevice(&cur));
+  if (cur != c.dev)
+    return set_error(IRLCU_EARG,
+                     "irlcu_rotate_volume_noalloc: device %d is current, but the library was initialised on device "
+                     "%d; make device %d current first",
+                     cur, c.dev, c.dev);
+  TRY(launch_rotate_noalloc(c.st, c.dev, angle, src, dst, n, nz));
   CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
 }

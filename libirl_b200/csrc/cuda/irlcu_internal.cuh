@@ -93,6 +93,7 @@ struct Ctx {
   irlcu_geom g{};
   int n = 0, nz = 0, nv = 0;
   size_t vox = 0, pln = 0;
+  int dev = -1;               // the device current at irlcu_init; c.st belongs to it
   cudaStream_t st = nullptr;
   cudaEvent_t ev[16];
   int nsub = 0;
@@ -195,7 +196,7 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
 
 // three-shear rotation of one device volume with every buffer in a static
 // device array (irlcu_rotate_volume_noalloc); enqueued on `st`
-int launch_rotate_noalloc(cudaStream_t st, float angle, const float *src, float *dst, int n, int nz);
+int launch_rotate_noalloc(cudaStream_t st, int dev, float angle, const float *src, float *dst, int n, int nz);
 
 // cumulative attenuation tables of nv views from rotated maps in tMu-like
 // buffer `rmu` (stride vox): writes E (and S if not null)

@@ -715,7 +715,7 @@ uint32_t g_na_host[IRLCU_NOALLOC_TAB_BYTES / 4];
 
 }  // namespace
 
-int launch_rotate_noalloc(cudaStream_t st, float angle, const float *src, float *dst, int n, int nz) {
+int launch_rotate_noalloc(cudaStream_t st, int dev, float angle, const float *src, float *dst, int n, int nz) {
   if (n < 1 || nz < 1 || n > IRLCU_NOALLOC_MAX_N)
     return set_error(IRLCU_EARG, "irlcu_rotate_volume_noalloc: n = %d, nz = %d outside 1 <= n <= %d, nz >= 1", n,
                      nz, IRLCU_NOALLOC_MAX_N);
@@ -742,8 +742,8 @@ int launch_rotate_noalloc(cudaStream_t st, float angle, const float *src, float 
   irl_shear_support(n, wi + L.st, wi + L.en);
   wi[L.views] = 0;
 
-  int dev = -1;
-  CU_TRY(cudaGetDevice(&dev));
+  // dev is the library's device and the current one (checked by the caller),
+  // so the symbol lookup below resolves on the device that runs `st`
   if (dev < 0 || dev >= NA_MAXDEV)
     return set_error(IRLCU_EARG, "irlcu_rotate_volume_noalloc: device %d beyond %d", dev, NA_MAXDEV);
   if (g_noalloc_addr[dev] == nullptr) {

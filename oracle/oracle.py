@@ -156,6 +156,18 @@ class OrProblem(C.Structure):
     ]
 
 
+def _threads() -> int:
+    """Host threads for the restatement's view loops: IRL_ORACLE_THREADS,
+    else every core this process may run on."""
+    env = os.environ.get("IRL_ORACLE_THREADS")
+    if env:
+        return max(1, int(env))
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def orc() -> C.CDLL:
     """The restatement library (oracle/src/irl_oracle.c)."""
     global _orc
@@ -175,8 +187,10 @@ def orc() -> C.CDLL:
         lib.or_osem.argtypes = [P, _I, _I, _I, _I, _I, _F, _F, _F, _F]
         lib.or_osem.restype = _I
         lib.or_initial_estimate.argtypes = [_I, _I, _I, _F, _F]
+        lib.or_set_threads.argtypes = [_I]
+        lib.or_set_threads(_threads())
         for f in ("or_shears_rotate", "or_rot3dpar", "or_conv2d_ypad", "or_esse_prepare", "or_esse_source",
-                  "or_project", "or_backproject", "or_genprj", "or_initial_estimate"):
+                  "or_project", "or_backproject", "or_genprj", "or_initial_estimate", "or_set_threads"):
             getattr(lib, f).restype = None
         _orc = lib
     return _orc

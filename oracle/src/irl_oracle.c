@@ -9,6 +9,7 @@
  */
 #include <complex.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -20,6 +21,68 @@
 #endif
 #define MAXF(a, b) ((a) > (b) ? (a) : (b))
 #define MINF(a, b) ((a) < (b) ? (a) : (b))
+
+/* ------------------------------------------------------------- threads */
+
+/* Views of a subset (and of IrlGenprj) are independent until their
+   backprojections are summed, so the restatement runs them on a pool of
+   host threads; everything order-dependent (the clamped accumulation of
+   prjbck.c:418-426, the EM update) stays serial, so the results do not
+   depend on the thread count. */
+static int g_threads = 1;
+
+void or_set_threads(int n)
+{
+	g_threads = n < 1 ? 1 : n;
+}
+
+typedef struct {
+	void (*fn)(void *ctx, int i);
+	void *ctx;
+	int count, next;
+	pthread_mutex_t mu;
+} par_job;
+
+static void *par_worker(void *arg)
+{
+	par_job *j = (par_job *)arg;
+	for (;;) {
+		int i;
+		pthread_mutex_lock(&j->mu);
+		i = j->next++;
+		pthread_mutex_unlock(&j->mu);
+		if (i >= j->count)
+			break;
+		j->fn(j->ctx, i);
+	}
+	return NULL;
+}
+
+static void par_for(int count, void (*fn)(void *ctx, int i), void *ctx)
+{
+	int nt = MINF(g_threads, count), t, started = 0;
+	pthread_t th[256];
+	par_job j;
+	if (nt > 256)
+		nt = 256;
+	if (nt <= 1) {
+		for (t = 0; t < count; ++t)
+			fn(ctx, t);
+		return;
+	}
+	j.fn = fn;
+	j.ctx = ctx;
+	j.count = count;
+	j.next = 0;
+	pthread_mutex_init(&j.mu, NULL);
+	for (t = 0; t < nt - 1; ++t)
+		if (pthread_create(&th[started], NULL, par_worker, &j) == 0)
+			++started;
+	par_worker(&j);
+	for (t = 0; t < started; ++t)
+		pthread_join(th[t], NULL);
+	pthread_mutex_destroy(&j.mu);
+}
 
 /* ------------------------------------------------------------ rotation */
 
@@ -317,24 +380,67 @@ void or_esse_prepare(const float *krnl, const float *kmu, int noffs, int nd, int
 
 /* exact circular convolution of a real [ky][kz][kx] grid with a real
    kernel grid (the realft3d / multrealft3d / realinvft3d chain) */
+/* The kernel grids are the same for every view, so their spectra are
+   computed once and kept (keyed by content, not only by address, since a
+   later problem may reuse a freed address); the spectrum is the same
+   deterministic transform either way. */
+#define SPEC_CACHE 4
+static struct {
+	float *key;
+	int kx, ky, kz;
+	double complex *spec;
+} g_spec[SPEC_CACHE];
+static int g_spec_next;
+static pthread_mutex_t g_spec_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static const double complex *kernel_spectrum(const float *k, int kx, int ky, int kz)
+{
+	size_t cnt = (size_t)kx * ky * kz, i;
+	double complex *K;
+	int e;
+	pthread_mutex_lock(&g_spec_mu);
+	for (e = 0; e < SPEC_CACHE; ++e)
+		if (g_spec[e].key != NULL && g_spec[e].kx == kx && g_spec[e].ky == ky && g_spec[e].kz == kz &&
+			memcmp(g_spec[e].key, k, sizeof(float) * cnt) == 0) {
+			K = g_spec[e].spec;
+			pthread_mutex_unlock(&g_spec_mu);
+			return K;
+		}
+	K = (double complex *)malloc(sizeof(double complex) * cnt);
+	for (i = 0; i < cnt; ++i)
+		K[i] = k[i];
+	dfft_c3d(K, kx, kz, ky, -1);
+	e = g_spec_next;
+	g_spec_next = (g_spec_next + 1) % SPEC_CACHE;
+	/* an evicted entry may still be in use by another thread's convolution
+	   only if more than SPEC_CACHE kernels are live at once; the oracle
+	   never has more than two per problem and one problem at a time */
+	free(g_spec[e].key);
+	free(g_spec[e].spec);
+	g_spec[e].key = (float *)malloc(sizeof(float) * cnt);
+	memcpy(g_spec[e].key, k, sizeof(float) * cnt);
+	g_spec[e].kx = kx;
+	g_spec[e].ky = ky;
+	g_spec[e].kz = kz;
+	g_spec[e].spec = K;
+	pthread_mutex_unlock(&g_spec_mu);
+	return K;
+}
+
 static void circ_conv3(const float *a, const float *k, float *out, int kx, int ky, int kz)
 {
 	size_t cnt = (size_t)kx * ky * kz, i;
 	double complex *A = (double complex *)malloc(sizeof(double complex) * cnt);
-	double complex *K = (double complex *)malloc(sizeof(double complex) * cnt);
-	for (i = 0; i < cnt; ++i) {
+	const double complex *K = kernel_spectrum(k, kx, ky, kz);
+	for (i = 0; i < cnt; ++i)
 		A[i] = a[i];
-		K[i] = k[i];
-	}
 	dfft_c3d(A, kx, kz, ky, -1);
-	dfft_c3d(K, kx, kz, ky, -1);
 	for (i = 0; i < cnt; ++i)
 		A[i] *= K[i];
 	dfft_c3d(A, kx, kz, ky, +1);
 	for (i = 0; i < cnt; ++i)
 		out[i] = (float)(creal(A[i]) / (double)cnt);
 	free(A);
-	free(K);
 }
 
 /* ExpandByFac (krnlprj3d.c:595-673): nearest expansion divided by c^3 and
@@ -521,12 +627,14 @@ void or_project(const or_problem *P, int model, int view, const float *est, cons
 	free(conv);
 }
 
-/* BackProject (prjbck.c:254-427), fPrimaryFac = fAtnFac = 1 */
-void or_backproject(const or_problem *P, int model, int view, const float *atn, const float *ratio, float *image)
+/* BackProject (prjbck.c:254-427), fPrimaryFac = fAtnFac = 1, up to the
+   unrotated volume un (the caller adds it to the image and clamps) */
+static void backproject_view(const or_problem *P, int model, int view, const float *atn, const float *ratio,
+	float *un)
 {
 	int n = P->n, nz = P->nz, r, atnm = model & 1, drfm = model & 2;
 	size_t pl = (size_t)nz * n, vox = pl * n, i;
-	float *ratn = NULL, *rot = (float *)malloc(sizeof(float) * vox), *un = (float *)malloc(sizeof(float) * vox);
+	float *ratn = NULL, *rot = (float *)malloc(sizeof(float) * vox);
 	float *sumatn = (float *)calloc(pl, sizeof(float)), *plane = (float *)malloc(sizeof(float) * pl);
 	float *conv = (float *)malloc(sizeof(float) * pl);
 	const int bck = P->bck_psf != NULL;
@@ -560,38 +668,64 @@ void or_backproject(const or_problem *P, int model, int view, const float *atn, 
 				sumatn[i] += (0.5 * ratn[(size_t)r * pl + i]);
 	}
 	rotate(P, -0.5 * M_PI - P->angle[view], rot, un);
-	for (i = 0; i < vox; i++)
-		image[i] += un[i];
-	for (i = 0; i < vox; i++)
-		if (image[i] < 1.0e-5)
-			image[i] = 0.0;
 	free(ratn);
 	free(rot);
-	free(un);
 	free(sumatn);
 	free(plane);
 	free(conv);
 }
 
-/* IrlGenprj view loop (irlgenprj.c:225-264) */
+/* image += un, then the clamp of prjbck.c:418-426 */
+static void add_clamped(float *image, const float *un, size_t vox)
+{
+	size_t i;
+	for (i = 0; i < vox; i++)
+		image[i] += un[i];
+	for (i = 0; i < vox; i++)
+		if (image[i] < 1.0e-5)
+			image[i] = 0.0;
+}
+
+void or_backproject(const or_problem *P, int model, int view, const float *atn, const float *ratio, float *image)
+{
+	size_t vox = (size_t)P->nz * P->n * P->n;
+	float *un = (float *)malloc(sizeof(float) * vox);
+	backproject_view(P, model, view, atn, ratio, un);
+	add_clamped(image, un, vox);
+	free(un);
+}
+
+/* IrlGenprj view loop (irlgenprj.c:225-264), the views on the thread pool */
+typedef struct {
+	const or_problem *P;
+	int model;
+	const float *act, *atn, *scatest;
+	float primary, *prj;
+} genprj_job;
+
+static void genprj_view(void *ctx, int a)
+{
+	const genprj_job *g = (const genprj_job *)ctx;
+	size_t pl = (size_t)g->P->nz * g->P->n, i;
+	float *calc = g->prj + pl * a;
+	or_project(g->P, g->model, a, g->act, g->atn, g->primary, calc);
+	if (g->scatest != NULL)
+		for (i = 0; i < pl; ++i)
+			calc[i] += g->scatest[pl * a + i];
+	for (i = 0; i < pl; ++i)
+		calc[i] = calc[i] * g->P->view_time[a] * g->P->sens[a];
+}
+
 void or_genprj(const or_problem *P, int model, const float *act, const float *atn, const float *scatest,
 	float primary, float *prj)
 {
 	size_t pl = (size_t)P->nz * P->n, i;
-	int a;
-	float *calc = (float *)malloc(sizeof(float) * pl), s;
-	for (a = 0; a < P->nviews; ++a) {
-		or_project(P, model, a, act, atn, primary, calc);
-		if (scatest != NULL)
-			for (i = 0; i < pl; ++i)
-				calc[i] += scatest[pl * a + i];
-		for (i = 0; i < pl; ++i)
-			prj[pl * a + i] = calc[i] * P->view_time[a] * P->sens[a];
-	}
+	genprj_job g = {P, model, act, atn, scatest, primary, prj};
+	float s;
+	par_for(P->nviews, genprj_view, &g);
 	s = 1.0 / (float)P->nviews;
 	for (i = 0; i < pl * P->nviews; ++i)
 		prj[i] *= s;
-	free(calc);
 }
 
 /* measured-bin mask helpers (osemrecon.c:92-184) with PixelWidth = BinWidth */
@@ -629,38 +763,110 @@ static void zero_nonmeasured(const or_problem *P, int v, const float *meas0, flo
 	}
 }
 
-/* vOsemRecon (osemrecon.c:557-897) without hooks, norm images in memory */
+/* one view of a subset: its backprojection un (not yet accumulated) */
+typedef struct {
+	const or_problem *P;
+	int prj_model, bck_model, model, this_s, next_s, srf, s, ns, per;
+	const float *meas, *atn, *scatest, *est;
+	float *scat, *calc, *c2, *un;   /* calc, c2: per member planes; un: per member volumes */
+	int norm_pass;
+} subset_job;
+
+static int subset_view(int s, int m, int ns)
+{
+	return s / 2 + (s % 2) * ns / 2 + m * ns;
+}
+
+static void subset_member(void *ctx, int m)
+{
+	const subset_job *j = (const subset_job *)ctx;
+	const or_problem *P = j->P;
+	size_t pl = (size_t)P->nz * P->n, vox = pl * P->n, i;
+	int a = subset_view(j->s, m, j->ns);
+	float *calc = j->calc + pl * m, *c2 = j->c2 + pl * m, *un = j->un + vox * m;
+	if (j->norm_pass) {
+		set_measured_to_one(P, a, j->meas + pl * a, calc);
+		for (i = 0; i < pl; ++i)
+			calc[i] *= P->view_time[a];
+		backproject_view(P, j->bck_model, a, j->atn, calc, un);
+		return;
+	}
+	or_project(P, j->model, a, j->est, j->atn, 1.0, calc);
+	for (i = 0; i < pl; ++i)
+		calc[i] *= P->view_time[a] * P->sens[a];
+	if (j->srf) {
+		if (!j->this_s) {
+			for (i = 0; i < pl; ++i)
+				calc[i] += j->scat[pl * a + i];
+		} else if (!j->next_s) {
+			or_project(P, j->prj_model & ~4, a, j->est, j->atn, 1.0, c2);
+			for (i = 0; i < pl; ++i)
+				c2[i] *= P->view_time[a];
+			for (i = 0; i < pl; ++i)
+				j->scat[pl * a + i] = calc[i] - c2[i];
+		}
+	}
+	if (j->scatest != NULL)
+		for (i = 0; i < pl; ++i)
+			calc[i] += j->scatest[pl * a + i];
+	zero_nonmeasured(P, a, j->meas, calc);
+	for (i = 0; i < pl; ++i)
+		calc[i] = calc[i] > 1e-20 ? j->meas[pl * a + i] / calc[i] : 0.0;
+	for (i = 0; i < pl; ++i)
+		calc[i] *= P->view_time[a];
+	backproject_view(P, j->bck_model, a, j->atn, calc, un);
+}
+
+/* vOsemRecon (osemrecon.c:557-897) without hooks, norm images in memory.
+   The members of a subset run on the thread pool; their backprojections
+   are then added to the update image in member order with the clamp of
+   prjbck.c:418-426, exactly as the serial loop does. */
 int or_osem(const or_problem *P, int prj_model, int bck_model, int srf_iters, int iterations, int per,
 	const float *meas, const float *atn, const float *scatest, float *est)
 {
 	int n = P->n, nz = P->nz, na = P->nviews, ns, s, m, it, srf = prj_model & 4, this_s = 0, next_s = 0;
 	size_t pl = (size_t)nz * n, vox = pl * n, i;
-	float *norm, *tmp = (float *)malloc(sizeof(float) * vox), *calc = (float *)malloc(sizeof(float) * pl);
-	float *scat = NULL, *c2 = (float *)malloc(sizeof(float) * pl);
+	float *norm, *tmp, *scat = NULL;
+	subset_job j;
 	if (per <= 0 || na % per)
 		return 1;
 	ns = na / per;
 	if (ns != 1 && ns % 2)
 		return 2;
 	norm = (float *)calloc(vox * ns, sizeof(float));
+	tmp = (float *)malloc(sizeof(float) * vox);
+	memset(&j, 0, sizeof(j));
+	j.P = P;
+	j.prj_model = prj_model;
+	j.bck_model = bck_model;
+	j.srf = srf;
+	j.ns = ns;
+	j.per = per;
+	j.meas = meas;
+	j.atn = atn;
+	j.scatest = scatest;
+	j.est = est;
+	j.calc = (float *)malloc(sizeof(float) * pl * per);
+	j.c2 = (float *)malloc(sizeof(float) * pl * per);
+	j.un = (float *)malloc(sizeof(float) * vox * per);
 	/* libirl allocates the stored scatter projections only when
 	   iNumSrfIterations > 0 (osemrecon.c:610-615) but adds them whenever
 	   scatter is not modelled in an iteration (osemrecon.c:743-745), a NULL
 	   dereference for iNumSrfIterations = 0; here they start at zero */
 	if (srf)
 		scat = (float *)calloc(pl * na, sizeof(float));
+	j.scat = scat;
+	j.norm_pass = 1;
 	for (s = 0; s < ns; ++s) {
 		float *nm = norm + vox * s;
-		for (m = 0; m < per; ++m) {
-			int a = s / 2 + (s % 2) * ns / 2 + m * ns;
-			set_measured_to_one(P, a, meas + pl * a, calc);
-			for (i = 0; i < pl; ++i)
-				calc[i] *= P->view_time[a];
-			or_backproject(P, bck_model, a, atn, calc, nm);
-		}
+		j.s = s;
+		par_for(per, subset_member, &j);
+		for (m = 0; m < per; ++m)
+			add_clamped(nm, j.un + vox * m, vox);
 		for (i = 0; i < vox; ++i)
 			nm[i] = nm[i] < 1e-6 ? 0.0 : 1.0 / nm[i];
 	}
+	j.norm_pass = 0;
 	if (srf)
 		next_s = 0 + 1 <= srf_iters;
 	for (it = 1; it <= iterations; ++it) {
@@ -670,43 +876,24 @@ int or_osem(const or_problem *P, int prj_model, int bck_model, int srf_iters, in
 			next_s = (it == iterations) ? this_s : (it + 1 <= srf_iters);
 			model = this_s ? prj_model : (prj_model & ~4);
 		}
+		j.model = model;
+		j.this_s = this_s;
+		j.next_s = next_s;
 		for (s = 0; s < ns; ++s) {
+			j.s = s;
+			par_for(per, subset_member, &j);
 			memset(tmp, 0, sizeof(float) * vox);
-			for (m = 0; m < per; ++m) {
-				int a = s / 2 + (s % 2) * ns / 2 + m * ns;
-				or_project(P, model, a, est, atn, 1.0, calc);
-				for (i = 0; i < pl; ++i)
-					calc[i] *= P->view_time[a] * P->sens[a];
-				if (srf) {
-					if (!this_s) {
-						for (i = 0; i < pl; ++i)
-							calc[i] += scat[pl * a + i];
-					} else if (!next_s) {
-						or_project(P, prj_model & ~4, a, est, atn, 1.0, c2);
-						for (i = 0; i < pl; ++i)
-							c2[i] *= P->view_time[a];
-						for (i = 0; i < pl; ++i)
-							scat[pl * a + i] = calc[i] - c2[i];
-					}
-				}
-				if (scatest != NULL)
-					for (i = 0; i < pl; ++i)
-						calc[i] += scatest[pl * a + i];
-				zero_nonmeasured(P, a, meas, calc);
-				for (i = 0; i < pl; ++i)
-					calc[i] = calc[i] > 1e-20 ? meas[pl * a + i] / calc[i] : 0.0;
-				for (i = 0; i < pl; ++i)
-					calc[i] *= P->view_time[a];
-				or_backproject(P, bck_model, a, atn, calc, tmp);
-			}
+			for (m = 0; m < per; ++m)
+				add_clamped(tmp, j.un + vox * m, vox);
 			for (i = 0; i < vox; ++i)
 				est[i] *= tmp[i] * norm[vox * s + i];
 		}
 	}
 	free(norm);
 	free(tmp);
-	free(calc);
-	free(c2);
+	free(j.calc);
+	free(j.c2);
+	free(j.un);
 	free(scat);
 	return 0;
 }

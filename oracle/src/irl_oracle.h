@@ -61,6 +61,9 @@ void or_genprj(const or_problem *P, int model, const float *act, const float *at
 int or_osem(const or_problem *P, int prj_model, int bck_model, int srf_iters, int iterations, int per_subset,
 	const float *meas, const float *atn, const float *scatest, float *est);
 void or_initial_estimate(int n, int nz, int nviews, const float *prj, float *est);
+/* host threads for the independent views of or_genprj and of each or_osem
+   subset (default 1); results do not depend on it */
+void or_set_threads(int n);
 
 #ifdef __cplusplus
 }

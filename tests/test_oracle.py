@@ -165,3 +165,22 @@ def test_reference_fft_table_genprj_matches_oracle_without_pad(orc):
     want = orc.Problem(case, pad_len=0, avg_len=0).genprj()
     for vi in range(case.nviews):
         assert rel_l2(prj[vi], want[vi]) <= 1e-6, (vi, rel_l2(prj[vi], want[vi]))
+
+
+def test_oracle_threads_do_not_change_results(orc):
+    """The restatement runs the views of IrlGenprj and of each OSEM subset on
+    host threads and adds the backprojections in view order afterwards, so
+    one thread and several give the same bits."""
+    case = W.full128(seed=2300, n=24, nviews=8, subsets=2, iterations=2, drf_max_offs=5)
+    out = {}
+    for t in (1, 4):
+        orc.orc().or_set_threads(t)
+        try:
+            pr = orc.Problem(case)
+            prj = pr.genprj()
+            est = pr.osem(W.poisson_counts(prj, 1e5, 2300), 2, 4)
+        finally:
+            orc.orc().or_set_threads(orc._threads())
+        out[t] = (prj, est)
+    assert np.array_equal(out[1][0], out[4][0])
+    assert np.array_equal(out[1][1], out[4][1])
