@@ -189,6 +189,26 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
 #define IRLCU_NOALLOC_MAX_N 1024
 int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz);
 
+/* Iteration-callback snapshots of the estimate, overlapped with the next
+   iteration: irlcu_snapshot_begin(slot) queues, after the work queued so
+   far, a copy of the estimate in external layout into the slot's pinned
+   host buffer (slot 0 or 1); irlcu_snapshot_end(slot, &p) waits for that
+   copy and sets p to the buffer, valid until the slot's next begin or the
+   context's end. */
+int irlcu_snapshot_begin(int slot);
+int irlcu_snapshot_end(int slot, float **host);
+
+/* Body-contour orbit edges for ComputeOrbit (computeorbit.c:81-147): img
+   is the thresholded n x n body image (host); for each view, rotated by
+   (sn[v], cs[v]) onto an m x m grid with the bilinear rotator of
+   rot3dpar.c:19-198, consumed[v] is one more than the first row (from
+   row 0, the detector side) that holds a positive sample, or m/2 when the
+   first m/2 rows hold none, which is the row count libirl's search loop
+   leaves behind.  Synchronous; needs no context (allocates its own small
+   device buffers). */
+int irlcu_orbit_edges(const float *img, int n, int m, const float *sn, const float *cs, int nviews,
+	int *consumed);
+
 /* synchronous wall-clock of the last batched call's stages, for tracing */
 int irlcu_stage_times(float *ms, int nmax);
 
@@ -214,6 +234,15 @@ int irlcu_sur_get_weights(irlcu_sur *net, float *host, size_t n);
 int irlcu_sur_set_weights(irlcu_sur *net, const float *host, size_t n);
 /* x: device BF16 [B][32][32][32][3] (channels last); y, t: device FP32 [B][128*128] */
 int irlcu_sur_forward(irlcu_sur *net, int B, const void *x, float *y);
+/* Test hook for the bounded waits of the tensor-core convolutions: how many
+   times a stage-refill wait polls its mbarrier before it gives up (default
+   and maximum 4,194,304); returns the previous value.  With 0 every such
+   wait runs out at once: the kernel sets its error flag, issues no further
+   copies or MMAs, waits for its copies in flight and (at the full limit)
+   for its last MMAs, frees its TMEM and returns, and the entry point
+   returns IRLCU_ECUDA ("... wait timed out").  The output of that call is
+   undefined; the context stays usable. */
+unsigned irlcu_sur_test_refill_wait(unsigned polls);
 /* mean squared error against t and its gradient (grad_host: nparams floats, or NULL) */
 int irlcu_sur_gradient(irlcu_sur *net, int B, const void *x, const float *t, float *loss, float *grad_host);
 /* one Adam step (beta 0.9 / 0.999) at learning rate lr; *loss before the step */

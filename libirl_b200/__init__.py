@@ -99,6 +99,8 @@ def _declare_irlcu(lib):
     lib.irlcu_sur_set_weights.argtypes = [V, F, S]
     lib.irlcu_sur_forward.restype = I
     lib.irlcu_sur_forward.argtypes = [V, I, V, V]
+    lib.irlcu_sur_test_refill_wait.restype = C.c_uint
+    lib.irlcu_sur_test_refill_wait.argtypes = [C.c_uint]
     lib.irlcu_sur_gradient.restype = I
     lib.irlcu_sur_gradient.argtypes = [V, I, V, V, C.POINTER(C.c_float), F]
     lib.irlcu_sur_train_step.restype = I

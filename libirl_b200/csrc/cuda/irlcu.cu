@@ -203,6 +203,14 @@ static void free_ctx(Ctx *c) {
   drf_fft_work_free(*c);
   esse_free(*c);
   free_rotate_scratch(*c);
+  for (int k = 0; k < 2; ++k) {
+    if (c->snap_copied[k]) cudaEventSynchronize(c->snap_copied[k]);
+    dfree(c->snap[k]);
+    if (c->snap_host[k]) cudaFreeHost(c->snap_host[k]);
+    if (c->snap_made[k]) cudaEventDestroy(c->snap_made[k]);
+    if (c->snap_copied[k]) cudaEventDestroy(c->snap_copied[k]);
+  }
+  if (c->snap_st) cudaStreamDestroy(c->snap_st);
   for (auto &e : c->ev) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -534,6 +542,41 @@ int irlcu_download_external(int buf, float *host) {
   CU_TRY(cudaMemcpyAsync(host, c.wbck, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
   CU_TRY(cudaStreamSynchronize(c.st));
   if (c.sur) TRY(sur_tc_status(c.st));
+  return IRLCU_OK;
+}
+
+// The iteration callback's copy of the estimate without stalling the
+// device: the external-layout snapshot is taken on the context stream right
+// after the iteration's kernels, then copied to pinned host memory on a
+// stream of its own, so that the next iteration's kernels (queued by the
+// host meanwhile) run during the copy and the callback.
+int irlcu_snapshot_begin(int slot) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (slot < 0 || slot > 1) return set_error(IRLCU_EARG, "snapshot slot %d", slot);
+  if (!c.est) return set_error(IRLCU_ESTATE, "no estimate to snapshot");
+  if (!c.snap_st) CU_TRY(cudaStreamCreateWithFlags(&c.snap_st, cudaStreamNonBlocking));
+  if (!c.snap[slot]) {
+    TRY(dalloc(&c.snap[slot], c.vox));
+    CU_TRY(cudaMallocHost(&c.snap_host[slot], c.vox * sizeof(float)));
+    CU_TRY(cudaEventCreateWithFlags(&c.snap_made[slot], cudaEventDisableTiming));
+    CU_TRY(cudaEventCreateWithFlags(&c.snap_copied[slot], cudaEventDisableTiming));
+  }
+  k_to_external<<<592, 256, 0, c.st>>>(c.est, c.snap[slot], c.n, c.nz);
+  CU_LAUNCHED();
+  CU_TRY(cudaEventRecord(c.snap_made[slot], c.st));
+  CU_TRY(cudaStreamWaitEvent(c.snap_st, c.snap_made[slot], 0));
+  CU_TRY(cudaMemcpyAsync(c.snap_host[slot], c.snap[slot], c.vox * sizeof(float), cudaMemcpyDeviceToHost, c.snap_st));
+  CU_TRY(cudaEventRecord(c.snap_copied[slot], c.snap_st));
+  return IRLCU_OK;
+}
+
+int irlcu_snapshot_end(int slot, float **host) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  if (slot < 0 || slot > 1 || !c.snap_copied[slot]) return set_error(IRLCU_ESTATE, "no snapshot in slot %d", slot);
+  CU_TRY(cudaEventSynchronize(c.snap_copied[slot]));
+  *host = c.snap_host[slot];
   return IRLCU_OK;
 }
 

@@ -150,6 +150,13 @@ struct Ctx {
   float *sur_work = nullptr;              // pooling work of max_batch views
   float *sur_static = nullptr;            // pooled mu and exp(-S) channels of every view (BF16 pairs)
   bool sur_static_ok = false;             // ... computed from the current attenuation tables
+  // estimate snapshots for the iteration callback (irlcu_snapshot_*): a
+  // device copy in external layout and a pinned host copy per slot, copied
+  // on their own stream while the next iteration runs
+  float *snap[2] = {nullptr, nullptr};
+  float *snap_host[2] = {nullptr, nullptr};
+  cudaStream_t snap_st = nullptr;
+  cudaEvent_t snap_made[2] = {nullptr, nullptr}, snap_copied[2] = {nullptr, nullptr};
   // three-shear intermediate for slices beyond shared memory, grown on use
   mutable float *xscratch = nullptr;
   mutable size_t xscratch_elems = 0;

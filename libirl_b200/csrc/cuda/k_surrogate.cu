@@ -326,6 +326,7 @@ constexpr int TC_MAXCH = 640;  // k chunks (of 8) of one CTA's k range: K / 8 <=
 constexpr unsigned TC_WAIT_LIMIT = 1u << 22;
 
 __device__ int g_tc_error;
+unsigned g_tc_refill_limit = TC_WAIT_LIMIT;  // host: polls of a stage-refill wait
 
 template <int N>
 struct TcCfg {
@@ -351,8 +352,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (unsigned it = 0; it < TC_WAIT_LIMIT; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned limit = TC_WAIT_LIMIT) {
+  for (unsigned it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -369,8 +370,13 @@ __device__ __forceinline__ void cp16(uint32_t dst, const void *src, bool ok) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0) : "memory");
 }
 
+// refill_limit: polls of a stage-refill wait (TC_WAIT_LIMIT; a test sets 0,
+// which makes those waits run out at once); the final wait for the last
+// MMAs always polls up to TC_WAIT_LIMIT, so no MMA is in flight when the
+// TMEM is freed
 template <int N>
-__global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const bf16 *__restrict__ X) {
+__global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const bf16 *__restrict__ X,
+                                                   unsigned refill_limit) {
   using Cfg = TcCfg<N>;
   extern __shared__ __align__(128) unsigned char tcs[];
   unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)tcs + 127) & ~(uintptr_t)127);
@@ -483,7 +489,7 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
     if (nt < nk) {
       if (it >= 1) {
         const int pt = it - 1;
-        if (!mbar_wait(smem_addr(&bars[pt % TC_S]), (pt / TC_S) & 1)) {
+        if (!mbar_wait(smem_addr(&bars[pt % TC_S]), (pt / TC_S) & 1, refill_limit)) {
           if (tid == 0) atomicExch(&g_tc_error, 1);
           abort_flag = 1;
         }
@@ -606,10 +612,10 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = n
   if (conv && tc_usable(a, *conv, X)) {
     const dim3 tgrid((a.M + TC_BM - 1) / TC_BM, 1, a.splits);
     switch (a.N) {
-      case 32: TC_TRY(tc_attr<32>()); k_conv_tc<32><<<tgrid, TC_NT, TcCfg<32>::SMEM, st>>>(a, *conv, X); break;
-      case 64: TC_TRY(tc_attr<64>()); k_conv_tc<64><<<tgrid, TC_NT, TcCfg<64>::SMEM, st>>>(a, *conv, X); break;
-      case 128: TC_TRY(tc_attr<128>()); k_conv_tc<128><<<tgrid, TC_NT, TcCfg<128>::SMEM, st>>>(a, *conv, X); break;
-      default: TC_TRY(tc_attr<256>()); k_conv_tc<256><<<tgrid, TC_NT, TcCfg<256>::SMEM, st>>>(a, *conv, X); break;
+      case 32: TC_TRY(tc_attr<32>()); k_conv_tc<32><<<tgrid, TC_NT, TcCfg<32>::SMEM, st>>>(a, *conv, X, g_tc_refill_limit); break;
+      case 64: TC_TRY(tc_attr<64>()); k_conv_tc<64><<<tgrid, TC_NT, TcCfg<64>::SMEM, st>>>(a, *conv, X, g_tc_refill_limit); break;
+      case 128: TC_TRY(tc_attr<128>()); k_conv_tc<128><<<tgrid, TC_NT, TcCfg<128>::SMEM, st>>>(a, *conv, X, g_tc_refill_limit); break;
+      default: TC_TRY(tc_attr<256>()); k_conv_tc<256><<<tgrid, TC_NT, TcCfg<256>::SMEM, st>>>(a, *conv, X, g_tc_refill_limit); break;
     }
     CU_LAUNCHED();
   } else {
@@ -1602,6 +1608,12 @@ int irlcu_sur_set_weights(irlcu_sur *s, const float *host, size_t n) {
   CU_LAUNCHED();
   CU_TRY(cudaStreamSynchronize(s->st));
   return IRLCU_OK;
+}
+
+unsigned irlcu_sur_test_refill_wait(unsigned polls) {
+  const unsigned prev = g_tc_refill_limit;
+  g_tc_refill_limit = polls < TC_WAIT_LIMIT ? polls : TC_WAIT_LIMIT;
+  return prev;
 }
 
 int irlcu_sur_forward(irlcu_sur *s, int B, const void *x, float *y) {

@@ -1,125 +1,111 @@
 /*
- * irl_orbit.c -- ComputeOrbit of libirl_b200 (libirl computeorbit.c:21-150).
+ * irl_orbit.c -- ComputeOrbit (irl.h; libirl computeorbit.c:21-150): the
+ * camera's centre-of-rotation distance (CFCR) per view.
  *
- * The body outline is rotated onto a sqrt(2)-larger grid with the bilinear
- * rotator (rot3dpar.c:19-198) for each view and the first non-empty row
- * from the detector gives the camera radius.  A single 2D image per view is
- * far below the size where a GPU launch pays, so this runs on the host with
- * the same arithmetic as the device rotator.
+ *   type 0: circular; every view gets fMargin.
+ *   type 1: body contour; each view's camera sits fMargin (or
+ *           pfMargins[view]) outside the body, whose outline is the part
+ *           of the 2D image above the threshold.
+ *   type 2: as 1, in L-mode: views i and i + NumViews/2 come from one
+ *           camera configuration, so both get the larger of their two
+ *           distances.
+ *
+ * For type 1/2 the body's extent towards each view's detector is the
+ * device kernel irlcu_orbit_edges (k_orbit.cu).  It scans, for all views
+ * at once, the image rotated onto a sqrt(2)-larger grid for the first row
+ * that holds body.  This file does the rest on the host:
+ *   - the threshold, applied in place to the caller's image as libirl
+ *     does;
+ *   - the grid side (ceil(sqrt 2 n), with n's parity);
+ *   - each view's rotation sine and cosine from libm;
+ *   - the radius arithmetic in libirl's operand types.
+ * Any failure is trapped and returned as 1, with the message in
+ * pchIrlErrorString.
  */
 #include <math.h>
+#include <setjmp.h>
 #include <stdlib.h>
-#include <string.h>
 
+#include "irl_err.h"
 #include "irl_host.h"
+#include "irlcu.h"
 
-/* bilinear rotation of one n_old x n_old slice onto n_new x n_new */
-static void rot2d(float fAngle, const float *Old, float *New, int OldDim, int NewDim)
+#define ORBIT_E_MEMORY 1
+#define ORBIT_E_TYPE 2
+
+/* pixels at or below the threshold become 0: fThresh > 0 is a fraction of
+   the maximum, fThresh <= 0 minus an absolute level */
+static void orbit_threshold(float *img, int count, float fThresh)
 {
-	int NewX, NewY, OldX, OldY, HeadPixel, TailPixel, NumPix;
-	float FloatX, FloatY, X, Y, z0, z1, z2, z3, z01, z23, z0123;
-	float NewAxis, OldAxis, Radius, Sin, Cos;
-	int z0out, z1out, z2out, z3out;
-	Sin = (float)sin(fAngle);
-	Cos = (float)cos(fAngle);
-	memset(New, 0, sizeof(float) * NewDim * NewDim);
-	NewAxis = 0.5 * (NewDim - 1);
-	OldAxis = 0.5 * (OldDim - 1);
-	Radius = 0.5 * NewDim;
-	for (NewY = 0; NewY < NewDim; NewY++) {
-		Y = NewY - NewAxis;
-		NumPix = (int)(sqrt(Radius * Radius - (Radius - NewY - .5) * (Radius - NewY - .5)) + .5);
-		NumPix *= 2;
-		HeadPixel = (int)(0.5 * (NewDim - NumPix));
-		TailPixel = HeadPixel + NumPix - 1;
-		for (NewX = HeadPixel; NewX <= TailPixel; NewX++) {
-			X = NewX - NewAxis;
-			FloatX = X * Cos - Y * Sin + OldAxis;
-			FloatY = X * Sin + Y * Cos + OldAxis;
-			OldX = (int)FloatX;
-			OldY = (int)FloatY;
-			z0out = z1out = z2out = z3out = 0;
-			if (OldX < 0 || OldX >= OldDim)
-				z0out = z1out = 1;
-			if (OldY < 0 || OldY >= OldDim)
-				z0out = z2out = 1;
-			if (OldX + 1 < 0 || OldX + 1 >= OldDim)
-				z2out = z3out = 1;
-			if (OldY + 1 < 0 || OldY + 1 >= OldDim)
-				z1out = z3out = 1;
-			z0 = z0out ? 0.0f : Old[OldY * OldDim + OldX];
-			z1 = z1out ? 0.0f : Old[(OldY + 1) * OldDim + OldX];
-			z2 = z2out ? 0.0f : Old[OldY * OldDim + OldX + 1];
-			z3 = z3out ? 0.0f : Old[(OldY + 1) * OldDim + OldX + 1];
-			z01 = z0 + (FloatY - OldY) * (z1 - z0);
-			z23 = z2 + (FloatY - OldY) * (z3 - z2);
-			if (FloatY < 0) {
-				z01 = z0;
-				z23 = z2;
-			}
-			z0123 = z01 + (FloatX - OldX) * (z23 - z01);
-			if (FloatX < 0)
-				z0123 = z01;
-			New[NewY * NewDim + NewX] = z0123;
-		}
+	float level, top;
+	int i;
+	if (fThresh <= 0.0f) {
+		level = -fThresh;
+	} else {
+		top = img[0];
+		for (i = 1; i < count; ++i)
+			if (img[i] > top)
+				top = img[i];
+		level = top * fThresh;
 	}
+	for (i = 0; i < count; ++i)
+		if (img[i] <= level)
+			img[i] = 0.0f;
 }
 
 int ComputeOrbit(float *pfPixels, IrlParms_t *psParms, float fMargin, float *pfMargins, float fThresh,
 	int OrbitType, PrjView_t *psViews)
 {
-	int iNang = psParms->NumViews, iNdim = psParms->NumPixels, iNumRotPix, iPix, iAng, iRow;
-	float fPixSize = psParms->BinWidth, fPixThresh = 0.0f, fMax, fRadius, fSum;
-	float *pfRotPix;
+	const int nviews = psParms->NumViews, n = psParms->NumPixels;
+	const float pix = psParms->BinWidth;
+	/* volatile: read after a longjmp back to the trap */
+	float *volatile sc = NULL;
+	int *volatile rows = NULL;
+	int side, v;
+	jmp_buf env;
 	if (OrbitType == 0) {
-		for (iAng = 0; iAng < iNang; ++iAng)
-			psViews[iAng].CFCR = fMargin;
+		for (v = 0; v < nviews; ++v)
+			psViews[v].CFCR = fMargin;
 		return 0;
-	} else if (OrbitType > 2 || OrbitType < 0) {
-		return 2;
 	}
-	if (fThresh <= 0.0) {
-		fPixThresh = -fThresh;
-	} else {
-		fMax = pfPixels[0];
-		for (iPix = 1; iPix < iNdim * iNdim; ++iPix)
-			fMax = pfPixels[iPix] > fMax ? pfPixels[iPix] : fMax;
-		fPixThresh = fMax * fThresh;
+	/* libirl rejects only types above 2 (computeorbit.c:81-84); a negative
+	   type runs the contour search as type 1 does */
+	if (OrbitType > 2)
+		return ORBIT_E_TYPE;
+	if (setjmp(env)) {
+		irl_untrap();
+		free(sc);
+		free(rows);
+		return ORBIT_E_MEMORY;
 	}
-	for (iPix = 0; iPix < iNdim * iNdim; ++iPix)
-		if (pfPixels[iPix] <= fPixThresh)
-			pfPixels[iPix] = 0.0;
-	iNumRotPix = (int)ceil(sqrt(2.0) * (double)iNdim);
-	if ((iNumRotPix % 2) != (iNdim % 2))
-		iNumRotPix++;
-	pfRotPix = (float *)malloc(sizeof(float) * iNumRotPix * iNumRotPix);
-	if (pfRotPix == NULL)
-		return 1;
-	for (iAng = 0; iAng < iNang; ++iAng) {
-		float fAngle = psViews[iAng].Angle;
-		int k;
-		rot2d((float)(0.5 * M_PI + fAngle), pfPixels, pfRotPix, iNdim, iNumRotPix);
-		fSum = 0.0;
-		for (iRow = 0; iRow < iNumRotPix / 2 && fSum <= 0.0; ++iRow) {
-			fSum = 0.0f;
-			for (k = 0; k < iNumRotPix; ++k)
-				fSum += pfRotPix[iRow * iNumRotPix + k];
+	irl_trap(&env);
+	orbit_threshold(pfPixels, n * n, fThresh);
+	side = (int)ceil(sqrt(2.0) * (double)n);
+	side += (side & 1) != (n & 1);
+	sc = (float *)irl_malloc(sizeof(float) * 2 * nviews, "orbit rotations");
+	rows = (int *)irl_malloc(sizeof(int) * nviews, "orbit edges");
+	for (v = 0; v < nviews; ++v) {
+		/* rows parallel to the detector, row 0 the farthest from the centre
+		   towards it: the rotation libirl applies, at float angle */
+		const float a = (float)(0.5 * M_PI + psViews[v].Angle);
+		sc[v] = (float)sin(a);
+		sc[nviews + v] = (float)cos(a);
+	}
+	irl_cu(irlcu_orbit_edges(pfPixels, n, side, sc, sc + nviews, nviews, rows), "ComputeOrbit");
+	for (v = 0; v < nviews; ++v) {
+		/* half the grid minus the rows outside the body, in cm */
+		float r = (float)(((double)(float)side / 2.0 - (double)(float)rows[v]) * (double)pix);
+		r += pfMargins != NULL ? pfMargins[v] : fMargin;
+		psViews[v].CFCR = r;
+	}
+	if (OrbitType == 2)
+		for (v = 0; v < nviews / 2; ++v) {
+			float *a = &psViews[v].CFCR, *b = &psViews[v + nviews / 2].CFCR;
+			const float far = *a > *b ? *a : *b;
+			*a = *b = far;
 		}
-		fRadius = ((float)iNumRotPix / 2.0 - (float)iRow) * fPixSize;
-		if (pfMargins != NULL)
-			fRadius += pfMargins[iAng];
-		else
-			fRadius += fMargin;
-		psViews[iAng].CFCR = fRadius;
-	}
-	if (OrbitType == 2) {
-		for (iAng = 0; iAng < iNang / 2; ++iAng) {
-			if (psViews[iAng].CFCR > psViews[iAng + iNang / 2].CFCR)
-				psViews[iAng + iNang / 2].CFCR = psViews[iAng].CFCR;
-			else
-				psViews[iAng].CFCR = psViews[iAng + iNang / 2].CFCR;
-		}
-	}
-	free(pfRotPix);
+	irl_untrap();
+	free(sc);
+	free(rows);
 	return 0;
 }

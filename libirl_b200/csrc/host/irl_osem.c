@@ -410,11 +410,13 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 			irl_fatal(IRL_E_VALUE, "SrfSetup", "scatter modelling needs an attenuation map");
 		irl_esse_prepare(krnl_fname, &S.p, ip->SrfCollapseFac, &S.esse);
 	}
+	irl_msg(5, "Done scatter kernel (%.3f s)\n", now_s() - t0);
 	{
 		irl_detector *d;
 		/* libirl calls vSetupDrfTables unconditionally (irlosem.c:158-160) */
 		irl_setup_drf_tables(&S.p, op, S.views, drf_fname, &d);
 	}
+	irl_msg(5, "Done DRF tables (%.3f s)\n", now_s() - t0);
 	S.vox = (size_t)S.p.n * S.p.nz * S.p.n;
 	S.prjn = (size_t)S.p.n * S.p.nz * S.p.nviews;
 	S.tmp = (float *)irl_malloc(sizeof(float) * S.vox, "IrlOsem:Temp");
@@ -444,10 +446,12 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		irl_reorder(S.p.n, S.p.nz, S.p.n, recon, S.tmp);
 		cb(0, S.tmp);
 	}
+	irl_msg(5, "Done host set-up (%.3f s)\n", now_s() - t0);
 	S.per = S.p.ang_per_subset;
 	S.max_batch = S.per > 32 ? 32 : S.per;
 	S.ns = irl_compute_subsets(S.p.nviews, S.per, &S.ang);
 	irl_device_setup(&S.p, S.views, atn, &S.esse, g_irl_adv.bFastRotate, S.max_batch);
+	irl_msg(5, "Done device set-up (%.3f s)\n", now_s() - t0);
 	irl_cu(irlcu_upload(IRLCU_BUF_PRJ, 0, prj, S.prjn), "IrlOsem");
 	irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, recon, S.vox), "IrlOsem");
 	if (scatest != NULL)
@@ -493,8 +497,26 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 	return 0;
 }
 
-/* one OSEM iteration: subset loop of osemrecon.c:637-883 */
-static void one_iteration(void)
+static int any_hook(void)
+{
+	int h;
+	for (h = 0; h < 6; ++h)
+		if (g_irl_hooks[h] != NULL)
+			return 1;
+	return 0;
+}
+
+/* the iteration callback with the snapshot of iteration it */
+static void deliver_snapshot(int it)
+{
+	float *img = NULL;
+	irl_cu(irlcu_snapshot_end(it & 1, &img), "OsemRecon");
+	S.cb(it, img);
+}
+
+/* one OSEM iteration: subset loop of osemrecon.c:637-883; with deliver_cb
+   the iteration callback gets the result before this returns */
+static void one_iteration(int deliver_cb)
 {
 	irl_parms *p = &S.p;
 	int it = S.it + 1, s = 0, m, model = p->prj_model, mode = 0;
@@ -552,7 +574,7 @@ static void one_iteration(void)
 		sur_check(model);
 	/* bCheckIfSaveIteration is true for every iteration with libirl's
 	   SaveInterval of 1 (IrlSetup.c:87-88, osemrecon.c:513-555) */
-	if (S.cb != NULL) {
+	if (deliver_cb && S.cb != NULL) {
 		irl_cu(irlcu_download_external(IRLCU_BUF_EST, S.tmp), "OsemRecon");
 		S.cb(it, S.tmp);
 	}
@@ -573,8 +595,26 @@ int IrlOsemIterate(int niter)
 		return err;
 	}
 	irl_trap(&env);
-	for (k = 0; k < niter && S.it < S.p.iterations; ++k)
-		one_iteration();
+	if (S.cb == NULL || any_hook()) {
+		for (k = 0; k < niter && S.it < S.p.iterations; ++k)
+			one_iteration(1);
+	} else {
+		/* the callback of iteration i runs while iteration i + 1 computes:
+		   its estimate is snapshotted on the device after iteration i and
+		   copied to pinned memory on a stream of its own
+		   (irlcu_snapshot_*); the callback still sees every iteration's
+		   result, in order, before this call returns */
+		int pending = -1;
+		for (k = 0; k < niter && S.it < S.p.iterations; ++k) {
+			one_iteration(0);
+			irl_cu(irlcu_snapshot_begin(S.it & 1), "OsemRecon");
+			if (pending >= 0)
+				deliver_snapshot(pending);
+			pending = S.it;
+		}
+		if (pending >= 0)
+			deliver_snapshot(pending);
+	}
 	irl_untrap();
 	return 0;
 }

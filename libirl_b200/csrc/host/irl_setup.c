@@ -7,7 +7,6 @@
  * decide integer indices or table sizes keep libirl's float/double types so
  * the decisions are identical.
  */
-#include <complex.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -205,190 +204,7 @@ irl_view *irl_setup_views(IrlParms_t *ip, PrjView_t *pv)
 }
 
 /* ------------------------------------------------------------ GRF tables */
-
-/* in-place complex FFT (double), power-of-two n, kernel exp(sign i ...) */
-static void cfft(double complex *x, int n, int stride, int sign)
-{
-	int i, j, len;
-	for (i = 1, j = 0; i < n; ++i) {
-		int bit = n >> 1;
-		for (; j & bit; bit >>= 1)
-			j ^= bit;
-		j ^= bit;
-		if (i < j) {
-			double complex t = x[(long)i * stride];
-			x[(long)i * stride] = x[(long)j * stride];
-			x[(long)j * stride] = t;
-		}
-	}
-	for (len = 2; len <= n; len <<= 1) {
-		int h = len >> 1;
-		for (j = 0; j < h; ++j) {
-			double a = sign * 2.0 * M_PI * (double)j / (double)len;
-			double complex w = cos(a) + I * sin(a);
-			for (i = j; i < n; i += len) {
-				double complex u = x[(long)i * stride], t = x[(long)(i + h) * stride] * w;
-				x[(long)i * stride] = u + t;
-				x[(long)(i + h) * stride] = u - t;
-			}
-		}
-	}
-}
-
-/* GenDPSRF, gendrf.c:44-216 (parallel-hole collimator) */
-static void gen_dpsrf(double ColToSource, double ColThick, double ColToImage, double HoleDiam,
-	double BinSize, double IntrinsicFWHM, int MatSize, float *pDPSRF, int *pAliasing)
-{
-	double intarg, samwid, normsum, normfac, alpha, beta, xfreq, yfreq, freq, delf, ftmp;
-	double PsfZero, NewBinSize;
-	int BinRatio, MyMatSize, NewMatSize, ix, iy, ix1, iy1;
-	float *ft;
-	double complex *cx;
-
-	*pAliasing = 0;
-	intarg = M_PI * M_PI * IntrinsicFWHM * IntrinsicFWHM / (4.0 * log(2.0));
-	alpha = (ColToSource + ColToImage + ColThick) / ColThick;
-	beta = M_PI * alpha * HoleDiam;
-	samwid = M_PI * BinSize;
-	BinRatio = 20.0 * BinSize / beta + 0.5;
-	BinRatio = BinRatio < 1 ? 1 : BinRatio;
-	NewBinSize = BinSize / BinRatio;
-	PsfZero = HoleDiam * (ColToSource + ColToImage + ColThick) / ColThick;
-	NewMatSize = 4.0 * PsfZero / NewBinSize;
-	MyMatSize = 2;
-	while ((MyMatSize < NewMatSize) && (MyMatSize < 1024))
-		MyMatSize *= 2;
-	ft = (float *)irl_calloc(sizeof(float) * 2 * MyMatSize * MyMatSize, "GRF spectrum");
-	delf = 1.0 / ((double)MyMatSize * NewBinSize);
-	ft[0] = 1;
-	for (ix = 0; ix <= MyMatSize / 2; ++ix) {
-		xfreq = (double)ix * delf;
-		for (iy = 0; iy <= MyMatSize / 2; ++iy) {
-			if (ix == 0 && iy == 0)
-				continue;
-			yfreq = (double)iy * delf;
-			freq = hypot(yfreq, xfreq);
-			ftmp = 2.0 * j1(beta * freq) / (beta * freq);
-			ftmp = ftmp * ftmp * exp(-freq * freq * intarg);
-			if (samwid > 0.0)
-				ftmp *= sin(samwid * freq) / (freq * samwid);
-			ft[2 * (MyMatSize * iy + ix)] = ftmp;
-			if (iy != 0)
-				ft[2 * (MyMatSize * (MyMatSize - iy) + ix)] = ftmp;
-			if (ix != 0)
-				ft[2 * (MyMatSize * iy + (MyMatSize - ix))] = ftmp;
-			if (ix != 0 && iy != 0)
-				ft[2 * (MyMatSize * (MyMatSize - iy) + (MyMatSize - ix))] = ftmp;
-		}
-	}
-	/* inverse 2D transform of the (float-stored) spectrum, in double */
-	cx = (double complex *)irl_malloc(sizeof(double complex) * MyMatSize * MyMatSize, "GRF transform");
-	for (ix = 0; ix < MyMatSize * MyMatSize; ++ix)
-		cx[ix] = ft[2 * ix] + I * ft[2 * ix + 1];
-	for (iy = 0; iy < MyMatSize; ++iy)
-		cfft(cx + (long)iy * MyMatSize, MyMatSize, 1, +1);
-	for (ix = 0; ix < MyMatSize; ++ix)
-		cfft(cx + ix, MyMatSize, MyMatSize, +1);
-	for (ix = 0; ix < MyMatSize * MyMatSize; ++ix) {
-		ft[2 * ix] = (float)(creal(cx[ix]) / ((double)MyMatSize * MyMatSize));
-		ft[2 * ix + 1] = (float)(cimag(cx[ix]) / ((double)MyMatSize * MyMatSize));
-	}
-	free(cx);
-	NewMatSize = MIN(MyMatSize / 2, BinRatio * MatSize);
-	*pAliasing = MyMatSize > 2 * MatSize;
-	for (ix = 0; ix < MyMatSize * MyMatSize; ix += 2)
-		if (ft[ix] < 0)
-			ft[ix] = 0;
-	normsum = ft[0];
-	for (ix = BinRatio; ix < NewMatSize; ix += BinRatio)
-		normsum += 2.0 * (ft[2 * ix] + ft[2 * ix * MyMatSize]);
-	for (ix = BinRatio; ix < NewMatSize; ix += BinRatio)
-		for (iy = BinRatio; iy < NewMatSize; iy += BinRatio)
-			normsum += 4.0 * ft[2 * (ix + iy * MyMatSize)];
-	normfac = 1.0 / normsum;
-	for (ix = 0; ix < MatSize * MatSize; ++ix)
-		pDPSRF[ix] = 0.0;
-	for (ix = 0, ix1 = 0; ix < NewMatSize; ix += BinRatio, ix1++)
-		for (iy = 0, iy1 = 0; iy < NewMatSize; iy += BinRatio, iy1++)
-			pDPSRF[ix1 + iy1 * MatSize] = ft[2 * (ix + iy * MyMatSize)] * normfac;
-	free(ft);
-}
-
-/* gendrf, gendrf.c:218-427 (parallel hole) */
-void irl_gendrf(float fColThick, float fHoleDiam, float fGap, float fIntrinsic, float fMaxErr,
-	float fBinSize, float fDrfSpacing, float minDist, int NumDists, int NOffs, Drf_t *tab)
-{
-	int iDist, iXOffs, iYOffs, MaxOffsX = NOffs, MaxOffsY = NOffs, alias = 0;
-	float fColToSource;
-	float *q = (float *)irl_malloc(sizeof(float) * NOffs * NOffs, "quarter DPSF");
-	double dSum, dNormFac, dMinSum = 1.0 - fMaxErr;
-
-	for (iDist = 0, fColToSource = minDist; iDist < NumDists; iDist++, fColToSource += fDrfSpacing) {
-		if (fColToSource <= 0.0) {
-			for (iXOffs = 1; iXOffs < NOffs * NOffs; ++iXOffs)
-				q[iXOffs] = 0.0;
-			q[0] = 1.0;
-		} else {
-			gen_dpsrf(fColToSource, fColThick, fGap, fHoleDiam, fBinSize, fIntrinsic, NOffs, q, &alias);
-		}
-		if (alias)
-			irl_warn("gendrf", "Possible aliasing in DRF table computation at distance %.2f", fColToSource);
-		if (fMaxErr <= 0.0) {
-			MaxOffsX = MaxOffsY = NOffs;
-			dNormFac = 1.0;
-		} else {
-			/* grow the square until the enclosed sum exceeds 1 - fMaxErr */
-			int iXT, iYT, prevX = 1;
-			dSum = q[0];
-			iYOffs = 1;
-			for (iXOffs = 1; iXOffs < NOffs; iXOffs++) {
-				if (dSum > dMinSum)
-					break;
-				dSum += 2 * q[iXOffs];
-				iYOffs = iXOffs;
-				for (iYT = 1; iYT < iYOffs; iYT++)
-					for (iXT = (prevX + 1); iXT <= iXOffs; iXT++)
-						dSum += 4 * q[iYT * NOffs + iXT];
-				for (iXT = 1; iXT <= iXOffs; iXT++)
-					dSum += 4 * q[iYOffs * NOffs + iXT];
-				dSum += 2 * q[iYOffs * NOffs];
-				iYOffs++;
-				prevX = iXOffs;
-			}
-			MaxOffsX = iXOffs;
-			MaxOffsY = iXOffs;
-			dSum = q[0];
-			for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs) {
-				dSum += q[iXOffs] * 2.0;
-				dSum += q[iXOffs * NOffs] * 2.0;
-				for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
-					dSum += 4.0 * q[iXOffs + iYOffs * NOffs];
-			}
-			dNormFac = 1.0 / dSum;
-		}
-		tab[iDist].MaxOffsX = MaxOffsX;
-		tab[iDist].MaxOffsY = MaxOffsY;
-		tab[iDist].bFFTdone = 0;
-		{
-			const int w = 2 * MaxOffsX - 1, xs = MaxOffsX - 1, ys = MaxOffsY - 1;
-			float *P = (float *)irl_calloc(sizeof(float) * (2 * MaxOffsX - 1) * (2 * MaxOffsY - 1), "PSF");
-#define PP(y, x) P[(y) * w + (x)]
-			PP(ys, xs) = q[0] * dNormFac;
-			for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
-				PP(ys + iYOffs, xs) = PP(ys - iYOffs, xs) = q[NOffs * iYOffs] * dNormFac;
-			for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs)
-				PP(ys, xs + iXOffs) = PP(ys, xs - iXOffs) = q[iXOffs] * dNormFac;
-			for (iYOffs = 1; iYOffs < MaxOffsY; ++iYOffs)
-				for (iXOffs = 1; iXOffs < MaxOffsX; ++iXOffs)
-					PP(ys + iYOffs, xs + iXOffs) = PP(ys - iYOffs, xs + iXOffs) =
-						PP(ys + iYOffs, xs - iXOffs) = PP(ys - iYOffs, xs - iXOffs) =
-							q[NOffs * iYOffs + iXOffs] * dNormFac;
-#undef PP
-			tab[iDist].Psf = P;
-		}
-	}
-	free(q);
-}
+/* irl_gendrf (the GRF table generator) lives in irl_grf.c */
 
 /* vComputeDrfs, IrlSetup.c:243-334 */
 static void compute_drfs(DrfTab_t *t, float fPixelWidth, float fBinWidth, int iReconMatSize, float fMinDist,

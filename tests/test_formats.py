@@ -88,10 +88,19 @@ def test_krnl_swapped_reads_numxyoffs(product, tmp_path):
         assert np.array_equal(got, k)
 
 
-def test_gendrf_matches_reference_and_is_normalised(product, orc):
-    nd, noffs = 6, 16
+# (col thick, hole diam, gap, intrinsic FWHM, max error, bin, spacing, first distance), distances, NOffs
+GENDRF_CASES = [
+    ((2.405, 0.111, 0.64, 0.38, 0.05, 0.4, 0.4, 3.0), 6, 16),
+    ((2.405, 0.111, 0.64, 0.38, 0.0, 0.3125, 0.3125, -1.0), 10, 64),   # no truncation; distances <= 0
+    ((3.5, 0.15, 1.0, 0.3, 0.01, 0.1, 0.2, 0.5), 8, 32),
+    ((2.0, 0.2, 0.5, 0.5, 0.002, 0.05, 0.6, 10.0), 5, 40),             # oversampled (ratio > 1), wide
+    ((2.405, 0.111, 0.64, 0.38, 0.02, 0.2, 1.0, 1.0), 40, 128),
+]
+
+
+@pytest.mark.parametrize("args,nd,noffs", GENDRF_CASES)
+def test_gendrf_matches_reference_and_is_normalised(product, orc, args, nd, noffs):
     tab = (api.Drf * nd)()
-    args = (2.405, 0.111, 0.64, 0.38, 0.05, 0.4, 0.4, 3.0)
     product.irl_gendrf(*args, nd, noffs, tab)
     for i in range(nd):
         d = tab[i]
@@ -108,7 +117,7 @@ def test_gendrf_matches_reference_and_is_normalised(product, orc):
             cnt = (2 * rt[i].MaxOffsY - 1) * (2 * rt[i].MaxOffsX - 1)
             a = np.ctypeslib.as_array(tab[i].Psf, shape=(cnt,))
             b = np.ctypeslib.as_array(rt[i].Psf, shape=(cnt,))
-            assert np.allclose(a, b, rtol=1e-5, atol=1e-7)
+            assert np.allclose(a, b, rtol=1e-6, atol=1e-9)
 
 
 def _genprj(lib, case, drf_name, krnl_name=None):

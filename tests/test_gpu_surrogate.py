@@ -160,3 +160,67 @@ def test_osem_surrogate_fallback(product, tmp_path):
         assert not np.array_equal(rec, plain)
     finally:
         product.IrlSetScatterSurrogate(None, 0.0)
+
+
+def test_trained_surrogate_ablation_full128(product, tmp_path):
+    """What the committed network gains: on the full 128^3 / 120-view / 8 x 10
+    case (Poisson data from the GPU ESSE path), the reconstruction with the
+    learned scatter model (ESSE fallback above 2 % view NRMSE) is within 1 %
+    image NRMSE of the ESSE reconstruction, and much closer to it than the
+    reconstruction with no scatter model (iNumSrfIterations = 0)."""
+    if not os.path.exists(SU.DEFAULT_WEIGHTS):
+        pytest.skip("no committed surrogate weights")
+    case = W.full128(seed=2000)
+    files = case.write_tables(str(tmp_path))
+    p, o, v = case.parms(), case.options(), case.views()
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    assert product.IrlGenprj(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), None, None,
+                             api.fptr(act), api.fptr(atn), api.fptr(prj), 1.0, None, None) == 0
+    meas = W.poisson_counts(prj, case.counts, 2000)
+    esse = _osem(product, case, files, meas, 10)
+    product.IrlSetScatterSurrogate(SU.DEFAULT_WEIGHTS.encode(), 0.02)
+    try:
+        learned = _osem(product, case, files, meas, 10)
+    finally:
+        product.IrlSetScatterSurrogate(None, 0.0)
+    none_case = W.full128(seed=2000, with_srf=True)
+    none_case.srf_iters = 0
+    p, o, v = none_case.parms(), none_case.options(), none_case.views()
+    atn, rec, m = none_case.atn.copy(), np.zeros_like(case.act), meas.copy()
+    assert product.IrlOsem(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), api.ITER_CB(), None,
+                           api.fptr(atn), api.fptr(m), api.fptr(rec), None, None) == 0
+    ref = float(np.linalg.norm(esse))
+    err_learned = float(np.linalg.norm(learned - esse)) / ref
+    err_none = float(np.linalg.norm(rec - esse)) / ref
+    assert err_learned <= 0.01, err_learned
+    assert err_learned < 0.25 * err_none, (err_learned, err_none)
+
+
+def test_tensor_core_wait_time_out_is_an_error_and_recoverable(product):
+    """The bounded mbarrier waits of the tcgen05 convolutions: with the
+    stage-refill waits limited to 0 polls every such wait runs out; the
+    kernel abandons its tile (its last MMAs are still awaited before the
+    TMEM is freed), the entry point returns an error with a message, and
+    the next call with the normal limit succeeds and gives the same output
+    as before."""
+    torch = _torch()
+    rng = np.random.default_rng(12)
+    net = SU.Network(product, 4, seed=13)
+    try:
+        _, xd = _inputs(rng, 4)
+        y0 = torch.zeros((4, 128 * 128), dtype=torch.float32, device="cuda")
+        y1 = torch.full_like(y0, -1.0)
+        net.forward(4, xd.data_ptr(), y0.data_ptr())
+        prev = product.irlcu_sur_test_refill_wait(0)
+        try:
+            rc = product.irlcu_sur_forward(net.ptr, 4, C.c_void_p(xd.data_ptr()), C.c_void_p(y1.data_ptr()))
+        finally:
+            product.irlcu_sur_test_refill_wait(prev)
+        assert rc != 0
+        assert b"timed out" in product.irlcu_error_string()
+        net.forward(4, xd.data_ptr(), y1.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(y0, y1)
+    finally:
+        net.close()
