@@ -173,6 +173,8 @@ static void free_ctx(Ctx *c) {
   dfree(c->rot.col_f2);
   dfree(c->rot.sn);
   dfree(c->rot.cs);
+  dfree(c->rot.col_rng);
+  dfree(c->rot.row_rng);
   dfree(c->sup_start);
   dfree(c->sup_end);
   dfree(c->est);
@@ -277,6 +279,8 @@ int irlcu_init(const irlcu_geom *g) {
   TRY(dalloc(&c->rot.col_f2, (size_t)2 * n * R));
   TRY(dalloc(&c->rot.sn, (size_t)R));
   TRY(dalloc(&c->rot.cs, (size_t)R));
+  TRY(dalloc(&c->rot.col_rng, (size_t)2 * n * R));
+  TRY(dalloc(&c->rot.row_rng, (size_t)n * R));
   TRY(dalloc(&c->sup_start, (size_t)n));
   TRY(dalloc(&c->sup_end, (size_t)n));
   {
@@ -348,6 +352,7 @@ int irlcu_set_angles(const float *angles) {
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  TRY(launch_shear_ranges(c, 0, R));
   return IRLCU_OK;
 }
 
@@ -1052,6 +1057,7 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2 + (size_t)r * 2 * n, cf2.data(), 2 * n * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn + r, &sn, 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs + r, &cs, 4, cudaMemcpyHostToDevice, alloc_stream()));
+  TRY(launch_shear_ranges(c, r, 1));
   int zero = 0;
   TRY(upload_views(&zero, 1, nullptr));
   const float *s = src;

@@ -763,6 +763,135 @@ __global__ void __launch_bounds__(128) k_conv_first(ConvGeom g, const bf16 *__re
   }
 }
 
+// The first layer (3 input channels, 27 taps: K = 81) on the tensor cores.
+// Its 3-channel rows do not come in the 16-byte channel chunks that
+// k_conv_tc gathers, so each thread builds its output position's whole A
+// row in registers (the 27 taps x 3 channels, zero outside the input and
+// past K, padded to K = 96) and stores it in the K-major no-swizzle
+// layout; the weights [32][81] are staged the same way.  Thread 0 issues
+// six M128 x N32 x K16 BF16 MMAs into a 32-column TMEM accumulator and
+// commits to an mbarrier (bounded wait, as in k_conv_tc); the epilogue adds
+// the bias, applies the ReLU and stores BF16.  One CTA of 128 threads per
+// 128 output positions.  The products are summed in the tensor cores'
+// order, not the direct kernels', so the outputs agree with them to FP32
+// rounding.
+constexpr int C0_KC = 12;                    // K chunks of 8: K = 96 >= 81
+constexpr int C0_A = TC_BM * C0_KC * 16;     // A tile bytes
+constexpr int C0_B = 32 * C0_KC * 16;        // B tile bytes
+constexpr size_t C0_SMEM = (size_t)C0_A + C0_B + 64 + 128;
+
+__global__ void __launch_bounds__(TC_NT) k_conv0_tc(ConvGeom g, const bf16 *__restrict__ x,
+                                                    const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                    bf16 *__restrict__ y) {
+  extern __shared__ __align__(128) unsigned char c0s[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)c0s + 127) & ~(uintptr_t)127);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + C0_A + C0_B);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long M = (long long)g.b * g.dout * g.hout * g.wout;
+  const long long m = (long long)blockIdx.x * TC_BM + tid;
+  const uint32_t sA = smem_addr(base), sB = sA + C0_A;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(32));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // this thread's A row: the 81 inputs of output position m, k = tap * 3 + c
+  {
+    uint32_t pk[C0_KC * 4];
+#pragma unroll
+    for (int q = 0; q < C0_KC * 4; ++q) pk[q] = 0u;
+    if (m < M) {
+      long long r = m;
+      const int ow = (int)(r % g.wout);
+      r /= g.wout;
+      const int oh = (int)(r % g.hout);
+      r /= g.hout;
+      const int od = (int)(r % g.dout);
+      const int b = (int)(r / g.dout);
+#pragma unroll
+      for (int tap = 0; tap < FIRST_TAPS; ++tap) {
+        const int td = tap / 9, th = (tap / 3) % 3, tw = tap % 3;
+        const int id = od * g.s + td - 1, ih = oh * g.s + th - 1, iw = ow * g.s + tw - 1;
+        if (id < 0 || id >= g.di || ih < 0 || ih >= g.hi || iw < 0 || iw >= g.wi) continue;
+        const unsigned short *px = reinterpret_cast<const unsigned short *>(x + in_off(g, b, id, ih, iw, 0));
+#pragma unroll
+        for (int c = 0; c < FIRST_CI; ++c) {
+          const int k = tap * FIRST_CI + c;
+          const uint32_t v = __ldg(px + c);
+          pk[k >> 1] |= (k & 1) ? (v << 16) : v;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < C0_KC; ++q)
+      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sA + q * (TC_BM * 16) + tid * 16),
+                   "r"(pk[4 * q]), "r"(pk[4 * q + 1]), "r"(pk[4 * q + 2]), "r"(pk[4 * q + 3]));
+  }
+  // B: weight row n, chunk q (k = 8q .. 8q+7; zero at k >= 81)
+  {
+    const unsigned short *wu = reinterpret_cast<const unsigned short *>(w);
+    for (int e = tid; e < 32 * C0_KC; e += TC_NT) {
+      const int n = e / C0_KC, q = e - n * C0_KC;
+      uint32_t h[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = 8 * q + i;
+        const uint32_t v = k < FIRST_TAPS * FIRST_CI ? (uint32_t)__ldg(wu + n * (FIRST_TAPS * FIRST_CI) + k) : 0u;
+        h[i >> 1] |= (i & 1) ? (v << 16) : v;
+      }
+      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sB + q * (32 * 16) + n * 16), "r"(h[0]),
+                   "r"(h[1]), "r"(h[2]), "r"(h[3]));
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {
+#pragma unroll
+    for (int kk = 0; kk < C0_KC / 2; ++kk) {
+      const uint64_t ad = umma_desc(sA + kk * 2 * (TC_BM * 16), TC_BM * 16, 128);
+      const uint64_t bd = umma_desc(sB + kk * 2 * (32 * 16), 32 * 16, 128);
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+          "l"(ad), "l"(bd), "r"(TcCfg<32>::IDESC), "r"(kk > 0 ? 1u : 0u), "r"(0), "r"(0), "r"(0), "r"(0));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(bar))
+                 : "memory");
+  }
+  const bool ok = mbar_wait(smem_addr(bar), 0);
+  if (!ok && lane == 0) atomicExch(&g_tc_error, 1);
+  const bool all_ok = __syncthreads_and(ok);  // uniform: the TMEM loads are warp-collective
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (all_ok) {
+#pragma unroll
+    for (int c0 = 0; c0 < 32; c0 += 8) {
+      uint32_t v[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < M) {
+        __align__(16) bf16 h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(fmaxf(__uint_as_float(v[q]) + bias[c0 + q], 0.f));
+        *reinterpret_cast<uint4 *>(y + m * 32 + c0) = *reinterpret_cast<const uint4 *>(h);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32));
+}
+
 // The first layer for an even output width: two adjacent output positions
 // (ow, ow + 1) per thread, so that every shared-memory weight load feeds
 // both.  Each output accumulates its products in the order k_conv_first does
@@ -1306,6 +1435,17 @@ static const bf16 *layer_input(const irlcu_sur &s, int i) {
 }
 
 // forward over the B samples in act[0]; FP32 output [B][128*128] in s.out
+// the first layer on the tensor cores unless IRLCU_SUR_TC=0 (then the
+// direct FP32 kernels k_conv_first / k_conv_first2)
+static bool conv0_tc_usable() {
+  static int env = -1;
+  if (env < 0) {
+    const char *e = getenv("IRLCU_SUR_TC");
+    env = (e && e[0] == '0') ? 0 : 1;
+  }
+  return env == 1;
+}
+
 static int sur_forward(irlcu_sur &s, int B) {
   const int nl = (int)s.L.size();
   for (int i = 0; i < nl; ++i) {
@@ -1319,7 +1459,15 @@ static int sur_forward(irlcu_sur &s, int B) {
     }
     const long long M = (long long)B * l.g.dout * l.g.hout * l.g.wout;
     if (i == 0 && l.g.ci == FIRST_CI && l.g.co == FIRST_CO && l.g.kd == 3) {
-      if ((l.g.wout & 1) == 0)
+      if (conv0_tc_usable()) {
+        static bool attr = false;
+        if (!attr) {
+          CU_TRY(cudaFuncSetAttribute(k_conv0_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C0_SMEM));
+          attr = true;
+        }
+        k_conv0_tc<<<(unsigned)((M + TC_BM - 1) / TC_BM), TC_NT, C0_SMEM, s.st>>>(l.g, s.act[0], s.wb + l.woff,
+                                                                               s.w + l.boff, s.act[1]);
+      } else if ((l.g.wout & 1) == 0)
         k_conv_first2<<<(unsigned)((M / 2 + 127) / 128), 128, 0, s.st>>>(l.g, s.act[0], s.wb + l.woff,
                                                                         s.w + l.boff, s.act[1]);
       else
