@@ -693,7 +693,7 @@ def run_reference(args):
     tmp = tempfile.mkdtemp(prefix="irlbench_ref_")
     files = case.write_tables(tmp)
     shms = []
-    pool = None
+    pool = acc_pool = None
     try:
         for size in (vox * 4, nv * pl * 4, per * vox * 4):
             shms.append(shared_memory.SharedMemory(create=True, size=size))
@@ -728,14 +728,23 @@ def run_reference(args):
         inside = np.hypot(xx, yy) <= n / 2
         est.reshape(n, nz, n)[:] = np.where(inside[:, None, :], avg, np.float32(0.0))
         upd = np.zeros((vox,), np.float32)
+        from concurrent.futures import ThreadPoolExecutor
+        acc_pool = ThreadPoolExecutor(max_workers=procs)
+        chunks = [(vox * i // 16, vox * (i + 1) // 16) for i in range(16)]
+
+        def accumulate(s, lo, hi):
+            # the worker processes are idle meanwhile, so the ordered clamped
+            # accumulation and the EM update run on host threads, a slab each
+            u = upd[lo:hi]
+            u[:] = 0.0
+            for m in range(per):
+                np.add(u, slots[m, lo:hi], out=u)
+                np.copyto(u, 0.0, where=u < 1e-5)
+            est[lo:hi] *= u * norms[s, lo:hi]
 
         def sub_iteration(s):
             pool.map(_ref_member, [(v, m) for m, v in enumerate(subset_views[s])], chunksize=1)
-            upd[:] = 0.0
-            for m in range(per):
-                np.add(upd, slots[m], out=upd)
-                upd[upd < 1e-5] = 0.0
-            est[:] *= upd * norms[s]
+            list(acc_pool.map(lambda c: accumulate(s, *c), chunks))
 
         for i in range(args.warmup):
             sub_iteration(i % ns)
@@ -752,6 +761,8 @@ def run_reference(args):
         if pool is not None:
             pool.close()
             pool.join()
+        if acc_pool is not None:
+            acc_pool.shutdown()
         for m in shms:
             m.close()
             m.unlink()

@@ -3,6 +3,13 @@
     python -m libirl_b200.surrogate.train --phantoms 200 --val 16 --steps 6000 \
         --out libirl_b200/surrogate/sur128.bin --summary sur128.json
 
+At the learned-scatter configuration's scale (3600 / 200 / 200 phantoms,
+training pairs generated in streamed chunks):
+
+    python -m libirl_b200.surrogate.train --phantoms 3600 --val 200 --test 200 \
+        --chunk 400 --steps 24000 --init libirl_b200/surrogate/sur128.bin \
+        --out libirl_b200/surrogate/sur128.bin --summary libirl_b200/surrogate/sur128_train.json
+
 Training pairs come from the library's GPU ESSE path (irlcu_sur_pairs): for
 every seeded full128 phantom (the 128^3 config-2 generator of
 libirl_b200.workloads, a different seed per phantom) and each of its 120
@@ -105,10 +112,90 @@ def nrmse(net, X, T, idx, batch):
     return np.concatenate(out)
 
 
+def _stats(e):
+    return {"mean": float(e.mean()), "median": float(np.median(e)), "p90": float(np.percentile(e, 90)),
+            "max": float(e.max()), "frac_le_1pct": float((e <= 0.01).mean()),
+            "frac_le_2pct": float((e <= 0.02).mean())}
+
+
+def train_streaming(args, lib):
+    """Training at the scale of the learned-scatter configuration: 3600
+    training, 200 validation and 200 test phantoms (seeds seed0 + i, split
+    by seed), 120 views each.  The training phantoms' pairs are generated
+    in chunks of --chunk phantoms and each chunk gets its share of the
+    steps (the phantoms are independent draws, so this is streaming SGD
+    over every training phantom without holding all 432,000 views);
+    validation and test pairs stay resident."""
+    import torch
+    ntr, nval, nte = args.phantoms, args.val, args.test
+    val_seeds = [args.seed0 + ntr + i for i in range(nval)]
+    te_seeds = [args.seed0 + ntr + nval + i for i in range(nte)]
+    t0 = time.time()
+    Xv, Tv, _ = generate(lib, val_seeds, workers=args.workers)
+    Xt, Tt, _ = generate(lib, te_seeds, workers=args.workers)
+    t_gen = time.time() - t0
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234)
+    net = SU.Network(lib, args.batch, seed=17)
+    if args.init:
+        net.set_weights(SU.load_weights(args.init))
+    curve, val_curve = [], []
+    step, t_train = 0, 0.0
+    nchunks = (ntr + args.chunk - 1) // args.chunk
+    for ci in range(nchunks):
+        seeds = [args.seed0 + i for i in range(ci * args.chunk, min(ntr, (ci + 1) * args.chunk))]
+        t = time.time()
+        X, T, _ = generate(lib, seeds, workers=args.workers)
+        t_gen += time.time() - t
+        n = X.shape[0]
+        stop = args.steps * (ci + 1) // nchunks
+        t = time.time()
+        while step < stop:
+            warm = min(1.0, (step + 1) / 200.0)
+            lr = args.lr * warm * (0.02 + 0.98 * 0.5 * (1.0 + math.cos(math.pi * step / args.steps)))
+            idx = torch.randint(0, n, (args.batch,), device="cuda", generator=g)
+            xb = X.index_select(0, idx).contiguous()
+            tb = T.index_select(0, idx).contiguous()
+            torch.cuda.synchronize()
+            loss = net.train_step(args.batch, xb.data_ptr(), tb.data_ptr(), lr)
+            if step % 200 == 0 or step == args.steps - 1:
+                curve.append((step, loss))
+                print(f"chunk {ci} step {step} loss {loss:.4e} lr {lr:.2e}", flush=True)
+            step += 1
+        t_train += time.time() - t
+        del X, T
+        torch.cuda.empty_cache()
+        ev = nrmse(net, Xv, Tv, torch.arange(0, min(Xv.shape[0], 2400), device="cuda"), args.batch)
+        val_curve.append((step, float(ev.mean())))
+        print(f"chunk {ci}: validation NRMSE mean {ev.mean():.4f}", flush=True)
+    ev = nrmse(net, Xv, Tv, torch.arange(0, Xv.shape[0], device="cuda"), args.batch)
+    et = nrmse(net, Xt, Tt, torch.arange(0, Xt.shape[0], device="cuda"), args.batch)
+    SU.save_weights(args.out, net.get_weights())
+    summ = {
+        "phantoms": ntr, "val_phantoms": nval, "test_phantoms": nte, "views_per_phantom": 120,
+        "training_views": ntr * 120, "chunk_phantoms": args.chunk, "steps": args.steps, "batch": args.batch,
+        "lr": args.lr, "init": args.init and os.path.basename(args.init), "seed0": args.seed0,
+        "generate_s": round(t_gen, 1), "train_s": round(t_train, 1),
+        "ms_per_step": round(1000 * t_train / max(1, args.steps), 2),
+        "loss_curve": [(s_, float(f"{l_:.4e}")) for s_, l_ in curve],
+        "val_nrmse_curve": [(s_, round(v_, 5)) for s_, v_ in val_curve],
+        "val_nrmse": _stats(ev), "test_nrmse": _stats(et),
+        "weights": os.path.relpath(args.out, ROOT) if args.out.startswith(ROOT) else args.out,
+    }
+    print(json.dumps(summ))
+    if args.summary:
+        with open(args.summary, "w") as f:
+            json.dump(summ, f, indent=1)
+    net.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--phantoms", type=int, default=200, help="training phantoms")
     ap.add_argument("--val", type=int, default=16, help="held-out phantoms")
+    ap.add_argument("--test", type=int, default=0, help="test phantoms (with --chunk)")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="generate the training pairs in chunks of this many phantoms (streaming)")
     ap.add_argument("--seed0", type=int, default=40000)
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=32)
@@ -122,6 +209,8 @@ def main(argv=None):
     import torch
     import libirl_b200 as L
     lib = L.load()
+    if args.chunk > 0:
+        return train_streaming(args, lib)
     t0 = time.time()
     seeds = [args.seed0 + i for i in range(args.phantoms + args.val)]
     X, T, _ = generate(lib, seeds, workers=args.workers)
