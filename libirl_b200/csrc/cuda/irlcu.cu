@@ -173,8 +173,6 @@ static void free_ctx(Ctx *c) {
   dfree(c->rot.col_f2);
   dfree(c->rot.sn);
   dfree(c->rot.cs);
-  dfree(c->rot.col_rng);
-  dfree(c->rot.row_rng);
   dfree(c->sup_start);
   dfree(c->sup_end);
   dfree(c->est);
@@ -207,8 +205,7 @@ static void free_ctx(Ctx *c) {
   free_rotate_scratch(*c);
   for (int k = 0; k < 2; ++k) {
     if (c->snap_copied[k]) cudaEventSynchronize(c->snap_copied[k]);
-    dfree(c->snap[k]);
-    if (c->snap_host[k]) cudaFreeHost(c->snap_host[k]);
+    dfree(c->snap[k]);  // snap_host[k] belongs to the process-wide pinned pair
     if (c->snap_made[k]) cudaEventDestroy(c->snap_made[k]);
     if (c->snap_copied[k]) cudaEventDestroy(c->snap_copied[k]);
   }
@@ -279,8 +276,6 @@ int irlcu_init(const irlcu_geom *g) {
   TRY(dalloc(&c->rot.col_f2, (size_t)2 * n * R));
   TRY(dalloc(&c->rot.sn, (size_t)R));
   TRY(dalloc(&c->rot.cs, (size_t)R));
-  TRY(dalloc(&c->rot.col_rng, (size_t)2 * n * R));
-  TRY(dalloc(&c->rot.row_rng, (size_t)n * R));
   TRY(dalloc(&c->sup_start, (size_t)n));
   TRY(dalloc(&c->sup_end, (size_t)n));
   {
@@ -352,7 +347,6 @@ int irlcu_set_angles(const float *angles) {
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
-  TRY(launch_shear_ranges(c, 0, R));
   return IRLCU_OK;
 }
 
@@ -555,18 +549,34 @@ int irlcu_download_external(int buf, float *host) {
 // after the iteration's kernels, then copied to pinned host memory on a
 // stream of its own, so that the next iteration's kernels (queued by the
 // host meanwhile) run during the copy and the callback.
+// The pinned host pair is kept for the process and reused by every later
+// context (pinning 2 x 8 MB takes milliseconds, more than a short
+// reconstruction's callbacks save).  Only the session with a callback uses
+// it, one at a time, and a context waits for its copies before it ends.
+static float *g_pin[2] = {nullptr, nullptr};
+static size_t g_pin_cap = 0;
+
 int irlcu_snapshot_begin(int slot) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
   if (slot < 0 || slot > 1) return set_error(IRLCU_EARG, "snapshot slot %d", slot);
   if (!c.est) return set_error(IRLCU_ESTATE, "no estimate to snapshot");
   if (!c.snap_st) CU_TRY(cudaStreamCreateWithFlags(&c.snap_st, cudaStreamNonBlocking));
+  if (g_pin_cap < c.vox) {
+    for (int k = 0; k < 2; ++k) {
+      if (g_pin[k]) CU_TRY(cudaFreeHost(g_pin[k]));
+      g_pin[k] = nullptr;
+    }
+    g_pin_cap = 0;
+    for (int k = 0; k < 2; ++k) CU_TRY(cudaMallocHost(&g_pin[k], c.vox * sizeof(float)));
+    g_pin_cap = c.vox;
+  }
   if (!c.snap[slot]) {
     TRY(dalloc(&c.snap[slot], c.vox));
-    CU_TRY(cudaMallocHost(&c.snap_host[slot], c.vox * sizeof(float)));
     CU_TRY(cudaEventCreateWithFlags(&c.snap_made[slot], cudaEventDisableTiming));
     CU_TRY(cudaEventCreateWithFlags(&c.snap_copied[slot], cudaEventDisableTiming));
   }
+  c.snap_host[slot] = g_pin[slot];
   k_to_external<<<592, 256, 0, c.st>>>(c.est, c.snap[slot], c.n, c.nz);
   CU_LAUNCHED();
   CU_TRY(cudaEventRecord(c.snap_made[slot], c.st));
@@ -1057,7 +1067,6 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2 + (size_t)r * 2 * n, cf2.data(), 2 * n * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn + r, &sn, 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs + r, &cs, 4, cudaMemcpyHostToDevice, alloc_stream()));
-  TRY(launch_shear_ranges(c, r, 1));
   int zero = 0;
   TRY(upload_views(&zero, 1, nullptr));
   const float *s = src;

@@ -24,11 +24,6 @@ struct RotTabs {
   int *col_sh;
   float *col_f1, *col_f2;
   float *sn, *cs;
-  // the parts of the three-shear intermediates the output needs
-  // (launch_shear_ranges): per column c < mdim, lo | hi << 16, the rows
-  // whose y-sheared value pass 3 reads; per row, the columns of X pass 2
-  // reads (lo > hi: none).  Null where a kernel does not use them.
-  int *col_rng, *row_rng;
 };
 
 // Fourier-domain form of a DRF table (k_drf_fft.cu): planes on an Mz x Mx
@@ -205,10 +200,6 @@ extern long long g_launch_count;
 // rotation of nv volumes: dst[v] = rotate(src[v or shared], tab rot_base+views[v])
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
                   size_t dst_stride, const int *dviews, int nv, int rot_base);
-
-// needed-range tables (RotTabs::col_rng / row_rng) of rotations
-// [r0, r0 + count), from their headers and shift tables
-int launch_shear_ranges(const Ctx &c, int r0, int count);
 
 // three-shear rotation of one device volume with every buffer in a static
 // device array (irlcu_rotate_volume_noalloc); enqueued on `st`

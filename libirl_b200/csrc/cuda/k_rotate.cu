@@ -272,11 +272,6 @@ __global__ void __launch_bounds__(SH_TX *SH_TY) k_shear_smem(const float *__rest
 //     from the next lane;
 //   flipped (columns): a lane per j (consecutive columns of the source),
 //     walking a quarter of the i range with the tap carried along.
-// packed [lo, hi] ranges of the needed-range tables (k_shear_ranges below)
-constexpr int RNG_EMPTY = 0xFFFF;  // lo = 0xFFFF, hi = 0
-__device__ __forceinline__ int rng_lo(int v) { return v & 0xFFFF; }
-__device__ __forceinline__ int rng_hi(int v) { return v >> 16; }
-
 __device__ __forceinline__ int shear_tap(const RotHdr &h, int n, int sh, int i) {
   return h.b180 ? n - i - (sh - h.iadd + 1) : i + sh - h.iadd;
 }
@@ -305,25 +300,21 @@ __device__ __forceinline__ ShearRow shear_row(const RotHdr &h, int n, int j, con
   return r;
 }
 
-// X row j is computed at the columns [lo, hi] of its needed range (t_rrng)
 __device__ __forceinline__ void shear_pass1_rows(const float *__restrict__ s, int rs, float *s_x, int xld, int n,
                                                  const RotHdr &h, const int *t_rsh, const float *t_rf1,
-                                                 const float *t_rf2, const int *t_st, const int *t_en,
-                                                 const int *t_rrng, int warp, int lane) {
+                                                 const float *t_rf2, const int *t_st, const int *t_en, int warp,
+                                                 int lane) {
   for (int j = warp; j < n; j += SH_TY) {
-    const int clo = rng_lo(t_rrng[j]), chi = rng_hi(t_rrng[j]);
-    if (clo > chi) continue;
     const ShearRow r = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
     const float *line = s + (h.b180 ? n - j - 1 : j) * rs + r.c0;  // tap(i) at line[dir i]
     float *xr = s_x + j * xld;
-    const int i00 = clo + lane;
-    float v = (i00 >= r.la && i00 <= r.lb) ? __ldg(line + r.dir * i00) : 0.f;
-    for (int i0 = clo; i0 <= chi; i0 += SH_TX) {
+    float v = (lane >= r.la && lane <= r.lb) ? __ldg(line + r.dir * lane) : 0.f;
+    for (int i0 = 0; i0 < h.mdim; i0 += SH_TX) {
       const int i = i0 + lane, inx = i + SH_TX;
       const float vn = (inx >= r.la && inx <= r.lb) ? __ldg(line + r.dir * inx) : 0.f;
       // second tap of i = tap(i + 1): the next lane's, lane 0's next chunk for lane 31
       const float sec = __shfl_sync(0xffffffffu, lane == 0 ? vn : v, (lane + 1) & (SH_TX - 1));
-      if (i <= chi) xr[i] = (i >= r.lo && i < r.vb) ? lerp2(r.f1, v, r.f2, sec) : 0.f;
+      if (i < h.mdim) xr[i] = (i >= r.lo && i < r.vb) ? lerp2(r.f1, v, r.f2, sec) : 0.f;
       v = vn;
     }
   }
@@ -331,21 +322,17 @@ __device__ __forceinline__ void shear_pass1_rows(const float *__restrict__ s, in
 
 __device__ __forceinline__ void shear_pass1_cols(const float *__restrict__ s, int rs, float *s_x, int xld, int n,
                                                  const RotHdr &h, const int *t_rsh, const float *t_rf1,
-                                                 const float *t_rf2, const int *t_st, const int *t_en,
-                                                 const int *t_rrng, int tid) {
+                                                 const float *t_rf2, const int *t_st, const int *t_en, int tid) {
   constexpr int NCH = 4;  // i chunks per j
   const int nt = SH_TX * SH_TY;
+  const int per = (h.mdim + NCH - 1) / NCH;
   for (int e = tid; e < n * NCH; e += nt) {
     const int ch = e / n, j = e - ch * n;
-    const int clo = rng_lo(t_rrng[j]), chi = rng_hi(t_rrng[j]);
-    if (clo > chi) continue;
-    const int per = (chi - clo + NCH) / NCH;
-    const int i0 = clo + ch * per, i1 = min(chi + 1, i0 + per);
-    if (i0 >= i1) continue;
     const ShearRow r = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
     const int step = r.dir * rs;
     const float *col = s + (h.b180 ? j : n - j - 1) + r.c0 * rs;  // tap(i) at col[i step]
     float *xc = s_x + j * xld;
+    const int i0 = ch * per, i1 = min(h.mdim, i0 + per);
     float v = (i0 >= r.la && i0 <= r.lb) ? __ldg(col + i0 * step) : 0.f;
     const float *pn = col + (i0 + 1) * step;
     for (int i = i0; i < i1; ++i, pn += step) {
@@ -369,7 +356,6 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
   float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
   int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
   float *t_cf1 = reinterpret_cast<float *>(t_csh + xld), *t_cf2 = t_cf1 + xld;
-  int *t_crng = reinterpret_cast<int *>(t_cf2 + xld), *t_rrng = t_crng + xld;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH_TY;
   const int k = blockIdx.x, v = blockIdx.y;
   const int r = rot_base + views[v];
@@ -383,19 +369,17 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
     t_rf2[i] = T.row_f2[(size_t)r * n + i];
     t_st[i] = sup_st[i];
     t_en[i] = sup_en[i];
-    t_rrng[i] = T.row_rng[(size_t)r * n + i];
   }
   for (int i = tid; i < h.mdim; i += nt) {
     t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
     t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
     t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
-    t_crng[i] = T.col_rng[(size_t)r * 2 * n + i];
   }
   __syncthreads();
   if (h.b90)
-    shear_pass1_cols(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, t_rrng, tid);
+    shear_pass1_cols(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, tid);
   else
-    shear_pass1_rows(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, t_rrng, ty, tx);
+    shear_pass1_rows(s, rs, s_x, xld, n, h, t_rsh, t_rf1, t_rf2, t_st, t_en, ty, tx);
   __syncthreads();
   // pass 2: Y[j][c] = lerp(X[j+jt][c], X[j+jt+1][c]) for jj = j + iadd in
   // [max(0, -jt), min(mdim, mdim - jt - 1)), else 0; X rows outside [0, n)
@@ -404,32 +388,26 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
   // rows already written (at or past the step's first row for jt >= 0,
   // walking down; at or before its last row for jt < 0, walking up), so
   // every load sees X.
-  // Only the rows [ja, jb] of column c that pass 3 reads (t_crng) are
-  // computed; the walk starts at the end of that range it reads away from.
   for (int c = ty; c < h.mdim; c += SH_TY) {
-    const int ja = rng_lo(t_crng[c]), jb = rng_hi(t_crng[c]);
-    if (ja > jb) continue;
     const int jt = t_csh[c];
     const float w1 = t_cf1[c], w2 = t_cf2[c];
     const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
     float *col = s_x + c;
     if (jt >= 0) {
-      for (int j0 = ja; j0 <= jb; j0 += SH_TX) {
+      for (int j0 = 0; j0 < n; j0 += SH_TX) {
         const int j = j0 + tx, r0 = j + jt;
-        const bool act = j <= jb;
-        const float x0 = (act && r0 < n) ? col[r0 * xld] : 0.f;
-        const float x1 = (act && r0 + 1 < n) ? col[(r0 + 1) * xld] : 0.f;
+        const float x0 = (j < n && r0 < n) ? col[r0 * xld] : 0.f;
+        const float x1 = (j < n && r0 + 1 < n) ? col[(r0 + 1) * xld] : 0.f;
         __syncwarp();
-        if (act) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        if (j < n) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
       }
     } else {
-      for (int j0 = jb; j0 >= ja; j0 -= SH_TX) {
+      for (int j0 = n - 1; j0 >= 0; j0 -= SH_TX) {
         const int j = j0 - tx, r0 = j + jt;
-        const bool act = j >= ja;
-        const float x0 = (act && r0 >= 0) ? col[r0 * xld] : 0.f;
-        const float x1 = (act && r0 + 1 >= 0) ? col[(r0 + 1) * xld] : 0.f;
+        const float x0 = (j >= 0 && r0 >= 0) ? col[r0 * xld] : 0.f;
+        const float x1 = (j >= 0 && r0 + 1 >= 0) ? col[(r0 + 1) * xld] : 0.f;
         __syncwarp();
-        if (act) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        if (j >= 0) col[j * xld] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
       }
     }
     __syncwarp();
@@ -453,6 +431,159 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
       y = yn;
     }
   }
+}
+
+// Two-slice form of the column-walk shear: one CTA of 32 x SH2_TY threads
+// rotates the adjacent slices k0 = 2 blockIdx.x and k0 + 1 of one view.
+// Both slices use the same rotation, so every shift, weight, bound and
+// address is computed once for the pair: the intermediate image holds
+// float2 pairs (slice k0, slice k0 + 1), each shared-memory access moves
+// both values, and only the loads, shuffles, products and global stores are
+// per slice.  The passes and every rounding are those of k_shear_cw, so the
+// output is the same bit for bit.  For an odd slice count the last CTA has
+// one slice; its second lane reads nothing and stores nothing.
+constexpr int SH2_TY = 32;
+
+__global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__restrict__ src, size_t src_stride,
+                                                               float *__restrict__ dst, size_t dst_stride,
+                                                               const int *__restrict__ views, int rot_base,
+                                                               RotTabs T, const int *__restrict__ sup_st,
+                                                               const int *__restrict__ sup_en, int n, int nz,
+                                                               int xld) {
+  extern __shared__ float sm[];
+  float2 *s_x = reinterpret_cast<float2 *>(sm);  // n * xld pairs
+  int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xld);
+  int *t_st = t_rsh + n, *t_en = t_st + n;
+  float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
+  int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
+  float *t_cf1 = reinterpret_cast<float *>(t_csh + xld), *t_cf2 = t_cf1 + xld;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH2_TY;
+  const int k0 = 2 * blockIdx.x, v = blockIdx.y;
+  const bool two = k0 + 1 < nz;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  const float *s = src + (size_t)v * src_stride + (size_t)k0 * n;  // slice k0 + 1 at s + n
+  float *d = dst + (size_t)v * dst_stride + (size_t)k0 * n;
+  const int rs = nz * n;
+  for (int i = tid; i < n; i += nt) {
+    t_rsh[i] = T.row_sh[(size_t)r * n + i];
+    t_rf1[i] = T.row_f1[(size_t)r * n + i];
+    t_rf2[i] = T.row_f2[(size_t)r * n + i];
+    t_st[i] = sup_st[i];
+    t_en[i] = sup_en[i];
+  }
+  for (int i = tid; i < h.mdim; i += nt) {
+    t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
+    t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
+    t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
+  }
+  __syncthreads();
+  const float2 zero2 = make_float2(0.f, 0.f);
+  if (!h.b90) {
+    // pass 1, rows: a warp per row, the second tap from the next lane
+    for (int j = ty; j < n; j += SH2_TY) {
+      const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+      const float *line = s + (h.b180 ? n - j - 1 : j) * rs + rw.c0;  // tap(i) at line[dir i]
+      float2 *xr = s_x + j * xld;
+      const bool in0 = tx >= rw.la && tx <= rw.lb;
+      float a0 = in0 ? __ldg(line + rw.dir * tx) : 0.f;
+      float a1 = (in0 && two) ? __ldg(line + rw.dir * tx + n) : 0.f;
+      for (int i0 = 0; i0 < h.mdim; i0 += SH_TX) {
+        const int i = i0 + tx, inx = i + SH_TX;
+        const bool in = inx >= rw.la && inx <= rw.lb;
+        const float *pp = line + rw.dir * inx;
+        const float b0 = in ? __ldg(pp) : 0.f, b1 = (in && two) ? __ldg(pp + n) : 0.f;
+        const float c0 = __shfl_sync(0xffffffffu, tx == 0 ? b0 : a0, (tx + 1) & (SH_TX - 1));
+        const float c1 = __shfl_sync(0xffffffffu, tx == 0 ? b1 : a1, (tx + 1) & (SH_TX - 1));
+        if (i < h.mdim)
+          xr[i] = (i >= rw.lo && i < rw.vb) ? make_float2(lerp2(rw.f1, a0, rw.f2, c0), lerp2(rw.f1, a1, rw.f2, c1))
+                                            : zero2;
+        a0 = b0;
+        a1 = b1;
+      }
+    }
+  } else {
+    // pass 1, columns (90-degree flips): a thread per (chunk, j) walks i
+    constexpr int NCH = 4;
+    const int per = (h.mdim + NCH - 1) / NCH;
+    for (int e = tid; e < n * NCH; e += nt) {
+      const int ch = e / n, j = e - ch * n;
+      const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+      const int step = rw.dir * rs;
+      const float *col = s + (h.b180 ? j : n - j - 1) + rw.c0 * rs;  // tap(i) at col[i step]
+      float2 *xc = s_x + j * xld;
+      const int i0 = ch * per, i1 = min(h.mdim, i0 + per);
+      const bool in0 = i0 >= rw.la && i0 <= rw.lb;
+      float a0 = in0 ? __ldg(col + i0 * step) : 0.f;
+      float a1 = (in0 && two) ? __ldg(col + i0 * step + n) : 0.f;
+      const float *pn = col + (i0 + 1) * step;
+      for (int i = i0; i < i1; ++i, pn += step) {
+        const bool in = i + 1 >= rw.la && i + 1 <= rw.lb;
+        const float b0 = in ? __ldg(pn) : 0.f, b1 = (in && two) ? __ldg(pn + n) : 0.f;
+        xc[i] = (i >= rw.lo && i < rw.vb) ? make_float2(lerp2(rw.f1, a0, rw.f2, b0), lerp2(rw.f1, a1, rw.f2, b1))
+                                          : zero2;
+        a0 = b0;
+        a1 = b1;
+      }
+    }
+  }
+  __syncthreads();
+  // pass 2: the y shear in place, a warp per column (see k_shear_cw)
+  for (int c = ty; c < h.mdim; c += SH2_TY) {
+    const int jt = t_csh[c];
+    const float w1 = t_cf1[c], w2 = t_cf2[c];
+    const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
+    float2 *col = s_x + c;
+    if (jt >= 0) {
+      for (int j0 = 0; j0 < n; j0 += SH_TX) {
+        const int j = j0 + tx, r0 = j + jt;
+        const float2 x0 = (j < n && r0 < n) ? col[r0 * xld] : zero2;
+        const float2 x1 = (j < n && r0 + 1 < n) ? col[(r0 + 1) * xld] : zero2;
+        __syncwarp();
+        if (j < n)
+          col[j * xld] = (j >= jlo && j < jhi) ? make_float2(lerp2(w1, x0.x, w2, x1.x), lerp2(w1, x0.y, w2, x1.y))
+                                               : zero2;
+      }
+    } else {
+      for (int j0 = n - 1; j0 >= 0; j0 -= SH_TX) {
+        const int j = j0 - tx, r0 = j + jt;
+        const float2 x0 = (j >= 0 && r0 >= 0) ? col[r0 * xld] : zero2;
+        const float2 x1 = (j >= 0 && r0 + 1 >= 0) ? col[(r0 + 1) * xld] : zero2;
+        __syncwarp();
+        if (j >= 0)
+          col[j * xld] = (j >= jlo && j < jhi) ? make_float2(lerp2(w1, x0.x, w2, x1.x), lerp2(w1, x0.y, w2, x1.y))
+                                               : zero2;
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // pass 3: the second x shear, a warp per row, the second tap from the next lane
+  for (int j = ty; j < n; j += SH2_TY) {
+    const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float2 *yr = s_x + j * xld;
+    float *orow = d + (size_t)j * rs;
+    int a = tx + off;
+    float2 y = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
+    for (int x0 = 0; x0 < n; x0 += SH_TX) {
+      const int x = x0 + tx;
+      a += SH_TX;
+      const float2 yn = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
+      const float s0 = __shfl_sync(0xffffffffu, tx == 0 ? yn.x : y.x, (tx + 1) & (SH_TX - 1));
+      const float s1 = __shfl_sync(0xffffffffu, tx == 0 ? yn.y : y.y, (tx + 1) & (SH_TX - 1));
+      if (x < n) {
+        const bool in = x >= xa && x < xb;
+        orow[x] = in ? lerp2(f1, y.x, f2, s0) : 0.f;
+        if (two) orow[x + n] = in ? lerp2(f1, y.y, f2, s1) : 0.f;
+      }
+      y = yn;
+    }
+  }
+}
+
+static size_t shear2_smem_bytes(int n, int xld) {
+  return sizeof(float2) * (size_t)n * xld + sizeof(float) * (5 * (size_t)n + 3 * (size_t)xld);
 }
 
 static size_t shear_smem_bytes(int n, int xld, bool stage) {
@@ -570,58 +701,6 @@ __global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, flo
 }
 
 
-// Needed ranges of the column-walk shear's intermediates, one CTA per
-// rotation.  Pass 3 writes output (j, x) for x in [st_j + 1, en_j - 1) from
-// y-sheared row j at columns a, a + 1 with a = x + sh_j + iadd: columns
-// [st_j + 1 + sh_j + iadd, en_j - 1 + sh_j + iadd] of row j, clipped to
-// [0, mdim).  Column c's range is the hull of the rows that read it.  Pass
-// 2 computes Y(j, c) of those rows from X rows j + jt_c and j + jt_c + 1,
-// so X row r is needed at the hull of the columns whose row range, shifted
-// by jt_c (and one more row), holds r.  Everything outside these ranges is
-// never read, so the kernel skips it and its output is unchanged.
-__global__ void k_shear_ranges(RotTabs T, const int *__restrict__ sup_st, const int *__restrict__ sup_en, int n,
-                               int r0) {
-  const int r = r0 + blockIdx.x;
-  const RotHdr h = load_hdr(T, r);
-  const int *rsh = T.row_sh + (size_t)r * n;
-  const int *csh = T.col_sh + (size_t)r * 2 * n;
-  int *crng = T.col_rng + (size_t)r * 2 * n;
-  int *rrng = T.row_rng + (size_t)r * n;
-  for (int c = threadIdx.x; c < 2 * n; c += blockDim.x) {
-    int lo = RNG_EMPTY, hi = 0;
-    if (c < h.mdim)
-      for (int j = 0; j < n; ++j) {
-        const int off = rsh[j] + h.iadd, xa = sup_st[j] + 1, xb = sup_en[j] - 1;
-        if (xa >= xb) continue;
-        if (c >= xa + off && c <= xb + off) {
-          lo = min(lo, j);
-          hi = j;
-        }
-      }
-    crng[c] = lo | (hi << 16);
-  }
-  __syncthreads();
-  for (int row = threadIdx.x; row < n; row += blockDim.x) {
-    int lo = RNG_EMPTY, hi = 0;
-    for (int c = 0; c < h.mdim; ++c) {
-      const int v = crng[c], jl = rng_lo(v), jh = rng_hi(v);
-      if (jl > jh) continue;
-      if (row >= jl + csh[c] && row <= jh + csh[c] + 1) {
-        lo = min(lo, c);
-        hi = c;
-      }
-    }
-    rrng[row] = lo | (hi << 16);
-  }
-}
-
-int launch_shear_ranges(const Ctx &c, int r0, int count) {
-  if (count <= 0) return IRLCU_OK;
-  k_shear_ranges<<<count, 256, 0, c.st>>>(c.rot, c.sup_start, c.sup_end, c.n, r0);
-  CU_LAUNCHED();
-  return IRLCU_OK;
-}
-
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
                   const int *dviews, int nv, int rot_base) {
   if (nv <= 0) return IRLCU_OK;
@@ -646,8 +725,22 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   // column-walk form unless IRLCU_SHEAR_STAGE selects the fused one; its
   // X rows get an odd stride (bank-conflict-free column walks)
   const int xo = xld | 1;
-  // + the needed-range tables of one rotation (xo + n ints)
-  const size_t smc = shear_smem_bytes(n, xo, false) + sizeof(int) * ((size_t)xo + n);
+  const size_t smc = shear_smem_bytes(n, xo, false);
+  // two slices per CTA where their pair image fits (IRLCU_SHEAR_PAIR=0
+  // keeps one slice per CTA)
+  const char *pair_env = getenv("IRLCU_SHEAR_PAIR");
+  const size_t smc2 = shear2_smem_bytes(n, xo);
+  if (!env && !(pair_env && pair_env[0] == '0') && smc2 <= (size_t)maxsm) {
+    static size_t s_cw2 = 0;
+    if (smc2 > s_cw2) {
+      CU_TRY(cudaFuncSetAttribute(k_shear_cw2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc2));
+      s_cw2 = smc2;
+    }
+    k_shear_cw2<<<dim3((nz + 1) / 2, nv), dim3(SH_TX, SH2_TY), smc2, c.st>>>(
+        src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xo);
+    CU_LAUNCHED();
+    return IRLCU_OK;
+  }
   if (!env && smc <= (size_t)maxsm) {
     static size_t s_cw = 0;
     if (smc > s_cw) {

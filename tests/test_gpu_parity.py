@@ -67,21 +67,26 @@ def gpu_osem(lib, case, files, meas, iterations=None, opts=None, parms=None, krn
 
 # ------------------------------------------------------------- rotations
 
-@pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (200, 1)])
-@pytest.mark.parametrize("fast", [1, 0, "fused"])
+@pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (128, 5), (200, 1)])
+@pytest.mark.parametrize("fast", [1, 0, "fused", "single"])
 def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     """Both rotators bit for bit against the oracle; the three-shear one in
-    its column-walk form (default) and its fused-pass form."""
+    its two-slice column-walk form (default where the slice pair fits shared
+    memory), its one-slice column-walk form and its fused-pass form."""
     import libirl_b200 as L
     if fast == "fused":
         monkeypatch.setenv("IRLCU_SHEAR_STAGE", "0")
+        fast = 1
+    if fast == "single":
+        monkeypatch.setenv("IRLCU_SHEAR_PAIR", "0")
         fast = 1
     rng = np.random.default_rng(n * 7 + nz)
     vol = rng.random((n, nz, n), dtype=np.float32)
     g = L.IrlcuGeom(n, nz, 1, fast, 1)
     L.check(product, product.irlcu_init(C.byref(g)))
     try:
-        for a in rng.uniform(-7, 7, 9).astype(np.float32):
+        angles = np.concatenate([rng.uniform(-7, 7, 9), [np.pi / 2, -np.pi / 2, np.pi, 0.0]]).astype(np.float32)
+        for a in angles:
             out = np.zeros_like(vol)
             L.check(product, product.irlcu_rotate_volume(float(a), api.fptr(vol), api.fptr(out), 0, 0))
             ref = np.zeros_like(vol)
