@@ -68,7 +68,7 @@ def gpu_osem(lib, case, files, meas, iterations=None, opts=None, parms=None, krn
 # ------------------------------------------------------------- rotations
 
 @pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (128, 5), (200, 1)])
-@pytest.mark.parametrize("fast", [1, 0, "fused", "single"])
+@pytest.mark.parametrize("fast", [1, 0, "fused", "single", "pair"])
 def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     """Both rotators bit for bit against the oracle; the three-shear one in
     its two-slice column-walk form (default where the slice pair fits shared
@@ -77,8 +77,8 @@ def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     if fast == "fused":
         monkeypatch.setenv("IRLCU_SHEAR_STAGE", "0")
         fast = 1
-    if fast == "single":
-        monkeypatch.setenv("IRLCU_SHEAR_PAIR", "0")
+    if fast in ("single", "pair"):
+        monkeypatch.setenv("IRLCU_SHEAR_PAIR", "0" if fast == "single" else "1")
         fast = 1
     rng = np.random.default_rng(n * 7 + nz)
     vol = rng.random((n, nz, n), dtype=np.float32)
@@ -248,6 +248,21 @@ def test_osem_scatter_modelling(product, orc, tmp_path, srf_iters):
     meas = W.poisson_counts(pr.genprj(), 2e5, 2200)
     got = gpu_osem(product, case, files, meas, parms={"iNumSrfIterations": srf_iters})
     want = orc.to_external(pr.osem(meas, 3, 4, srf_iters=srf_iters))
+    assert rel_l2(got, want) <= IMAGE_TOL
+
+
+@pytest.mark.parametrize("pair", ["0", "1"])
+def test_osem_shear_forms(product, orc, tmp_path, monkeypatch, pair):
+    """The one-slice and two-slice shear kernels in both of their uses, the
+    rotation of the shared estimate and the unrotation of the per-view
+    backprojections, through a whole reconstruction."""
+    monkeypatch.setenv("IRLCU_SHEAR_PAIR", pair)
+    case = W.full128(seed=2210, n=48, nz=33, nviews=8, subsets=2, iterations=2, drf_max_offs=6, with_srf=False)
+    files = case.write_tables(str(tmp_path))
+    pr = orc.Problem(case)
+    meas = W.poisson_counts(pr.genprj(), 2e5, 2210)
+    got = gpu_osem(product, case, files, meas)
+    want = orc.to_external(pr.osem(meas, 2, 4))
     assert rel_l2(got, want) <= IMAGE_TOL
 
 
