@@ -81,6 +81,10 @@ void irl_esse_free(irl_esse_host *e);
 void irl_gendrf(float col_thick, float hole_diam, float gap, float intrinsic, float max_err,
 	float bin_size, float drf_spacing, float min_dist, int ndist, int noffs, Drf_t *tab);
 
+/* the initial estimate from a precomputed irl_projection_sum */
+float *irl_initial_estimate_sum(const irl_parms *p, int contour_support, float atn_thresh,
+	const irl_view *views, float prj_sum, const float *atn, float *init);
+float irl_projection_sum(const float *prj, size_t count);
 float *irl_initial_estimate(const irl_parms *p, int contour_support, float atn_thresh,
 	const irl_view *views, const float *prj, const float *atn, float *init);
 

@@ -12,6 +12,7 @@
  * callback) + IrlOsemIterate (the iterations) + IrlOsemEnd (result copy and
  * release); the three are exported (include/irl_b200.h).
  */
+#include <pthread.h>
 #include <setjmp.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -383,18 +384,42 @@ int IrlGetScatterSurrogateNrmse(float *pfNrmse, int iNumViews)
 	return 0;
 }
 
+/* libirl's serial float sum of the projections (the initial estimate's
+   mean) runs on a helper thread while the scatter kernel and the DRF tables
+   are read and prepared; it only reads the caller's projections, which
+   nothing changes before it is joined */
+typedef struct {
+	const float *prj;
+	size_t count;
+	float sum;
+} prj_sum_job;
+
+static void *prj_sum_thread(void *arg)
+{
+	prj_sum_job *j = (prj_sum_job *)arg;
+	j->sum = irl_projection_sum(j->prj, j->count);
+	return NULL;
+}
+
 int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
 	void (*cb)(int, float *), float *scatest, float *atn, float *prj, float *recon, char *logname, char *msgname)
 {
 	jmp_buf env;
 	int err, m;
 	double t0 = now_s();
+	/* static: read after a longjmp back to the trap (the library keeps one
+	   session per process) */
+	static prj_sum_job sum_job;
+	static pthread_t sum_th;
+	static volatile int sum_running;
 	if (S.open)
 		session_close();
 	memset(&S, 0, sizeof(S));
 	S.open = 1;
 	S.hook_norm = -1;
 	if ((err = setjmp(env)) != 0) {
+		if (sum_running)
+			pthread_join(sum_th, NULL);
 		fprintf(stderr, "FATAL ERROR Trapped: err_num=%d\nErrMsg=%s\n", err, irl_last_error());
 		irl_msg(1, "aborted\n");
 		irl_untrap();
@@ -402,8 +427,18 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		return err;
 	}
 	irl_trap(&env);
+	sum_running = 0;
 	open_logs(logname, msgname, op->iMsgLevel, &S.logfp, &S.msgfp);
 	irl_setup_parms(ip, op, atn, krnl_fname, &S.p);
+	if (!op->bReconIsInitEst && prj != NULL) {
+		sum_job.prj = prj;
+		sum_job.count = (size_t)S.p.n * S.p.nz * S.p.nviews;
+		sum_job.sum = 0.0f;
+		if (pthread_create(&sum_th, NULL, prj_sum_thread, &sum_job) == 0)
+			sum_running = 1;
+		else
+			sum_job.sum = irl_projection_sum(prj, sum_job.count);
+	}
 	S.views = irl_setup_views(ip, pv);
 	if (S.p.model & MODEL_SRF) {
 		if (atn == NULL)
@@ -425,7 +460,14 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		memcpy(atn, S.tmp, sizeof(float) * S.vox);
 	}
 	if (!op->bReconIsInitEst) {
-		irl_initial_estimate(&S.p, op->bUseContourSupport, op->fAtnMapThresh, S.views, prj, atn, recon);
+		if (sum_running) {
+			pthread_join(sum_th, NULL);
+			sum_running = 0;
+		}
+		if (prj == NULL)
+			irl_fatal(IRL_E_VALUE, "IrlOsem", "no projections given");
+		irl_initial_estimate_sum(&S.p, op->bUseContourSupport, op->fAtnMapThresh, S.views, sum_job.sum, atn,
+			recon);
 	} else {
 		irl_reorder(S.p.nz, S.p.n, S.p.n, recon, S.tmp);
 		memcpy(recon, S.tmp, sizeof(float) * S.vox);

@@ -615,15 +615,31 @@ static void mask_range(size_t lo, size_t hi, void *c)
 }
 
 /* pfComputeInitialEstimate, initial_est.c:29-158 (internal layout) */
+/* libirl's float sum of all projection bins, in index order
+   (initial_est.c:89-95) */
+float irl_projection_sum(const float *prj, size_t count)
+{
+	float fSum = 0.0f;
+	size_t i;
+	for (i = 0; i < count; ++i)
+		fSum += prj[i];
+	return fSum;
+}
+
 float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const irl_view *views, const float *prj,
 	const float *atn, float *init)
 {
+	return irl_initial_estimate_sum(p, contour, thresh, views,
+		irl_projection_sum(prj, (size_t)p->n * p->nz * p->nviews), atn, init);
+}
+
+float *irl_initial_estimate_sum(const irl_parms *p, int contour, float thresh, const irl_view *views, float fSum,
+	const float *atn, float *init)
+{
 	int n = p->n, nz = p->nz, na = p->nviews, a, s, r, c2, use_map = 0;
-	size_t i, tot = (size_t)n * nz * na;
-	float fNum = (float)(n * n * nz), fAvg, fSum = 0.0f, fMapThresh = 0.0f;
+	size_t i;
+	float fNum = (float)(n * n * nz), fAvg, fMapThresh = 0.0f;
 	fNum *= M_PI / 4.0;
-	for (i = 0; i < tot; ++i)
-		fSum += prj[i];
 	fAvg = fSum / (fNum * na);
 	if (atn != NULL) {
 		fMapThresh = thresh;
