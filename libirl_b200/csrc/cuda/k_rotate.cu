@@ -465,6 +465,15 @@ __global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__r
   const float *s = src + (size_t)v * src_stride + (size_t)k0 * n;  // slice k0 + 1 at s + n
   float *d = dst + (size_t)v * dst_stride + (size_t)k0 * n;
   const int rs = nz * n;
+  // the pair's source rows (row y of both slices: 2n contiguous floats)
+  // into L2 while the tables load, so that pass 1's walks find them there
+  {
+    const int lines = (2 * n * 4 + 127) / 128, rb = two ? 2 * n * 4 : n * 4;
+    for (int e = tid; e < n * lines; e += nt) {
+      const int y = e / lines, o = (e - y * lines) * 128;
+      if (o < rb) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(s + (size_t)y * rs) + o));
+    }
+  }
   for (int i = tid; i < n; i += nt) {
     t_rsh[i] = T.row_sh[(size_t)r * n + i];
     t_rf1[i] = T.row_f1[(size_t)r * n + i];
