@@ -186,6 +186,8 @@ def run_b200(args):
     lib.irlcu_grids(grids)
     tune = (C.c_float * 2)()
     lib.irlcu_drf_tuning(tune)
+    shear_ms, shear_form = (C.c_float * 4)(), (C.c_int * 2)()
+    lib.irlcu_shear_tuning(shear_ms, shear_form)
     stream = torch.cuda.ExternalStream(lib.irlcu_stream())
     if lib.IrlOsemIterate(Wm):
         raise RuntimeError(lib.pchIrlErrorString().decode())
@@ -290,7 +292,11 @@ def run_b200(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, Poisson data)",
         "config": bench_config(world),
         "tuning": {"drf_engine": ("fourier-domain %dx%d grid" % (grids[0], grids[1])) if grids[0] else "direct",
-                   "drf_autotune_ms": {"direct": round(tune[0], 3), "fourier": round(tune[1], 3)}},
+                   "drf_autotune_ms": {"direct": round(tune[0], 3), "fourier": round(tune[1], 3)},
+                   "shear_autotune_ms": {
+                       src: {"one_slice": round(shear_ms[2 * k], 4), "two_slice": round(shear_ms[2 * k + 1], 4),
+                             "kept": "two_slice" if shear_form[k] == 1 else "one_slice"}
+                       for k, src in enumerate(("shared_source_rotation", "per_view_source_unrotation"))}},
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "stages_ms_per_iteration": {k: {**s, "ms": round(s["ms"] / P, 3)} for k, s in stages.items()},
         "learned_scatter": learned,

@@ -189,6 +189,13 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
 #define IRLCU_NOALLOC_MAX_N 1024
 int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz);
 
+/* The shape autotuner's last decision for the three-shear rotation (made
+   per (n, nz, batch) when a context's angles are set): ms[0..1] one- and
+   two-slice kernel time for a batch rotated from a shared source, ms[2..3]
+   the same for a batch with a source per view; form[k] = 1 where the
+   two-slice kernel was kept. */
+int irlcu_shear_tuning(float ms[4], int form[2]);
+
 /* Iteration-callback snapshots of the estimate, overlapped with the next
    iteration: irlcu_snapshot_begin(slot) queues, after the work queued so
    far, a copy of the estimate in external layout into the slot's pinned

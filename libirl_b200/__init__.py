@@ -70,6 +70,8 @@ def _declare_irlcu(lib):
     lib.irl_compute_subsets.argtypes = [I, I, C.POINTER(C.POINTER(C.c_int))]
     lib.irlcu_drf_tuning.restype = I
     lib.irlcu_drf_tuning.argtypes = [C.POINTER(C.c_float)]
+    lib.irlcu_shear_tuning.restype = I
+    lib.irlcu_shear_tuning.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_int)]
     lib.irlcu_grids.restype = I
     lib.irlcu_grids.argtypes = [C.POINTER(C.c_int)]
     lib.irlcu_stream.restype = C.c_void_p

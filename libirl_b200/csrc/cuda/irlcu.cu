@@ -309,6 +309,8 @@ void irlcu_shutdown(void) {
   g_ctx = nullptr;
 }
 
+static int shear_autotune(Ctx &c);
+
 int irlcu_set_angles(const float *angles) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
@@ -347,6 +349,94 @@ int irlcu_set_angles(const float *angles) {
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
+  if (c.g.fast_rotate) TRY(shear_autotune(c));
+  return IRLCU_OK;
+}
+
+// ------------------------------------------------------ shape autotuner
+// The three-shear rotation has two kernel shapes: one slice per CTA (two
+// CTAs per SM) and two slices per CTA (one 1024-thread CTA per SM, shared
+// index work).  Which is faster depends on where the source comes from, so
+// both are timed for each use, a batch of views rotated from one shared
+// volume (the estimate, the attenuation map) and unrotated from a volume
+// per view (the backprojections), and the faster is kept.  Decisions are
+// cached per (n, nz, batch) for the process; IRLCU_SHEAR_PAIR overrides.
+struct ShearKey {
+  int n, nz, batch;
+  bool operator==(const ShearKey &o) const { return n == o.n && nz == o.nz && batch == o.batch; }
+};
+struct ShearTune {
+  int form[2];
+  float ms[2][2];  // [source kind][one slice, two slices]
+};
+static std::vector<std::pair<ShearKey, ShearTune>> g_shear_cache;
+static ShearTune g_shear_last = {{-1, -1}, {{0.f, 0.f}, {0.f, 0.f}}};
+
+static int upload_views(const int *views, int nv, const irlcu_view_parm *vp);
+
+static int shear_autotune(Ctx &c) {
+  if (getenv("IRLCU_SHEAR_PAIR")) return IRLCU_OK;
+  const int B = std::min(c.g.max_batch, c.nv);
+  const ShearKey key{c.n, c.nz, B};
+  for (const auto &e : g_shear_cache)
+    if (e.first == key) {
+      c.shear_form[0] = e.second.form[0];
+      c.shear_form[1] = e.second.form[1];
+      g_shear_last = e.second;
+      return IRLCU_OK;
+    }
+  std::vector<int> views(B);
+  for (int i = 0; i < B; ++i) views[i] = i;
+  TRY(upload_views(views.data(), B, nullptr));
+  ShearTune t{};
+  // The timed work follows the iteration's data flow, so that each kernel
+  // meets its sources where the iteration leaves them: the rotation of a
+  // shared volume that was just written (the estimate after an update),
+  // then the unrotation of the B volumes that rotation just wrote (the
+  // backprojections).  Both shapes alternate within every repetition, so
+  // clock and cache drift affect them alike; repetition 0 is a warm-up.
+  constexpr int REPS = 4;
+  cudaEvent_t ev[REPS][2][3];
+  for (auto &r : ev)
+    for (auto &f : r)
+      for (auto &e : f) CU_TRY(cudaEventCreate(&e));
+  int rc = IRLCU_OK;
+  for (int rep = 0; rep < REPS && rc == IRLCU_OK; ++rep)
+    for (int form = 0; form < 2 && rc == IRLCU_OK; ++form) {
+      c.shear_form[0] = c.shear_form[1] = form;
+      cudaEventRecord(ev[rep][form][0], c.st);
+      rc = launch_rotate(c, c.wrot, 0, c.wbck, c.vox, c.dviews, B, 0);
+      cudaEventRecord(ev[rep][form][1], c.st);
+      if (rc == IRLCU_OK) rc = launch_rotate(c, c.wbck, c.vox, c.wrot, c.vox, c.dviews, B, c.nv);
+      cudaEventRecord(ev[rep][form][2], c.st);
+    }
+  if (rc == IRLCU_OK && cudaStreamSynchronize(c.st) != cudaSuccess) rc = set_error(IRLCU_ECUDA, "shear tuning");
+  for (int rep = 1; rep < REPS && rc == IRLCU_OK; ++rep)
+    for (int form = 0; form < 2; ++form)
+      for (int kind = 0; kind < 2; ++kind) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[rep][form][kind], ev[rep][form][kind + 1]);
+        t.ms[kind][form] += ms / (REPS - 1);
+      }
+  for (auto &r : ev)
+    for (auto &f : r)
+      for (auto &e : f) cudaEventDestroy(e);
+  if (rc != IRLCU_OK) return rc;
+  for (int kind = 0; kind < 2; ++kind) {
+    t.form[kind] = t.ms[kind][1] > 0.f && t.ms[kind][1] < t.ms[kind][0] ? 1 : 0;
+    c.shear_form[kind] = t.form[kind];
+  }
+  g_shear_cache.push_back({key, t});
+  g_shear_last = t;
+  return IRLCU_OK;
+}
+
+int irlcu_shear_tuning(float ms[4], int form[2]) {
+  for (int k = 0; k < 2; ++k) {
+    ms[2 * k] = g_shear_last.ms[k][0];
+    ms[2 * k + 1] = g_shear_last.ms[k][1];
+    form[k] = g_shear_last.form[k];
+  }
   return IRLCU_OK;
 }
 
@@ -368,8 +458,6 @@ struct TuneKey {
 };
 static std::vector<std::pair<TuneKey, bool>> g_tune_cache;
 static float g_tune_ms[2] = {0.f, 0.f};  // last timing: direct, Fourier domain
-
-static int upload_views(const int *views, int nv, const irlcu_view_parm *vp);
 
 static int time_drf(Ctx &c, const DrfDev &D, int B, float *ms) {
   for (int rep = 0; rep < 2; ++rep) {

@@ -94,6 +94,10 @@ struct Ctx {
   int n = 0, nz = 0, nv = 0;
   size_t vox = 0, pln = 0;
   int dev = -1;               // the device current at irlcu_init; c.st belongs to it
+  // three-shear kernel per source kind (0: one source shared by all views,
+  // 1: a source per view): 0 one slice per CTA, 1 two slices per CTA,
+  // -1 not tuned (launch_rotate's default); set by the shape autotuner
+  int shear_form[2] = {-1, -1};
   cudaStream_t st = nullptr;
   cudaEvent_t ev[16];
   int nsub = 0;

@@ -735,15 +735,14 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   // X rows get an odd stride (bank-conflict-free column walks)
   const int xo = xld | 1;
   const size_t smc = shear_smem_bytes(n, xo, false);
-  // two slices per CTA where their pair image fits, for a source shared by
-  // all views (src_stride 0: the estimate, read from L2).  Measured on the
-  // 128^3 subset: 118 against 133 us there; for per-view sources streamed
-  // from DRAM (the unrotation) the one-slice form's second resident CTA
-  // hides the load latency better (150 against 164 us).
-  // IRLCU_SHEAR_PAIR = 0 / 1 forces either form.
+  // two slices per CTA where their pair image fits, as the shape autotuner
+  // decided for this kind of source (one volume shared by all views, or one
+  // per view; Ctx::shear_form), else by default.  IRLCU_SHEAR_PAIR = 0 / 1
+  // forces either form.
   const char *pair_env = getenv("IRLCU_SHEAR_PAIR");
   const size_t smc2 = shear2_smem_bytes(n, xo);
-  const bool pair = pair_env ? pair_env[0] == '1' : src_stride == 0;
+  const int kind = src_stride == 0 ? 0 : 1, tuned = c.shear_form[kind];
+  const bool pair = pair_env ? pair_env[0] == '1' : (tuned >= 0 ? tuned == 1 : true);
   if (!env && pair && smc2 <= (size_t)maxsm) {
     static size_t s_cw2 = 0;
     if (smc2 > s_cw2) {

@@ -127,3 +127,32 @@ def test_drf_autotuner_keeps_the_faster_engine(product, tmp_path, monkeypatch):
         product.IrlOsemEnd(None)
     assert ms[0] > 0 and ms[1] > 0
     assert (grids[0] > 0) == (ms[1] < ms[0]), (list(grids), list(ms))
+
+
+def test_shear_autotuner_keeps_the_faster_kernel(product, orc, tmp_path, monkeypatch):
+    """The shape autotuner times the one- and two-slice shear kernels for a
+    shared source and for per-view sources when a context's angles are set,
+    keeps the faster of each, and the reconstruction with the kept kernels
+    still matches the oracle."""
+    monkeypatch.delenv("IRLCU_SHEAR_PAIR", raising=False)
+    # a geometry no other test uses, so the decision is measured here
+    case = W.full128(seed=3601, n=72, nz=40, nviews=8, subsets=2, iterations=2, drf_max_offs=5, with_srf=False)
+    files = case.write_tables(str(tmp_path))
+    pr = orc.Problem(case)
+    meas = W.poisson_counts(pr.genprj(), 1e5, 3601)
+    p, o, v = case.parms(), case.options(), case.views()
+    atn, prj, rec = case.atn.copy(), meas.copy(), np.zeros_like(case.act)
+    rc = product.IrlOsemBegin(C.byref(p), C.byref(o), v, dup(files["drf"]), None, api.ITER_CB(), None,
+                              api.fptr(atn), api.fptr(prj), api.fptr(rec), None, None)
+    assert rc == 0, product.pchIrlErrorString()
+    try:
+        ms, form = (C.c_float * 4)(), (C.c_int * 2)()
+        assert product.irlcu_shear_tuning(ms, form) == 0
+        assert product.IrlOsemIterate(case.iterations) == 0, product.pchIrlErrorString()
+    finally:
+        assert product.IrlOsemEnd(api.fptr(rec)) == 0
+    assert all(m > 0 for m in ms), list(ms)
+    for k in range(2):
+        assert form[k] == (1 if ms[2 * k + 1] < ms[2 * k] else 0), (list(ms), list(form))
+    want = orc.to_external(pr.osem(meas, case.iterations, case.nviews // case.subsets))
+    assert float(np.linalg.norm(rec - want) / np.linalg.norm(want)) <= 1e-3
