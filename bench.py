@@ -186,8 +186,6 @@ def run_b200(args):
     lib.irlcu_grids(grids)
     tune = (C.c_float * 2)()
     lib.irlcu_drf_tuning(tune)
-    shear_ms, shear_form = (C.c_float * 4)(), (C.c_int * 2)()
-    lib.irlcu_shear_tuning(shear_ms, shear_form)
     stream = torch.cuda.ExternalStream(lib.irlcu_stream())
     if lib.IrlOsemIterate(Wm):
         raise RuntimeError(lib.pchIrlErrorString().decode())
@@ -209,6 +207,10 @@ def run_b200(args):
     if failed:
         raise RuntimeError("another rank's timed iterations failed")
     ms_step = ms_total / K
+
+    # the shape autotuner decided during the warm-up iterations
+    shear_ms, shear_form = (C.c_float * 4)(), (C.c_int * 2)()
+    lib.irlcu_shear_tuning(shear_ms, shear_form)
 
     # --- stage profile over one more iteration (separate from the timing)
     lib.irlcu_profile_enable(1)

@@ -189,12 +189,19 @@ int irlcu_rotate_volume(float angle, const float *src, float *dst, int pb_flag, 
 #define IRLCU_NOALLOC_MAX_N 1024
 int irlcu_rotate_volume_noalloc(float angle, const float *src, float *dst, int n, int nz);
 
-/* The shape autotuner's last decision for the three-shear rotation (made
-   per (n, nz, batch) when a context's angles are set): ms[0..1] one- and
-   two-slice kernel time for a batch rotated from a shared source, ms[2..3]
-   the same for a batch with a source per view; form[k] = 1 where the
-   two-slice kernel was kept. */
+/* The shape autotuner's last decision for the three-shear rotation, made
+   from a context's first two whole iterations (irlcu_osem_iteration runs
+   the first with the one-slice and the second with the two-slice kernel,
+   timing every rotation launch) and cached per (n, nz, batch) for the
+   process: ms[0..1] one- and two-slice time per iteration of the rotations
+   from the shared estimate, ms[2..3] the same for the unrotations of the
+   per-view backprojections; form[k] = 1 where the two-slice kernel was
+   kept. */
 int irlcu_shear_tuning(float ms[4], int form[2]);
+/* Switches the trial iterations on or off (default on; IrlOsemBatch turns
+   them off so that the host never waits for the device between problems);
+   returns the previous setting. */
+int irlcu_shape_trials(int on);
 
 /* Iteration-callback snapshots of the estimate, overlapped with the next
    iteration: irlcu_snapshot_begin(slot) queues, after the work queued so

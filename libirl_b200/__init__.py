@@ -72,6 +72,8 @@ def _declare_irlcu(lib):
     lib.irlcu_drf_tuning.argtypes = [C.POINTER(C.c_float)]
     lib.irlcu_shear_tuning.restype = I
     lib.irlcu_shear_tuning.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_int)]
+    lib.irlcu_shape_trials.restype = I
+    lib.irlcu_shape_trials.argtypes = [I]
     lib.irlcu_grids.restype = I
     lib.irlcu_grids.argtypes = [C.POINTER(C.c_int)]
     lib.irlcu_stream.restype = C.c_void_p

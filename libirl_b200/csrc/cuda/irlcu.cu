@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <vector>
 
 #include "irlcu_internal.cuh"
@@ -210,6 +211,11 @@ static void free_ctx(Ctx *c) {
     if (c->snap_copied[k]) cudaEventDestroy(c->snap_copied[k]);
   }
   if (c->snap_st) cudaStreamDestroy(c->snap_st);
+  for (auto &v : c->trial_ev)
+    for (auto &e : v) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
   for (auto &e : c->ev) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -309,8 +315,6 @@ void irlcu_shutdown(void) {
   g_ctx = nullptr;
 }
 
-static int shear_autotune(Ctx &c);
-
 int irlcu_set_angles(const float *angles) {
   TRY(need_ctx());
   Ctx &c = *g_ctx;
@@ -349,93 +353,97 @@ int irlcu_set_angles(const float *angles) {
   CU_TRY(cudaMemcpyAsync(c.rot.col_f2, cf2.data(), cf2.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.sn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
   CU_TRY(cudaMemcpyAsync(c.rot.cs, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, alloc_stream()));
-  if (c.g.fast_rotate) TRY(shear_autotune(c));
   return IRLCU_OK;
 }
 
 // ------------------------------------------------------ shape autotuner
 // The three-shear rotation has two kernel shapes: one slice per CTA (two
 // CTAs per SM) and two slices per CTA (one 1024-thread CTA per SM, shared
-// index work).  Which is faster depends on where the source comes from, so
-// both are timed for each use, a batch of views rotated from one shared
-// volume (the estimate, the attenuation map) and unrotated from a volume
-// per view (the backprojections), and the faster is kept.  Decisions are
-// cached per (n, nz, batch) for the process; IRLCU_SHEAR_PAIR overrides.
+// index work).  Which is faster depends on where a launch finds its
+// source and on what runs around it, which a stand-alone timing at set-up
+// did not reproduce.  So the shapes are tried on the real work: the first
+// two whole iterations of a context (irlcu_osem_iteration) run eagerly, the
+// first with the one-slice and the second with the two-slice kernel, every
+// rotation launch timed with events, per source kind (one volume shared by
+// all views: the estimate; a volume per view: the backprojections).  From
+// the third iteration on, each kind keeps the shape with the smaller total,
+// before any iteration is captured into a graph.  Both shapes give the
+// same bits, so the trial iterations are ordinary iterations.
+// IRLCU_SHEAR_PAIR = 0 / 1 skips the trial and forces a shape.
+static float g_shear_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+static int g_shear_form[2] = {-1, -1};
+static bool g_shape_trials = true;  // off inside IrlOsemBatch (no host waits)
 struct ShearKey {
   int n, nz, batch;
   bool operator==(const ShearKey &o) const { return n == o.n && nz == o.nz && batch == o.batch; }
 };
-struct ShearTune {
-  int form[2];
-  float ms[2][2];  // [source kind][one slice, two slices]
-};
-static std::vector<std::pair<ShearKey, ShearTune>> g_shear_cache;
-static ShearTune g_shear_last = {{-1, -1}, {{0.f, 0.f}, {0.f, 0.f}}};
+static std::vector<std::pair<ShearKey, std::array<int, 2>>> g_shear_cache;  // per geometry, for the process
 
-static int upload_views(const int *views, int nv, const irlcu_view_parm *vp);
-
-static int shear_autotune(Ctx &c) {
-  if (getenv("IRLCU_SHEAR_PAIR")) return IRLCU_OK;
-  const int B = std::min(c.g.max_batch, c.nv);
-  const ShearKey key{c.n, c.nz, B};
-  for (const auto &e : g_shear_cache)
-    if (e.first == key) {
-      c.shear_form[0] = e.second.form[0];
-      c.shear_form[1] = e.second.form[1];
-      g_shear_last = e.second;
-      return IRLCU_OK;
-    }
-  std::vector<int> views(B);
-  for (int i = 0; i < B; ++i) views[i] = i;
-  TRY(upload_views(views.data(), B, nullptr));
-  ShearTune t{};
-  // The timed work follows the iteration's data flow, so that each kernel
-  // meets its sources where the iteration leaves them: the rotation of a
-  // shared volume that was just written (the estimate after an update),
-  // then the unrotation of the B volumes that rotation just wrote (the
-  // backprojections).  Both shapes alternate within every repetition, so
-  // clock and cache drift affect them alike; repetition 0 is a warm-up.
-  constexpr int REPS = 4;
-  cudaEvent_t ev[REPS][2][3];
-  for (auto &r : ev)
-    for (auto &f : r)
-      for (auto &e : f) CU_TRY(cudaEventCreate(&e));
-  int rc = IRLCU_OK;
-  for (int rep = 0; rep < REPS && rc == IRLCU_OK; ++rep)
-    for (int form = 0; form < 2 && rc == IRLCU_OK; ++form) {
-      c.shear_form[0] = c.shear_form[1] = form;
-      cudaEventRecord(ev[rep][form][0], c.st);
-      rc = launch_rotate(c, c.wrot, 0, c.wbck, c.vox, c.dviews, B, 0);
-      cudaEventRecord(ev[rep][form][1], c.st);
-      if (rc == IRLCU_OK) rc = launch_rotate(c, c.wbck, c.vox, c.wrot, c.vox, c.dviews, B, c.nv);
-      cudaEventRecord(ev[rep][form][2], c.st);
-    }
-  if (rc == IRLCU_OK && cudaStreamSynchronize(c.st) != cudaSuccess) rc = set_error(IRLCU_ECUDA, "shear tuning");
-  for (int rep = 1; rep < REPS && rc == IRLCU_OK; ++rep)
-    for (int form = 0; form < 2; ++form)
-      for (int kind = 0; kind < 2; ++kind) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev[rep][form][kind], ev[rep][form][kind + 1]);
-        t.ms[kind][form] += ms / (REPS - 1);
-      }
-  for (auto &r : ev)
-    for (auto &f : r)
-      for (auto &e : f) cudaEventDestroy(e);
-  if (rc != IRLCU_OK) return rc;
+// sums the finished trial iteration's launch times into trial_ms[.][form]
+static int shear_trial_collect(Ctx &c, int form) {
   for (int kind = 0; kind < 2; ++kind) {
-    t.form[kind] = t.ms[kind][1] > 0.f && t.ms[kind][1] < t.ms[kind][0] ? 1 : 0;
-    c.shear_form[kind] = t.form[kind];
+    float tot = 0.f;
+    for (auto &e : c.trial_ev[kind]) {
+      float ms = 0.f;
+      if (cudaEventSynchronize(e.second) == cudaSuccess && cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess)
+        tot += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    c.trial_ev[kind].clear();
+    c.trial_ms[kind][form] = tot;
   }
-  g_shear_cache.push_back({key, t});
-  g_shear_last = t;
   return IRLCU_OK;
+}
+
+// advances the trial before iteration launches; returns true while the
+// coming iteration is a trial iteration (to be run eagerly)
+static bool shear_trial_step(Ctx &c) {
+  if (!c.g.fast_rotate || c.shear_trial >= 3 || getenv("IRLCU_SHEAR_PAIR")) return false;
+  const ShearKey key{c.n, c.nz, std::min(c.g.max_batch, c.nv)};
+  if (c.shear_trial == 0) {
+    for (const auto &e : g_shear_cache)
+      if (e.first == key) {
+        c.shear_form[0] = e.second[0];
+        c.shear_form[1] = e.second[1];
+        c.shear_trial = 3;
+        return false;
+      }
+    if (!g_shape_trials) return false;
+    c.trial_form = 0;
+    c.shear_trial = 1;
+    return true;
+  }
+  shear_trial_collect(c, c.trial_form);
+  if (c.shear_trial == 1) {
+    c.trial_form = 1;
+    c.shear_trial = 2;
+    return true;
+  }
+  c.trial_form = -1;
+  c.shear_trial = 3;
+  for (int kind = 0; kind < 2; ++kind) {
+    const float one = c.trial_ms[kind][0], two = c.trial_ms[kind][1];
+    c.shear_form[kind] = (two > 0.f && two < one) ? 1 : 0;
+    g_shear_ms[kind][0] = one;
+    g_shear_ms[kind][1] = two;
+    g_shear_form[kind] = c.shear_form[kind];
+  }
+  g_shear_cache.push_back({key, {c.shear_form[0], c.shear_form[1]}});
+  return false;
+}
+
+int irlcu_shape_trials(int on) {
+  const int prev = g_shape_trials ? 1 : 0;
+  g_shape_trials = on != 0;
+  return prev;
 }
 
 int irlcu_shear_tuning(float ms[4], int form[2]) {
   for (int k = 0; k < 2; ++k) {
-    ms[2 * k] = g_shear_last.ms[k][0];
-    ms[2 * k + 1] = g_shear_last.ms[k][1];
-    form[k] = g_shear_last.form[k];
+    ms[2 * k] = g_shear_ms[k][0];
+    ms[2 * k + 1] = g_shear_ms[k][1];
+    form[k] = g_shear_form[k];
   }
   return IRLCU_OK;
 }
@@ -458,6 +466,8 @@ struct TuneKey {
 };
 static std::vector<std::pair<TuneKey, bool>> g_tune_cache;
 static float g_tune_ms[2] = {0.f, 0.f};  // last timing: direct, Fourier domain
+
+static int upload_views(const int *views, int nv, const irlcu_view_parm *vp);
 
 static int time_drf(Ctx &c, const DrfDev &D, int B, float *ms) {
   for (int rep = 0; rep < 2; ++rep) {
@@ -937,6 +947,12 @@ int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mod
   // stage profiling needs the eager launches (events around every stage)
   if (g_prof_on) return run_subsets(c, model, bck_model, use_scatest, scat_mode);
   const int key = (model & 15) | (bck_model & 15) << 4 | (use_scatest ? 1 : 0) << 8 | scat_mode << 9;
+  if (shear_trial_step(c)) {  // a shape-autotuner trial iteration: eager, its rotations timed
+    bool seen = false;
+    for (int k : c.graph_seen) seen |= k == key;
+    if (!seen) c.graph_seen.push_back(key);
+    return run_subsets(c, model, bck_model, use_scatest, scat_mode);
+  }
   for (const GraphRec &g : c.graphs)
     if (g.key == key) {
       CU_TRY(cudaGraphLaunch(g.exec, c.st));

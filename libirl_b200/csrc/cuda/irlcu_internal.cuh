@@ -97,7 +97,14 @@ struct Ctx {
   // three-shear kernel per source kind (0: one source shared by all views,
   // 1: a source per view): 0 one slice per CTA, 1 two slices per CTA,
   // -1 not tuned (launch_rotate's default); set by the shape autotuner
-  int shear_form[2] = {-1, -1};
+  mutable int shear_form[2] = {-1, -1};
+  // shape autotuner trial (irlcu_osem_iteration): state 0 pending, 1 and 2
+  // the trial iterations with form 0 and 1 in flight, 3 decided; while a
+  // trial iteration runs, launch_rotate times every launch (events per kind)
+  int shear_trial = 0;
+  mutable int trial_form = -1;
+  mutable std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trial_ev[2];
+  float trial_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [kind][form], ms per iteration
   cudaStream_t st = nullptr;
   cudaEvent_t ev[16];
   int nsub = 0;

@@ -591,6 +591,143 @@ __global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__r
   }
 }
 
+// Column-split form, for slices whose intermediate image does not fit
+// shared memory (n = 256: 256 x 277 floats): one CTA per (slice, view).
+// Pass 2 treats every column of X on its own, so the CTA runs passes 1 and
+// 2 for one block of columns at a time in shared memory and stores each
+// finished block of Y to a global work area (row-major, ldy per row); pass
+// 3 then reads Y's rows from there (just written, from L2).  Every value is
+// computed and rounded as in k_shear_cw, so the output is the same bit for
+// bit.  SPLIT_CB columns per block (the last may be shorter).
+constexpr int SPLIT_CB = 144;
+
+__global__ void __launch_bounds__(SH_TX *SH_TY, 1) k_shear_split(const float *__restrict__ src, size_t src_stride,
+                                                                float *__restrict__ dst, size_t dst_stride,
+                                                                float *__restrict__ ywork, int ldy,
+                                                                const int *__restrict__ views, int rot_base,
+                                                                RotTabs T, const int *__restrict__ sup_st,
+                                                                const int *__restrict__ sup_en, int n, int nz) {
+  constexpr int XS = SPLIT_CB | 1;  // odd stride: conflict-free column walks
+  extern __shared__ float sm[];
+  float *s_x = sm;  // n * XS
+  int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * XS);
+  int *t_st = t_rsh + n, *t_en = t_st + n;
+  float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
+  int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
+  float *t_cf1 = reinterpret_cast<float *>(t_csh + 2 * n), *t_cf2 = t_cf1 + 2 * n;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH_TY;
+  const int k = blockIdx.x, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  const float *s = src + (size_t)v * src_stride + (size_t)k * n;
+  float *d = dst + (size_t)v * dst_stride + (size_t)k * n;
+  float *yw = ywork + ((size_t)v * nz + k) * (size_t)n * ldy;
+  const int rs = nz * n;
+  for (int i = tid; i < n; i += nt) {
+    t_rsh[i] = T.row_sh[(size_t)r * n + i];
+    t_rf1[i] = T.row_f1[(size_t)r * n + i];
+    t_rf2[i] = T.row_f2[(size_t)r * n + i];
+    t_st[i] = sup_st[i];
+    t_en[i] = sup_en[i];
+  }
+  for (int i = tid; i < h.mdim; i += nt) {
+    t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
+    t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
+    t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
+  }
+  __syncthreads();
+  for (int c0 = 0; c0 < h.mdim; c0 += SPLIT_CB) {
+    const int c1 = min(h.mdim, c0 + SPLIT_CB);
+    // pass 1 for columns [c0, c1): X[j][i] at s_x[j XS + i - c0]
+    if (!h.b90) {
+      for (int j = ty; j < n; j += SH_TY) {
+        const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+        const float *line = s + (h.b180 ? n - j - 1 : j) * rs + rw.c0;
+        float *xr = s_x + j * XS;  // column i at xr[i - c0]
+        const int i00 = c0 + tx;
+        float a = (i00 >= rw.la && i00 <= rw.lb) ? __ldg(line + rw.dir * i00) : 0.f;
+        for (int i0 = c0; i0 < c1; i0 += SH_TX) {
+          const int i = i0 + tx, inx = i + SH_TX;
+          const float b = (inx >= rw.la && inx <= rw.lb) ? __ldg(line + rw.dir * inx) : 0.f;
+          const float sec = __shfl_sync(0xffffffffu, tx == 0 ? b : a, (tx + 1) & (SH_TX - 1));
+          if (i < c1) xr[i - c0] = (i >= rw.lo && i < rw.vb) ? lerp2(rw.f1, a, rw.f2, sec) : 0.f;
+          a = b;
+        }
+      }
+    } else {
+      constexpr int NCH = 4;
+      const int per = (c1 - c0 + NCH - 1) / NCH;
+      for (int e = tid; e < n * NCH; e += nt) {
+        const int ch = e / n, j = e - ch * n;
+        const int i0 = c0 + ch * per, i1 = min(c1, i0 + per);
+        if (i0 >= i1) continue;
+        const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+        const int step = rw.dir * rs;
+        const float *col = s + (h.b180 ? j : n - j - 1) + rw.c0 * rs;
+        float *xc = s_x + j * XS;  // column i at xc[i - c0]
+        float a = (i0 >= rw.la && i0 <= rw.lb) ? __ldg(col + i0 * step) : 0.f;
+        const float *pn = col + (i0 + 1) * step;
+        for (int i = i0; i < i1; ++i, pn += step) {
+          const float b = (i + 1 >= rw.la && i + 1 <= rw.lb) ? __ldg(pn) : 0.f;
+          xc[i - c0] = (i >= rw.lo && i < rw.vb) ? lerp2(rw.f1, a, rw.f2, b) : 0.f;
+          a = b;
+        }
+      }
+    }
+    __syncthreads();
+    // pass 2 in place for the block's columns (see k_shear_cw), then Y to ywork
+    for (int c = c0 + ty; c < c1; c += SH_TY) {
+      const int jt = t_csh[c];
+      const float w1 = t_cf1[c], w2 = t_cf2[c];
+      const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
+      float *col = s_x + (c - c0);
+      if (jt >= 0) {
+        for (int j0 = 0; j0 < n; j0 += SH_TX) {
+          const int j = j0 + tx, r0 = j + jt;
+          const float x0 = (j < n && r0 < n) ? col[r0 * XS] : 0.f;
+          const float x1 = (j < n && r0 + 1 < n) ? col[(r0 + 1) * XS] : 0.f;
+          __syncwarp();
+          if (j < n) col[j * XS] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        }
+      } else {
+        for (int j0 = n - 1; j0 >= 0; j0 -= SH_TX) {
+          const int j = j0 - tx, r0 = j + jt;
+          const float x0 = (j >= 0 && r0 >= 0) ? col[r0 * XS] : 0.f;
+          const float x1 = (j >= 0 && r0 + 1 >= 0) ? col[(r0 + 1) * XS] : 0.f;
+          __syncwarp();
+          if (j >= 0) col[j * XS] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    for (int j = ty; j < n; j += SH_TY)
+      for (int c = c0 + tx; c < c1; c += SH_TX) yw[(size_t)j * ldy + c] = s_x[j * XS + (c - c0)];
+    __syncthreads();
+  }
+  // pass 3 from the Y rows in ywork (written above by this CTA)
+  for (int j = ty; j < n; j += SH_TY) {
+    const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float *yr = yw + (size_t)j * ldy;
+    float *orow = d + (size_t)j * rs;
+    int a = tx + off;
+    float y = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
+    for (int x0 = 0; x0 < n; x0 += SH_TX) {
+      const int x = x0 + tx;
+      a += SH_TX;
+      const float yn = (a >= 0 && a < h.mdim) ? yr[a] : 0.f;
+      const float sec = __shfl_sync(0xffffffffu, tx == 0 ? yn : y, (tx + 1) & (SH_TX - 1));
+      if (x < n) orow[x] = (x >= xa && x < xb) ? lerp2(f1, y, f2, sec) : 0.f;
+      y = yn;
+    }
+  }
+}
+
+static size_t shear_split_smem_bytes(int n) {
+  return sizeof(float) * ((size_t)n * (SPLIT_CB | 1) + 5 * (size_t)n + 3 * 2 * (size_t)n);
+}
+
 static size_t shear2_smem_bytes(int n, int xld) {
   return sizeof(float2) * (size_t)n * xld + sizeof(float) * (5 * (size_t)n + 3 * (size_t)xld);
 }
@@ -710,8 +847,28 @@ __global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, flo
 }
 
 
+static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
+                              const int *dviews, int nv, int rot_base);
+
+// During a shape-autotuner trial iteration every three-shear launch is
+// bracketed by events, per source kind (irlcu_osem_iteration sums them).
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
                   const int *dviews, int nv, int rot_base) {
+  const bool timed = c.trial_form >= 0 && c.g.fast_rotate && !c.capturing && nv > 0;
+  if (!timed) return launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base);
+  const int kind = src_stride == 0 ? 0 : 1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CU_TRY(cudaEventCreate(&e0));
+  CU_TRY(cudaEventCreate(&e1));
+  c.trial_ev[kind].push_back({e0, e1});
+  CU_TRY(cudaEventRecord(e0, c.st));
+  const int rc = launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base);
+  CU_TRY(cudaEventRecord(e1, c.st));
+  return rc;
+}
+
+static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
+                              const int *dviews, int nv, int rot_base) {
   if (nv <= 0) return IRLCU_OK;
   const int n = c.n, nz = c.nz;
   if (!c.g.fast_rotate) {
@@ -741,7 +898,7 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
   // forces either form.
   const char *pair_env = getenv("IRLCU_SHEAR_PAIR");
   const size_t smc2 = shear2_smem_bytes(n, xo);
-  const int kind = src_stride == 0 ? 0 : 1, tuned = c.shear_form[kind];
+  const int kind = src_stride == 0 ? 0 : 1, tuned = c.trial_form >= 0 ? c.trial_form : c.shear_form[kind];
   const bool pair = pair_env ? pair_env[0] == '1' : (tuned >= 0 ? tuned == 1 : true);
   if (!env && pair && smc2 <= (size_t)maxsm) {
     static size_t s_cw2 = 0;
@@ -786,6 +943,30 @@ int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
     else
       k_shear_smem<false><<<grid, dim3(SH_TX, SH_TY), smem, c.st>>>(src, src_stride, dst, dst_stride, dviews,
                                                                    rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xld);
+    CU_LAUNCHED();
+    return IRLCU_OK;
+  }
+  // column-split form where its block of columns fits (IRLCU_SHEAR_SPLIT=0
+  // keeps the two global-memory kernels below)
+  const char *split_env = getenv("IRLCU_SHEAR_SPLIT");
+  const size_t sms = shear_split_smem_bytes(n);
+  if (!env && !(split_env && split_env[0] == '0') && sms <= (size_t)maxsm) {
+    const size_t needy = (size_t)nv * nz * n * xld;
+    if (needy > c.xscratch_elems) {
+      dev_free(c.xscratch, c.st);
+      c.xscratch = nullptr;
+      c.xscratch_elems = 0;
+      CU_TRY(dev_alloc_t(&c.xscratch, needy, c.st));
+      c.xscratch_elems = needy;
+    }
+    static size_t s_split = 0;
+    if (sms > s_split) {
+      CU_TRY(cudaFuncSetAttribute(k_shear_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+      s_split = sms;
+    }
+    k_shear_split<<<dim3(nz, nv), dim3(SH_TX, SH_TY), sms, c.st>>>(src, src_stride, dst, dst_stride, c.xscratch,
+                                                                   xld, dviews, rot_base, c.rot, c.sup_start,
+                                                                   c.sup_end, n, nz);
     CU_LAUNCHED();
     return IRLCU_OK;
   }

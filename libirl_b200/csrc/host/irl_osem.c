@@ -731,7 +731,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 {
 	jmp_buf env;
 	parked_session **h = NULL;
-	int p, m, err = 0;
+	int p, m, err = 0, trials = 1;
 	if ((err = setjmp(env)) != 0) {
 		irl_untrap();
 		return err;
@@ -749,6 +749,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 		irl_fatal(IRL_E_VALUE, "IrlOsemBatch", "an IrlOsemBegin session is open");
 	h = (parked_session **)irl_calloc(sizeof(parked_session *) * nprob, "batch sessions");
 	irl_untrap();
+	trials = irlcu_shape_trials(0);  /* no host waits inside the pipelined batch */
 	/* pipelined: problem p is set up and all its iterations are enqueued
 	   (asynchronous device work on its own stream); the host then sets up
 	   p + 1 while the device runs p, and ends p - 1 */
@@ -781,6 +782,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 			err = e;
 	}
 	free(h);
+	irlcu_shape_trials(trials);
 	return err;
 }
 

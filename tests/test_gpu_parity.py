@@ -67,18 +67,22 @@ def gpu_osem(lib, case, files, meas, iterations=None, opts=None, parms=None, krn
 
 # ------------------------------------------------------------- rotations
 
-@pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (128, 5), (200, 1)])
-@pytest.mark.parametrize("fast", [1, 0, "fused", "single", "pair"])
+@pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (128, 5), (200, 1), (256, 2)])
+@pytest.mark.parametrize("fast", [1, 0, "fused", "single", "pair", "global"])
 def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     """Both rotators bit for bit against the oracle; the three-shear one in
-    its two-slice column-walk form (default where the slice pair fits shared
-    memory), its one-slice column-walk form and its fused-pass form."""
+    its two-slice and one-slice column-walk forms, its fused-pass form, and
+    for slices beyond shared memory (n = 256) its column-split form
+    (default) and its global-memory form."""
     import libirl_b200 as L
     if fast == "fused":
         monkeypatch.setenv("IRLCU_SHEAR_STAGE", "0")
         fast = 1
     if fast in ("single", "pair"):
         monkeypatch.setenv("IRLCU_SHEAR_PAIR", "0" if fast == "single" else "1")
+        fast = 1
+    if fast == "global":  # slices beyond shared memory: the two global-memory kernels, not the column split
+        monkeypatch.setenv("IRLCU_SHEAR_SPLIT", "0")
         fast = 1
     rng = np.random.default_rng(n * 7 + nz)
     vol = rng.random((n, nz, n), dtype=np.float32)
