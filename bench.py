@@ -877,6 +877,73 @@ def run_batch32(args):
         "data": "synthetic (seeded phantoms, Poisson data)"}
 
 
+def _recon256(lib, case, files, meas, iterations, srf_iters=None):
+    from libirl_b200 import api
+    p, o, v = case.parms(), case.options(), case.views()
+    o.bFFTConvolve = 1
+    p.NumIterations = iterations
+    p.iNumSrfIterations = iterations if srf_iters is None else srf_iters
+    atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+    rc = lib.IrlOsem(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(), None,
+                     api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+    if rc:
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    return rec
+
+
+def large256_learned(lib, case, files, meas, K, Wm, esse_ms, torch):
+    """The 256^3 photopeak window with the learned scatter surrogate trained
+    on 256^3 phantoms (libirl_b200/surrogate/sur256.bin): device time per
+    iteration after the first (ESSE) iteration, and the image NRMSE of the
+    8-iteration reconstruction against the ESSE one and without scatter."""
+    from libirl_b200 import api
+    from libirl_b200 import surrogate as SU
+    if not os.path.exists(SU.WEIGHTS_256):
+        return {"unavailable": "no trained 256^3 weights (libirl_b200/surrogate/sur256.bin)"}
+    lib.IrlSetScatterSurrogate(SU.WEIGHTS_256.encode(), 0.02)
+    try:
+        p, o, v = case.parms(), case.options(), case.views()
+        o.bFFTConvolve = 1
+        p.NumIterations = 1 + Wm + K
+        p.iNumSrfIterations = p.NumIterations
+        atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+        rc = lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(),
+                              None, api.fptr(atn), api.fptr(m), api.fptr(rec), None, None)
+        if rc:
+            raise RuntimeError(lib.pchIrlErrorString().decode())
+        try:
+            lib.IrlOsemIterate(1 + Wm)
+            nr = np.zeros(case.nviews, np.float32)
+            lib.IrlGetScatterSurrogateNrmse(api.fptr(nr), case.nviews)
+            stream = torch.cuda.ExternalStream(lib.irlcu_stream())
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.IrlOsemIterate(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rc:
+                raise RuntimeError(lib.pchIrlErrorString().decode())
+            ms = e0.elapsed_time(e1) / K
+        finally:
+            lib.IrlOsemEnd(None)
+        sur_img = _recon256(lib, case, files, meas, case.iterations)
+    finally:
+        lib.IrlSetScatterSurrogate(None, 0.0)
+    esse_img = _recon256(lib, case, files, meas, case.iterations)
+    none_img = _recon256(lib, case, files, meas, case.iterations, srf_iters=0)
+    ref = np.linalg.norm(esse_img)
+    return {
+        "ms_per_iteration": round(ms, 2), "esse_ms_per_iteration": round(esse_ms, 2),
+        "speedup_vs_esse": round(esse_ms / ms, 3) if ms > 0 else None,
+        "image_nrmse_vs_esse": round(float(np.linalg.norm(sur_img - esse_img) / ref), 5),
+        "image_nrmse_no_scatter_vs_esse": round(float(np.linalg.norm(none_img - esse_img) / ref), 5),
+        "views_on_esse": int((nr > 0.02).sum()),
+        "view_nrmse": {"mean": round(float(nr.mean()), 5), "max": round(float(nr.max()), 5)},
+        "reconstruction": f"{case.iterations} iterations of {case.subsets} subsets, scatter model in all",
+    }
+
+
 def run_large256(args):
     """Config 5: 256^3, 128 views, 16 subsets, 65 x 65 DRF on libirl's FFT
     convolution path, ESSE; IrlGenprj of the photopeak and the lower
@@ -926,8 +993,10 @@ def run_large256(args):
         ms = e0.elapsed_time(e1) / K
     finally:
         lib.IrlOsemEnd(api.fptr(rec))
+    learned = large256_learned(lib, pp, fpp, meas, K, Wm, ms, torch)
     return {
         "metric": "ms per OSEM iteration, 256^3/128 views/16 subsets, 65x65 FFT DRF + ESSE, 1 B200",
+        "learned_scatter": learned,
         "value": round(ms, 2), "unit": "ms", "n_gpus": 1, "steps": K, "warmup": Wm, "higher_is_better": False,
         "genprj_s": {"photopeak": round(g_pp, 3), "lower_window": round(g_lw, 3)},
         "image_finite": bool(np.all(np.isfinite(rec))),

@@ -716,8 +716,8 @@ static int upload_views(const int *views, int nv, const irlcu_view_parm *vp) {
 // the surrogate's iteration-invariant input channels of every view, from
 // the current per-view mu and S tables (not inside a graph capture)
 static int sur_static_ensure(Ctx &c) {
-  if (c.sur_static_ok || !c.tMu || !c.tS || (c.n & 3) || c.n != c.nz) return IRLCU_OK;
-  const size_t P = (size_t)(c.n / 4) * (c.n / 4) * (c.n / 4);
+  if (c.sur_static_ok || !c.tMu || !c.tS || c.n % (4 * SUR_P) || c.n != c.nz) return IRLCU_OK;
+  const size_t P = (size_t)SUR_P * SUR_P * SUR_P;
   if (!c.sur_static) TRY(dalloc(&c.sur_static, (size_t)c.nv * P));  // one BF16 pair per float
   TRY(launch_sur_static(c.st, c.tMu, c.tS, c.nv, c.n, c.vox, c.sur_static));
   c.sur_static_ok = true;
@@ -788,7 +788,7 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
                             sur_input(c.sur), c.sur_work));
     const float *y = nullptr;
     TRY(sur_infer(c.sur, c.st, nv, &y));
-    return launch_scale_views(c.st, y, c.sur_scale, out, (int)c.pln, nv, 1);
+    return launch_scale_views_up(c.st, y, c.sur_scale, out, c.n, nv, 1);
   }
   if (model & MODEL_SRF_BIT) {
     if (!c.esse.on && !c.esse.zero) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
@@ -997,14 +997,14 @@ int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mod
 // pooling work buffer of max_batch views
 static int sur_work_ensure(Ctx &c) {
   if (c.sur_work) return IRLCU_OK;
-  const size_t P = (size_t)(c.n / 4) * (c.n / 4) * (c.n / 4);
+  const size_t P = (size_t)SUR_P * SUR_P * SUR_P;
   return dalloc(&c.sur_work, (size_t)c.g.max_batch * (P + SUR_POOL_PARTS));
 }
 
 static int sur_geometry(const Ctx &c, irlcu_sur *net, int model) {
   if (!net) return set_error(IRLCU_EARG, "surrogate: null network");
-  if (c.n != 128 || c.nz != 128)
-    return set_error(IRLCU_EARG, "surrogate: the network takes 128^3 volumes (here %d x %d)", c.n, c.nz);
+  if ((c.n != 128 && c.n != 256) || c.nz != c.n)
+    return set_error(IRLCU_EARG, "surrogate: the network takes 128^3 or 256^3 volumes (here %d x %d)", c.n, c.nz);
   if (!(model & MODEL_SRF_BIT) || !c.esse.on || !c.tS || !c.tMu)
     return set_error(IRLCU_ESTATE, "surrogate: the scatter model (ESSE) must be set up");
   return IRLCU_OK;
@@ -1026,14 +1026,15 @@ int irlcu_sur_pairs(int nv, const int *views, int model, void *x_out, float *t_o
   Ctx &c = *g_ctx;
   if (nv < 1 || nv > c.g.max_batch)
     return set_error(IRLCU_EARG, "surrogate pairs: batch %d outside 1..%d", nv, c.g.max_batch);
-  if (c.n != 128 || c.nz != 128) return set_error(IRLCU_EARG, "surrogate pairs: 128^3 volumes only");
+  if ((c.n != 128 && c.n != 256) || c.nz != c.n)
+    return set_error(IRLCU_EARG, "surrogate pairs: 128^3 or 256^3 volumes only");
   if (!(model & MODEL_SRF_BIT) || !c.esse.on || !c.tS || !c.tMu)
     return set_error(IRLCU_ESTATE, "surrogate pairs: ESSE is not set up");
   TRY(upload_views(views, nv, nullptr));
   TRY(esse_scatter(c, nv, views, model, c.wprj));
   TRY(sur_work_ensure(c));
   TRY(launch_sur_inputs(c.st, c.wrot, c.vox, c.tMu, c.tS, c.dviews, nv, c.n, c.vox, scale_out, x_out, c.sur_work));
-  TRY(launch_div_views(c.st, c.wprj, scale_out, t_out, (int)c.pln, nv));
+  TRY(launch_div_views_down(c.st, c.wprj, scale_out, t_out, c.n, nv));
   CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
 }
@@ -1057,7 +1058,7 @@ int irlcu_sur_check(irlcu_sur *net, int nv, const int *views, int model, float *
       break;
     const float *yd = nullptr;
     if ((rc = sur_infer(net, c.st, nb, &yd))) break;
-    if ((rc = launch_scale_views(c.st, yd, scale, c.wprj2, (int)c.pln, nb, 0))) break;
+    if ((rc = launch_scale_views_up(c.st, yd, scale, c.wprj2, c.n, nb, 0))) break;
     if (cudaMemcpyAsync(y.data(), c.wprj2, sizeof(float) * c.pln * nb, cudaMemcpyDeviceToHost, c.st) ||
         cudaMemcpyAsync(t.data(), c.wprj, sizeof(float) * c.pln * nb, cudaMemcpyDeviceToHost, c.st) ||
         cudaStreamSynchronize(c.st)) {

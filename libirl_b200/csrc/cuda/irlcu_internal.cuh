@@ -259,7 +259,9 @@ int sur_max_batch(const irlcu_sur *s);
 int sur_tc_status(cudaStream_t st);
 void *sur_input(irlcu_sur *s);
 int sur_infer(irlcu_sur *s, cudaStream_t st, int B, const float **y);
-// work: nv * ((n/4)^3 + SUR_POOL_PARTS) floats
+// The network's input grid: SUR_P^3 means of (n / SUR_P)^3 voxels (n a
+// multiple of 4 SUR_P: 128 or 256).  work: nv * (SUR_P^3 + SUR_POOL_PARTS) floats
+constexpr int SUR_P = 32;
 constexpr int SUR_POOL_PARTS = 128;
 int launch_sur_static(cudaStream_t st, const float *mu, const float *S, int nviews, int n, size_t vox, void *stat);
 int launch_sur_inputs_static(cudaStream_t st, const float *act, size_t act_stride, const void *stat,
@@ -269,6 +271,10 @@ int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, cons
 int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size_t n);
 int launch_scale_views(cudaStream_t st, const float *x, const float *s, float *y, int P, int nb, int accumulate);
 int launch_div_views(cudaStream_t st, const float *a, const float *s, float *out, int P, int nb);
+// the network's 128 x 128 output onto n x n projections (bilinear) and n x n
+// targets onto 128 x 128 (f x f means); n = 128 is the plain scale / divide
+int launch_scale_views_up(cudaStream_t st, const float *x, const float *s, float *y, int n, int nb, int accumulate);
+int launch_div_views_down(cudaStream_t st, const float *a, const float *s, float *out, int n, int nb);
 
 // ESSE effective source: src[v] = rot[v]*primary + effsrc(rot[v], view)
 int esse_setup(Ctx &c, const irlcu_esse *e);

@@ -1134,8 +1134,9 @@ __global__ void __launch_bounds__(POOL_NT) k_pool_inputs(const float *__restrict
                                                          const int *__restrict__ views, size_t vox, int n,
                                                          float *__restrict__ pa, float *__restrict__ part,
                                                          bf16 *__restrict__ out) {
-  const int P = n / 4;
+  const int P = SUR_P, f = n / SUR_P;
   const int tot = P * P * P;
+  const float inv = 1.f / (float)(f * f * f);
   const int b = blockIdx.y;
   const int view = views[b];
   const float *a = act + (size_t)b * act_stride;
@@ -1146,22 +1147,23 @@ __global__ void __launch_bounds__(POOL_NT) k_pool_inputs(const float *__restrict
   for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
     const int px = e % P, pz = (e / P) % P, py = e / (P * P);
     float sa = 0.f, sm = 0.f, se = 0.f;
-    for (int dy = 0; dy < 4; ++dy)
-      for (int dz = 0; dz < 4; ++dz) {
-        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
-        const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
-        const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
-        const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
-        sa += (va.x + va.y) + (va.z + va.w);
-        sm += (vm.x + vm.y) + (vm.z + vm.w);
-        se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
-      }
-    const float mean_a = sa * (1.f / 64.f);
+    for (int dy = 0; dy < f; ++dy)
+      for (int dz = 0; dz < f; ++dz)
+        for (int dx = 0; dx < f; dx += 4) {
+          const size_t i = ((size_t)(f * py + dy) * n + (f * pz + dz)) * n + f * px + dx;
+          const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
+          const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
+          const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
+          sa += (va.x + va.y) + (va.z + va.w);
+          sm += (vm.x + vm.y) + (vm.z + vm.w);
+          se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
+        }
+    const float mean_a = sa * inv;
     pa[(size_t)b * tot + e] = mean_a;
     psum += mean_a;
     bf16 *o = out + ((size_t)b * tot + e) * 3;
-    o[1] = __float2bfloat16(sm * (10.f / 64.f));
-    o[2] = __float2bfloat16(se * (1.f / 64.f));
+    o[1] = __float2bfloat16(sm * (10.f * inv));
+    o[2] = __float2bfloat16(se * inv);
   }
   red[threadIdx.x] = psum;
   __syncthreads();
@@ -1176,33 +1178,36 @@ __global__ void __launch_bounds__(POOL_NT) k_pool_inputs(const float *__restrict
 // every view, [view][P^3][2], pooled once per reconstruction
 __global__ void __launch_bounds__(POOL_NT) k_pool_static(const float *__restrict__ mu, const float *__restrict__ S,
                                                          size_t vox, int n, bf16 *__restrict__ stat) {
-  const int P = n / 4;
+  const int P = SUR_P, f = n / SUR_P;
   const int tot = P * P * P;
+  const float inv = 1.f / (float)(f * f * f);
   const int view = blockIdx.y;
   const float *m = mu + (size_t)view * vox;
   const float *sd = S + (size_t)view * vox;
   for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
     const int px = e % P, pz = (e / P) % P, py = e / (P * P);
     float sm = 0.f, se = 0.f;
-    for (int dy = 0; dy < 4; ++dy)
-      for (int dz = 0; dz < 4; ++dz) {
-        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
-        const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
-        const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
-        sm += (vm.x + vm.y) + (vm.z + vm.w);
-        se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
-      }
+    for (int dy = 0; dy < f; ++dy)
+      for (int dz = 0; dz < f; ++dz)
+        for (int dx = 0; dx < f; dx += 4) {
+          const size_t i = ((size_t)(f * py + dy) * n + (f * pz + dz)) * n + f * px + dx;
+          const float4 vm = __ldg(reinterpret_cast<const float4 *>(m + i));
+          const float4 vs = __ldg(reinterpret_cast<const float4 *>(sd + i));
+          sm += (vm.x + vm.y) + (vm.z + vm.w);
+          se += (__expf(-vs.x) + __expf(-vs.y)) + (__expf(-vs.z) + __expf(-vs.w));
+        }
     bf16 *o = stat + ((size_t)view * tot + e) * 2;
-    o[0] = __float2bfloat16(sm * (10.f / 64.f));
-    o[1] = __float2bfloat16(se * (1.f / 64.f));
+    o[0] = __float2bfloat16(sm * (10.f * inv));
+    o[1] = __float2bfloat16(se * inv);
   }
 }
 
 // activity channel only: 4^3 means and their partial sums
 __global__ void __launch_bounds__(POOL_NT) k_pool_act(const float *__restrict__ act, size_t act_stride, int n,
                                                       float *__restrict__ pa, float *__restrict__ part) {
-  const int P = n / 4;
+  const int P = SUR_P, f = n / SUR_P;
   const int tot = P * P * P;
+  const float inv = 1.f / (float)(f * f * f);
   const int b = blockIdx.y;
   const float *a = act + (size_t)b * act_stride;
   __shared__ float red[POOL_NT];
@@ -1210,13 +1215,14 @@ __global__ void __launch_bounds__(POOL_NT) k_pool_act(const float *__restrict__ 
   for (int e = blockIdx.x * POOL_NT + threadIdx.x; e < tot; e += gridDim.x * POOL_NT) {
     const int px = e % P, pz = (e / P) % P, py = e / (P * P);
     float sa = 0.f;
-    for (int dy = 0; dy < 4; ++dy)
-      for (int dz = 0; dz < 4; ++dz) {
-        const size_t i = ((size_t)(4 * py + dy) * n + (4 * pz + dz)) * n + 4 * px;
-        const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
-        sa += (va.x + va.y) + (va.z + va.w);
-      }
-    const float mean_a = sa * (1.f / 64.f);
+    for (int dy = 0; dy < f; ++dy)
+      for (int dz = 0; dz < f; ++dz)
+        for (int dx = 0; dx < f; dx += 4) {
+          const size_t i = ((size_t)(f * py + dy) * n + (f * pz + dz)) * n + f * px + dx;
+          const float4 va = __ldg(reinterpret_cast<const float4 *>(a + i));
+          sa += (va.x + va.y) + (va.z + va.w);
+        }
+    const float mean_a = sa * inv;
     pa[(size_t)b * tot + e] = mean_a;
     psum += mean_a;
   }
@@ -1286,6 +1292,43 @@ __global__ void k_div_views(const float *__restrict__ a, const float *__restrict
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
     const float sc = s[e / P];
     out[e] = sc > 0.f ? a[e] / sc : 0.f;
+  }
+}
+
+// Projections larger than the network's SUR_OUT x SUR_OUT output (n = 256):
+// y[b][z][x] (+)= s[b] * the output bilinearly interpolated at the pixel's
+// centre ((u + 0.5) / f - 0.5 in output pixels, clamped at the edges)
+constexpr int SUR_OUT = 128;
+__global__ void k_scale_views_up(const float *__restrict__ x, const float *__restrict__ s, float *__restrict__ y,
+                                 int n, int nb, int accumulate) {
+  const int f = n / SUR_OUT;
+  const size_t P = (size_t)n * n, tot = (size_t)nb * P;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(e / P), r = (int)(e - (size_t)b * P), zz = r / n, xx = r - zz * n;
+    const float tz = fminf(fmaxf((zz + 0.5f) / f - 0.5f, 0.f), (float)(SUR_OUT - 1));
+    const float tx = fminf(fmaxf((xx + 0.5f) / f - 0.5f, 0.f), (float)(SUR_OUT - 1));
+    const int z0 = min((int)tz, SUR_OUT - 2), x0 = min((int)tx, SUR_OUT - 2);
+    const float wz = tz - z0, wx = tx - x0;
+    const float *q = x + (size_t)b * SUR_OUT * SUR_OUT + (size_t)z0 * SUR_OUT + x0;
+    const float v0 = q[0] + wx * (q[1] - q[0]), v1 = q[SUR_OUT] + wx * (q[SUR_OUT + 1] - q[SUR_OUT]);
+    const float v = (v0 + wz * (v1 - v0)) * s[b];
+    y[e] = accumulate ? y[e] + v : v;
+  }
+}
+
+// training targets of projections larger than the output: f x f means / s[b]
+__global__ void k_div_views_down(const float *__restrict__ a, const float *__restrict__ s, float *__restrict__ out,
+                                 int n, int nb) {
+  const int f = n / SUR_OUT;
+  const size_t P = (size_t)SUR_OUT * SUR_OUT, tot = (size_t)nb * P;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(e / P), r = (int)(e - (size_t)b * P), zz = r / SUR_OUT, xx = r - zz * SUR_OUT;
+    const float *q = a + (size_t)b * n * n + (size_t)zz * f * n + (size_t)xx * f;
+    float acc = 0.f;
+    for (int i = 0; i < f; ++i)
+      for (int j = 0; j < f; ++j) acc += q[(size_t)i * n + j];
+    const float sc = s[b];
+    out[e] = sc > 0.f ? acc / (float)(f * f) / sc : 0.f;
   }
 }
 
@@ -1631,7 +1674,7 @@ int launch_sur_static(cudaStream_t st, const float *mu, const float *S, int nvie
 
 int launch_sur_inputs_static(cudaStream_t st, const float *act, size_t act_stride, const void *stat,
                              const int *dviews, int nv, int n, float *scale, void *out, float *work) {
-  const int P = n / 4, tot = P * P * P;
+  const int P = SUR_P, tot = P * P * P;
   const int nparts = SUR_POOL_PARTS;
   float *pa = work, *part = work + (size_t)nv * tot;
   dim3 grid(nparts, nv);
@@ -1645,7 +1688,7 @@ int launch_sur_inputs_static(cudaStream_t st, const float *act, size_t act_strid
 
 int launch_sur_inputs(cudaStream_t st, const float *act, size_t act_stride, const float *mu, const float *S,
                       const int *dviews, int nv, int n, size_t vox, float *scale, void *out, float *work) {
-  const int P = n / 4, tot = P * P * P;
+  const int P = SUR_P, tot = P * P * P;
   const int nparts = SUR_POOL_PARTS;
   float *pa = work, *part = work + (size_t)nv * tot;
   dim3 grid(nparts, nv);
@@ -1664,6 +1707,22 @@ int launch_sub(cudaStream_t st, const float *a, const float *b, float *out, size
 
 int launch_scale_views(cudaStream_t st, const float *x, const float *s, float *y, int P, int nb, int accumulate) {
   k_scale_views<<<grid_for((long long)P * nb), 256, 0, st>>>(x, s, y, P, nb, accumulate);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_scale_views_up(cudaStream_t st, const float *x, const float *s, float *y, int n, int nb, int accumulate) {
+  if (n == SUR_OUT) return launch_scale_views(st, x, s, y, n * n, nb, accumulate);
+  if (n % SUR_OUT) return set_error(IRLCU_EARG, "surrogate output: n = %d is not a multiple of %d", n, SUR_OUT);
+  k_scale_views_up<<<grid_for((long long)n * n * nb), 256, 0, st>>>(x, s, y, n, nb, accumulate);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
+int launch_div_views_down(cudaStream_t st, const float *a, const float *s, float *out, int n, int nb) {
+  if (n == SUR_OUT) return launch_div_views(st, a, s, out, n * n, nb);
+  if (n % SUR_OUT) return set_error(IRLCU_EARG, "surrogate targets: n = %d is not a multiple of %d", n, SUR_OUT);
+  k_div_views_down<<<grid_for((long long)SUR_OUT * SUR_OUT * nb), 256, 0, st>>>(a, s, out, n, nb);
   CU_LAUNCHED();
   return IRLCU_OK;
 }

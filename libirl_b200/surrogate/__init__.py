@@ -20,6 +20,9 @@ import numpy as np
 MAGIC = b"IRLSUR01"
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "sur128.bin")
+# the same network trained on the 256^3 / 128-view phantoms (inputs pooled
+# 8 x 8 x 8, output interpolated to 256 x 256)
+WEIGHTS_256 = os.path.join(HERE, "sur256.bin")
 INPUT_SHAPE = (32, 32, 32, 3)
 OUTPUT_SIZE = 128 * 128
 MODEL_SRF = 7  # projector bits: attenuation 1 | DRF 2 | scatter 4

@@ -57,11 +57,20 @@ def _phantom(seed):
     return W.full128(seed=seed)
 
 
-def generate(lib, seeds, workers=8, batch=15):
+def _phantom256(seed):
+    return W.large256(seed=seed)
+
+
+# workload -> (phantom maker, views per phantom)
+WORKLOADS = {"full128": (_phantom, 120), "large256": (_phantom256, 128)}
+
+
+def generate(lib, seeds, workers=8, workload="full128"):
     """Network inputs X, normalised targets T and scales S of every view of
-    every phantom, on the device."""
+    every phantom, on the device (targets of 256^3 phantoms as 2 x 2 means
+    of their 256 x 256 scatter projections)."""
     import torch
-    nv = 120
+    maker, nv = WORKLOADS[workload]
     N = len(seeds) * nv
     X = torch.empty((N,) + SU.INPUT_SHAPE, dtype=torch.bfloat16, device="cuda")
     T = torch.empty((N, SU.OUTPUT_SIZE), dtype=torch.float32, device="cuda")
@@ -71,8 +80,9 @@ def generate(lib, seeds, workers=8, batch=15):
     k = 0
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
-        for case in pool.imap(_phantom, seeds):
-            assert case.nviews == nv and case.n == 128
+        for case in pool.imap(maker, seeds):
+            assert case.nviews == nv and case.n in (128, 256)
+            batch = case.nviews // case.subsets
             files = case.write_tables(tmp)
             p, o, v = case.parms(), case.options(), case.views()
             o.bReconIsInitEst = 1  # the phantom is the estimate
@@ -131,8 +141,8 @@ def train_streaming(args, lib):
     val_seeds = [args.seed0 + ntr + i for i in range(nval)]
     te_seeds = [args.seed0 + ntr + nval + i for i in range(nte)]
     t0 = time.time()
-    Xv, Tv, _ = generate(lib, val_seeds, workers=args.workers)
-    Xt, Tt, _ = generate(lib, te_seeds, workers=args.workers)
+    Xv, Tv, _ = generate(lib, val_seeds, workers=args.workers, workload=args.workload)
+    Xt, Tt, _ = generate(lib, te_seeds, workers=args.workers, workload=args.workload)
     t_gen = time.time() - t0
     g = torch.Generator(device="cuda")
     g.manual_seed(1234)
@@ -145,7 +155,7 @@ def train_streaming(args, lib):
     for ci in range(nchunks):
         seeds = [args.seed0 + i for i in range(ci * args.chunk, min(ntr, (ci + 1) * args.chunk))]
         t = time.time()
-        X, T, _ = generate(lib, seeds, workers=args.workers)
+        X, T, _ = generate(lib, seeds, workers=args.workers, workload=args.workload)
         t_gen += time.time() - t
         n = X.shape[0]
         stop = args.steps * (ci + 1) // nchunks
@@ -172,8 +182,9 @@ def train_streaming(args, lib):
     et = nrmse(net, Xt, Tt, torch.arange(0, Xt.shape[0], device="cuda"), args.batch)
     SU.save_weights(args.out, net.get_weights())
     summ = {
-        "phantoms": ntr, "val_phantoms": nval, "test_phantoms": nte, "views_per_phantom": 120,
-        "training_views": ntr * 120, "chunk_phantoms": args.chunk, "steps": args.steps, "batch": args.batch,
+        "workload": args.workload, "phantoms": ntr, "val_phantoms": nval, "test_phantoms": nte,
+        "views_per_phantom": WORKLOADS[args.workload][1], "training_views": ntr * WORKLOADS[args.workload][1],
+        "chunk_phantoms": args.chunk, "steps": args.steps, "batch": args.batch,
         "lr": args.lr, "init": args.init and os.path.basename(args.init), "seed0": args.seed0,
         "generate_s": round(t_gen, 1), "train_s": round(t_train, 1),
         "ms_per_step": round(1000 * t_train / max(1, args.steps), 2),
@@ -194,6 +205,8 @@ def main(argv=None):
     ap.add_argument("--phantoms", type=int, default=200, help="training phantoms")
     ap.add_argument("--val", type=int, default=16, help="held-out phantoms")
     ap.add_argument("--test", type=int, default=0, help="test phantoms (with --chunk)")
+    ap.add_argument("--workload", default="full128", choices=sorted(WORKLOADS),
+                    help="phantom generator: full128 (128^3, 120 views) or large256 (256^3, 128 views)")
     ap.add_argument("--chunk", type=int, default=0,
                     help="generate the training pairs in chunks of this many phantoms (streaming)")
     ap.add_argument("--seed0", type=int, default=40000)

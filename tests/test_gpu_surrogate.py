@@ -224,3 +224,44 @@ def test_tensor_core_wait_time_out_is_an_error_and_recoverable(product):
         assert torch.equal(y0, y1)
     finally:
         net.close()
+
+
+def test_trained_surrogate_256_ablation(product, tmp_path):
+    """The network trained on 256^3 phantoms (inputs pooled 8 x 8 x 8, the
+    128 x 128 output interpolated to 256 x 256) inside the 256^3 / 128-view /
+    16-subset reconstruction with the 65x65 FFT DRF: within 1 % image NRMSE
+    of the ESSE reconstruction and far closer to it than without scatter."""
+    if not os.path.exists(SU.WEIGHTS_256):
+        pytest.skip("no committed 256^3 surrogate weights")
+    case = W.large256(seed=5000, iterations=4)
+    files = case.write_tables(str(tmp_path))
+    p, o, v = case.parms(), case.options(), case.views()
+    o.bFFTConvolve = 1
+    act, atn = case.act.copy(), case.atn.copy()
+    prj = np.zeros((case.nviews, case.nz, case.n), np.float32)
+    assert product.IrlGenprj(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), None, None,
+                             api.fptr(act), api.fptr(atn), api.fptr(prj), 1.0, None, None) == 0
+    meas = W.poisson_counts(prj, case.counts, 5000)
+
+    def recon(srf_iters=None):
+        p, o, v = case.parms(), case.options(), case.views()
+        o.bFFTConvolve = 1
+        if srf_iters is not None:
+            p.iNumSrfIterations = srf_iters
+        atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+        assert product.IrlOsem(C.byref(p), C.byref(o), v, dup(files["drf"]), dup(files["krnl"]), api.ITER_CB(), None,
+                               api.fptr(atn), api.fptr(m), api.fptr(rec), None, None) == 0, product.pchIrlErrorString()
+        return rec
+
+    esse = recon()
+    product.IrlSetScatterSurrogate(SU.WEIGHTS_256.encode(), 0.02)
+    try:
+        learned = recon()
+    finally:
+        product.IrlSetScatterSurrogate(None, 0.0)
+    none = recon(srf_iters=0)
+    ref = float(np.linalg.norm(esse))
+    err_learned = float(np.linalg.norm(learned - esse)) / ref
+    err_none = float(np.linalg.norm(none - esse)) / ref
+    assert err_learned <= 0.01, err_learned
+    assert err_learned < 0.25 * err_none, (err_learned, err_none)
