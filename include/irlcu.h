@@ -58,15 +58,19 @@ typedef struct {
 	                             the PSF's own extent (work accounting) */
 } irlcu_drf;
 
-/* ESSE scatter model (krnlprj3d.c:349-365, 676-954) */
+/* ESSE scatter model (krnlprj3d.c:349-365, 676-954).  The kernel comes in
+   its KRNL-file form (one quadrant, [ndepths][noffs][noffs]); the device
+   expands it to the grids K and K (mu - mu_avg) of pfReorder3dKrnl
+   (krnlprj3d.c:43-128, irlcu_esse_expand) and transforms them. */
 typedef struct {
 	int kx, ky, kz;           /* FFT grid: offsets (x), depths (y), slices (z) */
 	int collapse;             /* SrfCollapseFac */
-	int nterms;               /* Taylor terms, 1..3 */
+	int nterms;               /* Taylor terms, 1 or 2 */
 	float mu0, mu_avg, pix, cntr_pix_fac;
-	const float *krnl;        /* reordered kernel, [ky][kz][kx], host */
-	const float *kmu;         /* K * (mu - mu_avg) (nterms > 1), host */
-	const float *kmu2;        /* K * (mu - mu_avg)^2 (nterms > 2), host */
+	int noffs, ndepths;       /* NumXYoffs, NumDists */
+	const float *krnl;        /* pfKrnl, [ndepths][noffs][noffs], host */
+	const float *mu;          /* pfKrnlMu, same layout, host */
+	float kmu_outside;        /* K (mu - mu_avg) where K is 0 */
 } irlcu_esse;
 
 /* per-view scalars of the OSEM update (osemrecon.c:727-827) */
@@ -86,6 +90,9 @@ int irlcu_set_angles(const float *angles);
 /* DRF tables: which = 0 projector, 1 backprojector */
 int irlcu_set_drf(int which, const irlcu_drf *d);
 int irlcu_set_esse(const irlcu_esse *e);
+/* The ESSE grid of one term (0: K, 1: K (mu - mu_avg)), [ky][kz][kx], as
+   irlcu_set_esse builds it on the device, copied to host memory out. */
+int irlcu_esse_expand(const irlcu_esse *e, int term, float *out);
 /* measured-bin mask of each view: nviews*n column flags (1 measured) */
 int irlcu_set_column_mask(const unsigned char *mask);
 
@@ -98,15 +105,29 @@ int irlcu_set_column_mask(const unsigned char *mask);
 #define IRLCU_BUF_UPDATE 5   /* subset update image, volume */
 #define IRLCU_BUF_NORM 6     /* inverted norm image of subset `index`, volume */
 int irlcu_upload(int buf, int index, const float *host, size_t count);
+/* irlcu_upload on the context's copy stream: it does not wait for the
+   kernels queued on the library stream, and returns once the copy has
+   landed, so that later work sees it.  The buffer must exist and no queued
+   kernel may use it.  Callable from a helper thread of the calling one
+   (never at the same time as an irlcu call that changes the context). */
+int irlcu_upload_now(int buf, int index, const float *host, size_t count);
 int irlcu_download(int buf, int index, float *host, size_t count);
 int irlcu_zero(int buf, int index);
 /* a volume buffer copied to the host in libirl's external layout
    [z][y][x] (the transposition runs on the device) */
 int irlcu_download_external(int buf, float *host);
+/* a volume given in libirl's external layout [z][y][x] into a volume
+   buffer (internal layout [y][z][x]; the transposition runs on the device),
+   each value multiplied by scale when scale > 0 and scale != 1 (one float
+   multiply, as irlosem.c:212-215 scales the attenuation map) and set to 0
+   when below 0 with clamp (vZeroNeg).  The host array may be changed once
+   the call returns; the device work is queued on the library stream. */
+int irlcu_upload_external(int buf, const float *host, float scale, int clamp);
 int irlcu_alloc_norm(int nsubsets);
 
 /* Builds the per-view rotated attenuation tables from IRLCU_BUF_ATN
-   (rotated map, cumulative half-pixel sums and exp(-sum)). */
+   (rotated map, cumulative half-pixel sums and exp(-sum)).  Asynchronous:
+   returns once the work is queued on the library stream. */
 int irlcu_prepare_attenuation(int need_srf);
 
 /* Raw projections of the estimate for views[0..nv) into host or device
@@ -145,7 +166,8 @@ int irlcu_ctx_attach(void *ctx);
 
 /* Normalisation image of one subset (osemrecon.c:282-320): backprojects
    the measured-bin mask times ViewTime of each view, clamps after each,
-   inverts with a 1e-6 floor and stores it as NORM[subset]. */
+   inverts with a 1e-6 floor and stores it as NORM[subset].  Asynchronous:
+   returns once the work is queued on the library stream. */
 int irlcu_norm_subset(int nv, const int *views, const float *view_time,
 	int bck_model, int subset);
 

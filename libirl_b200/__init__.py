@@ -50,10 +50,16 @@ def _declare_irlcu(lib):
     lib.irlcu_set_angles.argtypes = [F]
     lib.irlcu_upload.restype = I
     lib.irlcu_upload.argtypes = [I, I, F, S]
+    lib.irlcu_upload_now.restype = I
+    lib.irlcu_upload_now.argtypes = [I, I, F, S]
+    lib.irlcu_esse_expand.restype = I
+    lib.irlcu_esse_expand.argtypes = [C.c_void_p, I, F]
     lib.irlcu_download.restype = I
     lib.irlcu_download.argtypes = [I, I, F, S]
     lib.irlcu_download_external.restype = I
     lib.irlcu_download_external.argtypes = [I, F]
+    lib.irlcu_upload_external.restype = I
+    lib.irlcu_upload_external.argtypes = [I, F, C.c_float, I]
     lib.irlcu_rotate_volume.restype = I
     lib.irlcu_rotate_volume.argtypes = [C.c_float, F, F, I, I]
     lib.irlcu_rotate_volume_noalloc.restype = I

@@ -211,6 +211,7 @@ static void free_ctx(Ctx *c) {
     if (c->snap_copied[k]) cudaEventDestroy(c->snap_copied[k]);
   }
   if (c->snap_st) cudaStreamDestroy(c->snap_st);
+  if (c->up_st) cudaStreamDestroy(c->up_st);
   for (auto &v : c->trial_ev)
     for (auto &e : v) {
       cudaEventDestroy(e.first);
@@ -244,6 +245,22 @@ __global__ void k_to_external(const float *__restrict__ in, float *__restrict__ 
   }
 }
 
+// the inverse of k_to_external, with irlosem.c's scaling and clamp of the
+// attenuation map folded in (one float multiply, then x < 0 -> +0)
+__global__ void k_from_external(const float *__restrict__ in, float *__restrict__ out, int n, int nz, float scale,
+                                int clamp) {
+  const size_t vox = (size_t)n * nz * n;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < vox; e += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(e % n);
+    const size_t r = e / n;
+    const int z = (int)(r % nz), y = (int)(r / nz);
+    float v = in[((size_t)z * n + y) * n + x];
+    if (scale > 0.0f && scale != 1.0f) v = __fmul_rn(v, scale);
+    if (clamp && v < 0.0f) v = 0.0f;
+    out[e] = v;
+  }
+}
+
 }  // namespace irlcu
 
 using namespace irlcu;
@@ -271,6 +288,7 @@ int irlcu_init(const irlcu_geom *g) {
   g_ctx = c;
   CU_TRY(cudaGetDevice(&c->dev));
   CU_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CU_TRY(cudaStreamCreateWithFlags(&c->up_st, cudaStreamNonBlocking));
   for (auto &e : c->ev) CU_TRY(cudaEventCreate(&e));
   const int n = c->n, R = 2 * c->nv;
   TRY(dalloc(&c->rot.hdr, (size_t)4 * R));
@@ -307,6 +325,9 @@ int irlcu_init(const irlcu_geom *g) {
   CU_TRY(cudaMemsetAsync(c->upd, 0, c->vox * sizeof(float), alloc_stream()));
   std::vector<unsigned char> ones((size_t)c->nv * n, 3);
   CU_TRY(cudaMemcpyAsync(c->colmask, ones.data(), ones.size(), cudaMemcpyHostToDevice, alloc_stream()));
+  // the buffers are zeroed before irlcu_upload_now may write them from the
+  // copy stream
+  CU_TRY(cudaStreamSynchronize(c->st));
   return IRLCU_OK;
 }
 
@@ -605,6 +626,20 @@ int irlcu_upload(int buf, int index, const float *host, size_t count) {
   return IRLCU_OK;
 }
 
+int irlcu_upload_now(int buf, int index, const float *host, size_t count) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  CU_TRY(cudaSetDevice(c.dev));  // the calling thread may be a helper thread
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, index, &p, &cap, false));
+  if (!p) return set_error(IRLCU_ESTATE, "buffer %d not allocated", buf);
+  if (count > cap) return set_error(IRLCU_EARG, "upload of %zu floats exceeds buffer %d (%zu)", count, buf, cap);
+  CU_TRY(cudaMemcpyAsync(p, host, count * 4, cudaMemcpyHostToDevice, c.up_st));
+  CU_TRY(cudaStreamSynchronize(c.up_st));
+  return IRLCU_OK;
+}
+
 int irlcu_download(int buf, int index, float *host, size_t count) {
   TRY(need_ctx());
   float *p;
@@ -639,6 +674,22 @@ int irlcu_download_external(int buf, float *host) {
   CU_TRY(cudaMemcpyAsync(host, c.wbck, c.vox * 4, cudaMemcpyDeviceToHost, c.st));
   CU_TRY(cudaStreamSynchronize(c.st));
   if (c.sur) TRY(sur_tc_status(c.st));
+  return IRLCU_OK;
+}
+
+int irlcu_upload_external(int buf, const float *host, float scale, int clamp) {
+  TRY(need_ctx());
+  Ctx &c = *g_ctx;
+  float *p;
+  size_t cap;
+  TRY(buf_ptr(buf, 0, &p, &cap, true));
+  if (!p || cap != c.vox) return set_error(IRLCU_EARG, "buffer %d is not a volume", buf);
+  // into wbck (vox * max_batch floats); the host array is free once the
+  // copy has landed, before the transposition is queued
+  CU_TRY(cudaMemcpyAsync(c.wbck, host, c.vox * 4, cudaMemcpyHostToDevice, c.st));
+  CU_TRY(cudaStreamSynchronize(c.st));
+  k_from_external<<<592, 256, 0, c.st>>>(c.wbck, p, c.n, c.nz, scale, clamp);
+  CU_LAUNCHED();
   return IRLCU_OK;
 }
 
@@ -745,7 +796,6 @@ int irlcu_prepare_attenuation(int need_srf) {
     TRY(launch_atn_tables(c, rmu, c.tE + (size_t)v0 * c.vox, need_srf ? c.tS + (size_t)v0 * c.vox : nullptr, nb));
   }
   if (need_srf && c.sur) TRY(sur_static_ensure(c));
-  CU_TRY(cudaStreamSynchronize(c.st));
   return IRLCU_OK;
 }
 
@@ -1140,7 +1190,6 @@ int irlcu_norm_subset(int nv, const int *views, const float *view_time, int bck_
     TRY(launch_backproject(c, planes, c.dviews, nb, E, drf, 1.0f, c.wbck));
     const bool last = v0 + nb >= nv;
     TRY(launch_unrotate_accumulate(c, c.wbck, c.dviews, nb, norm, 1, last ? ACC_INVERT : 0, nullptr, nullptr));
-    CU_TRY(cudaStreamSynchronize(c.st));
   }
   return IRLCU_OK;
 }

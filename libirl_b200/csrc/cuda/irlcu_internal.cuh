@@ -106,6 +106,7 @@ struct Ctx {
   mutable std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trial_ev[2];
   float trial_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [kind][form], ms per iteration
   cudaStream_t st = nullptr;
+  cudaStream_t up_st = nullptr;  // irlcu_upload_now: copies beside the queued kernels
   cudaEvent_t ev[16];
   int nsub = 0;
 

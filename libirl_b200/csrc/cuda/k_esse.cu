@@ -870,6 +870,58 @@ void esse_free(Ctx &c) {
   c.ew = EsseWork{};
 }
 
+// pfReorder3dKrnl (krnlprj3d.c:43-128) read backwards: each grid point
+// [z][y][x] of the oxd x oyd x ozd grid finds the file value that lands on
+// it, if any.  Offsets below the half-widths xmin = min(noffs, oxd/2) map
+// to themselves, their mirrors oxd - ix (ix > 0) back; depth plane z holds
+// file depth ozd/2 + ndepths/2 - 1 - u, u the plane before the half-axis
+// rotation.  Term 0 writes K (0 elsewhere), term 1 K (mu - mu_avg) (one
+// float subtraction and one product; `outside` elsewhere).
+__global__ void k_esse_expand(const float *__restrict__ kf, const float *__restrict__ mf, int noffs, int ndepths,
+                              int oxd, int oyd, int ozd, int term, float mu_avg, float outside,
+                              float *__restrict__ grid) {
+  const size_t total = (size_t)oxd * oyd * ozd;
+  const int xmin = min(noffs, oxd / 2), ymin = min(noffs, oyd / 2);
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(g % oxd);
+    const size_t r = g / oxd;
+    const int y = (int)(r % oyd), z = (int)(r / oyd);
+    const int ix = x < xmin ? x : (x >= oxd - xmin + 1 ? oxd - x : -1);
+    const int iy = y < ymin ? y : (y >= oyd - ymin + 1 ? oyd - y : -1);
+    const int u = z < ozd / 2 ? z + ozd / 2 : z - ozd / 2;
+    const int iz = ozd / 2 + ndepths / 2 - 1 - u;
+    float v;
+    if (ix >= 0 && iy >= 0 && iz >= 0 && iz < ndepths) {
+      const size_t f = (size_t)ix + (size_t)noffs * (iy + (size_t)noffs * iz);
+      v = term == 0 ? kf[f] : __fmul_rn(__fsub_rn(mf[f], mu_avg), kf[f]);
+    } else {
+      v = term == 0 ? 0.0f : outside;
+    }
+    grid[g] = v;
+  }
+}
+
+// the file-form kernel of e on the device (two arrays of noffs^2 * ndepths)
+static int esse_file_upload(Ctx &c, const irlcu_esse *e, float **dk, float **dm) {
+  *dk = *dm = nullptr;
+  if (e->noffs <= 0 || e->ndepths <= 0 || !e->krnl || !e->mu)
+    return set_error(IRLCU_EARG, "ESSE kernel of %d x %d x %d offsets", e->noffs, e->noffs, e->ndepths);
+  const size_t fc = (size_t)e->noffs * e->noffs * e->ndepths;
+  CU_TRY(dev_alloc(reinterpret_cast<void **>(dk), sizeof(float) * fc, c.st));
+  CU_TRY(dev_alloc(reinterpret_cast<void **>(dm), sizeof(float) * fc, c.st));
+  CU_TRY(cudaMemcpyAsync(*dk, e->krnl, sizeof(float) * fc, cudaMemcpyHostToDevice, c.st));
+  CU_TRY(cudaMemcpyAsync(*dm, e->mu, sizeof(float) * fc, cudaMemcpyHostToDevice, c.st));
+  return IRLCU_OK;
+}
+
+// the grid of one term: pfReorder3dKrnl's (oxd, oyd, ozd) = (kx, kz, ky)
+static int esse_expand(Ctx &c, const irlcu_esse *e, const float *dk, const float *dm, int term, float *grid) {
+  k_esse_expand<<<148 * 8, 256, 0, c.st>>>(dk, dm, e->noffs, e->ndepths, e->kx, e->kz, e->ky, term, e->mu_avg,
+                                           e->kmu_outside, grid);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
 int esse_setup(Ctx &c, const irlcu_esse *e) {
   esse_free(c);
   if (!e) {  // scatter factor 0: the effective source is zero
@@ -925,26 +977,33 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.T[t]), sizeof(float) * (size_t)B * c.n * c.nz * w.nxv, c.st));
     CU_TRY(dev_alloc(reinterpret_cast<void **>(&w.Tc[t]), sizeof(float) * (size_t)B * c.n * w.nzv * w.nxv, c.st));
   }
-  // kernel spectra: forward transform of the full real grids
-  const float *hk[3] = {e->krnl, e->kmu, e->kmu2};
-  float *dgrid = nullptr;
-  CU_TRY(dev_alloc(reinterpret_cast<void **>(&dgrid), sizeof(float) * (size_t)E.kx * E.ky * E.kz, c.st));
-  for (int t = 0; t < E.nterms; ++t) {
-    CU_TRY(dev_alloc(reinterpret_cast<void **>(&E.kft[t]), sizeof(float2) * spec, c.st));
-    CU_TRY(cudaMemcpyAsync(dgrid, hk[t], sizeof(float) * (size_t)E.kx * E.ky * E.kz, cudaMemcpyHostToDevice, c.st));
+  // kernel spectra: the grids expanded from the file form on the device,
+  // then their forward transforms
+  {
+    float *dk = nullptr, *dm = nullptr, *dgrid = nullptr;
     float2 *ta = nullptr, *tb = nullptr;
-    CU_TRY(dev_alloc(reinterpret_cast<void **>(&ta), sizeof(float2) * spec, c.st));
-    CU_TRY(dev_alloc(reinterpret_cast<void **>(&tb), sizeof(float2) * spec, c.st));
-    int rc = fft3_forward(c.st, E, nullptr, dgrid, c.n, c.nz, 1, E.ky, E.kz, E.kx, 1, ta, tb, E.kft[t]);
-    CU_TRY(cudaStreamSynchronize(c.st));
+    int rc = esse_file_upload(c, e, &dk, &dm);
+    if (!rc && dev_alloc(reinterpret_cast<void **>(&dgrid), sizeof(float) * (size_t)E.kx * E.ky * E.kz, c.st))
+      rc = set_error(IRLCU_ENOMEM, "ESSE grid");
+    if (!rc && (dev_alloc(reinterpret_cast<void **>(&ta), sizeof(float2) * spec, c.st) ||
+                dev_alloc(reinterpret_cast<void **>(&tb), sizeof(float2) * spec, c.st)))
+      rc = set_error(IRLCU_ENOMEM, "ESSE transform work");
+    for (int t = 0; !rc && t < E.nterms; ++t) {
+      if (dev_alloc(reinterpret_cast<void **>(&E.kft[t]), sizeof(float2) * spec, c.st)) {
+        rc = set_error(IRLCU_ENOMEM, "ESSE kernel spectrum");
+        break;
+      }
+      rc = esse_expand(c, e, dk, dm, t, dgrid);
+      if (!rc) rc = fft3_forward(c.st, E, nullptr, dgrid, c.n, c.nz, 1, E.ky, E.kz, E.kx, 1, ta, tb, E.kft[t]);
+    }
+    if (!rc && cudaStreamSynchronize(c.st) != cudaSuccess) rc = set_error(IRLCU_ECUDA, "ESSE kernel spectra");
     dev_free(ta, c.st);
     dev_free(tb, c.st);
-    if (rc) {
-      dev_free(dgrid, c.st);
-      return rc;
-    }
+    dev_free(dgrid, c.st);
+    dev_free(dk, c.st);
+    dev_free(dm, c.st);
+    if (rc) return rc;
   }
-  dev_free(dgrid, c.st);
   // fused y-z kernel when the plane fits in shared memory: the register
   // form when the cropped rows of both terms fit the plane (nyv <= L/2),
   // else the pass form (IRLCU_ESSE_YZ=pass forces the latter)
@@ -1252,4 +1311,25 @@ static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int 
 extern "C" int irlcu_set_esse(const irlcu_esse *e) {
   if (!irlcu::g_ctx) return irlcu::set_error(IRLCU_ESTATE, "irlcu_init has not been called");
   return irlcu::esse_setup(*irlcu::g_ctx, e);
+}
+
+extern "C" int irlcu_esse_expand(const irlcu_esse *e, int term, float *out) {
+  using namespace irlcu;
+  if (!g_ctx) return set_error(IRLCU_ESTATE, "irlcu_init has not been called");
+  if (!e || !out || term < 0 || term > 1 || e->kx <= 0 || e->ky <= 0 || e->kz <= 0)
+    return set_error(IRLCU_EARG, "irlcu_esse_expand: bad arguments");
+  Ctx &c = *g_ctx;
+  const size_t total = (size_t)e->kx * e->ky * e->kz;
+  float *dk = nullptr, *dm = nullptr, *dgrid = nullptr;
+  int rc = esse_file_upload(c, e, &dk, &dm);
+  if (!rc && dev_alloc(reinterpret_cast<void **>(&dgrid), sizeof(float) * total, c.st))
+    rc = set_error(IRLCU_ENOMEM, "ESSE grid");
+  if (!rc) rc = esse_expand(c, e, dk, dm, term, dgrid);
+  if (!rc && cudaMemcpyAsync(out, dgrid, sizeof(float) * total, cudaMemcpyDeviceToHost, c.st) != cudaSuccess)
+    rc = set_error(IRLCU_ECUDA, "ESSE grid download");
+  if (!rc && cudaStreamSynchronize(c.st) != cudaSuccess) rc = set_error(IRLCU_ECUDA, "ESSE grid download");
+  dev_free(dgrid, c.st);
+  dev_free(dk, c.st);
+  dev_free(dm, c.st);
+  return rc;
 }

@@ -47,12 +47,17 @@ typedef struct {
 	DrfTab_t *drf;
 } irl_detector;
 
-/* ESSE scatter model prepared on the host (krnlprj3d.c:403-547) */
+/* ESSE scatter model prepared on the host (krnlprj3d.c:403-547): the
+   kernel in its file form, the weighted mean of mu over it and the FFT
+   grid the device expands it to (irlcu_esse) */
 typedef struct {
 	int on;                 /* 0 when the kernel's scatter factor is 0 */
 	int kx, ky, kz, collapse, nterms;
 	float mu0, mu_avg, pix, cntr_pix_fac;
-	float *krnl, *kmu, *kmu2;
+	int noffs, ndepths;     /* NumXYoffs, NumDists */
+	float *krnl_file;       /* [ndepths][noffs][noffs] */
+	float *mu_file;         /* [ndepths][noffs][noffs] */
+	float kmu_outside;      /* K (mu - mu_avg) where K is 0: (0 - mu_avg) * 0 */
 } irl_esse_host;
 
 void irl_setup_parms(IrlParms_t *ip, Options_t *op, float *atn, char *krnl_fname, irl_parms *p);
@@ -104,8 +109,12 @@ void irl_parallel_for(size_t n, size_t grain, irl_range_fn fn, void *ctx);
    slot 1 backprojector when any detector has a separate GRF table) */
 void irl_upload_drf(const irl_parms *p, irl_view *views, int ndet, irl_detector *dets);
 
-/* device set-up shared by IrlOsem and IrlGenprj: geometry, rotation
-   tables, measured-column masks, attenuation tables, DRF and ESSE */
+/* device set-up: irl_device_geometry (context, rotation tables,
+   measured-column masks), then the attenuation tables, then
+   irl_device_tables (DRF and ESSE); irl_device_setup runs all three, from
+   an attenuation map already in the internal layout */
+void irl_device_geometry(irl_parms *p, irl_view *views, int fast_rotate, int max_batch);
+void irl_device_tables(irl_parms *p, irl_view *views, const irl_esse_host *esse);
 void irl_device_setup(irl_parms *p, irl_view *views, const float *atn_internal,
 	const irl_esse_host *esse, int fast_rotate, int max_batch);
 

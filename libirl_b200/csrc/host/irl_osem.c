@@ -58,6 +58,13 @@ static double now_s(void)
 	return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
+/* set-up step timings at message level 6, from the start of IrlOsemBegin */
+static double g_mark_t0;
+static void mark(const char *what)
+{
+	irl_msg(6, "  mark %s (%.4f s)\n", what, now_s() - g_mark_t0);
+}
+
 /* ---------------------------------------------------------------- session */
 
 typedef struct {
@@ -222,37 +229,43 @@ static void scale_f(float *p, size_t n, float s)
 	irl_parallel_for(n, IRL_PAR_GRAIN, scale_range, &c);
 }
 
-/* shared device set-up of IrlOsem and IrlGenprj */
-void irl_device_setup(irl_parms *p, irl_view *views, const float *atn_internal, const irl_esse_host *esse,
-	int fast_rotate, int max_batch)
+/* device context, rotation tables and column masks: everything that
+   depends only on the geometry and the views */
+void irl_device_geometry(irl_parms *p, irl_view *views, int fast_rotate, int max_batch)
 {
 	irlcu_geom g;
 	float *angles = (float *)irl_malloc(sizeof(float) * p->nviews, "angles");
 	unsigned char *mask = (unsigned char *)irl_malloc((size_t)p->nviews * p->n, "column masks");
 	unsigned char *m1 = (unsigned char *)irl_malloc(p->n, "mask"), *m2 = (unsigned char *)irl_malloc(p->n, "mask");
-	int a, i;
+	int a, i, rc;
 	g.n = p->n;
 	g.nz = p->nz;
 	g.nviews = p->nviews;
 	g.fast_rotate = fast_rotate;
 	g.max_batch = max_batch;
-	irl_cu(irlcu_init(&g), "device set-up");
-	for (a = 0; a < p->nviews; ++a)
-		angles[a] = views[a].angle;
-	irl_cu(irlcu_set_angles(angles), "device set-up");
 	for (a = 0; a < p->nviews; ++a) {
+		angles[a] = views[a].angle;
 		/* PWid = PixelWidth / BinWidth = 1 (IrlSetup.c:65-66) */
-		float pw = p->pix / p->pix;
-		irl_measured_columns(views[a].left, pw, p->n, p->nbins, m1);
-		irl_norm_columns(views[a].left, views[a].right, pw, p->n, p->nbins, m2);
+		irl_measured_columns(views[a].left, p->pix / p->pix, p->n, p->nbins, m1);
+		irl_norm_columns(views[a].left, views[a].right, p->pix / p->pix, p->n, p->nbins, m2);
 		for (i = 0; i < p->n; ++i)
 			mask[(size_t)a * p->n + i] = (unsigned char)(m1[i] | (m2[i] << 1));
 	}
-	irl_cu(irlcu_set_column_mask(mask), "device set-up");
-	if (atn_internal != NULL) {
-		irl_cu(irlcu_upload(IRLCU_BUF_ATN, 0, atn_internal, (size_t)p->n * p->nz * p->n), "device set-up");
-		irl_cu(irlcu_prepare_attenuation((p->model & MODEL_SRF) != 0), "device set-up");
-	}
+	rc = irlcu_init(&g);
+	if (rc == 0)
+		rc = irlcu_set_angles(angles);
+	if (rc == 0)
+		rc = irlcu_set_column_mask(mask);
+	free(angles);
+	free(mask);
+	free(m1);
+	free(m2);
+	irl_cu(rc, "device set-up");
+}
+
+/* DRF tables and the ESSE kernel spectra */
+void irl_device_tables(irl_parms *p, irl_view *views, const irl_esse_host *esse)
+{
 	if (p->model & MODEL_DRF)
 		irl_upload_drf(p, views, 0, NULL);
 	if ((p->model & MODEL_SRF) && esse != NULL && esse->on) {
@@ -266,21 +279,32 @@ void irl_device_setup(irl_parms *p, irl_view *views, const float *atn_internal, 
 		e.mu_avg = esse->mu_avg;
 		e.pix = esse->pix;
 		e.cntr_pix_fac = esse->cntr_pix_fac;
-		e.krnl = esse->krnl;
-		e.kmu = esse->kmu;
-		e.kmu2 = esse->kmu2;
+		e.noffs = esse->noffs;
+		e.ndepths = esse->ndepths;
+		e.krnl = esse->krnl_file;
+		e.mu = esse->mu_file;
+		e.kmu_outside = esse->kmu_outside;
 		irl_cu(irlcu_set_esse(&e), "ESSE set-up");
 	} else if (p->model & MODEL_SRF) {
 		irl_cu(irlcu_set_esse(NULL), "ESSE set-up");
 	}
-	free(angles);
-	free(mask);
-	free(m1);
-	free(m2);
+}
+
+/* the whole device set-up of IrlGenprj, from an attenuation map already
+   in the internal layout */
+void irl_device_setup(irl_parms *p, irl_view *views, const float *atn_internal, const irl_esse_host *esse,
+	int fast_rotate, int max_batch)
+{
+	irl_device_geometry(p, views, fast_rotate, max_batch);
+	if (atn_internal != NULL) {
+		irl_cu(irlcu_upload(IRLCU_BUF_ATN, 0, atn_internal, (size_t)p->n * p->nz * p->n), "device set-up");
+		irl_cu(irlcu_prepare_attenuation((p->model & MODEL_SRF) != 0), "device set-up");
+	}
+	irl_device_tables(p, views, esse);
 }
 
 /* normalisation images of every subset (psComputeNormImages,
-   osemrecon.c:223-343) */
+   osemrecon.c:223-343), into the norm buffers irlcu_alloc_norm made */
 static void compute_norms(void)
 {
 	irl_parms *p = &S.p;
@@ -288,7 +312,6 @@ static void compute_norms(void)
 	float *img = NULL;
 	int s, m;
 	double t0 = now_s();
-	irl_cu(irlcu_alloc_norm(S.ns), "OsemRecon");
 	for (s = 0; s < S.ns; ++s) {
 		for (m = 0; m < S.per; ++m)
 			vt[m] = S.views[S.ang[s * S.per + m]].view_time;
@@ -384,42 +407,88 @@ int IrlGetScatterSurrogateNrmse(float *pfNrmse, int iNumViews)
 	return 0;
 }
 
-/* libirl's serial float sum of the projections (the initial estimate's
-   mean) runs on a helper thread while the scatter kernel and the DRF tables
-   are read and prepared; it only reads the caller's projections, which
-   nothing changes before it is joined */
+/* Host work of the set-up that runs on helper threads while the device
+   builds its tables.  Neither allocates nor raises an error (a failed
+   upload is returned in prj_job.rc).
+   - prj_job: libirl's serial float sum of the projections (the initial
+     estimate's mean, initial_est.c:89-95), then the clamp of the caller's
+     projections (irlosem.c:205), then their upload beside the queued
+     kernels; the sum reads them before the clamp, as libirl's does.
+   - atn_job: the caller's attenuation map reordered in place to the
+     internal layout (irlosem.c:170-176), through the session's temporary
+     volume.  It starts once the device has its own copy of the map. */
 typedef struct {
-	const float *prj;
+	float *prj;
 	size_t count;
+	int need_sum;
 	float sum;
-} prj_sum_job;
+	int rc;
+} prj_job;
 
-static void *prj_sum_thread(void *arg)
+typedef struct {
+	int n, nz;
+	float *atn, *tmp;
+} atn_job;
+
+static void *prj_thread(void *arg)
 {
-	prj_sum_job *j = (prj_sum_job *)arg;
-	j->sum = irl_projection_sum(j->prj, j->count);
+	prj_job *j = (prj_job *)arg;
+	if (j->need_sum)
+		j->sum = irl_projection_sum(j->prj, j->count);
+	zero_neg(j->prj, j->count);
+	j->rc = irlcu_upload_now(IRLCU_BUF_PRJ, 0, j->prj, j->count);
 	return NULL;
 }
 
+static void *atn_thread(void *arg)
+{
+	atn_job *j = (atn_job *)arg;
+	const size_t vox = (size_t)j->n * j->nz * j->n;
+	irl_reorder(j->nz, j->n, j->n, j->atn, j->tmp);
+	memcpy(j->atn, j->tmp, sizeof(float) * vox);
+	return NULL;
+}
+
+/* runs fn(arg) on a new thread, or here when none can be started */
+static int start_helper(pthread_t *th, void *(*fn)(void *), void *arg)
+{
+	if (pthread_create(th, NULL, fn, arg) == 0)
+		return 1;
+	fn(arg);
+	return 0;
+}
+
+/* The set-up keeps the device busy while the host works: the device gets
+   the attenuation map first (transposed, scaled and clamped on the device)
+   and builds the per-view tables while the host reads the scatter kernel
+   and the DRF tables; the normalisation images are queued before the host
+   computes the initial estimate and the caller-visible changes of its
+   arrays.  The results are those of libirl's serial order
+   (irlosem.c:150-243): every step reads what it read there. */
 int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, char *krnl_fname,
 	void (*cb)(int, float *), float *scatest, float *atn, float *prj, float *recon, char *logname, char *msgname)
 {
 	jmp_buf env;
 	int err, m;
 	double t0 = now_s();
+	g_mark_t0 = t0;
 	/* static: read after a longjmp back to the trap (the library keeps one
 	   session per process) */
-	static prj_sum_job sum_job;
-	static pthread_t sum_th;
-	static volatile int sum_running;
+	static prj_job pjob;
+	static atn_job ajob;
+	static pthread_t prj_th, atn_th;
+	static volatile int prj_running, atn_running;
 	if (S.open)
 		session_close();
 	memset(&S, 0, sizeof(S));
 	S.open = 1;
 	S.hook_norm = -1;
 	if ((err = setjmp(env)) != 0) {
-		if (sum_running)
-			pthread_join(sum_th, NULL);
+		if (prj_running)
+			pthread_join(prj_th, NULL);
+		if (atn_running)
+			pthread_join(atn_th, NULL);
+		prj_running = atn_running = 0;
 		fprintf(stderr, "FATAL ERROR Trapped: err_num=%d\nErrMsg=%s\n", err, irl_last_error());
 		irl_msg(1, "aborted\n");
 		irl_untrap();
@@ -427,24 +496,43 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		return err;
 	}
 	irl_trap(&env);
-	sum_running = 0;
+	prj_running = atn_running = 0;
 	open_logs(logname, msgname, op->iMsgLevel, &S.logfp, &S.msgfp);
 	irl_setup_parms(ip, op, atn, krnl_fname, &S.p);
-	if (!op->bReconIsInitEst && prj != NULL) {
-		sum_job.prj = prj;
-		sum_job.count = (size_t)S.p.n * S.p.nz * S.p.nviews;
-		sum_job.sum = 0.0f;
-		if (pthread_create(&sum_th, NULL, prj_sum_thread, &sum_job) == 0)
-			sum_running = 1;
-		else
-			sum_job.sum = irl_projection_sum(prj, sum_job.count);
-	}
+	S.vox = (size_t)S.p.n * S.p.nz * S.p.n;
+	S.prjn = (size_t)S.p.n * S.p.nz * S.p.nviews;
 	S.views = irl_setup_views(ip, pv);
-	if (S.p.model & MODEL_SRF) {
-		if (atn == NULL)
-			irl_fatal(IRL_E_VALUE, "SrfSetup", "scatter modelling needs an attenuation map");
-		irl_esse_prepare(krnl_fname, &S.p, ip->SrfCollapseFac, &S.esse);
+	if ((S.p.model & MODEL_SRF) && atn == NULL)
+		irl_fatal(IRL_E_VALUE, "SrfSetup", "scatter modelling needs an attenuation map");
+	S.tmp = (float *)irl_malloc(sizeof(float) * S.vox, "IrlOsem:Temp");
+	S.per = S.p.ang_per_subset;
+	S.max_batch = S.per > 32 ? 32 : S.per;
+	S.ns = irl_compute_subsets(S.p.nviews, S.per, &S.ang);
+	mark("parms and views");
+
+	/* device: geometry, then the attenuation map and its per-view tables
+	   (queued; they build while the host reads the kernel and DRF files) */
+	irl_device_geometry(&S.p, S.views, g_irl_adv.bFastRotate, S.max_batch);
+	if (prj == NULL)
+		irl_fatal(IRL_E_VALUE, "IrlOsem", "no projections given");
+	pjob.prj = prj;
+	pjob.count = S.prjn;
+	pjob.need_sum = !op->bReconIsInitEst;
+	pjob.sum = 0.0f;
+	pjob.rc = 0;
+	prj_running = start_helper(&prj_th, prj_thread, &pjob);
+	if (atn != NULL) {
+		irl_cu(irlcu_upload_external(IRLCU_BUF_ATN, atn, ip->fAtnScaleFac, 1), "IrlOsem");
+		irl_cu(irlcu_prepare_attenuation((S.p.model & MODEL_SRF) != 0), "IrlOsem");
+		ajob.n = S.p.n;
+		ajob.nz = S.p.nz;
+		ajob.atn = atn;
+		ajob.tmp = S.tmp;
+		atn_running = start_helper(&atn_th, atn_thread, &ajob);
 	}
+	mark("attenuation queued");
+	if (S.p.model & MODEL_SRF)
+		irl_esse_prepare(krnl_fname, &S.p, ip->SrfCollapseFac, &S.esse);
 	irl_msg(5, "Done scatter kernel (%.3f s)\n", now_s() - t0);
 	{
 		irl_detector *d;
@@ -452,27 +540,49 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		irl_setup_drf_tables(&S.p, op, S.views, drf_fname, &d);
 	}
 	irl_msg(5, "Done DRF tables (%.3f s)\n", now_s() - t0);
-	S.vox = (size_t)S.p.n * S.p.nz * S.p.n;
-	S.prjn = (size_t)S.p.n * S.p.nz * S.p.nviews;
-	S.tmp = (float *)irl_malloc(sizeof(float) * S.vox, "IrlOsem:Temp");
-	if (atn != NULL) {
-		irl_reorder(S.p.nz, S.p.n, S.p.n, atn, S.tmp);
-		memcpy(atn, S.tmp, sizeof(float) * S.vox);
+	irl_device_tables(&S.p, S.views, &S.esse);
+	irl_msg(5, "Done device set-up (%.3f s)\n", now_s() - t0);
+
+	if ((S.p.prj_model & MODEL_SRF) && S.p.srf_iters > 0) {
+		S.prjscat = (float *)irl_calloc(sizeof(float) * S.prjn, "OsemRecon:PrjScatEst");
+		irl_cu(irlcu_zero(IRLCU_BUF_PRJSCAT, 0), "IrlOsem");
 	}
-	if (!op->bReconIsInitEst) {
-		if (sum_running) {
-			pthread_join(sum_th, NULL);
-			sum_running = 0;
+	irl_cu(irlcu_alloc_norm(S.ns), "OsemRecon");
+	{
+		/* every subset's views on the device, for whole-iteration launches */
+		const int tot = S.ns * S.per;
+		irlcu_view_parm *all = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * tot, "subset views");
+		int i;
+		for (i = 0; i < tot; ++i) {
+			all[i].view_time = S.views[S.ang[i]].view_time;
+			all[i].sensitivity = S.views[S.ang[i]].sensitivity;
 		}
-		if (prj == NULL)
-			irl_fatal(IRL_E_VALUE, "IrlOsem", "no projections given");
-		irl_initial_estimate_sum(&S.p, op->bUseContourSupport, op->fAtnMapThresh, S.views, sum_job.sum, atn,
+		m = irlcu_set_subsets(S.ns, S.per, S.ang, all);
+		free(all);
+		irl_cu(m, "OsemRecon");
+	}
+	compute_norms();
+	mark("norms queued");
+
+	/* host: the initial estimate and the caller-visible changes of the
+	   attenuation map and the scatter estimate, while the norms run */
+	if (atn_running) {
+		pthread_join(atn_th, NULL);
+		atn_running = 0;
+	}
+	if (prj_running) {
+		pthread_join(prj_th, NULL);
+		prj_running = 0;
+	}
+	irl_cu(pjob.rc, "IrlOsem");
+	if (!op->bReconIsInitEst) {
+		irl_initial_estimate_sum(&S.p, op->bUseContourSupport, op->fAtnMapThresh, S.views, pjob.sum, atn,
 			recon);
 	} else {
 		irl_reorder(S.p.nz, S.p.n, S.p.n, recon, S.tmp);
 		memcpy(recon, S.tmp, sizeof(float) * S.vox);
 	}
-	zero_neg(prj, S.prjn);
+	mark("initial estimate");
 	if (atn != NULL) {
 		if (ip->fAtnScaleFac > 0 && ip->fAtnScaleFac != 1.0)
 			scale_f(atn, S.vox, ip->fAtnScaleFac);
@@ -489,36 +599,14 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 		cb(0, S.tmp);
 	}
 	irl_msg(5, "Done host set-up (%.3f s)\n", now_s() - t0);
-	S.per = S.p.ang_per_subset;
-	S.max_batch = S.per > 32 ? 32 : S.per;
-	S.ns = irl_compute_subsets(S.p.nviews, S.per, &S.ang);
-	irl_device_setup(&S.p, S.views, atn, &S.esse, g_irl_adv.bFastRotate, S.max_batch);
-	irl_msg(5, "Done device set-up (%.3f s)\n", now_s() - t0);
-	irl_cu(irlcu_upload(IRLCU_BUF_PRJ, 0, prj, S.prjn), "IrlOsem");
-	irl_cu(irlcu_upload(IRLCU_BUF_EST, 0, recon, S.vox), "IrlOsem");
+	/* beside the norms still running: no queued kernel reads the estimate */
+	irl_cu(irlcu_upload_now(IRLCU_BUF_EST, 0, recon, S.vox), "IrlOsem");
 	if (scatest != NULL)
 		irl_cu(irlcu_upload(IRLCU_BUF_SCATEST, 0, scatest, S.prjn), "IrlOsem");
 	S.use_scatest = scatest != NULL;
-	if ((S.p.prj_model & MODEL_SRF) && S.p.srf_iters > 0) {
-		S.prjscat = (float *)irl_calloc(sizeof(float) * S.prjn, "OsemRecon:PrjScatEst");
-		irl_cu(irlcu_zero(IRLCU_BUF_PRJSCAT, 0), "IrlOsem");
-	}
 	S.recon = recon;
 	S.cb = cb;
 	irl_msg(5, "Done Initialization (%.3f s)\n", now_s() - t0);
-	compute_norms();
-	{
-		/* every subset's views on the device, for whole-iteration launches */
-		const int tot = S.ns * S.per;
-		irlcu_view_parm *all = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * tot, "subset views");
-		int i;
-		for (i = 0; i < tot; ++i) {
-			all[i].view_time = S.views[S.ang[i]].view_time;
-			all[i].sensitivity = S.views[S.ang[i]].sensitivity;
-		}
-		irl_cu(irlcu_set_subsets(S.ns, S.per, S.ang, all), "OsemRecon");
-		free(all);
-	}
 	if (g_sur_fname != NULL && (S.p.prj_model & MODEL_SRF) && S.p.srf_iters > 0)
 		sur_load();
 	for (m = 0; m < 6; ++m)
@@ -535,6 +623,7 @@ int IrlOsemBegin(IrlParms_t *ip, Options_t *op, PrjView_t *pv, char *drf_fname, 
 	S.p.start_iteration = g_irl_adv.iStartIteration;
 	S.it = S.p.start_iteration;
 	S.vp = (irlcu_view_parm *)irl_calloc(sizeof(irlcu_view_parm) * S.per, "view parameters");
+	mark("set-up returns");
 	irl_untrap();
 	return 0;
 }
@@ -678,8 +767,10 @@ int IrlOsemEnd(float *recon)
 		for (s = 0; s < S.ns; ++s)
 			norm_file(S.p.norm_base, s, NULL, 0, 1);
 	}
+	g_mark_t0 = now_s();
 	if (recon != NULL)
 		irl_cu(irlcu_download_external(IRLCU_BUF_EST, recon), "IrlOsem");
+	mark("end: image download");
 	irl_untrap();
 	session_close();
 	return 0;

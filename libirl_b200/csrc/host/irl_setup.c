@@ -426,79 +426,82 @@ void irl_upload_drf(const irl_parms *p, irl_view *views, int ndet, irl_detector 
 
 /* ------------------------------------------------------------------- ESSE */
 
-/* pfReorder3dKrnl, krnlprj3d.c:43-128: one-quadrant kernel -> wrap-around
-   order [depth][slice][offset] with the depth axis flipped */
-static float *reorder_krnl(const float *in, int noffs, int ndepths, int oxd, int oyd, int ozd)
-{
-	float *out = (float *)irl_calloc(sizeof(float) * (size_t)oxd * oyd * ozd, "reordered kernel");
-	int xmin = MIN(noffs, oxd / 2), ymin = MIN(noffs, oyd / 2), izin, iy, ix;
-	for (izin = 0; izin < ndepths; ++izin) {
-		int izout = ozd / 2 - izin + ndepths / 2 - 1;
-		if (izout < 0 || izout >= ozd)
-			continue;
-		izout += izout < ozd / 2 ? ozd / 2 : -ozd / 2;
-		for (iy = 0; iy < ymin; iy++) {
-			for (ix = 0; ix < xmin; ix++) {
-				float v = in[ix + noffs * (iy + noffs * izin)];
-				int yo[2] = {iy, oyd - iy}, xo[2] = {ix, oxd - ix}, a, b;
-				for (a = 0; a < (iy > 0 ? 2 : 1); ++a)
-					for (b = 0; b < (ix > 0 ? 2 : 1); ++b)
-						out[xo[b] + (size_t)oxd * (yo[a] + (size_t)oyd * izout)] = v;
-			}
-		}
-	}
-	return out;
-}
+/* pfReorder3dKrnl, krnlprj3d.c:43-128, puts the file's one-quadrant kernel
+   [depth][y offset][x offset] into a wrap-around grid [depth][slice][offset]
+   of oxd x oyd x ozd with the depth axis flipped: offset ix < xmin =
+   min(noffs, oxd/2) lands on x = ix and, for ix > 0, on its mirror
+   oxd - ix; the same along y; depth izin on the plane
+   ozd/2 - izin + ndepths/2 - 1, rotated by half the axis.  Everything else
+   is 0.  The device builds the grids (irlcu_esse_expand); the host only
+   needs the grid indices that hold kernel values, in increasing order, with
+   the file index each one comes from. */
+typedef struct {
+	size_t count;
+	size_t *grid;   /* grid index, increasing */
+	int *file;      /* index into the file's arrays */
+} krnl_support_map;
 
-/* the grid indices reorder_krnl can write, in increasing order: depth
-   planes that a kernel distance lands on, and the x and y offsets below
-   the half-widths with their mirrors at the top of each axis */
-static size_t *krnl_support(int noffs, int ndepths, int oxd, int oyd, int ozd, size_t *count)
+static krnl_support_map krnl_support(int noffs, int ndepths, int oxd, int oyd, int ozd)
 {
 	int xmin = MIN(noffs, oxd / 2), ymin = MIN(noffs, oyd / 2), nxs = 0, nys = 0, iz, iy, ix, t;
 	int *xs = (int *)irl_malloc(sizeof(int) * 2 * (size_t)(xmin + 1), "kernel support");
+	int *xf = (int *)irl_malloc(sizeof(int) * 2 * (size_t)(xmin + 1), "kernel support");
 	int *ys = (int *)irl_malloc(sizeof(int) * 2 * (size_t)(ymin + 1), "kernel support");
-	unsigned char *zon = (unsigned char *)irl_calloc((size_t)ozd, "kernel support");
-	size_t *out, n = 0;
-	for (t = 0; t < xmin; ++t)
-		xs[nxs++] = t;
-	for (t = oxd - xmin + 1; t < oxd; ++t)
-		xs[nxs++] = t;
-	for (t = 0; t < ymin; ++t)
-		ys[nys++] = t;
-	for (t = oyd - ymin + 1; t < oyd; ++t)
-		ys[nys++] = t;
+	int *yf = (int *)irl_malloc(sizeof(int) * 2 * (size_t)(ymin + 1), "kernel support");
+	int *zin = (int *)irl_malloc(sizeof(int) * (size_t)ozd, "kernel support");
+	krnl_support_map m;
+	for (t = 0; t < xmin; ++t, ++nxs)
+		xs[nxs] = xf[nxs] = t;
+	for (t = oxd - xmin + 1; t < oxd; ++t, ++nxs) {
+		xs[nxs] = t;
+		xf[nxs] = oxd - t;
+	}
+	for (t = 0; t < ymin; ++t, ++nys)
+		ys[nys] = yf[nys] = t;
+	for (t = oyd - ymin + 1; t < oyd; ++t, ++nys) {
+		ys[nys] = t;
+		yf[nys] = oyd - t;
+	}
+	for (iz = 0; iz < ozd; ++iz)
+		zin[iz] = -1;
 	for (t = 0; t < ndepths; ++t) {
 		int z = ozd / 2 - t + ndepths / 2 - 1;
 		if (z < 0 || z >= ozd)
 			continue;
 		z += z < ozd / 2 ? ozd / 2 : -ozd / 2;
-		zon[z] = 1;
+		zin[z] = t;
 	}
-	out = (size_t *)irl_malloc(sizeof(size_t) * ((size_t)nxs * nys * ozd + 1), "kernel support");
+	m.count = 0;
+	m.grid = (size_t *)irl_malloc(sizeof(size_t) * ((size_t)nxs * nys * ozd + 1), "kernel support");
+	m.file = (int *)irl_malloc(sizeof(int) * ((size_t)nxs * nys * ozd + 1), "kernel support");
 	for (iz = 0; iz < ozd; ++iz)
-		if (zon[iz])
+		if (zin[iz] >= 0)
 			for (iy = 0; iy < nys; ++iy)
-				for (ix = 0; ix < nxs; ++ix)
-					out[n++] = xs[ix] + (size_t)oxd * (ys[iy] + (size_t)oyd * iz);
+				for (ix = 0; ix < nxs; ++ix) {
+					m.grid[m.count] = xs[ix] + (size_t)oxd * (ys[iy] + (size_t)oyd * iz);
+					m.file[m.count++] = xf[ix] + noffs * (yf[iy] + noffs * zin[iz]);
+				}
 	free(xs);
+	free(xf);
 	free(ys);
-	free(zon);
-	*count = n;
-	return out;
+	free(yf);
+	free(zin);
+	return m;
 }
 
 /* pvInitESSEScatterModel + pvInitScatterPrj, krnlprj3d.c:956-1009, 403-547,
    with libirl's hard-coded parameters "2 2 2 3" (IrlSetup.c:169-174):
-   xy pad 2, z pad 2, two Taylor terms, 3D geometry */
+   xy pad 2, z pad 2, two Taylor terms, 3D geometry.  The kernel stays in
+   its file form; its grids K and K (mu - mu_avg) are built on the device. */
 void irl_esse_prepare(const char *fname, const irl_parms *p, int c, irl_esse_host *e)
 {
 	const float xypad = 2, zpad = 2;
 	const int nterms = 2;
 	KrnlData_t *k;
 	int nx, ny, nz;
-	size_t i, cnt;
-	float fKs = 0.0f, fKMs = 0.0f, *mu;
+	size_t q, fcount;
+	float fKs = 0.0f, fKMs = 0.0f;
+	krnl_support_map sup;
 	memset(e, 0, sizeof(*e));
 	if (c < 1 || c > 4)
 		irl_fatal(IRL_E_VALUE, "SrfSetup", "srf_collapse_fac = %d: must be 1 (no collapse) to 4", c);
@@ -522,39 +525,34 @@ void irl_esse_prepare(const char *fname, const irl_parms *p, int c, irl_esse_hos
 	e->kx = nx;
 	e->ky = ny;
 	e->kz = nz;
-	e->krnl = reorder_krnl(k->pfKrnl, k->iNumXYoffs, k->iNumDists, nx, nz, ny);
-	mu = reorder_krnl(k->pfKrnlMu, k->iNumXYoffs, k->iNumDists, nx, nz, ny);
-	cnt = (size_t)nx * ny * nz;
-	/* libirl's float sums run over the whole grid in index order
+	e->noffs = k->iNumXYoffs;
+	e->ndepths = k->iNumDists;
+	fcount = (size_t)e->noffs * e->noffs * e->ndepths;
+	e->krnl_file = (float *)irl_malloc(sizeof(float) * fcount, "ESSE kernel");
+	e->mu_file = (float *)irl_malloc(sizeof(float) * fcount, "ESSE mu kernel");
+	memcpy(e->krnl_file, k->pfKrnl, sizeof(float) * fcount);
+	memcpy(e->mu_file, k->pfKrnlMu, sizeof(float) * fcount);
+	/* libirl's float sums run over the whole reordered grid in index order
 	   (krnlprj3d.c:495-510).  Outside the kernel's support both grids hold
 	   +0, and adding +0 (or the product +0 * 0) to a float sum that starts at
 	   +0 leaves it unchanged, so summing the support in the same order gives
-	   the same bits in a small fraction of the work. */
-	{
-		size_t ns = 0, q;
-		size_t *sup = krnl_support(k->iNumXYoffs, k->iNumDists, nx, nz, ny, &ns);
-		for (q = 0; q < ns; ++q) {
-			fKs += e->krnl[sup[q]];
-			fKMs += e->krnl[sup[q]] * mu[sup[q]];
-		}
-		if (fKs == 0.0) {
-			irl_warn("InitScatterPrj", "Sum of Krnl is 0!");
-			e->mu_avg = k->fKrnlMu0;
-		} else {
-			e->mu_avg = fKMs / fKs;
-		}
-		/* K (mu - mu_avg): outside the support (0 - mu_avg) * 0 everywhere */
-		e->kmu = (float *)irl_malloc(sizeof(float) * cnt, "K mu");
-		{
-			const float outside = (0.0f - e->mu_avg) * 0.0f;
-			for (i = 0; i < cnt; ++i)
-				e->kmu[i] = outside;
-		}
-		for (q = 0; q < ns; ++q)
-			e->kmu[sup[q]] = (mu[sup[q]] - e->mu_avg) * e->krnl[sup[q]];
-		free(sup);
+	   the same bits. */
+	sup = krnl_support(e->noffs, e->ndepths, nx, nz, ny);
+	for (q = 0; q < sup.count; ++q) {
+		const float kv = e->krnl_file[sup.file[q]];
+		fKs += kv;
+		fKMs += kv * e->mu_file[sup.file[q]];
 	}
-	free(mu);
+	free(sup.grid);
+	free(sup.file);
+	if (fKs == 0.0) {
+		irl_warn("InitScatterPrj", "Sum of Krnl is 0!");
+		e->mu_avg = k->fKrnlMu0;
+	} else {
+		e->mu_avg = fKMs / fKs;
+	}
+	/* K (mu - mu_avg) outside the support: (0 - mu_avg) * 0 */
+	e->kmu_outside = (0.0f - e->mu_avg) * 0.0f;
 	if (fabs(k->fPixSize - p->pix * c) > 0.02)
 		irl_warn("vInitESSEScatterModel", "Pixel size after collapse=%.3g, Pixel size in kernel=%.3g",
 			c * p->pix, k->fPixSize);
@@ -566,9 +564,8 @@ void irl_esse_prepare(const char *fname, const irl_parms *p, int c, irl_esse_hos
 
 void irl_esse_free(irl_esse_host *e)
 {
-	free(e->krnl);
-	free(e->kmu);
-	free(e->kmu2);
+	free(e->krnl_file);
+	free(e->mu_file);
 	memset(e, 0, sizeof(*e));
 }
 
@@ -590,28 +587,36 @@ static void zero_behind(int nd, float fSin, float fCos, float fRadius, float *pi
 	}
 }
 
+/* One pass over the estimate's rows (r, s) writes what libirl's three
+   passes leave (initial_est.c:97-157): the mean or the contour image, 0 where
+   the attenuation map is below the threshold, 0 outside the circle. */
 typedef struct {
 	float *init;
-	float v;
-	const float *atn;
+	float v;                      /* the mean, when img is NULL */
+	const float *img;             /* contour image [r][c], or NULL */
+	const unsigned char *outside; /* [r][c]: beyond the reconstruction circle */
+	const float *atn;             /* internal layout, or NULL for no map mask */
 	float thresh;
-} fill_ctx;
+	int n, nz;
+} init_ctx;
 
-static void fill_range(size_t lo, size_t hi, void *c)
+static void init_range(size_t lo, size_t hi, void *c)
 {
-	const fill_ctx *f = (const fill_ctx *)c;
-	size_t i;
-	for (i = lo; i < hi; ++i)
-		f->init[i] = f->v;
-}
-
-static void mask_range(size_t lo, size_t hi, void *c)
-{
-	const fill_ctx *f = (const fill_ctx *)c;
-	size_t i;
-	for (i = lo; i < hi; ++i)
-		if (f->atn[i] < f->thresh)
-			f->init[i] = 0.0;
+	const init_ctx *f = (const init_ctx *)c;
+	const int n = f->n;
+	size_t q;
+	int x;
+	for (q = lo; q < hi; ++q) {
+		const size_t r = q / (size_t)f->nz;
+		float *out = f->init + q * n;
+		const float *a = f->atn != NULL ? f->atn + q * n : NULL;
+		for (x = 0; x < n; ++x) {
+			float v = f->img != NULL ? f->img[x + r * n] : f->v;
+			if ((a != NULL && a[x] < f->thresh) || f->outside[r * n + x])
+				v = 0.0f;
+			out[x] = v;
+		}
+	}
 }
 
 /* pfComputeInitialEstimate, initial_est.c:29-158 (internal layout) */
@@ -636,7 +641,7 @@ float *irl_initial_estimate(const irl_parms *p, int contour, float thresh, const
 float *irl_initial_estimate_sum(const irl_parms *p, int contour, float thresh, const irl_view *views, float fSum,
 	const float *atn, float *init)
 {
-	int n = p->n, nz = p->nz, na = p->nviews, a, s, r, c2, use_map = 0;
+	int n = p->n, nz = p->nz, na = p->nviews, a, r, c2, use_map = 0;
 	size_t i;
 	float fNum = (float)(n * n * nz), fAvg, fMapThresh = 0.0f;
 	fNum *= M_PI / 4.0;
@@ -650,29 +655,20 @@ float *irl_initial_estimate_sum(const irl_parms *p, int contour, float thresh, c
 		else
 			use_map = fMapThresh > 0.0;
 	}
-	if (!contour) {
-		fill_ctx fc = {init, fAvg, NULL, 0.0f};
-		irl_parallel_for((size_t)n * nz * n, IRL_PAR_GRAIN, fill_range, &fc);
-	} else {
-		float *img = (float *)irl_malloc(sizeof(float) * n * n, "contour image");
-		for (i = 0; i < (size_t)n * n; ++i)
-			img[i] = fAvg;
-		for (a = 0; a < na; ++a) {
-			double d = views[a].angle;
-			zero_behind(n, (float)sin(d), (float)cos(d), views[a].cfcr / p->pix, img);
-		}
-		for (s = 0; s < nz; ++s)
-			for (r = 0; r < n; ++r)
-				for (c2 = 0; c2 < n; ++c2)
-					init[(size_t)r * nz * n + (size_t)s * n + c2] = img[c2 + r * n];
-		free(img);
-	}
-	if (use_map) {
-		fill_ctx mc = {init, 0.0f, atn, fMapThresh};
-		irl_parallel_for((size_t)n * nz * n, IRL_PAR_GRAIN, mask_range, &mc);
-	}
 	{
+		float *img = NULL;
+		unsigned char *outside = (unsigned char *)irl_malloc((size_t)n * n, "circle mask");
 		float fRadius = (float)n * 0.5, fX, fY, fCent = fRadius;
+		init_ctx ic;
+		if (contour) {
+			img = (float *)irl_malloc(sizeof(float) * n * n, "contour image");
+			for (i = 0; i < (size_t)n * n; ++i)
+				img[i] = fAvg;
+			for (a = 0; a < na; ++a) {
+				double d = views[a].angle;
+				zero_behind(n, (float)sin(d), (float)cos(d), views[a].cfcr / p->pix, img);
+			}
+		}
 		for (r = 0; r < n; ++r) {
 			fY = (float)r - fCent;
 			if (fY > 0)
@@ -681,11 +677,20 @@ float *irl_initial_estimate_sum(const irl_parms *p, int contour, float thresh, c
 				fX = (float)c2 - fCent;
 				if (fX > 0)
 					fX += 1;
-				if (hypot(fX, fY) > fRadius)
-					for (s = 0; s < nz; ++s)
-						init[(size_t)r * nz * n + (size_t)s * n + c2] = 0.0;
+				outside[(size_t)r * n + c2] = hypot(fX, fY) > fRadius;
 			}
 		}
+		ic.init = init;
+		ic.v = fAvg;
+		ic.img = img;
+		ic.outside = outside;
+		ic.atn = use_map ? atn : NULL;
+		ic.thresh = fMapThresh;
+		ic.n = n;
+		ic.nz = nz;
+		irl_parallel_for((size_t)n * nz, (IRL_PAR_GRAIN + n - 1) / n, init_range, &ic);
+		free(img);
+		free(outside);
 	}
 	return init;
 }
