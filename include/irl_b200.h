@@ -56,9 +56,11 @@ typedef struct {
 
 /* Runs nprob independent OSEM reconstructions, each exactly as IrlOsem
    would run it alone (same results).  Every problem has its own device
-   context and stream; they run pipelined: while the device iterates one
-   problem (all its iterations enqueued at once), the host sets up the next
-   and finishes the one before, so at most two are resident at a time.
+   context and stream; they run pipelined: while the device iterates the
+   problems enqueued so far (all iterations of each at once), the host sets
+   up the next.  Up to IRL_BATCH_DEPTH (environment, default 4) problems are
+   resident at a time, fewer when the next one might not fit in device
+   memory; the oldest is finished first.
    Not allowed with hooks, or with iSetupExtraPrjViewData /
    iSetupDetectors data pending (those are per-call state of IrlOsem).
    Returns 0, or the first non-zero iStatus. */

@@ -225,6 +225,10 @@ int irlcu_shear_tuning(float ms[4], int form[2]);
    returns the previous setting. */
 int irlcu_shape_trials(int on);
 
+/* Device memory that new contexts can use: cudaMemGetInfo's free bytes
+   plus what the stream-ordered pool holds unused; and the total. */
+int irlcu_mem_info(size_t *free_bytes, size_t *total_bytes);
+
 /* Iteration-callback snapshots of the estimate, overlapped with the next
    iteration: irlcu_snapshot_begin(slot) queues, after the work queued so
    far, a copy of the estimate in external layout into the slot's pinned

@@ -454,6 +454,23 @@ static bool shear_trial_step(Ctx &c) {
   return false;
 }
 
+int irlcu_mem_info(size_t *free_bytes, size_t *total_bytes) {
+  size_t fr = 0, tot = 0;
+  CU_TRY(cudaMemGetInfo(&fr, &tot));
+  // blocks the stream-ordered pool keeps for reuse count as free
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+      fr += (size_t)(reserved - used);
+  }
+  if (free_bytes) *free_bytes = fr;
+  if (total_bytes) *total_bytes = tot;
+  return IRLCU_OK;
+}
+
 int irlcu_shape_trials(int on) {
   const int prev = g_shape_trials ? 1 : 0;
   g_shape_trials = on != 0;

@@ -818,11 +818,29 @@ static int batch_end(parked_session **h, IrlOsemProblem_t *pp, int p, int err)
 	return e;
 }
 
+/* problems of a batch in flight at once (IRL_BATCH_DEPTH, default 4) */
+static int batch_depth(void)
+{
+	const char *e = getenv("IRL_BATCH_DEPTH");
+	int d = e != NULL ? atoi(e) : 4;
+	return d < 1 ? 1 : d > 64 ? 64 : d;
+}
+
+/* a generous estimate of one problem's device memory: the per-view
+   attenuation tables (three with the scatter model), the norm images and
+   the batch work space, in volumes */
+static double batch_need_bytes(const IrlOsemProblem_t *q)
+{
+	const IrlParms_t *ip = q->psIrlParms;
+	const double vox = (double)ip->NumPixels * ip->NumPixels * ip->NumSlices;
+	return 4.0 * vox * (3.0 * ip->NumViews + 96.0);
+}
+
 int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 {
 	jmp_buf env;
 	parked_session **h = NULL;
-	int p, m, err = 0, trials = 1;
+	int p, m, err = 0, trials = 1, depth, oldest = 0;
 	if ((err = setjmp(env)) != 0) {
 		irl_untrap();
 		return err;
@@ -841,11 +859,28 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 	h = (parked_session **)irl_calloc(sizeof(parked_session *) * nprob, "batch sessions");
 	irl_untrap();
 	trials = irlcu_shape_trials(0);  /* no host waits inside the pipelined batch */
+	depth = batch_depth();
 	/* pipelined: problem p is set up and all its iterations are enqueued
 	   (asynchronous device work on its own stream); the host then sets up
-	   p + 1 while the device runs p, and ends p - 1 */
+	   p + 1 while the device runs p and the problems before it.  Up to
+	   `depth` problems are in flight; the oldest is ended (waiting for its
+	   device work) before a new one would exceed that, or the device
+	   memory */
 	for (p = 0; p < nprob && !err; ++p) {
 		IrlOsemProblem_t *q = pp + p;
+		/* the oldest problems end first while the next one might not fit */
+		while (oldest < p && !err) {
+			size_t fr = 0;
+			if (p - oldest < depth && (irlcu_mem_info(&fr, NULL) != 0 || (double)fr >= batch_need_bytes(q)))
+				break;
+			{
+				const int e = batch_end(h, pp, oldest++, err);
+				if (!err)
+					err = e;
+			}
+		}
+		if (err)
+			break;
 		q->iStatus = IrlOsemBegin(q->psIrlParms, q->psOptions, q->psViews, q->pchDrfTabFname,
 			q->pchScatKrnlFname, NULL, q->pfScatterEstimate, q->pfAtnMap, q->pfPrjImage, q->pfReconImage,
 			NULL, NULL);
@@ -861,11 +896,6 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 			}
 		}
 		h[p] = session_park();
-		if (p > 0 && h[p - 1] != NULL) {
-			const int e = batch_end(h, pp, p - 1, err);
-			if (!err)
-				err = e;
-		}
 	}
 	for (p = 0; p < nprob; ++p) {
 		const int e = batch_end(h, pp, p, err);

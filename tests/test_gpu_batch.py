@@ -63,8 +63,18 @@ def _check_batch(product, cases, tmp_path):
         assert np.array_equal(rec, ref), f"problem {i}: {int((rec != ref).sum())} voxels differ"
 
 
-def test_batch_equals_separate_calls(product, tmp_path):
-    _check_batch(product, _cases(), tmp_path)
+@pytest.mark.parametrize("depth", ["1", "2", "4", "8"])
+def test_batch_equals_separate_calls(product, tmp_path, monkeypatch, depth):
+    """Any number of problems in flight (IRL_BATCH_DEPTH) gives the separate
+    calls' results."""
+    monkeypatch.setenv("IRL_BATCH_DEPTH", depth)
+    _check_batch(product, _cases() + _cases()[:2], tmp_path)
+
+
+def test_mem_info(product):
+    fr, tot = C.c_size_t(), C.c_size_t()
+    assert product.irlcu_mem_info(C.byref(fr), C.byref(tot)) == 0
+    assert 0 < fr.value <= tot.value
 
 
 def test_batch_small_problems_behind_a_large_one(product, tmp_path):
