@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(GNT) k_conv_gemm(GemmArgs a, ConvGeom g, const
 // g_tc_error, issues no further copies or MMAs, waits for its copies in
 // flight and (bounded) for its last commit, and frees its TMEM.
 constexpr int TC_BM = 128, TC_BK = 64, TC_NT = 128, TC_S = 4;
+static_assert(TC_BM == TC_NT && TC_NT == 128 && TC_BK % 32 == 0, "k_conv_tc's copy mapping: 4 threads per row");
 constexpr int TC_MAXCH = 640;  // k chunks (of 8) of one CTA's k range: K / 8 <= 576 here
 constexpr unsigned TC_WAIT_LIMIT = 1u << 22;
 
@@ -389,10 +390,15 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
   const int kb = a.splits > 1 ? blockIdx.z * a.kper : 0;
   const int ke = a.splits > 1 ? min(a.K, kb + a.kper) : a.K;
   const int nk = (ke - kb + TC_BK - 1) / TC_BK;
-  // this thread's A row: output position decoded once
-  int rb = -1, rd = 0, rh = 0, rw = 0;
-  {
-    const int m = m0 + tid;
+  // A rows this thread copies: rows rg * 32 + tid / 4 (rg < TC_BM / 32),
+  // output positions decoded once
+  constexpr int TC_RG = TC_BM / 32;
+  int rb[TC_RG], rd[TC_RG], rh[TC_RG], rw[TC_RG];
+#pragma unroll
+  for (int rg = 0; rg < TC_RG; ++rg) {
+    rb[rg] = -1;
+    rd[rg] = rh[rg] = rw[rg] = 0;
+    const int m = m0 + rg * 32 + (tid >> 2);
     if (m < a.M) {
       int r = m;
       const int ow = r % g.wout;
@@ -400,10 +406,10 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
       const int oh = r % g.hout;
       r /= g.hout;
       const int od = r % g.dout;
-      rb = r / g.dout;
-      rd = od * g.s - g.kd / 2;
-      rh = oh * g.s - g.kh / 2;
-      rw = ow * g.s - g.kw / 2;
+      rb[rg] = r / g.dout;
+      rd[rg] = od * g.s - g.kd / 2;
+      rh[rg] = oh * g.s - g.kh / 2;
+      rw[rg] = ow * g.s - g.kw / 2;
     }
   }
   // tap offsets of the k chunks of [kb, kb + nk TC_BK) (c = -1 past ke)
@@ -438,13 +444,23 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
   auto load_tile = [&](int t) {
     const uint32_t As = sbase + (t % TC_S) * Cfg::STAGE, Bs = As + Cfg::A_BYTES;
     const int k0 = kb + t * TC_BK;
+    // A: four consecutive threads copy four consecutive 16-byte chunks of
+    // one row (64 bytes of one tap's channels, contiguous in the input), so
+    // a warp's copies are 8 rows x 64 bytes of whole sectors, and its
+    // shared-memory stores of one chunk column cover the 32 banks once
 #pragma unroll
-    for (int q = 0; q < TC_BK / 8; ++q) {
+    for (int hq = 0; hq < TC_BK / 32; ++hq) {
+      const int q = hq * 4 + (tid & 3);
       const int2 e = ktab[t * (TC_BK / 8) + q];
-      const int id = rd + (e.x & 0xff), ih = rh + ((e.x >> 8) & 0xff), iw = rw + (e.x >> 16);
-      const bool ok = rb >= 0 && e.y >= 0 && id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi;
-      cp16(As + q * (TC_BM * 16) + tid * 16, ok ? (const void *)(X + in_off(g, rb, id, ih, iw, e.y)) : (const void *)X,
-           ok);
+#pragma unroll
+      for (int rg = 0; rg < TC_RG; ++rg) {
+        const int row = rg * 32 + (tid >> 2);
+        const int id = rd[rg] + (e.x & 0xff), ih = rh[rg] + ((e.x >> 8) & 0xff), iw = rw[rg] + (e.x >> 16);
+        const bool ok =
+            rb[rg] >= 0 && e.y >= 0 && id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi;
+        cp16(As + q * (TC_BM * 16) + row * 16,
+             ok ? (const void *)(X + in_off(g, rb[rg], id, ih, iw, e.y)) : (const void *)X, ok);
+      }
     }
     // B: 8 consecutive threads read one weight row's 8 chunks (128 bytes)
     for (int e = tid; e < N * (TC_BK / 8); e += TC_NT) {
