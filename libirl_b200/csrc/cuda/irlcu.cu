@@ -827,10 +827,15 @@ static bool sur_flagged(const Ctx &c, const int *hviews, int nv) {
 
 static int forward_batch(int nv, const int *hviews, int model, float primary, float *out, float *out_nosrf) {
   Ctx &c = *g_ctx;
+  RotCollapse col;
   {
     Stage s(IRLCU_ST_ROTATE, c.st);
     s.bytes = 8.0 * (double)c.vox * nv;  // read the estimate, write each rotated copy
-    TRY(launch_rotate(c, c.est, 0, c.wrot, c.vox, c.dviews, nv, 0));
+    // ESSE's collapse of the rotated volumes rides on the rotation when this
+    // batch takes the ESSE path
+    const bool esse_path = (model & MODEL_SRF_BIT) && c.esse.on && !(c.sur && !sur_flagged(c, hviews, nv));
+    if (!esse_path || !esse_collapse_target(c, nv, &col)) col.out = nullptr;
+    TRY(launch_rotate(c, c.est, 0, c.wrot, c.vox, c.dviews, nv, 0, col.out ? &col : nullptr));
   }
   const float *E = (model & MODEL_ATN_BIT) ? c.tE : nullptr;
   const DrfDev *drf = (model & MODEL_DRF_BIT) ? &c.drf[0] : nullptr;
@@ -861,7 +866,7 @@ static int forward_batch(int nv, const int *hviews, int model, float primary, fl
     if (!c.esse.on && !c.esse.zero) return set_error(IRLCU_ESTATE, "scatter model requested but not set up");
     if (!c.tS) return set_error(IRLCU_ESTATE, "scatter model needs the attenuation tables");
     Stage s(IRLCU_ST_ESSE, c.st);
-    TRY(launch_esse(c, c.wrot, c.dviews, nv, primary, c.wbck));
+    TRY(launch_esse(c, c.wrot, c.dviews, nv, primary, c.wbck, col.done));
     src = c.wbck;
     scale = 1.0f;
   }

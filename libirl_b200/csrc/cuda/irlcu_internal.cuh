@@ -209,9 +209,18 @@ extern long long g_launch_count;
 
 // ---- launchers (each defined in its kernel file) ----
 
+// ESSE's CollapseByFac by 2 of the rotated volumes, taken by the two-slice
+// shear while it writes them (out[v][y'][z'][x'], nyv x nzv x nxv per
+// view); `done` reports whether it did
+struct RotCollapse {
+  float *out = nullptr;
+  int nyv = 0, nzv = 0, nxv = 0;
+  bool done = false;
+};
+
 // rotation of nv volumes: dst[v] = rotate(src[v or shared], tab rot_base+views[v])
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst,
-                  size_t dst_stride, const int *dviews, int nv, int rot_base);
+                  size_t dst_stride, const int *dviews, int nv, int rot_base, RotCollapse *col = nullptr);
 
 // three-shear rotation of one device volume with every buffer in a static
 // device array (irlcu_rotate_volume_noalloc); enqueued on `st`
@@ -280,6 +289,9 @@ int launch_div_views_down(cudaStream_t st, const float *a, const float *s, float
 // ESSE effective source: src[v] = rot[v]*primary + effsrc(rot[v], view)
 int esse_setup(Ctx &c, const irlcu_esse *e);
 int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary,
-                float *src);
+                float *src, bool collapsed = false);
+// where the rotation may leave ESSE's collapsed input for a batch of nv
+// views (RotCollapse), or false when this ESSE set-up reads it otherwise
+bool esse_collapse_target(const Ctx &c, int nv, RotCollapse *col);
 
 }  // namespace irlcu

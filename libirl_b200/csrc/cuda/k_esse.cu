@@ -1058,7 +1058,21 @@ int esse_setup(Ctx &c, const irlcu_esse *e) {
 
 static int esse_expand_combine(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src);
 
-int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src) {
+bool esse_collapse_target(const Ctx &c, int nv, RotCollapse *col) {
+  const EsseDev &E = c.esse;
+  const EsseWork &w = c.ew;
+  if (!E.on || !E.fused || !E.yz_reg || !er_len_ok(E.kx) || E.collapse != 2 || nv > w.batch || !w.g[0] ||
+      (c.n & 1) || (c.nz & 1))
+    return false;
+  col->out = w.g[0];
+  col->nyv = w.nyv;
+  col->nzv = w.nzv;
+  col->nxv = w.nxv;
+  col->done = false;
+  return true;
+}
+
+int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float primary, float *src, bool collapsed) {
   EsseDev &E = c.esse;
   EsseWork &w = c.ew;
   if (!E.on) {
@@ -1092,13 +1106,25 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     const int lines = (nyv * nzv + 1) / 2;
     if (reg_rows) {
       TRY_ESSE(er_attrs(E.kx));
-      if (E.collapse > 1) {
+      if (E.collapse > 1 && collapsed) {
+        ra.pre = w.g[0];  // the two-slice rotation left the collapse there
+      } else if (E.collapse > 1) {
         // the collapse as its own streaming pass into g[0] (free until the
-        // x inverse writes it)
+        // x inverse writes it); in a shape-autotuner trial it counts with
+        // the rotation it follows, which the two-slice form folds it into
         const size_t tot = (size_t)nv * nyv * nzv * nxv;
+        const bool timed = c.trial_form >= 0 && !c.capturing;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (timed) {
+          CU_TRY(cudaEventCreate(&e0));
+          CU_TRY(cudaEventCreate(&e1));
+          c.trial_ev[0].push_back({e0, e1});
+          CU_TRY(cudaEventRecord(e0, c.st));
+        }
         k_esse_collapse<<<(unsigned)((tot + 255) / 256), 256, 0, c.st>>>(rot, c.vox, c.n, c.nz, E.collapse, nyv, nzv,
                                                                          nxv, nv, w.g[0]);
         CU_LAUNCHED();
+        if (timed) CU_TRY(cudaEventRecord(e1, c.st));
         ra.pre = w.g[0];
       }
       dim3 grid_((lines + ER_LW - 1) / ER_LW, nv);

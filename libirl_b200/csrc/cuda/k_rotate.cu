@@ -442,14 +442,23 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 2) k_shear_cw(const float *__res
 // per slice.  The passes and every rounding are those of k_shear_cw, so the
 // output is the same bit for bit.  For an odd slice count the last CTA has
 // one slice; its second lane reads nothing and stores nothing.
+//
+// With COL (even n, even slice count) the CTA also writes ESSE's
+// CollapseByFac by 2 of the pair (out[v][y/2][k0/2][x/2], nyv x nzv x n/2
+// per view): the 2 x 2 x 2 sums of its output values, added in the order of
+// the separate collapse (row y, then y + 1; slice k0, then k0 + 1; x, then
+// x + 1), so ESSE reads the same bits without a pass over the rotated
+// volumes.  Pass 3 then runs a warp per row pair.
 constexpr int SH2_TY = 32;
 
+template <bool COL>
 __global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__restrict__ src, size_t src_stride,
                                                                float *__restrict__ dst, size_t dst_stride,
                                                                const int *__restrict__ views, int rot_base,
                                                                RotTabs T, const int *__restrict__ sup_st,
                                                                const int *__restrict__ sup_en, int n, int nz,
-                                                               int xld) {
+                                                               int xld, float *__restrict__ col_out, int nyv,
+                                                               int nzv) {
   extern __shared__ float sm[];
   float2 *s_x = reinterpret_cast<float2 *>(sm);  // n * xld pairs
   int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xld);
@@ -457,6 +466,7 @@ __global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__r
   float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
   int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
   float *t_cf1 = reinterpret_cast<float *>(t_csh + xld), *t_cf2 = t_cf1 + xld;
+
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * SH2_TY;
   const int k0 = 2 * blockIdx.x, v = blockIdx.y;
   const bool two = k0 + 1 < nz;
@@ -568,25 +578,76 @@ __global__ void __launch_bounds__(SH_TX *SH2_TY, 1) k_shear_cw2(const float *__r
   }
   __syncthreads();
   // pass 3: the second x shear, a warp per row, the second tap from the next lane
-  for (int j = ty; j < n; j += SH2_TY) {
-    const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
-    const float f1 = t_rf1[j], f2 = t_rf2[j];
-    const float2 *yr = s_x + j * xld;
-    float *orow = d + (size_t)j * rs;
-    int a = tx + off;
-    float2 y = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
-    for (int x0 = 0; x0 < n; x0 += SH_TX) {
-      const int x = x0 + tx;
-      a += SH_TX;
-      const float2 yn = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
-      const float s0 = __shfl_sync(0xffffffffu, tx == 0 ? yn.x : y.x, (tx + 1) & (SH_TX - 1));
-      const float s1 = __shfl_sync(0xffffffffu, tx == 0 ? yn.y : y.y, (tx + 1) & (SH_TX - 1));
-      if (x < n) {
-        const bool in = x >= xa && x < xb;
-        orow[x] = in ? lerp2(f1, y.x, f2, s0) : 0.f;
-        if (two) orow[x + n] = in ? lerp2(f1, y.y, f2, s1) : 0.f;
+  if (!COL) {
+    for (int j = ty; j < n; j += SH2_TY) {
+      const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
+      const float f1 = t_rf1[j], f2 = t_rf2[j];
+      const float2 *yr = s_x + j * xld;
+      float *orow = d + (size_t)j * rs;
+      int a = tx + off;
+      float2 y = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
+      for (int x0 = 0; x0 < n; x0 += SH_TX) {
+        const int x = x0 + tx;
+        a += SH_TX;
+        const float2 yn = (a >= 0 && a < h.mdim) ? yr[a] : zero2;
+        const float s0 = __shfl_sync(0xffffffffu, tx == 0 ? yn.x : y.x, (tx + 1) & (SH_TX - 1));
+        const float s1 = __shfl_sync(0xffffffffu, tx == 0 ? yn.y : y.y, (tx + 1) & (SH_TX - 1));
+        if (x < n) {
+          const bool in = x >= xa && x < xb;
+          orow[x] = in ? lerp2(f1, y.x, f2, s0) : 0.f;
+          if (two) orow[x + n] = in ? lerp2(f1, y.y, f2, s1) : 0.f;
+        }
+        y = yn;
       }
-      y = yn;
+    }
+  } else {
+    // a warp per row pair (2p, 2p + 1), both rows a chunk at a time, so the
+    // collapse of each 2 x 2 x 2 block is added in registers
+    for (int p = ty; p < (n >> 1); p += SH2_TY) {
+      const int ja = 2 * p, jb = ja + 1;
+      const int offa = t_rsh[ja] + h.iadd, xaa = t_st[ja] + 1, xba = t_en[ja] - 1;
+      const int offb = t_rsh[jb] + h.iadd, xab = t_st[jb] + 1, xbb = t_en[jb] - 1;
+      const float f1a = t_rf1[ja], f2a = t_rf2[ja], f1b = t_rf1[jb], f2b = t_rf2[jb];
+      const float2 *yra = s_x + ja * xld, *yrb = s_x + jb * xld;
+      float *oa = d + (size_t)ja * rs, *ob = d + (size_t)jb * rs;
+      float *co = col_out + (((size_t)v * nyv + p) * nzv + (k0 >> 1)) * (n >> 1);
+      int aa = tx + offa, ab = tx + offb;
+      float2 ya = (aa >= 0 && aa < h.mdim) ? yra[aa] : zero2;
+      float2 yb = (ab >= 0 && ab < h.mdim) ? yrb[ab] : zero2;
+      for (int x0 = 0; x0 < n; x0 += SH_TX) {
+        const int x = x0 + tx;
+        aa += SH_TX;
+        ab += SH_TX;
+        const float2 yna = (aa >= 0 && aa < h.mdim) ? yra[aa] : zero2;
+        const float2 ynb = (ab >= 0 && ab < h.mdim) ? yrb[ab] : zero2;
+        const int src_lane = (tx + 1) & (SH_TX - 1);
+        const float sa0 = __shfl_sync(0xffffffffu, tx == 0 ? yna.x : ya.x, src_lane);
+        const float sa1 = __shfl_sync(0xffffffffu, tx == 0 ? yna.y : ya.y, src_lane);
+        const float sb0 = __shfl_sync(0xffffffffu, tx == 0 ? ynb.x : yb.x, src_lane);
+        const float sb1 = __shfl_sync(0xffffffffu, tx == 0 ? ynb.y : yb.y, src_lane);
+        float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+        if (x < n) {
+          const bool ina = x >= xaa && x < xba, inb = x >= xab && x < xbb;
+          a0 = ina ? lerp2(f1a, ya.x, f2a, sa0) : 0.f;
+          a1 = ina ? lerp2(f1a, ya.y, f2a, sa1) : 0.f;
+          b0 = inb ? lerp2(f1b, yb.x, f2b, sb0) : 0.f;
+          b1 = inb ? lerp2(f1b, yb.y, f2b, sb1) : 0.f;
+          oa[x] = a0;
+          oa[x + n] = a1;
+          ob[x] = b0;
+          ob[x + n] = b1;
+        }
+        // the next x of each value, from the next lane
+        const float na0 = __shfl_down_sync(0xffffffffu, a0, 1), na1 = __shfl_down_sync(0xffffffffu, a1, 1);
+        const float nb0 = __shfl_down_sync(0xffffffffu, b0, 1), nb1 = __shfl_down_sync(0xffffffffu, b1, 1);
+        if (!(tx & 1) && x < n) {
+          float t = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(0.f, a0), na0), a1), na1);
+          t = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(t, b0), nb0), b1), nb1);
+          co[x >> 1] = t;
+        }
+        ya = yna;
+        yb = ynb;
+      }
     }
   }
 }
@@ -848,27 +909,28 @@ __global__ void k_rot3dpar(const float *__restrict__ src, size_t src_stride, flo
 
 
 static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
-                              const int *dviews, int nv, int rot_base);
+                              const int *dviews, int nv, int rot_base, RotCollapse *col);
 
 // During a shape-autotuner trial iteration every three-shear launch is
 // bracketed by events, per source kind (irlcu_osem_iteration sums them).
 int launch_rotate(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
-                  const int *dviews, int nv, int rot_base) {
+                  const int *dviews, int nv, int rot_base, RotCollapse *col) {
   const bool timed = c.trial_form >= 0 && c.g.fast_rotate && !c.capturing && nv > 0;
-  if (!timed) return launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base);
+  if (!timed) return launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base, col);
   const int kind = src_stride == 0 ? 0 : 1;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CU_TRY(cudaEventCreate(&e0));
   CU_TRY(cudaEventCreate(&e1));
   c.trial_ev[kind].push_back({e0, e1});
   CU_TRY(cudaEventRecord(e0, c.st));
-  const int rc = launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base);
+  const int rc = launch_rotate_impl(c, src, src_stride, dst, dst_stride, dviews, nv, rot_base, col);
   CU_TRY(cudaEventRecord(e1, c.st));
   return rc;
 }
 
 static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride, float *dst, size_t dst_stride,
-                              const int *dviews, int nv, int rot_base) {
+                              const int *dviews, int nv, int rot_base, RotCollapse *col) {
+  if (col) col->done = false;
   if (nv <= 0) return IRLCU_OK;
   const int n = c.n, nz = c.nz;
   if (!c.g.fast_rotate) {
@@ -901,13 +963,31 @@ static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride,
   const int kind = src_stride == 0 ? 0 : 1, tuned = c.trial_form >= 0 ? c.trial_form : c.shear_form[kind];
   const bool pair = pair_env ? pair_env[0] == '1' : (tuned >= 0 ? tuned == 1 : true);
   if (!env && pair && smc2 <= (size_t)maxsm) {
+    // with the collapse where its buffers fit too (even n and slice count,
+    // the collapsed sizes those of the rotated volume)
+    const size_t smcc = smc2;
+    const bool fuse = col && col->out && !(n & 1) && !(nz & 1) && col->nyv == n / 2 && col->nzv == nz / 2 &&
+                      col->nxv == n / 2;
+    if (fuse) {
+      static size_t s_cw2c = 0;
+      if (smcc > s_cw2c) {
+        CU_TRY(cudaFuncSetAttribute(k_shear_cw2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smcc));
+        s_cw2c = smcc;
+      }
+      k_shear_cw2<true><<<dim3(nz / 2, nv), dim3(SH_TX, SH2_TY), smcc, c.st>>>(
+          src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xo, col->out,
+          col->nyv, col->nzv);
+      CU_LAUNCHED();
+      col->done = true;
+      return IRLCU_OK;
+    }
     static size_t s_cw2 = 0;
     if (smc2 > s_cw2) {
-      CU_TRY(cudaFuncSetAttribute(k_shear_cw2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc2));
+      CU_TRY(cudaFuncSetAttribute(k_shear_cw2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc2));
       s_cw2 = smc2;
     }
-    k_shear_cw2<<<dim3((nz + 1) / 2, nv), dim3(SH_TX, SH2_TY), smc2, c.st>>>(
-        src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xo);
+    k_shear_cw2<false><<<dim3((nz + 1) / 2, nv), dim3(SH_TX, SH2_TY), smc2, c.st>>>(
+        src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xo, nullptr, 0, 0);
     CU_LAUNCHED();
     return IRLCU_OK;
   }

@@ -270,6 +270,23 @@ def test_osem_shear_forms(product, orc, tmp_path, monkeypatch, pair):
     assert rel_l2(got, want) <= IMAGE_TOL
 
 
+def test_esse_collapse_in_two_slice_shear_is_bit_exact(product, tmp_path, monkeypatch):
+    """With ESSE at collapse 2 the two-slice shear also writes the collapsed
+    rotated volumes (CollapseByFac, krnlprj3d.c:559-592); the one-slice
+    shear leaves that to the separate collapse pass.  Projections and a
+    reconstruction must be the same bits either way."""
+    case = W.full128(seed=2230, n=64, nviews=8, subsets=2, iterations=2, collapse=2, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    out = {}
+    for pair in ("0", "1"):
+        monkeypatch.setenv("IRLCU_SHEAR_PAIR", pair)
+        prj = gpu_genprj(product, case, files)
+        meas = W.poisson_counts(prj, 2e5, 2230)
+        out[pair] = (prj, gpu_osem(product, case, files, meas))
+    assert np.array_equal(out["0"][0], out["1"][0])
+    assert np.array_equal(out["0"][1], out["1"][1])
+
+
 def test_osem_bilinear_rotator_and_callbacks(product, orc, tmp_path):
     case = W.plain64(seed=1300, n=32, nviews=8, subsets=2, iterations=3)
     files = case.write_tables(str(tmp_path))
