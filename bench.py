@@ -1005,6 +1005,47 @@ def run_large256(args):
         "data": "synthetic (seeded phantom, Poisson data)"}
 
 
+def run_kernel_times(args):
+    """Warm device time of every kernel of the full128 iteration: `--warmup`
+    iterations, then `--steps` iterations (CUDA-graph replay, ESSE in every
+    one) with CUPTI kernel records through torch.profiler, summed per kernel
+    and divided by the iteration count.  A diagnostic table, not a bench
+    line."""
+    import collections
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    import libirl_b200 as L
+    from libirl_b200 import api
+    torch.cuda.set_device(0)
+    L.build()
+    lib = L.load()
+    tmp = tempfile.mkdtemp(prefix="irlkt_")
+    case, files, meas = make_workload(lib, tmp, args.nviews, args.subsets)
+    K, Wm = args.steps, args.warmup
+    p, o, v = case.parms(), case.options(), case.views()
+    p.NumIterations = p.iNumSrfIterations = K + Wm
+    atn, rec, m = case.atn.copy(), np.zeros_like(case.act), meas.copy()
+    if lib.IrlOsemBegin(C.byref(p), C.byref(o), v, _dup(files["drf"]), _dup(files["krnl"]), api.ITER_CB(), None,
+                        api.fptr(atn), api.fptr(m), api.fptr(rec), None, None):
+        raise RuntimeError(lib.pchIrlErrorString().decode())
+    lib.IrlOsemIterate(Wm)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        lib.IrlOsemIterate(K)
+        torch.cuda.synchronize()
+    lib.IrlOsemEnd(api.fptr(rec))
+    tot, cnt = collections.defaultdict(float), collections.Counter()
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA:
+            name = e.name.split("(")[0].replace("void ", "").replace("irlcu::", "")
+            tot[name] += getattr(e, "device_time_total", 0.0)
+            cnt[name] += 1
+    s = sum(tot.values())
+    print("total us per iteration: %.1f" % (s / K))
+    for k, t in sorted(tot.items(), key=lambda x: -x[1]):
+        print("%-45s %5d launches %9.1f us/iter %5.1f%%" % (k[:45], cnt[k] // K, t / K, 100 * t / s))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -1022,7 +1063,12 @@ def main():
     ap.add_argument("--cpu-views", type=int, default=2)
     ap.add_argument("--workload", default="full128", choices=["full128", "batch32", "large256"],
                     help="full128 is the bench line (which also reports the others unless --no-extra)")
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="print the warm device time of every kernel of the full128 iteration instead")
     args = ap.parse_args()
+    if args.kernel_times:
+        run_kernel_times(args)
+        return
     if args.workload == "batch32":
         print(json.dumps(run_batch32(args)))
         return
