@@ -455,7 +455,11 @@ def make_roofline(prof, case, grids):
     if mz and mx:
         stages.append(("drf", (2, 4), per * n * 3 * 2 * (2 * b * mz * mx),
                        "k_dplane_fwd / k_dplane_fwd_finish / k_dplane_bck (Fourier-domain DRF, one CTA per plane)"))
-    stages.append(("rotate", (0,), per * 2 * b * vox, "k_shear_cw2 (three-shear rotation, two slices per CTA; with ESSE it also writes the 2x2x2 collapse)"))
+    # with ESSE at collapse 2 the rotation also writes the collapsed volume
+    col = b * vox // 8 if (kx and case.collapse == 2) else 0
+    stages.append(("rotate", (0,), per * (2 * b * vox + col),
+                   "k_shear_cw2 (three-shear rotation, two slices per CTA; with ESSE it also writes the 2x2x2 "
+                   "collapse, b*V/8 per view)"))
     stages.append(("unrotate", (5,), per * 3 * b * vox + 2 * b * vox, "k_shear_cw + k_accumulate"))
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal SIMT FP32 TFLOP/s (not measured)
     out = []
