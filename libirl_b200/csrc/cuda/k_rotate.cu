@@ -15,11 +15,14 @@
 //    osemrecon.c:317-320, 850-852).
 //
 // Volume layout [y][z][x]; a slice k is the set of rows y*nz*n + k*n.
+#include <cooperative_groups.h>
 #include <cstdio>
 #include <cstdlib>
 
 #include "irlcu_internal.cuh"
 #include "../host/irl_geom.h"
+
+namespace cg = cooperative_groups;
 
 namespace irlcu {
 
@@ -785,6 +788,142 @@ __global__ void __launch_bounds__(SH_TX *SH_TY, 1) k_shear_split(const float *__
   }
 }
 
+// Cluster form, for slices whose intermediate image does not fit one SM's
+// shared memory (n = 256: 256 x 277 floats): a cluster of two CTAs per
+// (slice, view), CTA q holding X's columns [q cb, q cb + cb).  Passes 1 and
+// 2 treat every column on its own, so each CTA runs them for its half;
+// after a cluster barrier pass 3 reads Y's rows from both halves (the
+// partner's through distributed shared memory), each CTA writing half of
+// the output rows, and a second barrier keeps both halves alive until both
+// CTAs are done.  Every value is computed and rounded as in k_shear_cw, so
+// the output is the same bit for bit.
+constexpr int CL_TY = 32;  // warps per CTA of the cluster form
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_TX *CL_TY, 1)
+    k_shear_cl2(const float *__restrict__ src, size_t src_stride, float *__restrict__ dst, size_t dst_stride,
+                const int *__restrict__ views, int rot_base, RotTabs T, const int *__restrict__ sup_st,
+                const int *__restrict__ sup_en, int n, int nz, int cb, int xs) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int q = (int)cl.block_rank();
+  extern __shared__ float sm[];
+  float *s_x = sm;  // n * xs: column c0 + i at s_x[j xs + i]
+  int *t_rsh = reinterpret_cast<int *>(s_x + (size_t)n * xs);
+  int *t_st = t_rsh + n, *t_en = t_st + n;
+  float *t_rf1 = reinterpret_cast<float *>(t_en + n), *t_rf2 = t_rf1 + n;
+  int *t_csh = reinterpret_cast<int *>(t_rf2 + n);
+  float *t_cf1 = reinterpret_cast<float *>(t_csh + 2 * n), *t_cf2 = t_cf1 + 2 * n;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SH_TX + tx, nt = SH_TX * CL_TY;
+  const int k = blockIdx.x >> 1, v = blockIdx.y;
+  const int r = rot_base + views[v];
+  const RotHdr h = load_hdr(T, r);
+  const float *s = src + (size_t)v * src_stride + (size_t)k * n;
+  float *d = dst + (size_t)v * dst_stride + (size_t)k * n;
+  const int rs = nz * n;
+  for (int i = tid; i < n; i += nt) {
+    t_rsh[i] = T.row_sh[(size_t)r * n + i];
+    t_rf1[i] = T.row_f1[(size_t)r * n + i];
+    t_rf2[i] = T.row_f2[(size_t)r * n + i];
+    t_st[i] = sup_st[i];
+    t_en[i] = sup_en[i];
+  }
+  for (int i = tid; i < h.mdim; i += nt) {
+    t_csh[i] = T.col_sh[(size_t)r * 2 * n + i];
+    t_cf1[i] = T.col_f1[(size_t)r * 2 * n + i];
+    t_cf2[i] = T.col_f2[(size_t)r * 2 * n + i];
+  }
+  __syncthreads();
+  const int c0 = q * cb, c1 = min(h.mdim, c0 + cb);  // empty when X is narrower than one half
+  // pass 1 for columns [c0, c1)
+  if (!h.b90) {
+    for (int j = ty; j < n; j += CL_TY) {
+      const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+      const float *line = s + (h.b180 ? n - j - 1 : j) * rs + rw.c0;
+      float *xr = s_x + j * xs;
+      const int i00 = c0 + tx;
+      float a = (i00 >= rw.la && i00 <= rw.lb) ? __ldg(line + rw.dir * i00) : 0.f;
+      for (int i0 = c0; i0 < c1; i0 += SH_TX) {
+        const int i = i0 + tx, inx = i + SH_TX;
+        const float b = (inx >= rw.la && inx <= rw.lb) ? __ldg(line + rw.dir * inx) : 0.f;
+        const float sec = __shfl_sync(0xffffffffu, tx == 0 ? b : a, (tx + 1) & (SH_TX - 1));
+        if (i < c1) xr[i - c0] = (i >= rw.lo && i < rw.vb) ? lerp2(rw.f1, a, rw.f2, sec) : 0.f;
+        a = b;
+      }
+    }
+  } else {
+    constexpr int NCH = 4;
+    const int per = (c1 - c0 + NCH - 1) / NCH;
+    for (int e = tid; e < n * NCH; e += nt) {
+      const int ch = e / n, j = e - ch * n;
+      const int i0 = c0 + ch * per, i1 = min(c1, i0 + per);
+      if (i0 >= i1) continue;
+      const ShearRow rw = shear_row(h, n, j, t_rsh, t_rf1, t_rf2, t_st, t_en);
+      const int step = rw.dir * rs;
+      const float *col = s + (h.b180 ? j : n - j - 1) + rw.c0 * rs;
+      float *xc = s_x + j * xs;
+      float a = (i0 >= rw.la && i0 <= rw.lb) ? __ldg(col + i0 * step) : 0.f;
+      const float *pn = col + (i0 + 1) * step;
+      for (int i = i0; i < i1; ++i, pn += step) {
+        const float b = (i + 1 >= rw.la && i + 1 <= rw.lb) ? __ldg(pn) : 0.f;
+        xc[i - c0] = (i >= rw.lo && i < rw.vb) ? lerp2(rw.f1, a, rw.f2, b) : 0.f;
+        a = b;
+      }
+    }
+  }
+  __syncthreads();
+  // pass 2 in place for the half's columns (see k_shear_cw)
+  for (int c = c0 + ty; c < c1; c += CL_TY) {
+    const int jt = t_csh[c];
+    const float w1 = t_cf1[c], w2 = t_cf2[c];
+    const int jlo = max(0, -jt) - h.iadd, jhi = min(h.mdim, h.mdim - jt - 1) - h.iadd;
+    float *col = s_x + (c - c0);
+    if (jt >= 0) {
+      for (int j0 = 0; j0 < n; j0 += SH_TX) {
+        const int j = j0 + tx, r0 = j + jt;
+        const float x0 = (j < n && r0 < n) ? col[r0 * xs] : 0.f;
+        const float x1 = (j < n && r0 + 1 < n) ? col[(r0 + 1) * xs] : 0.f;
+        __syncwarp();
+        if (j < n) col[j * xs] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+      }
+    } else {
+      for (int j0 = n - 1; j0 >= 0; j0 -= SH_TX) {
+        const int j = j0 - tx, r0 = j + jt;
+        const float x0 = (j >= 0 && r0 >= 0) ? col[r0 * xs] : 0.f;
+        const float x1 = (j >= 0 && r0 + 1 >= 0) ? col[(r0 + 1) * xs] : 0.f;
+        __syncwarp();
+        if (j >= 0) col[j * xs] = (j >= jlo && j < jhi) ? lerp2(w1, x0, w2, x1) : 0.f;
+      }
+    }
+    __syncwarp();
+  }
+  // both halves of Y complete
+  cl.sync();
+  const float *half0 = cl.map_shared_rank(s_x, 0), *half1 = cl.map_shared_rank(s_x, 1);
+  // pass 3 for rows [q n / 2, (q + 1) n / 2): Y[j][a] from the half that holds column a
+  const int jb = q * n / 2, je = (q + 1) * n / 2;
+  for (int j = jb + ty; j < je; j += CL_TY) {
+    const int off = t_rsh[j] + h.iadd, xa = t_st[j] + 1, xb = t_en[j] - 1;
+    const float f1 = t_rf1[j], f2 = t_rf2[j];
+    const float *y0 = half0 + (size_t)j * xs, *y1 = half1 + (size_t)j * xs;
+    float *orow = d + (size_t)j * rs;
+    int a = tx + off;
+    float y = (a >= 0 && a < h.mdim) ? (a < cb ? y0[a] : y1[a - cb]) : 0.f;
+    for (int x0 = 0; x0 < n; x0 += SH_TX) {
+      const int x = x0 + tx;
+      a += SH_TX;
+      const float yn = (a >= 0 && a < h.mdim) ? (a < cb ? y0[a] : y1[a - cb]) : 0.f;
+      const float sec = __shfl_sync(0xffffffffu, tx == 0 ? yn : y, (tx + 1) & (SH_TX - 1));
+      if (x < n) orow[x] = (x >= xa && x < xb) ? lerp2(f1, y, f2, sec) : 0.f;
+      y = yn;
+    }
+  }
+  // the partner may still read this CTA's half
+  cl.sync();
+}
+
+static size_t shear_cl2_smem_bytes(int n, int xs) {
+  return sizeof(float) * ((size_t)n * xs + 5 * (size_t)n + 3 * 2 * (size_t)n);
+}
+
 static size_t shear_split_smem_bytes(int n) {
   return sizeof(float) * ((size_t)n * (SPLIT_CB | 1) + 5 * (size_t)n + 3 * 2 * (size_t)n);
 }
@@ -1025,6 +1164,24 @@ static int launch_rotate_impl(const Ctx &c, const float *src, size_t src_stride,
                                                                    rot_base, c.rot, c.sup_start, c.sup_end, n, nz, xld);
     CU_LAUNCHED();
     return IRLCU_OK;
+  }
+  // cluster form where half of X fits one SM (IRLCU_SHEAR_CLUSTER=0 skips
+  // it for the column-split form below)
+  {
+    const char *cl_env = getenv("IRLCU_SHEAR_CLUSTER");
+    const int cb = (xld + 1) / 2, xs = cb | 1;
+    const size_t smcl = shear_cl2_smem_bytes(n, xs);
+    if (!env && !(cl_env && cl_env[0] == '0') && smcl <= (size_t)maxsm) {
+      static size_t s_cl = 0;
+      if (smcl > s_cl) {
+        CU_TRY(cudaFuncSetAttribute(k_shear_cl2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smcl));
+        s_cl = smcl;
+      }
+      k_shear_cl2<<<dim3(2 * nz, nv), dim3(SH_TX, CL_TY), smcl, c.st>>>(
+          src, src_stride, dst, dst_stride, dviews, rot_base, c.rot, c.sup_start, c.sup_end, n, nz, cb, xs);
+      CU_LAUNCHED();
+      return IRLCU_OK;
+    }
   }
   // column-split form where its block of columns fits (IRLCU_SHEAR_SPLIT=0
   // keeps the two global-memory kernels below)

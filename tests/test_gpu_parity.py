@@ -68,12 +68,12 @@ def gpu_osem(lib, case, files, meas, iterations=None, opts=None, parms=None, krn
 # ------------------------------------------------------------- rotations
 
 @pytest.mark.parametrize("n,nz", [(16, 3), (33, 2), (64, 4), (128, 2), (128, 5), (200, 1), (256, 2)])
-@pytest.mark.parametrize("fast", [1, 0, "fused", "single", "pair", "global"])
+@pytest.mark.parametrize("fast", [1, 0, "fused", "single", "pair", "split", "global"])
 def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     """Both rotators bit for bit against the oracle; the three-shear one in
     its two-slice and one-slice column-walk forms, its fused-pass form, and
-    for slices beyond shared memory (n = 256) its column-split form
-    (default) and its global-memory form."""
+    for slices beyond one SM's shared memory (n = 256) its two-CTA cluster
+    form (default), its column-split form and its global-memory form."""
     import libirl_b200 as L
     if fast == "fused":
         monkeypatch.setenv("IRLCU_SHEAR_STAGE", "0")
@@ -81,8 +81,10 @@ def test_rotation_bit_exact(product, orc, monkeypatch, n, nz, fast):
     if fast in ("single", "pair"):
         monkeypatch.setenv("IRLCU_SHEAR_PAIR", "0" if fast == "single" else "1")
         fast = 1
-    if fast == "global":  # slices beyond shared memory: the two global-memory kernels, not the column split
-        monkeypatch.setenv("IRLCU_SHEAR_SPLIT", "0")
+    if fast in ("split", "global"):  # slices beyond shared memory: not the cluster form
+        monkeypatch.setenv("IRLCU_SHEAR_CLUSTER", "0")
+        if fast == "global":  # the two global-memory kernels, not the column split
+            monkeypatch.setenv("IRLCU_SHEAR_SPLIT", "0")
         fast = 1
     rng = np.random.default_rng(n * 7 + nz)
     vol = rng.random((n, nz, n), dtype=np.float32)
