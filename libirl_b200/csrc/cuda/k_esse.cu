@@ -298,9 +298,10 @@ constexpr int CW = 16;
 template <int L>
 __global__ void k_fft_col(ColArgs a, const float2 *__restrict__ twg) {
   extern __shared__ __align__(16) float2 smc[];
+  constexpr int LS = L + 1;              // odd line stride: the kx-fastest loads and stores are conflict-free
   float2 *tw = smc;
-  float2 *sa = smc + L;                  // [CW][L]
-  float2 *sb = sa + CW * L;
+  float2 *sa = smc + L;                  // [CW][LS]
+  float2 *sb = sa + CW * LS;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twg[i];
   const int kx0 = blockIdx.x * CW, o = blockIdx.y, b = blockIdx.z;
   const int wv = min(CW, a.kxh - kx0);
@@ -313,14 +314,14 @@ __global__ void k_fft_col(ColArgs a, const float2 *__restrict__ twg) {
         v = a.in[(size_t)b * a.in_bs + (size_t)o * a.in_os + (size_t)p * a.in_ps + kx0 + w];
         if (a.mul[t]) v = cmul(v, __ldg(&a.mul[t][(size_t)o * a.mul_os + (size_t)p * a.mul_ps + kx0 + w]));
       }
-      sa[w * L + p] = v;
+      sa[w * LS + p] = v;
     }
     __syncthreads();
-    float2 *res = fft_lines<L>(sa, sb, CW, L, tw, a.s);
+    float2 *res = fft_lines<L>(sa, sb, CW, LS, tw, a.s);
     for (int e = threadIdx.x; e < a.out_valid * CW; e += blockDim.x) {
       const int p = e / CW, w = e - p * CW;
       if (w < wv)
-        a.out[t][(size_t)b * a.out_bs + (size_t)o * a.out_os + (size_t)p * a.out_ps + kx0 + w] = res[w * L + p];
+        a.out[t][(size_t)b * a.out_bs + (size_t)o * a.out_os + (size_t)p * a.out_ps + kx0 + w] = res[w * LS + p];
     }
   }
 }
@@ -761,7 +762,7 @@ static bool esse_len_ok(int L) {
 
 static int row_wr(int L) { return (L <= 128) ? 16 : (L <= 256 ? 4 : 2); }  // row_lines<L>()
 
-static int col_smem(int L) { return (int)(sizeof(float2) * (L + 2 * CW * L)); }
+static int col_smem(int L) { return (int)(sizeof(float2) * (L + 2 * CW * (L + 1))); }
 
 static int set_col_attr(int L) {
   const int sm = col_smem(L);
