@@ -763,6 +763,9 @@ static bool esse_len_ok(int L) {
 static int row_wr(int L) { return (L <= 128) ? 16 : (L <= 256 ? 4 : 2); }  // row_lines<L>()
 
 static int col_smem(int L) { return (int)(sizeof(float2) * (L + 2 * CW * (L + 1))); }
+// threads of a column-pass CTA: 512 for long lines (more warps to hide the
+// shared-memory passes), 256 below
+static int col_nt(int L) { return L >= 256 ? 512 : 256; }
 
 static int set_col_attr(int L) {
   const int sm = col_smem(L);
@@ -820,7 +823,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   za.s = 1.f;
   {
     dim3 grid_((kxh + CW - 1) / CW, nyv, nb);
-    LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), st, za, g_ctx->ew.twz);
+    LDISPATCH(E.kz, k_fft_col, grid_, col_nt(E.kz), col_smem(E.kz), st, za, g_ctx->ew.twz);
     CU_LAUNCHED();
   }
   // y lines (outer = z < Kz) -> out [nb][Ky][Kz][kxh]
@@ -840,7 +843,7 @@ static int fft3_forward(cudaStream_t st, const EsseDev &E, const float *rot, con
   ya.s = 1.f;
   {
     dim3 grid_((kxh + CW - 1) / CW, E.kz, nb);
-    LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), st, ya, g_ctx->ew.twy);
+    LDISPATCH(E.ky, k_fft_col, grid_, col_nt(E.ky), col_smem(E.ky), st, ya, g_ctx->ew.twy);
     CU_LAUNCHED();
   }
   return IRLCU_OK;
@@ -1216,7 +1219,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
   ya.s = -1.f;
   {
     dim3 grid_((kxh + CW - 1) / CW, E.kz, nv);
-    LDISPATCH(E.ky, k_fft_col, grid_, 256, col_smem(E.ky), c.st, ya, w.twy);
+    LDISPATCH(E.ky, k_fft_col, grid_, col_nt(E.ky), col_smem(E.ky), c.st, ya, w.twy);
     CU_LAUNCHED();
   }
   // inverse z -> D[t] [nv][nyv][nzv][kxh]
@@ -1236,7 +1239,7 @@ int launch_esse(Ctx &c, const float *rot, const int *dviews, int nv, float prima
     za.kxh = kxh;
     za.s = -1.f;
     dim3 grid_((kxh + CW - 1) / CW, nyv, nv);
-    LDISPATCH(E.kz, k_fft_col, grid_, 256, col_smem(E.kz), c.st, za, w.twz);
+    LDISPATCH(E.kz, k_fft_col, grid_, col_nt(E.kz), col_smem(E.kz), c.st, za, w.twz);
     CU_LAUNCHED();
   }
   // inverse x (real part, cropped, 1/(Kx Ky Kz)) -> g[t] [nv][nyv][nzv][nxv]
