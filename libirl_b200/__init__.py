@@ -80,6 +80,8 @@ def _declare_irlcu(lib):
     lib.irlcu_shear_tuning.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_int)]
     lib.irlcu_shape_trials.restype = I
     lib.irlcu_shape_trials.argtypes = [I]
+    lib.irlcu_iteration_graphs.restype = I
+    lib.irlcu_iteration_graphs.argtypes = [I]
     lib.irlcu_mem_info.restype = I
     lib.irlcu_mem_info.argtypes = [C.POINTER(S), C.POINTER(S)]
     lib.irlcu_grids.restype = I

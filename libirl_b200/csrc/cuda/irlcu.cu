@@ -471,6 +471,14 @@ int irlcu_mem_info(size_t *free_bytes, size_t *total_bytes) {
   return IRLCU_OK;
 }
 
+static bool g_graphs_on = true;  // off inside IrlOsemBatch (eager iterations)
+
+int irlcu_iteration_graphs(int on) {
+  const int prev = g_graphs_on ? 1 : 0;
+  g_graphs_on = on != 0;
+  return prev;
+}
+
 int irlcu_shape_trials(int on) {
   const int prev = g_shape_trials ? 1 : 0;
   g_shape_trials = on != 0;
@@ -1032,7 +1040,7 @@ int irlcu_osem_iteration(int model, int bck_model, int use_scatest, int scat_mod
       return IRLCU_OK;
     }
   const char *env = getenv("IRLCU_GRAPHS");
-  const bool graphs = !(env && !strcmp(env, "0"));
+  const bool graphs = g_graphs_on && !(env && !strcmp(env, "0"));
   bool seen = false;
   for (int k : c.graph_seen) seen |= k == key;
   if (!graphs || !seen) {

@@ -17,13 +17,16 @@
 //   D3 conv2d 128->64  k3 + ReLU, x2                    [64][64][64]
 //   D4 conv2d 64->32   k3 + ReLU, x2                    [128][128][32]
 //   D5 conv2d 32->1    k3 (linear)                      [128][128]
-// 1,653,153 parameters.  Every convolution is a BF16 tensor-core GEMM
-// (mma.sync m16n8k16, FP32 accumulate) with the bias and ReLU in its
-// epilogue: forward as an implicit GEMM that reads the channels-last input
-// directly; backward on explicit im2col columns for the weight gradient and
-// the input-gradient columns, folded back by a gather-form col2im.  Long
-// reductions are split over K and summed in a fixed order, so results are
-// deterministic.
+// 1,653,153 parameters.  Every convolution is a BF16 tensor-core GEMM on
+// tcgen05 (TMEM accumulator, FP32) with the bias and ReLU in its epilogue:
+// forward as an implicit GEMM that gathers the channels-last input directly
+// (k_conv0_tc, k_conv_tc); backward (k_gemm_tc) on explicit im2col columns,
+// transposed for the weight gradient, and on the input-gradient columns,
+// folded back by a gather-form col2im.  The last layer (one output
+// channel) keeps direct kernels and, for its input gradient, the
+// mma.sync m16n8k16 GEMM, which IRLCU_SUR_TC=0 also selects everywhere.
+// Long reductions are split over K and summed in a fixed order, so results
+// are deterministic.
 // Training: Adam on FP32 master weights, BF16 copies for the GEMMs.
 #include <algorithm>
 #include <cmath>
@@ -560,6 +563,144 @@ __global__ void __launch_bounds__(TC_NT) k_conv_tc(GemmArgs a, ConvGeom g, const
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
 }
 
+// Plain tcgen05 GEMM for training's backward pass, both operands K-major:
+// C(m, n) = sum_k A[m*sam + k] B[n*sbn + k] (sak = sbk = 1; K, sam, sbn
+// multiples of 8 and 16-byte aligned rows), FP32 output at
+// Cf[m*scm + n*scn], or raw split-K partials ws[z][M][N] that
+// k_splitk_reduce adds in slice order.  One CTA of 128 threads per 128
+// rows x NT columns (grid.y tiles N); the stage layout, the MMA issue, the
+// bounded waits and the TMEM epilogue are k_conv_tc's, with the gather
+// replaced by row copies: eight consecutive threads copy one row's 128
+// bytes of a k tile.  Rows past M or N and k past the CTA's range read 0.
+template <int NT>
+__global__ void __launch_bounds__(TC_NT) k_gemm_tc(GemmArgs a, unsigned refill_limit) {
+  using Cfg = TcCfg<NT>;
+  extern __shared__ __align__(128) unsigned char tcs[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)tcs + 127) & ~(uintptr_t)127);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + TC_S * Cfg::STAGE);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + TC_S);
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * NT;
+  const int kb = a.splits > 1 ? blockIdx.z * a.kper : 0;
+  const int ke = a.splits > 1 ? min(a.K, kb + a.kper) : a.K;
+  const int nk = (ke - kb + TC_BK - 1) / TC_BK;
+  if (tid == 0) {
+    for (int i = 0; i < TC_S; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[i])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    abort_flag = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(Cfg::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t sbase = smem_addr(base);
+  auto load_tile = [&](int t) {
+    const uint32_t As = sbase + (t % TC_S) * Cfg::STAGE, Bs = As + Cfg::A_BYTES;
+    const int k0 = kb + t * TC_BK;
+    for (int e = tid; e < TC_BM * (TC_BK / 8); e += TC_NT) {
+      const int row = e >> 3, q = e & 7, k = k0 + q * 8, m = m0 + row;
+      const bool ok = m < a.M && k < ke;
+      cp16(As + q * (TC_BM * 16) + row * 16, ok ? (const void *)(a.A + (size_t)m * a.sam + k) : (const void *)a.A,
+           ok);
+    }
+    for (int e = tid; e < NT * (TC_BK / 8); e += TC_NT) {
+      const int n = e >> 3, q = e & 7, k = k0 + q * 8, nn = n0 + n;
+      const bool ok = nn < a.N && k < ke;
+      cp16(Bs + q * (NT * 16) + n * 16, ok ? (const void *)(a.B + (size_t)nn * a.sbn + k) : (const void *)a.B, ok);
+    }
+  };
+#pragma unroll
+  for (int p = 0; p < TC_S - 1; ++p) {
+    if (p < nk) load_tile(p);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  int last_it = -1;
+  for (int it = 0; it < nk; ++it) {
+    const int st = it % TC_S;
+    asm volatile("cp.async.wait_group %0;" ::"n"(TC_S - 2) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (abort_flag) break;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = sbase + st * Cfg::STAGE, b0 = a0 + Cfg::A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 16; ++kk) {
+        const uint64_t ad = umma_desc(a0 + kk * 2 * (TC_BM * 16), TC_BM * 16, 128);
+        const uint64_t bd = umma_desc(b0 + kk * 2 * (NT * 16), NT * 16, 128);
+        const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(Cfg::IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&bars[st]))
+                   : "memory");
+    }
+    last_it = it;
+    const int nt = it + TC_S - 1;
+    if (nt < nk) {
+      if (it >= 1) {
+        const int pt = it - 1;
+        if (!mbar_wait(smem_addr(&bars[pt % TC_S]), (pt / TC_S) & 1, refill_limit)) {
+          if (tid == 0) atomicExch(&g_tc_error, 1);
+          abort_flag = 1;
+        }
+      }
+      load_tile(nt);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (last_it >= 0 && !mbar_wait(smem_addr(&bars[last_it % TC_S]), (last_it / TC_S) & 1)) {
+    if (tid == 0) atomicExch(&g_tc_error, 1);
+    abort_flag = 1;
+  }
+  __syncthreads();
+  const bool ok = !abort_flag;
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (ok && last_it >= 0) {
+    const int m = m0 + warp * 32 + lane;
+#pragma unroll
+    for (int c0 = 0; c0 < NT; c0 += 8) {
+      if (n0 + c0 >= a.N) break;  // uniform over the CTA
+      uint32_t v[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < a.M) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int n = n0 + c0 + q;
+          if (n >= a.N) break;
+          float f = __uint_as_float(v[q]);
+          if (a.splits > 1) {
+            a.ws[((size_t)blockIdx.z * a.M + m) * a.N + n] = f;
+          } else {
+            if (a.bias) f += a.bias[n];
+            if (a.relu) f = fmaxf(f, 0.f);
+            const long long o = (long long)m * a.scm + (long long)n * a.scn;
+            if (a.Cf) a.Cf[o] = f;
+            if (a.Cb) a.Cb[o] = __float2bfloat16(f);
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
+}
+
 __global__ void k_splitk_reduce(GemmArgs a) {
   const size_t tot = (size_t)a.M * a.N;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
@@ -654,6 +795,90 @@ static int gemm(cudaStream_t st, GemmArgs a, float *ws, const ConvGeom *conv = n
   return IRLCU_OK;
 }
 
+template <int NT>
+static int gemm_tc_attr() {
+  static bool done = false;
+  if (done) return IRLCU_OK;
+  CU_TRY(cudaFuncSetAttribute(k_gemm_tc<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<NT>::SMEM));
+  done = true;
+  return IRLCU_OK;
+}
+
+// the backward GEMMs on tcgen05 unless IRLCU_SUR_TC=0
+static bool bwd_tc_on() {
+  static int env = -1;
+  if (env < 0) {
+    const char *e = getenv("IRLCU_SUR_TC");
+    env = (e && e[0] == '0') ? 0 : 1;
+  }
+  return env == 1;
+}
+
+// k_gemm_tc over a GEMM with K-major operands (see there); the reduction
+// is split when the tile grid is small, summed by k_splitk_reduce in slice
+// order, so the result does not depend on scheduling
+static int gemm_tc(cudaStream_t st, GemmArgs a, float *ws) {
+  if (a.M <= 0 || a.N <= 0 || a.K <= 0) return IRLCU_OK;
+  if (a.sak != 1 || a.sbk != 1 || a.K % 8 || a.sam % 8 || a.sbn % 8 || ((uintptr_t)a.A & 15) ||
+      ((uintptr_t)a.B & 15))
+    return set_error(IRLCU_EARG, "tcgen05 GEMM needs K-major operands with 16-byte rows (K = %d)", a.K);
+  const int NT = a.N <= 32 ? 32 : a.N <= 64 ? 64 : a.N <= 128 ? 128 : 256;
+  const long long tm = (a.M + TC_BM - 1) / TC_BM, tn = (a.N + NT - 1) / NT;
+  if (tn > 65535) return set_error(IRLCU_EARG, "tcgen05 GEMM with N = %d too wide", a.N);
+  const long long per_sm = NT <= 64 ? 2 : 1;  // resident CTAs per SM (shared memory)
+  long long sp = std::min<long long>(per_sm * 148 / std::max<long long>(tm * tn, 1), a.K / 256);
+  int splits = (int)std::max<long long>(1, std::min<long long>(sp, 64));
+  while (splits > 1 && (size_t)splits * a.M * a.N > GEMM_WS_ELEMS) --splits;
+  a.splits = 1;
+  a.kper = a.K;
+  if (splits > 1) {
+    a.kper = ((a.K + splits - 1) / splits + TC_BK - 1) / TC_BK * TC_BK;
+    a.splits = (a.K + a.kper - 1) / a.kper;
+    a.ws = ws;
+  }
+  const dim3 grid((unsigned)tm, (unsigned)tn, a.splits);
+  switch (NT) {
+    case 32: TC_TRY(gemm_tc_attr<32>()); k_gemm_tc<32><<<grid, TC_NT, TcCfg<32>::SMEM, st>>>(a, g_tc_refill_limit); break;
+    case 64: TC_TRY(gemm_tc_attr<64>()); k_gemm_tc<64><<<grid, TC_NT, TcCfg<64>::SMEM, st>>>(a, g_tc_refill_limit); break;
+    case 128: TC_TRY(gemm_tc_attr<128>()); k_gemm_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, g_tc_refill_limit); break;
+    default: TC_TRY(gemm_tc_attr<256>()); k_gemm_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, g_tc_refill_limit); break;
+  }
+  CU_LAUNCHED();
+  if (a.splits > 1) {
+    const size_t tot = (size_t)a.M * a.N;
+    k_splitk_reduce<<<(unsigned)std::min<size_t>((tot + 255) / 256, 148 * 32), 256, 0, st>>>(a);
+    CU_LAUNCHED();
+  }
+  return IRLCU_OK;
+}
+
+// out[c][r] = in[r][c] for a rows x cols BF16 matrix: 32 x 32 tiles through
+// shared memory, grid (ceil(rows / 32), ceil(cols / 32)), block (32, 8)
+__global__ void k_transpose_bf16(const bf16 *__restrict__ in, bf16 *__restrict__ out, long long rows, int cols) {
+  __shared__ bf16 t[32][33];
+  const long long r0 = (long long)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const long long r = r0 + i;
+    const int c = c0 + threadIdx.x;
+    if (r < rows && c < cols) t[i][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int c = c0 + i;
+    const long long r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[(long long)c * rows + r] = t[threadIdx.x][i];
+  }
+}
+
+static int transpose_bf16(cudaStream_t st, const bf16 *in, bf16 *out, long long rows, int cols) {
+  const long long bx = (rows + 31) / 32;
+  if (bx > 0x7fffffffLL || (cols + 31) / 32 > 65535) return set_error(IRLCU_EARG, "transpose of %lld x %d", rows, cols);
+  k_transpose_bf16<<<dim3((unsigned)bx, (unsigned)((cols + 31) / 32)), dim3(32, 8), 0, st>>>(in, out, rows, cols);
+  CU_LAUNCHED();
+  return IRLCU_OK;
+}
+
 // ---------------------------------------------------------- conv helpers
 
 __host__ __device__ inline int conv_out(int in, int k, int s) { return (in + 2 * (k / 2) - k) / s + 1; }
@@ -681,6 +906,32 @@ __global__ void k_im2col(ConvGeom g, const bf16 *__restrict__ x, bf16 *__restric
     if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
       v = x[in_off(g, b, id, ih, iw, c)];
     col[e] = v;
+  }
+}
+
+// the same columns transposed, colT[k][m] (m contiguous): the K-major
+// operand of the weight-gradient GEMM, whose reduction runs over m
+__global__ void k_im2colT(ConvGeom g, const bf16 *__restrict__ x, bf16 *__restrict__ colT) {
+  const long long K = (long long)g.kd * g.kh * g.kw * g.ci;
+  const long long M = (long long)g.b * g.dout * g.hout * g.wout;
+  const long long tot = M * K;
+  const bf16 zero = __float2bfloat16(0.f);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e / M);
+    const long long m = e - (long long)k * M;
+    const int c = k % g.ci, tap = k / g.ci;
+    const int tw = tap % g.kw, th = (tap / g.kw) % g.kh, td = tap / (g.kw * g.kh);
+    long long r = m;
+    const int ow = (int)(r % g.wout); r /= g.wout;
+    const int oh = (int)(r % g.hout); r /= g.hout;
+    const int od = (int)(r % g.dout);
+    const int b = (int)(r / g.dout);
+    const int id = od * g.s + td - g.kd / 2, ih = oh * g.s + th - g.kh / 2, iw = ow * g.s + tw - g.kw / 2;
+    bf16 v = zero;
+    if (id >= 0 && id < g.di && ih >= 0 && ih < g.hi && iw >= 0 && iw < g.wi)
+      v = x[in_off(g, b, id, ih, iw, c)];
+    colT[e] = v;
   }
 }
 
@@ -1377,6 +1628,8 @@ struct irlcu_sur {
   float *dcol = nullptr;          // input-gradient columns
   float *gf = nullptr, *gf2 = nullptr;   // FP32 activation gradients
   irlcu::bf16 *gb = nullptr;      // BF16 gradient of the current layer output
+  irlcu::bf16 *gbT = nullptr;     // gb transposed [co][M] (tcgen05 weight gradient)
+  irlcu::bf16 *wT = nullptr;      // a layer's BF16 weights transposed [K][co] (tcgen05 input gradient)
   float *out = nullptr;           // network output [B][128*128]
   float *dout = nullptr;
   float *loss_part = nullptr;
@@ -1473,6 +1726,8 @@ static void sur_free(irlcu_sur *s) {
   cudaFree(s->gf);
   cudaFree(s->gf2);
   cudaFree(s->gb);
+  cudaFree(s->gbT);
+  cudaFree(s->wT);
   cudaFree(s->out);
   cudaFree(s->dout);
   cudaFree(s->loss_part);
@@ -1574,23 +1829,50 @@ static int sur_backward(irlcu_sur &s, int B) {
     const bf16 *yact = (i == nl - 1) ? nullptr : s.act[i + 1];
     k_relu_grad<<<grid_for(nout), 256, 0, s.st>>>(gcur, yact, s.gb, nout, (yact && l.relu) ? 1 : 0);
     CU_LAUNCHED();
-    k_im2col<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
-    CU_LAUNCHED();
-    // dW[n][k] = sum_m col[m][k] g[m][n]
-    GemmArgs a{};
-    a.A = s.col;  // A'(k, m) = col[m*K + k]
-    a.sam = 1;
-    a.sak = l.K;
-    a.B = s.gb;   // B'(m, n) = g[m*co + n]
-    a.sbk = l.g.co;
-    a.sbn = 1;
-    a.M = (int)l.K;
-    a.N = l.g.co;
-    a.K = (int)M;
-    a.Cf = s.g + l.woff;  // dW[n*K + k]
-    a.scm = 1;
-    a.scn = l.K;
-    STRY(gemm(s.st, a, s.ws));
+    // the tcgen05 GEMMs take K-major operands: the weight gradient reduces
+    // over the M output positions, so it reads the columns and the layer
+    // gradient transposed (M a multiple of 8 keeps their rows 16-byte
+    // aligned); the input gradient reduces over the co output channels
+    const bool tc_w = bwd_tc_on() && M % 8 == 0;
+    const bool tc_d = bwd_tc_on() && l.g.co % 8 == 0;
+    if (tc_w) {
+      k_im2colT<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
+      CU_LAUNCHED();
+      STRY(transpose_bf16(s.st, s.gb, s.gbT, M, l.g.co));
+      // dW[n][k] = sum_m colT[k][m] gT[n][m]
+      GemmArgs a{};
+      a.A = s.col;
+      a.sam = M;
+      a.sak = 1;
+      a.B = s.gbT;
+      a.sbn = M;
+      a.sbk = 1;
+      a.M = (int)l.K;
+      a.N = l.g.co;
+      a.K = (int)M;
+      a.Cf = s.g + l.woff;  // dW[n*K + k]
+      a.scm = 1;
+      a.scn = l.K;
+      STRY(gemm_tc(s.st, a, s.ws));
+    } else {
+      k_im2col<<<grid_for(M * l.K), 256, 0, s.st>>>(l.g, layer_input(s, i), s.col);
+      CU_LAUNCHED();
+      // dW[n][k] = sum_m col[m][k] g[m][n]
+      GemmArgs a{};
+      a.A = s.col;  // A'(k, m) = col[m*K + k]
+      a.sam = 1;
+      a.sak = l.K;
+      a.B = s.gb;   // B'(m, n) = g[m*co + n]
+      a.sbk = l.g.co;
+      a.sbn = 1;
+      a.M = (int)l.K;
+      a.N = l.g.co;
+      a.K = (int)M;
+      a.Cf = s.g + l.woff;  // dW[n*K + k]
+      a.scm = 1;
+      a.scn = l.K;
+      STRY(gemm(s.st, a, s.ws));
+    }
     k_bias_grad<<<l.g.co, 256, 0, s.st>>>(s.gb, M, l.g.co, s.g + l.boff);
     CU_LAUNCHED();
     if (i == 0) break;  // no gradient for the input
@@ -1599,16 +1881,24 @@ static int sur_backward(irlcu_sur &s, int B) {
     d.A = s.gb;
     d.sam = l.g.co;
     d.sak = 1;
-    d.B = s.wb + l.woff;  // B(n, k) = W[n*K + k]
-    d.sbk = l.K;
-    d.sbn = 1;
     d.M = (int)M;
     d.N = (int)l.K;
     d.K = l.g.co;
     d.Cf = s.dcol;
     d.scm = l.K;
     d.scn = 1;
-    STRY(gemm(s.st, d, s.ws));
+    if (tc_d) {
+      STRY(transpose_bf16(s.st, s.wb + l.woff, s.wT, l.g.co, (int)l.K));
+      d.B = s.wT;  // B(k, n) = WT[k*co + n]
+      d.sbn = l.g.co;
+      d.sbk = 1;
+      STRY(gemm_tc(s.st, d, s.ws));
+    } else {
+      d.B = s.wb + l.woff;  // B(n, k) = W[n*K + k]
+      d.sbk = l.K;
+      d.sbn = 1;
+      STRY(gemm(s.st, d, s.ws));
+    }
     const long long nin = (long long)layer_in_elems(l, B);
     k_col2im<<<grid_for(nin), 256, 0, s.st>>>(l.g, s.dcol, gnext);
     CU_LAUNCHED();
@@ -1774,10 +2064,11 @@ int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
       (rc = dmalloc(&s->wb, P)))
     return fail(rc);
   const int B = max_batch;
-  size_t colmax = 0, actmax = 0;
+  size_t colmax = 0, actmax = 0, wmax = 0;
   s->act.assign(s->L.size() + 1, nullptr);
   for (size_t i = 0; i < s->L.size(); ++i) {
     const Layer &l = s->L[i];
+    wmax = std::max(wmax, (size_t)l.K * l.g.co);
     const size_t M = (size_t)B * l.g.dout * l.g.hout * l.g.wout;
     colmax = std::max(colmax, M * (size_t)l.K);
     actmax = std::max(actmax, std::max(layer_in_elems(l, B), layer_out_elems(l, B)));
@@ -1787,7 +2078,8 @@ int irlcu_sur_create(int max_batch, unsigned long long seed, irlcu_sur **out) {
   }
   if ((rc = dmalloc(&s->fold, layer_out_elems(s->L[2], B))) || (rc = dmalloc(&s->col, colmax)) ||
       (rc = dmalloc(&s->dcol, colmax)) || (rc = dmalloc(&s->gf, actmax)) || (rc = dmalloc(&s->gf2, actmax)) ||
-      (rc = dmalloc(&s->gb, actmax)) || (rc = dmalloc(&s->out, (size_t)B * 128 * 128)) ||
+      (rc = dmalloc(&s->gb, actmax)) || (rc = dmalloc(&s->gbT, actmax)) || (rc = dmalloc(&s->wT, wmax)) ||
+      (rc = dmalloc(&s->out, (size_t)B * 128 * 128)) ||
       (rc = dmalloc(&s->dout, (size_t)B * 128 * 128)) || (rc = dmalloc(&s->loss_part, (size_t)B)) ||
       (rc = dmalloc(&s->ws, GEMM_WS_ELEMS)))
     return fail(rc);

@@ -840,7 +840,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 {
 	jmp_buf env;
 	parked_session **h = NULL;
-	int p, m, err = 0, trials = 1, depth, oldest = 0;
+	int p, m, err = 0, trials = 1, graphs = 1, depth, oldest = 0;
 	if ((err = setjmp(env)) != 0) {
 		irl_untrap();
 		return err;
@@ -859,6 +859,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 	h = (parked_session **)irl_calloc(sizeof(parked_session *) * nprob, "batch sessions");
 	irl_untrap();
 	trials = irlcu_shape_trials(0);  /* no host waits inside the pipelined batch */
+	graphs = irlcu_iteration_graphs(0);  /* eager iterations: faster with problems in flight */
 	depth = batch_depth();
 	/* pipelined: problem p is set up and all its iterations are enqueued
 	   (asynchronous device work on its own stream); the host then sets up
@@ -904,6 +905,7 @@ int IrlOsemBatch(int nprob, IrlOsemProblem_t *pp)
 	}
 	free(h);
 	irlcu_shape_trials(trials);
+	irlcu_iteration_graphs(graphs);
 	return err;
 }
 
