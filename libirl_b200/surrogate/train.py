@@ -200,6 +200,31 @@ def train_streaming(args, lib):
     net.close()
 
 
+def time_steps(args, lib):
+    """Wall time of training steps (forward, loss, backward, Adam; each
+    step ends with a stream synchronisation) at --batch on seeded random
+    inputs and targets, after 3 untimed steps; no pairs are generated and
+    no weights are written."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(99)
+    B = args.batch
+    x = torch.rand((B,) + SU.INPUT_SHAPE, device="cuda", generator=g).to(torch.bfloat16)
+    t = torch.rand((B, SU.OUTPUT_SIZE), device="cuda", generator=g)
+    torch.cuda.synchronize()
+    net = SU.Network(lib, B, seed=17)
+    try:
+        for _ in range(3):
+            net.train_step(B, x.data_ptr(), t.data_ptr(), 1e-4)
+        t0 = time.perf_counter()
+        for _ in range(args.time_steps):
+            loss = net.train_step(B, x.data_ptr(), t.data_ptr(), 1e-4)
+        ms = 1000.0 * (time.perf_counter() - t0) / args.time_steps
+    finally:
+        net.close()
+    print(json.dumps({"batch": B, "steps": args.time_steps, "ms_per_step": round(ms, 3), "loss": loss}))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--phantoms", type=int, default=200, help="training phantoms")
@@ -217,11 +242,15 @@ def main(argv=None):
     ap.add_argument("--init", default=None, help="start from this weights file")
     ap.add_argument("--out", default=SU.DEFAULT_WEIGHTS)
     ap.add_argument("--summary", default=None)
+    ap.add_argument("--time-steps", type=int, default=0,
+                    help="only time this many training steps on seeded random data (no pairs, no weights written)")
     args = ap.parse_args(argv)
 
     import torch
     import libirl_b200 as L
     lib = L.load()
+    if args.time_steps > 0:
+        return time_steps(args, lib)
     if args.chunk > 0:
         return train_streaming(args, lib)
     t0 = time.time()
