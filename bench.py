@@ -818,7 +818,8 @@ def run_batch32(args):
     """Config 3: 32 seeded problems of uneven size (N 64..128, 60..120
     views, 4..12 subsets, DRF + ESSE), 5 iterations each: IrlOsemBatch
     against the same 32 IrlOsem calls one after another, wall time, after
-    one untimed batch pass (table autotuning and module loading)."""
+    one untimed batch pass (table autotuning and module loading); medians
+    of three alternating rounds."""
     import torch  # noqa: F401  (CUDA context for the library)
     import libirl_b200 as L
     from libirl_b200 import api, workloads as W
@@ -860,14 +861,24 @@ def run_batch32(args):
         return time.perf_counter() - t0, out
 
     batch()
-    seq_s, seq_imgs = sequential()
-    bat_s, bat_imgs = batch()
-    same = all(np.array_equal(a, b) for a, b in zip(seq_imgs, bat_imgs))
+    # the small problems make both forms sensitive to host load on a shared
+    # machine, so each is timed in three alternating rounds and the medians
+    # are reported (every sample beside them)
+    samples = {"sequential": [], "batched": [], "sequential_1it": [], "batched_1it": []}
+    same = True
+    for _ in range(3):
+        seq_s, seq_imgs = sequential()
+        bat_s, bat_imgs = batch()
+        same = same and all(np.array_equal(a, b) for a, b in zip(seq_imgs, bat_imgs))
+        # the iteration phase alone: 5 iterations minus 1 (set-up and the
+        # first iteration cancel)
+        seq1, _ = sequential(1)
+        bat1, _ = batch(1)
+        for k, t in (("sequential", seq_s), ("batched", bat_s), ("sequential_1it", seq1), ("batched_1it", bat1)):
+            samples[k].append(round(t, 3))
+    seq_s, bat_s = float(np.median(samples["sequential"])), float(np.median(samples["batched"]))
+    seq1, bat1 = float(np.median(samples["sequential_1it"])), float(np.median(samples["batched_1it"]))
     iters = sum(c.iterations for c, _, _ in data)
-    # the iteration phase alone: 5 iterations minus 1 (set-up and the first
-    # iteration cancel)
-    seq1, _ = sequential(1)
-    bat1, _ = batch(1)
     it_seq, it_bat = seq_s - seq1, bat_s - bat1
     return {
         "metric": "wall s for 32 uneven OSEM reconstructions (5 iterations each), 1 B200", "value": round(bat_s, 3),
@@ -876,6 +887,7 @@ def run_batch32(args):
         "ms_per_problem_iteration": round(1000 * bat_s / iters, 3), "identical_to_sequential": bool(same),
         "iterations_2_to_5_s": {"batched": round(it_bat, 3), "sequential": round(it_seq, 3),
                                 "speedup": round(it_seq / it_bat, 3) if it_bat > 0 else None},
+        "samples_s": samples, "timing": "median of 3 alternating rounds",
         "config": {"workload": "batch32: " + ", ".join(f"{c.n}^3/{c.nviews}v/{c.subsets}s" for c, _, _ in data),
                    "includes": "set-up (tables, norm images) and result copies of every problem"},
         "data": "synthetic (seeded phantoms, Poisson data)"}

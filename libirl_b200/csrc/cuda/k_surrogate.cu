@@ -676,7 +676,24 @@ __global__ void __launch_bounds__(TC_NT) k_gemm_tc(GemmArgs a, unsigned refill_l
                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                    : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (m < a.M) {
+      // eight consecutive columns of a row-major FP32 output (the split-K
+      // partials, or Cf with scn = 1) go out as two 16-byte stores: one
+      // whole 32-byte sector per thread instead of eight scalar stores
+      float *vrow = nullptr;
+      if (m < a.M && n0 + c0 + 8 <= a.N) {
+        if (a.splits > 1) {
+          if ((a.N & 3) == 0) vrow = a.ws + ((size_t)blockIdx.z * a.M + m) * a.N + n0 + c0;
+        } else if (a.scn == 1 && (a.scm & 3) == 0 && a.Cf && !a.Cb && !a.bias && !a.relu &&
+                   ((uintptr_t)a.Cf & 15) == 0) {
+          vrow = a.Cf + (long long)m * a.scm + n0 + c0;
+        }
+      }
+      if (vrow) {
+        reinterpret_cast<float4 *>(vrow)[0] =
+            make_float4(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]), __uint_as_float(v[3]));
+        reinterpret_cast<float4 *>(vrow)[1] =
+            make_float4(__uint_as_float(v[4]), __uint_as_float(v[5]), __uint_as_float(v[6]), __uint_as_float(v[7]));
+      } else if (m < a.M) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int n = n0 + c0 + q;

@@ -375,6 +375,51 @@ def test_osem_norm_files_and_errors(product, tmp_path):
     assert rc != 0 and b"not even" in product.pchIrlErrorString()
 
 
+def test_backprojection_per_view_through_norm_images(product, orc, tmp_path):
+    """BackProject of one view (prjbck.c:254-427) on its own: with one view
+    per subset, each subset's norm image is the inverted backprojection of
+    that view's measured-bin mask times its ViewTime (osemrecon.c:282-320),
+    here all bins (positive data, the detector spanning the slice).  The
+    norm files written during IrlOsem are read at the iteration-0 callback
+    and inverted back; every view's backprojection (attenuation + DRF, the
+    backprojector model) is compared with the oracle's or_backproject,
+    within the per-view tolerance on the voxels both keep (the 1e-6 floor of
+    the inversion may fall either way on a voxel at the threshold)."""
+    case = W.full128(seed=2060, n=32, nviews=8, subsets=8, iterations=1, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    base = str(tmp_path / "nrm")
+    ns = case.nviews
+    got = {}
+
+    def cb(it, _img):
+        if it == 0:
+            for s in range(ns):
+                got[s] = np.fromfile(f"{base}.norm.{s}.dat", dtype=np.float32).reshape(case.n, case.nz, case.n)
+
+    meas = np.ones((case.nviews, case.nz, case.n), np.float32)
+    gpu_osem(product, case, files, meas, parms={"pchNormImageBase": base.encode()}, cb=api.ITER_CB(cb))
+    assert len(got) == ns
+    order = C.POINTER(C.c_int)()
+    assert product.irl_compute_subsets(case.nviews, 1, C.byref(order)) == ns
+    views = [order[s] for s in range(ns)]
+    assert sorted(views) == list(range(ns))
+    pr = orc.Problem(case)
+    bck_model = pr.model(srf=False)
+    ones = np.ones((case.nz, case.n), np.float32)
+    for s, v in enumerate(views):
+        ref = np.zeros((case.n, case.nz, case.n), np.float32)
+        orc.orc().or_backproject(C.byref(pr.P), bck_model, v, api.fptr(pr.atn), api.fptr(ones), api.fptr(ref))
+        norm = got[s]
+        both = (norm > 0) & (ref >= np.float32(1e-6))
+        assert both.sum() > 0.5 * (ref >= np.float32(1e-6)).sum(), f"view {v}: backprojection support lost"
+        flips = int(((norm > 0) != (ref >= np.float32(1e-6))).sum())
+        assert flips <= max(2, int(1e-3 * both.sum())), f"view {v}: {flips} voxels on opposite sides of the floor"
+        bp = np.zeros_like(ref)
+        bp[both] = 1.0 / norm[both].astype(np.float64)
+        err = rel_l2(bp[both], ref[both])
+        assert err <= VIEW_TOL, f"view {v}: backprojection relL2 {err:.3e}"
+
+
 # --------------------------------------------------------- full-size checks
 
 @pytest.mark.parametrize("engine", ["direct", "fft"])
