@@ -819,7 +819,7 @@ def run_batch32(args):
     views, 4..12 subsets, DRF + ESSE), 5 iterations each: IrlOsemBatch
     against the same 32 IrlOsem calls one after another, wall time, after
     one untimed batch pass (table autotuning and module loading); medians
-    of three alternating rounds."""
+    of three alternating repeats."""
     import torch  # noqa: F401  (CUDA context for the library)
     import libirl_b200 as L
     from libirl_b200 import api, workloads as W
@@ -862,7 +862,7 @@ def run_batch32(args):
 
     batch()
     # the small problems make both forms sensitive to host load on a shared
-    # machine, so each is timed in three alternating rounds and the medians
+    # machine, so each is timed in three alternating repeats and the medians
     # are reported (every sample beside them)
     samples = {"sequential": [], "batched": [], "sequential_1it": [], "batched_1it": []}
     same = True
@@ -887,7 +887,7 @@ def run_batch32(args):
         "ms_per_problem_iteration": round(1000 * bat_s / iters, 3), "identical_to_sequential": bool(same),
         "iterations_2_to_5_s": {"batched": round(it_bat, 3), "sequential": round(it_seq, 3),
                                 "speedup": round(it_seq / it_bat, 3) if it_bat > 0 else None},
-        "samples_s": samples, "timing": "median of 3 alternating rounds",
+        "samples_s": samples, "timing": "median of 3 alternating repeats",
         "config": {"workload": "batch32: " + ", ".join(f"{c.n}^3/{c.nviews}v/{c.subsets}s" for c, _, _ in data),
                    "includes": "set-up (tables, norm images) and result copies of every problem"},
         "data": "synthetic (seeded phantoms, Poisson data)"}
