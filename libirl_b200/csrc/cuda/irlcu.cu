@@ -112,6 +112,13 @@ cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t st) {
     if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
     uint64_t keep = UINT64_MAX;
     if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    // a block freed on another context's stream is not handed out with an
+    // inserted wait on that stream: with several reconstructions in flight
+    // (IrlOsemBatch) such a wait, followed by this function's stream
+    // synchronisation, would hold the host until the other problem's queued
+    // work reached the free
+    int no = 0;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no)) != cudaSuccess) return e;
     ready[dev] = true;
   }
   if ((e = cudaMallocAsync(p, bytes, st)) != cudaSuccess) return e;
