@@ -129,6 +129,48 @@ def test_oracle_vs_reference_live_osem_padding(orc):
     assert np.array_equal(pr.genprj(), prj)
 
 
+def test_oracle_backproject_single_view_matches_reference(orc, tmp_path):
+    """BackProject of one view on a constant projection (prjbck.c:254-427,
+    attenuation + DRF, three-shear unrotation): the per-view term of a norm
+    image (osemrecon.c:282-320), which the GPU single-view backprojection
+    test compares with or_backproject.  Here or_backproject is compared
+    with the reference's own BackProject for every view of the same
+    elliptical-orbit case: they agree to float rounding (about 2e-7
+    relative L2 with this case's non-separable 11 x 11 PSFs; a few ulp on
+    individual voxels, from the convolution's summation order)."""
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    case = W.full128(seed=2060, n=32, nviews=8, subsets=8, iterations=1, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    ref = orc.ref()
+    F, I, FL = api.FLOAT_P, C.c_int, C.c_float
+    ref.BackProject.restype = None
+    ref.BackProject.argtypes = [I, I, I, I, FL, I, FL, FL, C.POINTER(api.DrfTab), C.c_void_p, F, F, F, FL, FL,
+                                I, I, I, I]
+    title, col = C.c_char_p(), C.c_char_p()
+    tab = ref.sReadDrfTab(files["drf"].encode(), C.byref(title), C.byref(col))
+    tab.psBckDrfTab = None
+    n, nz = case.n, case.nz
+    pr = orc.Problem(case)
+    ones = np.ones((nz, n), np.float32)
+    model = pr.model(srf=False)
+    assert model == 3
+    ref.InitPrj(nz, n, n, 7)  # every work image, as IrlOsem with a scatter model sets up
+    try:
+        for v in range(case.nviews):
+            want = np.zeros((n, nz, n), np.float32)
+            atn, ratio = pr.atn.copy(), ones.copy()
+            ref.BackProject(nz, n, n, model, case.pix, v, float(case.angles[v]), float(case.cfcr[v]), C.byref(tab),
+                            None, api.fptr(atn), api.fptr(ratio), api.fptr(want), 1.0, 1.0, 0, 0, 0, 1)
+            got = np.zeros_like(want)
+            orc.orc().or_backproject(C.byref(pr.P), model, v, api.fptr(pr.atn), api.fptr(ones), api.fptr(got))
+            assert want.max() > 0.5
+            err = rel_l2(got, want)
+            assert err <= 1e-6, f"view {v}: relL2 {err:.3e}"
+    finally:
+        ref.FreePrj()
+
+
 def test_reference_fft_convolution_is_zero_padded_direct(orc):
     """libirl's FFT convolution branch (PadSwap + realft3d + conv2dPsfFFT on a
     2N x 2Nz grid) equals the direct "same" convolution with no axial
