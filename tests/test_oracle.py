@@ -135,9 +135,7 @@ def test_oracle_backproject_single_view_matches_reference(orc, tmp_path):
     image (osemrecon.c:282-320), which the GPU single-view backprojection
     test compares with or_backproject.  Here or_backproject is compared
     with the reference's own BackProject for every view of the same
-    elliptical-orbit case: they agree to float rounding (about 2e-7
-    relative L2 with this case's non-separable 11 x 11 PSFs; a few ulp on
-    individual voxels, from the convolution's summation order)."""
+    elliptical-orbit case, bit for bit."""
     if not _have_ref(orc):
         pytest.skip("compiled reference not available")
     case = W.full128(seed=2060, n=32, nviews=8, subsets=8, iterations=1, drf_max_offs=6)
@@ -150,6 +148,7 @@ def test_oracle_backproject_single_view_matches_reference(orc, tmp_path):
     title, col = C.c_char_p(), C.c_char_p()
     tab = ref.sReadDrfTab(files["drf"].encode(), C.byref(title), C.byref(col))
     tab.psBckDrfTab = None
+    tab.bFFTconvolve = 0  # sReadDrfTab leaves it unset; IrlSetup.c:577 sets it from the options
     n, nz = case.n, case.nz
     pr = orc.Problem(case)
     ones = np.ones((nz, n), np.float32)
@@ -165,8 +164,7 @@ def test_oracle_backproject_single_view_matches_reference(orc, tmp_path):
             got = np.zeros_like(want)
             orc.orc().or_backproject(C.byref(pr.P), model, v, api.fptr(pr.atn), api.fptr(ones), api.fptr(got))
             assert want.max() > 0.5
-            err = rel_l2(got, want)
-            assert err <= 1e-6, f"view {v}: relL2 {err:.3e}"
+            assert np.array_equal(got, want), f"view {v}: relL2 {rel_l2(got, want):.3e}"
     finally:
         ref.FreePrj()
 
