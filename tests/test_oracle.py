@@ -169,6 +169,42 @@ def test_oracle_backproject_single_view_matches_reference(orc, tmp_path):
         ref.FreePrj()
 
 
+def test_oracle_project_single_view_matches_reference(orc, tmp_path):
+    """Project of one view (prjbck.c:68-252, attenuation + DRF, three-shear
+    rotation of activity and attenuation) from or_project against the
+    reference's own Project, every view of the elliptical-orbit case, bit
+    for bit."""
+    if not _have_ref(orc):
+        pytest.skip("compiled reference not available")
+    case = W.full128(seed=2061, n=32, nviews=8, subsets=8, iterations=1, drf_max_offs=6)
+    files = case.write_tables(str(tmp_path))
+    ref = orc.ref()
+    F, I, FL = api.FLOAT_P, C.c_int, C.c_float
+    ref.Project.restype = None
+    ref.Project.argtypes = [I, I, I, I, FL, I, FL, FL, C.POINTER(api.DrfTab), C.c_void_p, F, F, F, FL, FL,
+                            I, I, I, I, I]
+    title, col = C.c_char_p(), C.c_char_p()
+    tab = ref.sReadDrfTab(files["drf"].encode(), C.byref(title), C.byref(col))
+    tab.psBckDrfTab = None
+    tab.bFFTconvolve = 0  # sReadDrfTab leaves it unset; IrlSetup.c:577 sets it from the options
+    n, nz = case.n, case.nz
+    pr = orc.Problem(case)
+    model = pr.model(srf=False)
+    ref.InitPrj(nz, n, n, 7)
+    try:
+        for v in range(case.nviews):
+            want = np.zeros((nz, n), np.float32)
+            atn, act = pr.atn.copy(), pr.act.copy()
+            ref.Project(nz, n, n, model, case.pix, v, float(case.angles[v]), float(case.cfcr[v]), C.byref(tab),
+                        None, api.fptr(atn), api.fptr(act), api.fptr(want), 1.0, 1.0, 0, 0, 0, 0, 1)
+            got = np.zeros_like(want)
+            orc.orc().or_project(C.byref(pr.P), model, v, api.fptr(pr.act), api.fptr(pr.atn), 1.0, api.fptr(got))
+            assert want.max() > 0
+            assert np.array_equal(got, want), f"view {v}: relL2 {rel_l2(got, want):.3e}"
+    finally:
+        ref.FreePrj()
+
+
 def test_reference_fft_convolution_is_zero_padded_direct(orc):
     """libirl's FFT convolution branch (PadSwap + realft3d + conv2dPsfFFT on a
     2N x 2Nz grid) equals the direct "same" convolution with no axial
