@@ -35,6 +35,8 @@ def test_drft_roundtrip_native_and_swapped(product, tmp_path):
     t = product.sReadDrfTab(f.encode(), C.byref(title), C.byref(col))
     assert t.iNumDistances == 7 and abs(t.fPixSize - 0.4) < 1e-7 and abs(t.fStartDistance - 5.0) < 1e-7
     assert title.value == b"table" and col.value == b"LEHR"
+    # fields libirl's reader leaves unset (drftabio.c:168-174) come back zeroed
+    assert t.bFFTconvolve == 0 and not t.psBckDrfTab
     for i, p in enumerate(psfs):
         d = t.psDrfs[i]
         assert (2 * d.MaxOffsY - 1, 2 * d.MaxOffsX - 1) == p.shape
